@@ -1,0 +1,416 @@
+"""Host-side mirror of the reference's hot-path interface over libcam.
+
+Two layers:
+
+* ``Context``: one CUDA device, its stream, cached FFT plans and scratch
+  buffers (cam_ctx).  Methods map 1:1 to the C ABI.
+* Reference-shaped entry points with the reference's names, argument meaning
+  and effects: ``getDensity_NGP/CIC/TSC`` (Headers/massFunctions.h:12-26),
+  ``do_fftw_r2c/c2r`` (Source/NumericalMethods.cpp:1718, :1818),
+  ``PowerSpectrumF.compute_power_spectrum_grid`` (Source/PowerSpectrumF.cpp:1739)
+  and ``Cwclass.get_CWC`` (Source/Cwclass.cpp:235).  Where the reference exits
+  on an error these raise ``CamError``.
+
+Arrays may be numpy (host) or torch CUDA tensors (device, same device as the
+context); results come back in the same kind of memory.
+"""
+from __future__ import annotations
+
+import ctypes
+import threading
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import CamError
+
+NGP, CIC, TSC = L.NGP, L.CIC, L.TSC
+F32, F64 = L.F32, L.F64
+
+
+def make_grid(n, box, d=None, mn=0.0) -> L.Grid:
+    n3 = (n, n, n) if np.isscalar(n) else tuple(n)
+    b3 = (box, box, box) if np.isscalar(box) else tuple(box)
+    m3 = (mn, mn, mn) if np.isscalar(mn) else tuple(mn)
+    if d is None:
+        d3 = tuple(float(np.float32(np.float32(b) / np.float32(k))) for b, k in zip(b3, n3))
+    else:
+        d3 = (d, d, d) if np.isscalar(d) else tuple(d)
+    g = L.Grid()
+    for a in range(3):
+        g.n[a], g.L[a], g.d[a], g.min[a] = int(n3[a]), float(b3[a]), float(d3[a]), float(m3[a])
+    return g
+
+
+def _f32(a):
+    if a is None or L.is_device(a):
+        return a
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+@dataclass
+class PkResult:
+    pk: np.ndarray
+    modes: np.ndarray
+    kvector: np.ndarray
+    n_obj: float
+    shot_noise: float
+    normal: float
+
+
+@dataclass
+class TwebResult:
+    labels: object
+    lambdas: object
+    counts: np.ndarray
+    ties: int
+    mean: float
+
+
+@dataclass
+class AssignResult:
+    mesh: object
+    n_in: int
+    n_lost: int
+    sum_mesh: float
+
+
+class Context:
+    """A cam_ctx on one device with an optional HBM budget (bytes)."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0):
+        self._lib = L.lib()
+        h = ctypes.c_void_p()
+        rc = self._lib.cam_ctx_create(device, hbm_budget, ctypes.byref(h))
+        if rc != L.CAM_OK:
+            raise CamError(rc, f"cannot create a context on device {device}")
+        self.h = h
+        self.device = device
+        self._lock = threading.Lock()
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._lib.cam_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != L.CAM_OK:
+            raise CamError(rc, self._lib.cam_last_error(self.h).decode())
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(self._lib.cam_kernel_launches(self.h))
+
+    def profile(self, on: bool = True):
+        self._check(self._lib.cam_profile_enable(self.h, int(on)))
+
+    def profile_read(self, reset: bool = True) -> dict:
+        """{kernel: (launches, total_ms)} since the last reset."""
+        buf = ctypes.create_string_buffer(1 << 16)
+        self._check(self._lib.cam_profile_read(self.h, buf, len(buf), int(reset)))
+        out = {}
+        for line in buf.value.decode().splitlines():
+            name, cnt, ms = line.rsplit(",", 2)
+            out[name] = (int(cnt), float(ms))
+        return out
+
+    def set_stream(self, stream_handle: int | None):
+        self._check(self._lib.cam_ctx_set_stream(self.h, stream_handle))
+
+    def sync(self):
+        self._check(self._lib.cam_ctx_sync(self.h))
+
+    # ---------------------------------------------------------------- helpers
+    def _particles(self, x, y, z, w):
+        dev = L.is_device(x)
+        x, y, z, w = _f32(x), _f32(y), _f32(z), _f32(w)
+        p = L.Particles()
+        p.n = int(x.shape[0])
+        p.x, p.y, p.z, p.w = L.ptr(x), L.ptr(y), L.ptr(z), L.ptr(w)
+        p.mem = L.MEM_DEVICE if dev else L.MEM_HOST
+        return p, (x, y, z, w), dev
+
+    @staticmethod
+    def _empty(shape, dtype, dev, like=None):
+        if dev:
+            import torch
+            tdt = {np.float32: torch.float32, np.float64: torch.float64, np.uint32: torch.int32,
+                   np.uint8: torch.uint8, np.int64: torch.int64, np.complex64: torch.complex64,
+                   np.complex128: torch.complex128}[dtype]
+            return torch.empty(shape, dtype=tdt, device=like.device)
+        return np.empty(shape, dtype)
+
+    # ---------------------------------------------------------------- assignment
+    def assign(self, x, y, z, w, grid: L.Grid, scheme: int, precision: int = F32, out=None) -> AssignResult:
+        p, keep, dev = self._particles(x, y, z, w)
+        shape = (grid.n[0], grid.n[1], grid.n[2])
+        dt = np.float64 if precision == F64 else np.float32
+        mesh = out if out is not None else self._empty(shape, dt, dev, x)
+        st = L.AssignStats()
+        self._check(self._lib.cam_assign(self.h, ctypes.byref(p), ctypes.byref(grid), scheme, precision,
+                                         L.ptr(mesh), L.MEM_DEVICE if dev else L.MEM_HOST, ctypes.byref(st)))
+        return AssignResult(mesh, st.n_in, st.n_lost, st.sum_mesh)
+
+    def count_ngp(self, x, y, z, grid: L.Grid) -> AssignResult:
+        p, keep, dev = self._particles(x, y, z, None)
+        shape = (grid.n[0], grid.n[1], grid.n[2])
+        out = self._empty(shape, np.uint32, dev, x)
+        st = L.AssignStats()
+        self._check(self._lib.cam_count_ngp(self.h, ctypes.byref(p), ctypes.byref(grid), L.ptr(out),
+                                            L.MEM_DEVICE if dev else L.MEM_HOST, ctypes.byref(st)))
+        return AssignResult(out, st.n_in, st.n_lost, st.sum_mesh)
+
+    def cell_keys(self, x, y, z, grid: L.Grid, scheme: int):
+        p, keep, dev = self._particles(x, y, z, None)
+        out = self._empty((p.n,), np.int64, dev, x)
+        self._check(self._lib.cam_cell_keys(self.h, ctypes.byref(p), ctypes.byref(grid), scheme, L.ptr(out),
+                                            L.MEM_DEVICE if dev else L.MEM_HOST))
+        return out
+
+    # ---------------------------------------------------------------- FFT
+    def fft_r2c(self, mesh):
+        dev = L.is_device(mesh)
+        n = mesh.shape[0]
+        prec = F64 if str(mesh.dtype).endswith("float64") else F32
+        cdt = np.complex128 if prec == F64 else np.complex64
+        if not dev:
+            mesh = np.ascontiguousarray(mesh)
+        out = self._empty((n, n, n // 2 + 1), cdt, dev, mesh)
+        self._check(self._lib.cam_fft_r2c(self.h, n, prec, L.ptr(mesh), L.ptr(out),
+                                          L.MEM_DEVICE if dev else L.MEM_HOST))
+        return out
+
+    def fft_c2r(self, spec):
+        dev = L.is_device(spec)
+        n = spec.shape[0]
+        prec = F64 if str(spec.dtype).endswith("complex128") else F32
+        rdt = np.float64 if prec == F64 else np.float32
+        if not dev:
+            spec = np.ascontiguousarray(spec)
+        out = self._empty((n, n, n), rdt, dev, spec)
+        self._check(self._lib.cam_fft_c2r(self.h, n, prec, L.ptr(spec), L.ptr(out),
+                                          L.MEM_DEVICE if dev else L.MEM_HOST))
+        return out
+
+    # ---------------------------------------------------------------- P(k)
+    @staticmethod
+    def pk_opts(scheme=CIC, nbins=0, ndel=1.0, DeltaKmin=0.0, mas_correction=True, sn_correction=True,
+                input_type=L.INPUT_DENSITY) -> L.PkOpts:
+        o = L.PkOpts()
+        o.scheme, o.mas_correction, o.sn_correction = scheme, int(mas_correction), int(sn_correction)
+        o.input_type, o.nbins, o.DeltaKmin, o.ndel = input_type, nbins, DeltaKmin, ndel
+        return o
+
+    def power(self, mesh, box: float, opts: L.PkOpts) -> PkResult:
+        dev = L.is_device(mesh)
+        n = mesh.shape[0]
+        prec = F64 if str(mesh.dtype).endswith("float64") else F32
+        if not dev:
+            mesh = np.ascontiguousarray(mesh)
+        nb = opts.nbins if opts.nbins > 0 else int(n / opts.ndel / 2)
+        pk = np.empty(nb); md = np.empty(nb, np.int64); kv = np.empty(nb)
+        info = L.PkInfo()
+        g = make_grid(n, box)
+        self._check(self._lib.cam_power(self.h, ctypes.byref(g), L.ptr(mesh), prec,
+                                        L.MEM_DEVICE if dev else L.MEM_HOST, ctypes.byref(opts),
+                                        L.ptr(pk), L.ptr(md), L.ptr(kv), ctypes.byref(info)))
+        return PkResult(pk, md, kv, info.n_obj, info.shot_noise, info.normal)
+
+    # ---------------------------------------------------------------- T-web
+    @staticmethod
+    def tweb_opts(R=0.0, lambda_th=0.0, tie_band=1e-5, input_type=L.INPUT_DENSITY) -> L.TwebOpts:
+        o = L.TwebOpts()
+        o.smoothing_R, o.lambda_th, o.tie_band, o.input_type = R, lambda_th, tie_band, input_type
+        return o
+
+    def tweb(self, mesh, box: float, opts: L.TwebOpts, want_lambdas=False) -> TwebResult:
+        dev = L.is_device(mesh)
+        n = mesh.shape[0]
+        prec = F64 if str(mesh.dtype).endswith("float64") else F32
+        if not dev:
+            mesh = np.ascontiguousarray(mesh)
+        labels = self._empty((n, n, n), np.uint8, dev, mesh)
+        lam = self._empty((3, n, n, n), np.float32, dev, mesh) if want_lambdas else None
+        st = L.TwebStats()
+        g = make_grid(n, box)
+        self._check(self._lib.cam_tweb(self.h, ctypes.byref(g), L.ptr(mesh), prec,
+                                       L.MEM_DEVICE if dev else L.MEM_HOST, ctypes.byref(opts),
+                                       L.ptr(labels), L.ptr(lam), L.MEM_DEVICE if dev else L.MEM_HOST,
+                                       ctypes.byref(st)))
+        return TwebResult(labels, lam, np.array(st.counts[:], np.int64), int(st.ties), st.mean)
+
+    # ---------------------------------------------------------------- job
+    def job(self, x, y, z, w, grid: L.Grid, scheme: int, precision=F32, pk: L.PkOpts | None = None,
+            tweb: L.TwebOpts | None = None, want_labels=False):
+        p, keep, dev = self._particles(x, y, z, w)
+        d = L.JobDesc()
+        d.parts, d.grid, d.scheme, d.precision = p, grid, scheme, precision
+        if pk is not None:
+            d.pk = pk
+        d.want_tweb = int(tweb is not None)
+        if tweb is not None:
+            d.tweb = tweb
+        r = L.JobResult()
+        nb = 0
+        if pk is not None:
+            nb = pk.nbins if pk.nbins > 0 else int(grid.n[0] / pk.ndel / 2)
+        pkv = np.empty(nb); md = np.empty(nb, np.int64); kv = np.empty(nb)
+        n = grid.n[0]
+        labels = np.empty((n, n, n), np.uint8) if (tweb is not None and want_labels) else None
+        r.pk, r.modes, r.kvector, r.labels = L.ptr(pkv), L.ptr(md), L.ptr(kv), L.ptr(labels)
+        self._check(self._lib.cam_job_run(self.h, ctypes.byref(d), ctypes.byref(r)))
+        return {
+            "pk": PkResult(pkv, md, kv, r.pk_info.n_obj, r.pk_info.shot_noise, r.pk_info.normal) if nb else None,
+            "assign": AssignResult(None, r.assign.n_in, r.assign.n_lost, r.assign.sum_mesh),
+            "tweb": TwebResult(labels, None, np.array(r.tweb.counts[:], np.int64), int(r.tweb.ties), r.tweb.mean)
+            if tweb is not None else None,
+        }
+
+
+_default: dict[int, Context] = {}
+_default_lock = threading.Lock()
+
+
+def default_context(device: int = 0) -> Context:
+    with _default_lock:
+        if device not in _default:
+            _default[device] = Context(device)
+        return _default[device]
+
+
+# ---------------------------------------------------------------------------
+# Reference-shaped entry points
+# ---------------------------------------------------------------------------
+
+def _getDensity(scheme, N1, N2, N3, L1, L2, L3, d1, d2, d3, min1, min2, min3, xp, yp, zp, Par_mass,
+                delta, weightmass):
+    g = make_grid((N1, N2, N3), (L1, L2, L3), (d1, d2, d3), (min1, min2, min3))
+    w = Par_mass if weightmass else None
+    prec = F64 if str(delta.dtype).endswith("float64") else F32
+    out = delta.reshape(N1, N2, N3) if hasattr(delta, "reshape") else delta
+    ctx = default_context()
+    res = ctx.assign(xp, yp, zp, w, g, scheme, prec, out=out)
+    return res.n_lost
+
+
+def getDensity_NGP(N1, N2, N3, L1, L2, L3, d1, d2, d3, min1, min2, min3, xp, yp, zp, Par_mass, delta,
+                   weightmass):
+    """Source/massFunctions.cpp:35 -- fills ``delta`` (N1*N2*N3) in place; returns NLOSS."""
+    return _getDensity(NGP, N1, N2, N3, L1, L2, L3, d1, d2, d3, min1, min2, min3, xp, yp, zp, Par_mass,
+                       delta, weightmass)
+
+
+def getDensity_CIC(N1, N2, N3, L1, L2, L3, d1, d2, d3, min1, min2, min3, xp, yp, zp, Par_mass, delta,
+                   weightmass):
+    """Source/massFunctions.cpp:678 -- fills ``delta`` in place; returns NLOSS."""
+    return _getDensity(CIC, N1, N2, N3, L1, L2, L3, d1, d2, d3, min1, min2, min3, xp, yp, zp, Par_mass,
+                       delta, weightmass)
+
+
+def getDensity_TSC(N1, N2, N3, L1, L2, L3, d1, d2, d3, min1, min2, min3, xp, yp, zp, Par_mass, delta,
+                   weightmass):
+    """Source/massFunctions.cpp:1050 -- fills ``delta`` in place; returns NLOSS."""
+    return _getDensity(TSC, N1, N2, N3, L1, L2, L3, d1, d2, d3, min1, min2, min3, xp, yp, zp, Par_mass,
+                       delta, weightmass)
+
+
+def do_fftw_r2c(Nft, data_in, data_out):
+    """Source/NumericalMethods.cpp:1718 -- unnormalised r2c into ``data_out``
+    (N, N, N/2+1) complex."""
+    res = default_context().fft_r2c(data_in.reshape(Nft, Nft, Nft))
+    data_out[...] = res.reshape(data_out.shape)
+
+
+def do_fftw_c2r(Nft, data_in, data_out):
+    """Source/NumericalMethods.cpp:1818 -- c2r divided by N^3 into ``data_out``."""
+    res = default_context().fft_c2r(data_in.reshape(Nft, Nft, Nft // 2 + 1))
+    data_out[...] = res.reshape(data_out.shape)
+
+
+@dataclass
+class Params:
+    """The Params getters the hot path reads (Headers/Params.h): _Nft, _Lbox,
+    _mass_assignment (0 NGP, 1 CIC, 2 TSC), _MAS_correction, _SN_correction,
+    _input_type ("density_grid" | "delta_grid"), _ndel_data, _DeltaKmin,
+    _lambdath; smoothing_R is the Gaussian radius applied before the T-web."""
+    Nft: int
+    Lbox: float
+    mass_assignment: int = CIC
+    MAS_correction: bool = True
+    SN_correction: bool = True
+    input_type: str = "density_grid"
+    ndel_data: float = 1.0
+    DeltaKmin: float = 0.0
+    Nnp_data: int = 0
+    lambdath: float = 0.0
+    smoothing_R: float = 0.0
+    tie_band: float = 1e-5
+    device: int = 0
+
+
+class PowerSpectrumF:
+    """Source/PowerSpectrumF.cpp:1739 (compute_power_spectrum_grid) with the
+    accessors of Headers/PowerSpectrumF.h."""
+
+    def __init__(self, params: Params):
+        self.params = params
+        self.pk0 = np.zeros(0)
+        self.modes_g = np.zeros(0, np.int64)
+        self.kvector_data = np.zeros(0)
+
+    def compute_power_spectrum_grid(self, data_in, write_to_file=False):
+        p = self.params
+        it = L.INPUT_DENSITY if p.input_type == "density_grid" else L.INPUT_DELTA
+        o = Context.pk_opts(p.mass_assignment, p.Nnp_data, p.ndel_data, p.DeltaKmin, p.MAS_correction,
+                            p.SN_correction, it)
+        mesh = data_in.reshape(p.Nft, p.Nft, p.Nft)
+        r = default_context(p.device).power(mesh, p.Lbox, o)
+        self.pk0, self.modes_g, self.kvector_data = r.pk, r.modes, r.kvector
+        self.shot_noise, self.normal_power, self.ngal = r.shot_noise, r.normal, r.n_obj
+        if write_to_file:
+            raise CamError(L.CAM_E_UNSUPPORTED, "file output is not part of the GPU path")
+
+    def _pk0(self, i):
+        return self.pk0[i]
+
+    def _nmodes_k(self, i):
+        return self.modes_g[i]
+
+    def _kvector_data(self, i):
+        return self.kvector_data[i]
+
+
+I_KNOT, I_FILAMENT, I_SHEET, I_VOID = 1, 2, 3, 4
+
+
+class Cwclass:
+    """Source/Cwclass.cpp:235 (get_CWC) with the public members lambda1..3,
+    CWClass and the volume fractions of Headers/Cwclass.h."""
+
+    def __init__(self, params: Params):
+        self.params = params
+
+    def get_CWC(self, delta):
+        p = self.params
+        it = L.INPUT_DELTA if p.input_type == "delta_grid" else L.INPUT_DENSITY
+        o = Context.tweb_opts(p.smoothing_R, p.lambdath, p.tie_band, it)
+        r = default_context(p.device).tweb(delta.reshape(p.Nft, p.Nft, p.Nft), p.Lbox, o, want_lambdas=True)
+        ng = float(p.Nft) ** 3
+        self.lambda1, self.lambda2, self.lambda3 = (r.lambdas[0].reshape(-1), r.lambdas[1].reshape(-1),
+                                                    r.lambdas[2].reshape(-1))
+        self.CWClass = r.labels.reshape(-1)
+        self.volume_knots, self.volume_filaments, self.volume_sheets, self.volume_voids = (
+            r.counts[0] / ng, r.counts[1] / ng, r.counts[2] / ng, r.counts[3] / ng)
+        self.ties = r.ties
+
+    do_CWC = get_CWC
+
+    def get_Tclassification(self, ig):
+        return int(self.CWClass[ig])

@@ -1,0 +1,596 @@
+// C ABI of libcam: contexts, scratch memory, deterministic reductions and
+// the entry points declared in include/cam.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "cam_internal.h"
+
+namespace cam {
+
+void *scratch(cam_ctx *ctx, const char *name, size_t bytes)
+{
+    bytes = std::max<size_t>(bytes, 256);
+    DevBuf &b = ctx->bufs[name];
+    if (b.cap >= bytes) return b.ptr;
+    const size_t want = std::max(bytes, b.cap + b.cap / 4);
+    if (ctx->budget && ctx->used - b.cap + want > ctx->budget)
+        throw Error{CAM_E_NOMEM, std::string("HBM budget exceeded allocating ") + name};
+    if (b.ptr) {
+        CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        CAM_CUDA_TRY(cudaFree(b.ptr));
+        ctx->used -= b.cap;
+        b.ptr = nullptr;
+        b.cap = 0;
+    }
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Error{CAM_E_NOMEM, std::string("cudaMalloc failed for ") + name + ": " + cudaGetErrorString(e)};
+    }
+    b.ptr = p;
+    b.cap = want;
+    ctx->used += want;
+    return p;
+}
+
+void prof_begin(cam_ctx *ctx, const char *name)
+{
+    if (!ctx->prof_on) return;
+    auto take = [&]() {
+        cudaEvent_t e;
+        if (!ctx->prof_pool.empty()) {
+            e = ctx->prof_pool.back();
+            ctx->prof_pool.pop_back();
+        } else {
+            CAM_CUDA_TRY(cudaEventCreate(&e));
+        }
+        return e;
+    };
+    ProfRecord r{name, take(), take()};
+    CAM_CUDA_TRY(cudaEventRecord(r.start, ctx->stream));
+    ctx->prof_pending.push_back(r);
+}
+
+void prof_end(cam_ctx *ctx)
+{
+    if (!ctx->prof_on || ctx->prof_pending.empty()) return;
+    CAM_CUDA_TRY(cudaEventRecord(ctx->prof_pending.back().stop, ctx->stream));
+}
+
+// Folds finished records into the per-name totals (synchronises).
+static void prof_collect(cam_ctx *ctx)
+{
+    if (ctx->prof_pending.empty()) return;
+    CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    for (auto &r : ctx->prof_pending) {
+        float ms = 0.f;
+        CAM_CUDA_TRY(cudaEventElapsedTime(&ms, r.start, r.stop));
+        auto &acc = ctx->prof_acc[r.name];
+        acc.first += 1;
+        acc.second += ms;
+        ctx->prof_pool.push_back(r.start);
+        ctx->prof_pool.push_back(r.stop);
+    }
+    ctx->prof_pending.clear();
+}
+
+void release_all(cam_ctx *ctx)
+{
+    for (auto &kv : ctx->bufs)
+        if (kv.second.ptr) cudaFree(kv.second.ptr);
+    ctx->bufs.clear();
+    ctx->used = 0;
+}
+
+namespace {
+
+constexpr int kRedBlocks = 2 * kNumSMs;
+
+template <typename T>
+__global__ void __launch_bounds__(256) partial_sum_kernel(const T *__restrict__ in, int64_t n, double *__restrict__ part)
+{
+    __shared__ double red[8];
+    // Static contiguous chunk per CTA: the summation order is fixed.
+    const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+    const int64_t beg = (int64_t)blockIdx.x * chunk, end = min(n, beg + chunk);
+    double acc = 0.0;
+    for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) acc += (double)in[i];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < 8; ++w) t += red[w];
+        part[blockIdx.x] = t;
+    }
+}
+
+__global__ void final_sum_kernel(const double *__restrict__ part, int np, double *__restrict__ out,
+                                 double divisor)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double t = 0.0;
+        for (int i = 0; i < np; ++i) t += part[i];
+        out[0] = t;
+        out[1] = t / divisor;
+    }
+}
+
+}  // namespace
+
+// out[0] = sum, out[1] = sum / n (FP64, fixed order).
+void reduce_sum_f64(cam_ctx *ctx, const double *in, int64_t n, double *out)
+{
+    auto *part = static_cast<double *>(scratch(ctx, "red.part", kRedBlocks * sizeof(double)));
+    CAM_LAUNCH(ctx, partial_sum_kernel<double>, kRedBlocks, 256, 0, in, n, part);
+    CAM_LAUNCH(ctx, final_sum_kernel, 1, 32, 0, part, kRedBlocks, out, (double)n);
+}
+
+void mesh_mean(cam_ctx *ctx, const void *mesh, int precision, int64_t ncell, double *d_out)
+{
+    auto *part = static_cast<double *>(scratch(ctx, "red.part", kRedBlocks * sizeof(double)));
+    if (precision == CAM_F32)
+        CAM_LAUNCH(ctx, partial_sum_kernel<float>, kRedBlocks, 256, 0, (const float *)mesh, ncell, part);
+    else
+        CAM_LAUNCH(ctx, partial_sum_kernel<double>, kRedBlocks, 256, 0, (const double *)mesh, ncell, part);
+    CAM_LAUNCH(ctx, final_sum_kernel, 1, 32, 0, part, kRedBlocks, d_out, (double)ncell);
+}
+
+}  // namespace cam
+
+using namespace cam;
+
+namespace {
+
+template <typename F>
+int guarded(cam_ctx *ctx, F &&f)
+{
+    if (!ctx) return CAM_E_INVAL;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    try {
+        CAM_CUDA_TRY(cudaSetDevice(ctx->device));
+        f();
+        ctx->err.clear();
+        return CAM_OK;
+    } catch (const Error &e) {
+        ctx->err = e.msg;
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        ctx->err = "host allocation failed";
+        return CAM_E_NOMEM;
+    } catch (...) {
+        ctx->err = "unexpected exception";
+        return CAM_E_CUDA;
+    }
+}
+
+size_t esize(int precision) { return precision == CAM_F64 ? 8 : 4; }
+
+void check_grid_cubic(const cam_grid *g)
+{
+    CAM_REQUIRE(g, CAM_E_INVAL, "null grid");
+    CAM_REQUIRE(g->n[0] == g->n[1] && g->n[1] == g->n[2], CAM_E_UNSUPPORTED, "FFT stages need a cubic mesh");
+    CAM_REQUIRE(g->L[0] > 0.f && std::isfinite(g->L[0]), CAM_E_INVAL, "box side must be > 0");
+}
+
+void check_prec(int p) { CAM_REQUIRE(p == CAM_F32 || p == CAM_F64, CAM_E_INVAL, "precision must be CAM_F32 or CAM_F64"); }
+void check_mem(int m) { CAM_REQUIRE(m == CAM_MEM_HOST || m == CAM_MEM_DEVICE, CAM_E_INVAL, "mem must be CAM_MEM_HOST or CAM_MEM_DEVICE"); }
+
+struct DevParticles {
+    const float *x, *y, *z, *w;
+    int64_t n;
+};
+
+DevParticles stage_particles(cam_ctx *ctx, const cam_particles *p)
+{
+    CAM_REQUIRE(p, CAM_E_INVAL, "null particles");
+    CAM_REQUIRE(p->n >= 0, CAM_E_INVAL, "negative particle count");
+    check_mem(p->mem);
+    CAM_REQUIRE(p->n == 0 || (p->x && p->y && p->z), CAM_E_INVAL, "null particle coordinates");
+    DevParticles d{};
+    d.n = p->n;
+    d.x = stage_in(ctx, "in.x", p->x, p->n, p->mem);
+    d.y = stage_in(ctx, "in.y", p->y, p->n, p->mem);
+    d.z = stage_in(ctx, "in.z", p->z, p->n, p->mem);
+    d.w = p->w ? stage_in(ctx, "in.w", p->w, p->n, p->mem) : nullptr;
+    return d;
+}
+
+cam_grid resolved(const cam_grid &g)
+{
+    cam_grid r = g;
+    for (int a = 0; a < 3; ++a)
+        if (r.d[a] == 0.f) r.d[a] = r.L[a] / (float)r.n[a];
+    return r;
+}
+
+int nbins_default(const cam_pk_opts &o, int64_t n)
+{
+    if (o.nbins > 0) return o.nbins;
+    return (int)((double)n / o.ndel / 2.0);  // Nnp_data = Nft / ndel_data / 2
+}
+
+// Power spectrum of a spectrum already on the device (split layout).
+void power_from_spectrum(cam_ctx *ctx, const Spectrum &s, float L, double n_obj, const cam_pk_opts &o,
+                         double *pk, int64_t *modes, double *kvec, cam_pk_info *info)
+{
+    const int nbins = nbins_default(o, s.n);
+    std::vector<double> sr(nbins), ss(nbins);
+    std::vector<int64_t> md(nbins);
+    power_bin(ctx, s, o, nbins, sr.data(), ss.data(), md.data());
+    const double vol = (double)L * (double)L * (double)L;
+    double normal, ngal;
+    if (o.input_type == CAM_INPUT_DENSITY) {
+        ngal = n_obj;
+        normal = ngal * ngal / vol;  // PowerSpectrumF.cpp:1764
+    } else {
+        ngal = 1.0;
+        const double ng = (double)s.n * s.n * s.n;
+        normal = ng * ng / vol;      // PowerSpectrumF.cpp:1775
+    }
+    const double sn = vol / ngal;   // PowerSpectrumF.cpp:1782
+    const double kf = 2.0 * M_PI / (double)L;
+    for (int b = 0; b < nbins; ++b) {
+        double v = 0.0;
+        if (md[b] > 0) {
+            v = sr[b] / ((double)md[b] * normal);
+            if (o.sn_correction) v -= sn * ss[b] / (double)md[b];
+        }
+        if (pk) pk[b] = v;
+        if (modes) modes[b] = md[b];
+        if (kvec) kvec[b] = kf * (o.DeltaKmin + ((double)b + 0.5) * o.ndel);  // PowerSpectrumF.cpp:1792
+    }
+    if (info) {
+        info->n_obj = ngal;
+        info->shot_noise = sn;
+        info->normal = normal;
+        info->kf = kf;
+    }
+}
+
+Spectrum alloc_spectrum(cam_ctx *ctx, int64_t n, int precision, const char *tag)
+{
+    Spectrum s;
+    s.n = n;
+    s.precision = precision;
+    const size_t cs = 2 * esize(precision);
+    s.main = scratch(ctx, (std::string(tag) + ".main").c_str(), (size_t)n * n * (n / 2) * cs);
+    s.nyq = scratch(ctx, (std::string(tag) + ".nyq").c_str(), (size_t)n * n * cs);
+    return s;
+}
+
+void validate_pk(const cam_pk_opts *o)
+{
+    CAM_REQUIRE(o, CAM_E_INVAL, "null P(k) options");
+    CAM_REQUIRE(o->scheme >= 0 && o->scheme <= 2, CAM_E_INVAL, "unknown window scheme");
+    CAM_REQUIRE(o->input_type == CAM_INPUT_DENSITY || o->input_type == CAM_INPUT_DELTA, CAM_E_INVAL, "unknown input type");
+    CAM_REQUIRE(o->ndel > 0.0 && std::isfinite(o->ndel), CAM_E_INVAL, "ndel must be > 0");
+    CAM_REQUIRE(o->nbins >= 0, CAM_E_INVAL, "nbins must be >= 0");
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *cam_version(void) { return "cosmicatlas-b200 0.1 (sm_100a)"; }
+
+int cam_ctx_create(int device, size_t hbm_budget, cam_ctx **out)
+{
+    if (!out) return CAM_E_INVAL;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        return CAM_E_INVAL;
+    }
+    auto *c = new (std::nothrow) cam_ctx;
+    if (!c) return CAM_E_NOMEM;
+    c->device = device;
+    c->budget = hbm_budget;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        delete c;
+        return CAM_E_CUDA;
+    }
+    c->stream = c->own_stream;
+    *out = c;
+    return CAM_OK;
+}
+
+int cam_ctx_destroy(cam_ctx *ctx)
+{
+    if (!ctx) return CAM_E_INVAL;
+    {
+        std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+        cudaSetDevice(ctx->device);
+        cudaStreamSynchronize(ctx->stream);
+        for (auto &kv : ctx->plans) delete kv.second;
+        for (auto &r : ctx->prof_pending) {
+            cudaEventDestroy(r.start);
+            cudaEventDestroy(r.stop);
+        }
+        for (auto e : ctx->prof_pool) cudaEventDestroy(e);
+        ctx->plans.clear();
+        release_all(ctx);
+        if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    }
+    delete ctx;
+    return CAM_OK;
+}
+
+int cam_ctx_set_stream(cam_ctx *ctx, void *stream)
+{
+    return guarded(ctx, [&] { ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream; });
+}
+
+int cam_ctx_sync(cam_ctx *ctx)
+{
+    return guarded(ctx, [&] { CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream)); });
+}
+
+const char *cam_last_error(cam_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int64_t cam_kernel_launches(cam_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
+int cam_profile_enable(cam_ctx *ctx, int on)
+{
+    return guarded(ctx, [&] {
+        prof_collect(ctx);
+        ctx->prof_on = on != 0;
+    });
+}
+
+int cam_profile_read(cam_ctx *ctx, char *buf, size_t len, int reset)
+{
+    return guarded(ctx, [&] {
+        CAM_REQUIRE(buf && len > 0, CAM_E_INVAL, "null buffer");
+        prof_collect(ctx);
+        std::string out;
+        for (auto &kv : ctx->prof_acc) {
+            char line[256];
+            snprintf(line, sizeof(line), "%s,%lld,%.6f\n", kv.first.c_str(), (long long)kv.second.first,
+                     kv.second.second);
+            out += line;
+        }
+        CAM_REQUIRE(out.size() + 1 <= len, CAM_E_INVAL, "profile buffer too small");
+        memcpy(buf, out.c_str(), out.size() + 1);
+        if (reset) ctx->prof_acc.clear();
+    });
+}
+
+int cam_assign(cam_ctx *ctx, const cam_particles *parts, const cam_grid *grid, int scheme,
+               int precision, void *mesh_out, int out_mem, cam_assign_stats *stats)
+{
+    return guarded(ctx, [&] {
+        CAM_REQUIRE(grid && mesh_out, CAM_E_INVAL, "null grid or output");
+        check_prec(precision);
+        check_mem(out_mem);
+        const DevParticles d = stage_particles(ctx, parts);
+        const cam_grid g = resolved(*grid);
+        const int64_t ncell = g.n[0] * g.n[1] * g.n[2];
+        AssignOut out;
+        out.precision = precision;
+        out.mesh = out_mem == CAM_MEM_DEVICE ? mesh_out : scratch(ctx, "asg.mesh", ncell * esize(precision));
+        out.d_sum = static_cast<double *>(scratch(ctx, "asg.sum", 2 * sizeof(double)));
+        assign_device(ctx, d.x, d.y, d.z, d.w, d.n, g, scheme, out);
+        if (out_mem == CAM_MEM_HOST)
+            CAM_CUDA_TRY(cudaMemcpyAsync(mesh_out, out.mesh, ncell * esize(precision), cudaMemcpyDeviceToHost, ctx->stream));
+        double sum = 0.0;
+        CAM_CUDA_TRY(cudaMemcpyAsync(&sum, out.d_sum, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        if (stats) {
+            stats->n_in = out.n_in;
+            stats->n_lost = out.n_lost;
+            stats->sum_mesh = sum;
+        }
+    });
+}
+
+int cam_count_ngp(cam_ctx *ctx, const cam_particles *parts, const cam_grid *grid, uint32_t *counts_out,
+                  int out_mem, cam_assign_stats *stats)
+{
+    return guarded(ctx, [&] {
+        CAM_REQUIRE(grid && counts_out, CAM_E_INVAL, "null grid or output");
+        check_mem(out_mem);
+        CAM_REQUIRE(parts && parts->w == nullptr, CAM_E_INVAL, "integer counts take unweighted particles");
+        const DevParticles d = stage_particles(ctx, parts);
+        const cam_grid g = resolved(*grid);
+        const int64_t ncell = g.n[0] * g.n[1] * g.n[2];
+        AssignOut out;
+        out.precision = -1;
+        out.mesh = out_mem == CAM_MEM_DEVICE ? (void *)counts_out : scratch(ctx, "asg.mesh", ncell * 4);
+        out.d_sum = static_cast<double *>(scratch(ctx, "asg.sum", 2 * sizeof(double)));
+        assign_device(ctx, d.x, d.y, d.z, nullptr, d.n, g, CAM_NGP, out);
+        if (out_mem == CAM_MEM_HOST)
+            CAM_CUDA_TRY(cudaMemcpyAsync(counts_out, out.mesh, ncell * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        double sum = 0.0;
+        CAM_CUDA_TRY(cudaMemcpyAsync(&sum, out.d_sum, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        if (stats) {
+            stats->n_in = out.n_in;
+            stats->n_lost = out.n_lost;
+            stats->sum_mesh = sum;
+        }
+    });
+}
+
+int cam_cell_keys(cam_ctx *ctx, const cam_particles *parts, const cam_grid *grid, int scheme,
+                  int64_t *keys_out, int out_mem)
+{
+    return guarded(ctx, [&] {
+        CAM_REQUIRE(grid && keys_out, CAM_E_INVAL, "null grid or output");
+        check_mem(out_mem);
+        CAM_REQUIRE(scheme >= CAM_NGP && scheme <= CAM_TSC, CAM_E_INVAL, "unknown mass assignment scheme");
+        const DevParticles d = stage_particles(ctx, parts);
+        const cam_grid g = resolved(*grid);
+        int64_t *dk = out_mem == CAM_MEM_DEVICE ? keys_out
+                                                : static_cast<int64_t *>(scratch(ctx, "keys.out", std::max<int64_t>(d.n, 1) * 8));
+        cell_keys_device(ctx, d.x, d.y, d.z, d.n, g, scheme, dk);
+        if (out_mem == CAM_MEM_HOST && d.n > 0)
+            CAM_CUDA_TRY(cudaMemcpyAsync(keys_out, dk, d.n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+int cam_fft_r2c(cam_ctx *ctx, int64_t n, int precision, const void *in, void *out, int mem)
+{
+    return guarded(ctx, [&] {
+        CAM_REQUIRE(in && out, CAM_E_INVAL, "null FFT buffer");
+        check_prec(precision);
+        check_mem(mem);
+        FftPlan *plan = get_plan(ctx, n, precision);
+        const size_t es = esize(precision);
+        const size_t in_bytes = (size_t)n * n * n * es;
+        const size_t out_bytes = (size_t)n * n * (n / 2 + 1) * 2 * es;
+        const void *din = mem == CAM_MEM_DEVICE ? in : scratch(ctx, "fft.in", in_bytes);
+        if (mem == CAM_MEM_HOST) CAM_CUDA_TRY(cudaMemcpyAsync((void *)din, in, in_bytes, cudaMemcpyHostToDevice, ctx->stream));
+        Spectrum s = alloc_spectrum(ctx, n, precision, "fft.spec");
+        fft_r2c_split(ctx, plan, din, nullptr, s);
+        void *dout = mem == CAM_MEM_DEVICE ? out : scratch(ctx, "fft.out", out_bytes);
+        split_to_fftw(ctx, s, dout);
+        if (mem == CAM_MEM_HOST) CAM_CUDA_TRY(cudaMemcpyAsync(out, dout, out_bytes, cudaMemcpyDeviceToHost, ctx->stream));
+        CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+int cam_fft_c2r(cam_ctx *ctx, int64_t n, int precision, const void *in, void *out, int mem)
+{
+    return guarded(ctx, [&] {
+        CAM_REQUIRE(in && out, CAM_E_INVAL, "null FFT buffer");
+        check_prec(precision);
+        check_mem(mem);
+        FftPlan *plan = get_plan(ctx, n, precision);
+        const size_t es = esize(precision);
+        const size_t out_bytes = (size_t)n * n * n * es;
+        const size_t in_bytes = (size_t)n * n * (n / 2 + 1) * 2 * es;
+        const void *din = mem == CAM_MEM_DEVICE ? in : scratch(ctx, "fft.out", in_bytes);
+        if (mem == CAM_MEM_HOST) CAM_CUDA_TRY(cudaMemcpyAsync((void *)din, in, in_bytes, cudaMemcpyHostToDevice, ctx->stream));
+        Spectrum s = alloc_spectrum(ctx, n, precision, "fft.spec");
+        fftw_to_split(ctx, din, s);
+        void *dout = mem == CAM_MEM_DEVICE ? out : scratch(ctx, "fft.in", out_bytes);
+        fft_c2r_split(ctx, plan, s, dout, 1.0 / ((double)n * n * n));
+        if (mem == CAM_MEM_HOST) CAM_CUDA_TRY(cudaMemcpyAsync(out, dout, out_bytes, cudaMemcpyDeviceToHost, ctx->stream));
+        CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+int cam_power(cam_ctx *ctx, const cam_grid *grid, const void *mesh, int precision, int mem,
+              const cam_pk_opts *opts, double *pk, int64_t *modes, double *kvector, cam_pk_info *info)
+{
+    return guarded(ctx, [&] {
+        check_grid_cubic(grid);
+        CAM_REQUIRE(mesh, CAM_E_INVAL, "null mesh");
+        check_prec(precision);
+        check_mem(mem);
+        validate_pk(opts);
+        const int64_t n = grid->n[0];
+        FftPlan *plan = get_plan(ctx, n, precision);
+        const size_t bytes = (size_t)n * n * n * esize(precision);
+        const void *dm = mem == CAM_MEM_DEVICE ? mesh : scratch(ctx, "pk.mesh", bytes);
+        if (mem == CAM_MEM_HOST) CAM_CUDA_TRY(cudaMemcpyAsync((void *)dm, mesh, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        auto *dsum = static_cast<double *>(scratch(ctx, "pk.sum", 2 * sizeof(double)));
+        double hs[2] = {0.0, 0.0};
+        const double *sub = nullptr;
+        if (opts->input_type == CAM_INPUT_DENSITY) {
+            mesh_mean(ctx, dm, precision, n * n * n, dsum);
+            sub = dsum + 1;  // rho - N_gal / N^3 (PowerSpectrumF.cpp:1756-1762)
+        }
+        Spectrum s = alloc_spectrum(ctx, n, precision, "job.spec");
+        fft_r2c_split(ctx, plan, dm, sub, s);
+        if (sub) {
+            CAM_CUDA_TRY(cudaMemcpyAsync(hs, dsum, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
+            CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        }
+        power_from_spectrum(ctx, s, grid->L[0], hs[0], *opts, pk, modes, kvector, info);
+    });
+}
+
+int cam_tweb(cam_ctx *ctx, const cam_grid *grid, const void *mesh, int precision, int mem,
+             const cam_tweb_opts *opts, uint8_t *labels, float *lambdas, int out_mem, cam_tweb_stats *stats)
+{
+    return guarded(ctx, [&] {
+        check_grid_cubic(grid);
+        CAM_REQUIRE(mesh && opts, CAM_E_INVAL, "null mesh or options");
+        check_prec(precision);
+        check_mem(mem);
+        check_mem(out_mem);
+        CAM_REQUIRE(opts->input_type == CAM_INPUT_DENSITY || opts->input_type == CAM_INPUT_DELTA, CAM_E_INVAL,
+                    "unknown input type");
+        const int64_t n = grid->n[0], ncell = n * n * n;
+        FftPlan *plan = get_plan(ctx, n, precision);
+        const size_t bytes = (size_t)ncell * esize(precision);
+        const void *dm = mem == CAM_MEM_DEVICE ? mesh : scratch(ctx, "pk.mesh", bytes);
+        if (mem == CAM_MEM_HOST) CAM_CUDA_TRY(cudaMemcpyAsync((void *)dm, mesh, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        auto *dsum = static_cast<double *>(scratch(ctx, "tw.sum", 2 * sizeof(double)));
+        const double *sub = nullptr;
+        if (opts->input_type == CAM_INPUT_DENSITY) {
+            mesh_mean(ctx, dm, precision, ncell, dsum);
+            sub = dsum + 1;
+        }
+        Spectrum s = alloc_spectrum(ctx, n, precision, "job.spec");
+        fft_r2c_split(ctx, plan, dm, sub, s);
+        uint8_t *dl = labels ? (out_mem == CAM_MEM_DEVICE ? labels : static_cast<uint8_t *>(scratch(ctx, "tw.labels", ncell))) : nullptr;
+        float *dlam = lambdas ? (out_mem == CAM_MEM_DEVICE ? lambdas : static_cast<float *>(scratch(ctx, "tw.lam", 3 * ncell * 4))) : nullptr;
+        cam_tweb_stats st{};
+        tweb_device(ctx, plan, s, grid->L[0], sub, opts->input_type, *opts, dl, dlam, &st);
+        if (out_mem == CAM_MEM_HOST) {
+            if (labels) CAM_CUDA_TRY(cudaMemcpyAsync(labels, dl, ncell, cudaMemcpyDeviceToHost, ctx->stream));
+            if (lambdas) CAM_CUDA_TRY(cudaMemcpyAsync(lambdas, dlam, 3 * ncell * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        }
+        CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        if (stats) *stats = st;
+    });
+}
+
+int cam_job_run(cam_ctx *ctx, const cam_job_desc *job, cam_job_result *res)
+{
+    return guarded(ctx, [&] {
+        CAM_REQUIRE(job && res, CAM_E_INVAL, "null job or result");
+        check_grid_cubic(&job->grid);
+        check_prec(job->precision);
+        const bool want_pk = job->pk.nbins > 0 || job->pk.ndel > 0.0;
+        if (want_pk) validate_pk(&job->pk);
+        const cam_grid g = resolved(job->grid);
+        const int64_t n = g.n[0], ncell = n * n * n;
+        const DevParticles d = stage_particles(ctx, &job->parts);
+        FftPlan *plan = get_plan(ctx, n, job->precision);
+        AssignOut out;
+        out.precision = job->precision;
+        out.mesh = scratch(ctx, "job.mesh", ncell * esize(job->precision));
+        auto *dsum = static_cast<double *>(scratch(ctx, "job.sum", 2 * sizeof(double)));
+        out.d_sum = dsum;
+        assign_device(ctx, d.x, d.y, d.z, d.w, d.n, g, job->scheme, out);
+        // FFT of rho - mean, mean from the deposit's exact per-brick sums.
+        Spectrum s = alloc_spectrum(ctx, n, job->precision, "job.spec");
+        fft_r2c_split(ctx, plan, out.mesh, dsum + 1, s);
+        double hs[2] = {0.0, 0.0};
+        CAM_CUDA_TRY(cudaMemcpyAsync(hs, dsum, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
+        CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        res->assign.n_in = out.n_in;
+        res->assign.n_lost = out.n_lost;
+        res->assign.sum_mesh = hs[0];
+        if (want_pk) {
+            cam_pk_opts po = job->pk;
+            power_from_spectrum(ctx, s, g.L[0], hs[0], po, res->pk, res->modes, res->kvector, &res->pk_info);
+        }
+        if (job->want_tweb) {
+            uint8_t *dl = res->labels ? static_cast<uint8_t *>(scratch(ctx, "tw.labels", ncell)) : nullptr;
+            cam_tweb_opts to = job->tweb;
+            tweb_device(ctx, plan, s, g.L[0], dsum + 1, to.input_type, to, dl, nullptr, &res->tweb);
+            if (dl) {
+                CAM_CUDA_TRY(cudaMemcpyAsync(res->labels, dl, ncell, cudaMemcpyDeviceToHost, ctx->stream));
+                CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+            }
+        }
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,554 @@
+// Particle -> mesh mass assignment (NGP / CIC / TSC) for sm_100a.
+//
+// Replaces getDensity_NGP / getDensity_CIC / getDensity_TSC,
+// Source/massFunctions.cpp:35-98, :678-790, :1050-1165.
+//
+// Pipeline (no float atomics, bitwise deterministic):
+//   1. bin_count   : per particle, the reference's FP32 home cell (bit-exact
+//                    key), the mesh bricks its stencil touches, and a count
+//                    per brick (integer atomics).  Also lost particles and
+//                    max |w|.
+//   2. scan        : exclusive scan of the brick counts.
+//   3. bin_scatter : per particle, one 16-byte payload per touched brick:
+//                    home cell relative to the brick, the exact fractional
+//                    offset in fixed point, the weight.
+//   4. deposit     : one CTA per brick accumulates its payloads into a
+//                    shared-memory tile of int64 fixed-point cell sums.
+//                    Integer sums do not depend on the order the payloads
+//                    arrived in, so the gather is deterministic; the tile is
+//                    then written once, coalesced, as FP32/FP64 (or uint32
+//                    counts for NGP).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "cam_internal.h"
+
+namespace cam {
+namespace {
+
+constexpr int kBinThreads = 256;
+constexpr int kDepositThreads = 256;
+
+__device__ __forceinline__ int wrapi(int v, int n)
+{
+    if (v >= n) v -= n;
+    if (v < 0) v += n;
+    if (v < 0 || v >= n) v = ((v % n) + n) % n;
+    return v;
+}
+
+// Reference FP32 home cell (see orc_keys / ref_home in the oracle).
+// NGP: x on [min, min+L); CIC: x - d/2 wrapped once by +-L then [min, min+L);
+// TSC: x on [min, min+L].  i = floor((x-min)/d) in IEEE float, then mod N.
+template <int SCHEME>
+__device__ __forceinline__ bool home_cell(const float p[3], const AssignGeom &g, int c[3])
+{
+    float q[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float v = p[a];
+        if (SCHEME == CAM_CIC) {
+            v = __fsub_rn(v, __fmul_rn(0.5f, g.d[a]));
+            if (v < 0.0f) v = __fadd_rn(v, g.L[a]);
+            if (v >= g.L[a]) v = __fsub_rn(v, g.L[a]);
+        }
+        q[a] = v;
+    }
+    bool ok = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float hi = __fadd_rn(g.mn[a], g.L[a]);
+        ok = ok && (SCHEME == CAM_TSC ? (q[a] >= g.mn[a] && q[a] <= hi)
+                                      : (q[a] >= g.mn[a] && q[a] < hi));
+    }
+    if (!ok) return false;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float u = __fdiv_rn(__fsub_rn(q[a], g.mn[a]), g.d[a]);
+        int i = (int)floorf(u);
+        c[a] = i % g.n[a];  // fmod(float(i), float(N)) for 0 <= i < 2^24
+    }
+    return true;
+}
+
+// Exact offset t = (x - min)/d - 1/2 - c in cells, nearest periodic image,
+// in FP32 with error-free transformations: TwoSum for x - min and a fused
+// multiply-add for the subtraction of (c + 1/2) d (the product is exact
+// inside the FMA).  |error| ~ 2e-7 cells.
+__device__ __forceinline__ float exact_offset(float x, float mn, float d, int c, int n)
+{
+    const float hi = __fsub_rn(x, mn);
+    const float bb = __fsub_rn(hi, x);
+    const float lo = __fadd_rn(__fsub_rn(x, __fsub_rn(hi, bb)), __fsub_rn(-mn, bb));
+    const float u = __fdiv_rn(hi, d);
+    float ci = (float)c + 0.5f;
+    const float diff = u - ci;
+    if (diff > 0.5f * (float)n) ci += (float)n;
+    else if (diff < -0.5f * (float)n) ci -= (float)n;
+    const float r = __fadd_rn(__fmaf_rn(-ci, d, hi), lo);
+    return __fdiv_rn(r, d);
+}
+
+template <int SCHEME>
+struct Stencil {
+    static constexpr int W = SCHEME == CAM_NGP ? 1 : (SCHEME == CAM_CIC ? 2 : 3);
+    static constexpr int FIRST = SCHEME == CAM_TSC ? -1 : 0;
+};
+
+// Payload word per axis: bits 26..31 = home cell relative to the brick + 8,
+// bits 0..25 = round(t * 2^24) + 2^24 (t in [-1, 3)).
+__device__ __forceinline__ uint32_t pack_axis(int cl, float t)
+{
+    int tq = __float2int_rn(t * 16777216.0f) + 16777216;
+    tq = min(max(tq, 0), (1 << 26) - 1);
+    return ((uint32_t)(cl + 8) << 26) | (uint32_t)tq;
+}
+__device__ __forceinline__ void unpack_axis(uint32_t v, int &cl, float &t)
+{
+    cl = (int)(v >> 26) - 8;
+    t = (float)((int)(v & 0x3FFFFFFu) - 16777216) * (1.0f / 16777216.0f);
+}
+
+__device__ __forceinline__ int brick_linear(const AssignGeom &g, int b0, int b1, int b2)
+{
+    return (b0 * g.nb[1] + b1) * g.nb[2] + b2;
+}
+
+// Passes 1 and 3.  COUNT: count per brick, lost particles, max |w|.
+// SCATTER: write one payload per touched brick at cursor[brick]++.
+template <int SCHEME, bool SCATTER>
+__global__ void __launch_bounds__(kBinThreads)
+bin_kernel(const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z,
+           const float *__restrict__ w, int64_t np, AssignGeom g, uint32_t *__restrict__ counter,
+           uint4 *__restrict__ payload, unsigned long long *__restrict__ lost,
+           unsigned int *__restrict__ wmax_bits)
+{
+    using St = Stencil<SCHEME>;
+    const int lane = threadIdx.x & 31;
+    unsigned long long my_lost = 0;
+    unsigned int my_wmax = 0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < np; base += stride) {
+        const int64_t p = base + threadIdx.x;
+        const bool inrange = p < np;
+        float pos[3] = {0.f, 0.f, 0.f};
+        float wt = 1.0f;
+        if (inrange) {
+            pos[0] = __ldcs(x + p);
+            pos[1] = __ldcs(y + p);
+            pos[2] = __ldcs(z + p);
+            if (w) wt = __ldcs(w + p);
+        }
+        int c[3] = {0, 0, 0};
+        const bool valid = inrange && home_cell<SCHEME>(pos, g, c);
+        if (!SCATTER) {
+            if (inrange && !valid) ++my_lost;
+            if (valid && w) my_wmax = max(my_wmax, __float_as_uint(fabsf(wt)));
+        }
+        // Bricks touched along each axis: 1 or 2.
+        int bl[3], nbx[3];
+        float t[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const int lo = wrapi(c[a] + St::FIRST, g.n[a]);
+            const int hi = wrapi(c[a] + St::FIRST + St::W - 1, g.n[a]);
+            bl[a] = lo / g.b[a];
+            const int bh = hi / g.b[a];
+            nbx[a] = (bh == bl[a]) ? 1 : 2;
+            if (SCHEME != CAM_NGP && SCATTER && valid)
+                t[a] = exact_offset(pos[a], g.mn[a], g.d[a], c[a], g.n[a]);
+        }
+        // First target (lowest brick on every axis) with warp aggregation.
+        const int key0 = valid ? brick_linear(g, bl[0], bl[1], bl[2]) : -1;
+        const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+        uint32_t slot0 = 0;
+        if (valid) {
+            const unsigned peers = __match_any_sync(vmask, key0);
+            const int leader = __ffs(peers) - 1;
+            const int rank = __popc(peers & ((1u << lane) - 1));
+            uint32_t base_slot = 0;
+            if (lane == leader) base_slot = atomicAdd(counter + key0, (uint32_t)__popc(peers));
+            base_slot = __shfl_sync(peers, base_slot, leader);
+            slot0 = base_slot + rank;
+        }
+        if (!valid) continue;
+        // Payloads / counts for every touched brick.
+#pragma unroll
+        for (int i0 = 0; i0 < 2; ++i0) {
+            if (i0 >= nbx[0]) break;
+            const int b0 = (bl[0] + i0) % g.nb[0];
+#pragma unroll
+            for (int i1 = 0; i1 < 2; ++i1) {
+                if (i1 >= nbx[1]) break;
+                const int b1 = (bl[1] + i1) % g.nb[1];
+#pragma unroll
+                for (int i2 = 0; i2 < 2; ++i2) {
+                    if (i2 >= nbx[2]) break;
+                    const int b2 = (bl[2] + i2) % g.nb[2];
+                    const bool first = (i0 | i1 | i2) == 0;
+                    const int key = brick_linear(g, b0, b1, b2);
+                    uint32_t slot;
+                    if (first) slot = slot0;
+                    else slot = atomicAdd(counter + key, 1u);
+                    if (SCATTER) {
+                        const int o[3] = {b0 * g.b[0], b1 * g.b[1], b2 * g.b[2]};
+                        uint32_t word[3];
+#pragma unroll
+                        for (int a = 0; a < 3; ++a) {
+                            int cl = c[a] - o[a];
+                            if (cl > (g.n[a] >> 1)) cl -= g.n[a];
+                            if (cl < -(g.n[a] >> 1)) cl += g.n[a];
+                            word[a] = pack_axis(cl, t[a]);
+                        }
+                        payload[slot] = make_uint4(word[0], word[1], word[2], __float_as_uint(wt));
+                    }
+                }
+            }
+        }
+    }
+    if (!SCATTER) {
+        // Warp reductions, one atomic per warp.
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            my_lost += __shfl_down_sync(0xffffffffu, my_lost, off);
+            my_wmax = max(my_wmax, __shfl_down_sync(0xffffffffu, my_wmax, off));
+        }
+        if (lane == 0) {
+            if (my_lost) atomicAdd(lost, my_lost);
+            if (my_wmax) atomicMax(wmax_bits, my_wmax);
+        }
+    }
+}
+
+// Exclusive scan of the brick counts (single CTA, 1024 threads x 8 items per
+// round).  start[nb] = total.  cursor := start for the scatter pass.
+__global__ void __launch_bounds__(1024)
+scan_kernel(const uint32_t *__restrict__ count, uint32_t *__restrict__ start,
+            uint32_t *__restrict__ cursor, int nb)
+{
+    __shared__ uint32_t warp_sums[32];
+    __shared__ uint32_t carry_s;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    if (tid == 0) carry_s = 0;
+    __syncthreads();
+    constexpr int ITEMS = 8;
+    for (int base = 0; base < nb; base += 1024 * ITEMS) {
+        uint32_t v[ITEMS];
+        uint32_t sum = 0;
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i) {
+            const int idx = base + tid * ITEMS + i;
+            v[i] = idx < nb ? count[idx] : 0u;
+            sum += v[i];
+        }
+        uint32_t incl = sum;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t o = __shfl_up_sync(0xffffffffu, incl, off);
+            if (lane >= off) incl += o;
+        }
+        if (lane == 31) warp_sums[wid] = incl;
+        __syncthreads();
+        if (wid == 0) {
+            uint32_t ws = warp_sums[lane];
+            uint32_t wi = ws;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const uint32_t o = __shfl_up_sync(0xffffffffu, wi, off);
+                if (lane >= off) wi += o;
+            }
+            warp_sums[lane] = wi - ws;  // exclusive
+        }
+        __syncthreads();
+        uint32_t run = carry_s + warp_sums[wid] + incl - sum;
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i) {
+            const int idx = base + tid * ITEMS + i;
+            if (idx < nb) {
+                start[idx] = run;
+                cursor[idx] = run;
+            }
+            run += v[i];
+        }
+        __syncthreads();
+        if (tid == 1023) carry_s = run;
+        __syncthreads();
+    }
+    if (tid == 0) start[nb] = carry_s;
+}
+
+template <typename OutT>
+__device__ __forceinline__ OutT convert_out(long long q, int s);
+template <>
+__device__ __forceinline__ float convert_out<float>(long long q, int s)
+{
+    return __double2float_rn(ldexp((double)q, -s));
+}
+template <>
+__device__ __forceinline__ double convert_out<double>(long long q, int s)
+{
+    return ldexp((double)q, -s);
+}
+template <>
+__device__ __forceinline__ uint32_t convert_out<uint32_t>(long long q, int s)
+{
+    return (uint32_t)(q >> s);
+}
+
+// Pass 4: one CTA per brick.
+template <int SCHEME, typename OutT>
+__global__ void __launch_bounds__(kDepositThreads)
+deposit_kernel(const uint4 *__restrict__ payload, const uint32_t *__restrict__ start,
+               AssignGeom g, const unsigned int *__restrict__ wmax_bits, int weighted,
+               OutT *__restrict__ mesh, double *__restrict__ brick_sum)
+{
+    using St = Stencil<SCHEME>;
+    extern __shared__ long long tile[];
+    __shared__ long long red[kDepositThreads / 32];
+    const int B = blockIdx.x;
+    const int B2 = B % g.nb[2];
+    const int B1 = (B / g.nb[2]) % g.nb[1];
+    const int B0 = B / (g.nb[2] * g.nb[1]);
+    const int o[3] = {B0 * g.b[0], B1 * g.b[1], B2 * g.b[2]};
+    const int e[3] = {min(g.b[0], g.n[0] - o[0]), min(g.b[1], g.n[1] - o[1]),
+                      min(g.b[2], g.n[2] - o[2])};
+    const int ncell = e[0] * e[1] * e[2];
+    for (int i = threadIdx.x; i < ncell; i += blockDim.x) tile[i] = 0;
+    __syncthreads();
+
+    const uint32_t beg = start[B], end = start[B + 1];
+    const uint32_t P = end - beg;
+    // Fixed-point scale 2^s with P * max|w| * 2^s < 2^61: no cell sum can
+    // overflow int64, whatever the order of accumulation.
+    const float wmax = weighted ? __uint_as_float(*wmax_bits) : 1.0f;
+    int ex = 0;
+    frexp((double)max(P, 1u) * (double)(wmax > 0.f ? wmax : 1.0f), &ex);
+    const int s = 61 - ex;
+
+    for (uint32_t p = beg + threadIdx.x; p < end; p += blockDim.x) {
+        const uint4 v = payload[p];
+        int cl[3];
+        float t[3];
+        unpack_axis(v.x, cl[0], t[0]);
+        unpack_axis(v.y, cl[1], t[1]);
+        unpack_axis(v.z, cl[2], t[2]);
+        const float ws = scalbnf(__uint_as_float(v.w), s);
+        float wa[3][St::W];
+        int li[3][St::W];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            if (SCHEME == CAM_NGP) {
+                wa[a][0] = 1.0f;
+            } else if (SCHEME == CAM_CIC) {
+                wa[a][0] = 1.0f - t[a];
+                wa[a][St::W - 1] = t[a];
+            } else {
+                const float hm = 0.5f - t[a], hp = 0.5f + t[a];
+                wa[a][0] = 0.5f * hm * hm;
+                wa[a][1] = 0.75f - t[a] * t[a];
+                wa[a][St::W - 1] = 0.5f * hp * hp;
+            }
+#pragma unroll
+            for (int sidx = 0; sidx < St::W; ++sidx) {
+                // Global cell of this stencil point, wrapped, then local
+                // index in the brick or -1 when it belongs to another brick.
+                const int gc = wrapi(o[a] + cl[a] + St::FIRST + sidx, g.n[a]);
+                const int lc = gc - o[a];
+                li[a][sidx] = (lc >= 0 && lc < e[a]) ? lc : -1;
+            }
+        }
+#pragma unroll
+        for (int ia = 0; ia < St::W; ++ia) {
+            if (li[0][ia] < 0) continue;
+#pragma unroll
+            for (int ja = 0; ja < St::W; ++ja) {
+                if (li[1][ja] < 0) continue;
+                const float wij = ws * wa[0][ia] * wa[1][ja];
+                const int row = (li[0][ia] * e[1] + li[1][ja]) * e[2];
+#pragma unroll
+                for (int ka = 0; ka < St::W; ++ka) {
+                    if (li[2][ka] < 0) continue;
+                    const long long q = __float2ll_rn(wij * wa[2][ka]);
+                    atomicAdd(reinterpret_cast<unsigned long long *>(tile + row + li[2][ka]),
+                              (unsigned long long)q);
+                }
+            }
+        }
+    }
+    __syncthreads();
+
+    long long acc = 0;
+    for (int i = threadIdx.x; i < ncell; i += blockDim.x) {
+        const int lk = i % e[2];
+        const int lj = (i / e[2]) % e[1];
+        const int lii = i / (e[2] * e[1]);
+        const long long q = tile[i];
+        acc += q;
+        const int64_t gidx = ((int64_t)(o[0] + lii) * g.n[1] + (o[1] + lj)) * g.n[2] + (o[2] + lk);
+        mesh[gidx] = convert_out<OutT>(q, s);
+    }
+    // Deterministic block sum of the integer cell sums.
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long tot = 0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) tot += red[i];
+        brick_sum[B] = ldexp((double)tot, -s);
+    }
+}
+
+// Keys only (cam_cell_keys).
+template <int SCHEME>
+__global__ void keys_kernel(const float *__restrict__ x, const float *__restrict__ y,
+                            const float *__restrict__ z, int64_t np, AssignGeom g,
+                            int64_t *__restrict__ keys)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t ncell = (int64_t)g.n[0] * g.n[1] * g.n[2];
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < np; p += stride) {
+        const float pos[3] = {x[p], y[p], z[p]};
+        int c[3];
+        keys[p] = home_cell<SCHEME>(pos, g, c)
+                      ? (int64_t)c[2] + (int64_t)g.n[2] * ((int64_t)c[1] + (int64_t)g.n[1] * c[0])
+                      : ncell;
+    }
+}
+
+int grid_for(int64_t work, int threads)
+{
+    const int64_t blocks = (work + threads - 1) / threads;
+    const int64_t cap = (int64_t)kNumSMs * 8;
+    return (int)std::max<int64_t>(1, std::min(blocks, cap));
+}
+
+}  // namespace
+
+AssignGeom make_geom(const cam_grid &gr, int scheme, int64_t np)
+{
+    AssignGeom g{};
+    for (int a = 0; a < 3; ++a) {
+        CAM_REQUIRE(gr.n[a] >= 1 && gr.n[a] <= (1 << 20), CAM_E_INVAL, "grid size out of range");
+        CAM_REQUIRE(std::isfinite(gr.L[a]) && gr.L[a] > 0.f, CAM_E_INVAL, "box side must be > 0");
+        g.n[a] = (int)gr.n[a];
+        g.L[a] = gr.L[a];
+        g.d[a] = gr.d[a] != 0.f ? gr.d[a] : gr.L[a] / (float)gr.n[a];
+        g.mn[a] = gr.min[a];
+        CAM_REQUIRE(std::isfinite(g.d[a]) && g.d[a] > 0.f, CAM_E_INVAL, "cell size must be > 0");
+        CAM_REQUIRE(std::isfinite(g.mn[a]), CAM_E_INVAL, "box origin must be finite");
+    }
+    // Brick extents: z 32 (128-byte rows), y and x 16; shrunk (to 4) while
+    // the mesh has too few bricks to fill the GPU.  TSC needs >= 3 cells
+    // per brick axis unless one brick spans the axis.
+    g.b[2] = std::min(g.n[2], 32);
+    g.b[1] = std::min(g.n[1], 16);
+    g.b[0] = std::min(g.n[0], 16);
+    auto nbricks = [&]() {
+        int64_t t = 1;
+        for (int a = 0; a < 3; ++a) t *= (g.n[a] + g.b[a] - 1) / g.b[a];
+        return t;
+    };
+    const int64_t want = std::min<int64_t>(4 * kNumSMs, std::max<int64_t>(1, np / 4096));
+    while (nbricks() < want && (g.b[0] > 4 || g.b[1] > 4)) {
+        if (g.b[0] >= g.b[1] && g.b[0] > 4) g.b[0] = (g.b[0] + 1) / 2;
+        else g.b[1] = (g.b[1] + 1) / 2;
+    }
+    // A stencil of width <= 3 must never span three bricks: a partial last
+    // brick keeps at least 2 cells (shrink the brick until it does).
+    for (int a = 0; a < 3; ++a) {
+        while (g.b[a] < g.n[a] && g.n[a] % g.b[a] != 0 && g.n[a] % g.b[a] < 2 && g.b[a] > 3) --g.b[a];
+        g.nb[a] = (g.n[a] + g.b[a] - 1) / g.b[a];
+    }
+    (void)scheme;
+    return g;
+}
+
+template <int SCHEME>
+static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const float *z,
+                        const float *w, int64_t np, const AssignGeom &g, AssignOut &out)
+{
+    const int64_t nb = (int64_t)g.nb[0] * g.nb[1] * g.nb[2];
+    CAM_REQUIRE(nb < (1ll << 31), CAM_E_UNSUPPORTED, "too many mesh bricks");
+    auto *counter = static_cast<uint32_t *>(scratch(ctx, "asg.count", nb * sizeof(uint32_t)));
+    auto *start = static_cast<uint32_t *>(scratch(ctx, "asg.start", (nb + 1) * sizeof(uint32_t)));
+    auto *stats = static_cast<unsigned long long *>(scratch(ctx, "asg.stats", 64));
+    auto *bsum = static_cast<double *>(scratch(ctx, "asg.bsum", nb * sizeof(double)));
+    unsigned long long *d_lost = stats;
+    unsigned int *d_wmax = reinterpret_cast<unsigned int *>(stats + 1);
+    CAM_CUDA_TRY(cudaMemsetAsync(counter, 0, nb * sizeof(uint32_t), ctx->stream));
+    CAM_CUDA_TRY(cudaMemsetAsync(stats, 0, 64, ctx->stream));
+
+    const int gb = grid_for(np, kBinThreads);
+    if (np > 0)
+        CAM_LAUNCH_NAMED(ctx, "assign_bin_count", (bin_kernel<SCHEME, false>), gb, kBinThreads, 0, x, y, z, w, np, g,
+                   counter, (uint4 *)nullptr, d_lost, d_wmax);
+    CAM_LAUNCH_NAMED(ctx, "assign_scan", scan_kernel, 1, 1024, 0, counter, start, counter, (int)nb);
+
+    // Payload size and diagnostics back to the host (one synchronisation).
+    uint32_t total = 0;
+    unsigned long long hstats[2] = {0, 0};
+    CAM_CUDA_TRY(cudaMemcpyAsync(&total, start + nb, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    CAM_CUDA_TRY(cudaMemcpyAsync(hstats, stats, 16, cudaMemcpyDeviceToHost, ctx->stream));
+    CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    const unsigned int wmax_bits = (unsigned int)(hstats[1] & 0xffffffffu);
+    CAM_REQUIRE(!w || wmax_bits < 0x7f800000u, CAM_E_NONFINITE, "a particle weight is NaN or infinite");
+    out.n_lost = (int64_t)hstats[0];
+    out.n_in = np - out.n_lost;
+
+    uint4 *payload = static_cast<uint4 *>(scratch(ctx, "asg.payload", std::max<size_t>(total, 1) * sizeof(uint4)));
+    if (np > 0)
+        CAM_LAUNCH_NAMED(ctx, "assign_bin_scatter", (bin_kernel<SCHEME, true>), gb, kBinThreads, 0, x, y, z, w, np, g,
+                   counter, payload, d_lost, d_wmax);
+
+    const size_t smem = (size_t)g.b[0] * g.b[1] * g.b[2] * sizeof(long long);
+    CAM_REQUIRE(smem <= 200 * 1024, CAM_E_UNSUPPORTED, "brick tile too large");
+    const int weighted = w != nullptr;
+    auto launch_dep = [&](auto kern, auto *mesh) {
+        CAM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CAM_LAUNCH_NAMED(ctx, "assign_deposit", kern, (unsigned)nb, kDepositThreads, smem, payload, start, g, d_wmax,
+                   weighted, mesh, bsum);
+    };
+    if (out.precision == CAM_F32)
+        launch_dep(deposit_kernel<SCHEME, float>, static_cast<float *>(out.mesh));
+    else if (out.precision == CAM_F64)
+        launch_dep(deposit_kernel<SCHEME, double>, static_cast<double *>(out.mesh));
+    else
+        launch_dep(deposit_kernel<SCHEME, uint32_t>, static_cast<uint32_t *>(out.mesh));
+    if (out.d_sum) reduce_sum_f64(ctx, bsum, nb, out.d_sum);
+}
+
+void assign_device(cam_ctx *ctx, const float *x, const float *y, const float *z,
+                   const float *w, int64_t np, const cam_grid &grid, int scheme, AssignOut &out)
+{
+    CAM_REQUIRE(np >= 0, CAM_E_INVAL, "negative particle count");
+    CAM_REQUIRE(np == 0 || (x && y && z), CAM_E_INVAL, "null particle coordinates");
+    CAM_REQUIRE(np < (1ll << 31), CAM_E_UNSUPPORTED, "more than 2^31 particles per call");
+    const AssignGeom g = make_geom(grid, scheme, np);
+    if (out.precision == -1)
+        CAM_REQUIRE(scheme == CAM_NGP && w == nullptr, CAM_E_INVAL, "integer counts need unweighted NGP");
+    switch (scheme) {
+    case CAM_NGP: assign_impl<CAM_NGP>(ctx, x, y, z, w, np, g, out); break;
+    case CAM_CIC: assign_impl<CAM_CIC>(ctx, x, y, z, w, np, g, out); break;
+    case CAM_TSC: assign_impl<CAM_TSC>(ctx, x, y, z, w, np, g, out); break;
+    default: throw Error{CAM_E_INVAL, "unknown mass assignment scheme"};
+    }
+}
+
+void cell_keys_device(cam_ctx *ctx, const float *x, const float *y, const float *z, int64_t np,
+                      const cam_grid &grid, int scheme, int64_t *keys)
+{
+    const AssignGeom g = make_geom(grid, scheme, np);
+    if (np == 0) return;
+    const int gb = grid_for(np, 256);
+    switch (scheme) {
+    case CAM_NGP: CAM_LAUNCH(ctx, keys_kernel<CAM_NGP>, gb, 256, 0, x, y, z, np, g, keys); break;
+    case CAM_CIC: CAM_LAUNCH(ctx, keys_kernel<CAM_CIC>, gb, 256, 0, x, y, z, np, g, keys); break;
+    case CAM_TSC: CAM_LAUNCH(ctx, keys_kernel<CAM_TSC>, gb, 256, 0, x, y, z, np, g, keys); break;
+    default: throw Error{CAM_E_INVAL, "unknown mass assignment scheme"};
+    }
+}
+
+}  // namespace cam

@@ -1,0 +1,344 @@
+// 3D real-to-complex / complex-to-real FFT for sm_100a.
+//
+// Replaces do_fftw_r2c / do_fftw_c2r, Source/NumericalMethods.cpp:1718-1856
+// (a fresh FFTW_ESTIMATE plan per call there; here plans are built once per
+// (N, precision) and hold only a twiddle table).
+//
+// Layout.  Spectra are kept in a "split" layout: main[N][N][N/2] complex
+// (k < N/2) plus the Nyquist plane nyq[N][N] (k = N/2).  Every main row is
+// N/2 complex, a multiple of 16 bytes, so column tiles are aligned 128-byte
+// segments.  split_to_fftw / fftw_to_split convert to FFTW's [i][j][k<=N/2].
+//
+// Passes (each one HBM read + one HBM write of the array):
+//   rows  : along z, real rows of N packed as N/2 complex, half-length
+//           complex FFT plus the r2c untangling (or its inverse for c2r);
+//   cols  : along y or x, tiles of 16 (float) / 8 (double) consecutive
+//           columns x N rows staged in shared memory.
+// Inside a CTA the 1D transforms are mixed-radix (8, 4, 2, 3) Stockham
+// stages in shared memory.  Each thread keeps its butterflies' inputs in
+// registers across a barrier, so a stage reads and writes the same buffer.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "cam_fft_device.cuh"
+#include "cam_internal.h"
+
+namespace cam {
+
+struct FftPlan {
+    int64_t n = 0;
+    int precision = CAM_F32;
+    void *tw = nullptr;  // n roots exp(-2 pi i m / n), float2 or double2
+    Radices rad_n, rad_m;
+};
+
+namespace {
+
+// Column transforms: element (comp, plane, j, col) at
+// base + comp*ccomp + plane*pstride + j*jstride + col, col < ncols.
+template <typename T, bool INV>
+__global__ void __launch_bounds__(1024, 1)
+fft_cols_kernel(typename fftdev::CT<T>::t *base, int len, int ncols, int64_t jstride, int64_t pstride,
+                int64_t ccomp, Radices rd, const typename fftdev::CT<T>::t *__restrict__ tw, int twmul)
+{
+    using C = typename fftdev::CT<T>::t;
+    constexpr int W = fftdev::CT<T>::kCols;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *tile = reinterpret_cast<C *>(smem_raw);
+    const int col0 = blockIdx.x * W;
+    const int nc = min(W, ncols - col0);
+    C *g = base + (int64_t)blockIdx.z * ccomp + (int64_t)blockIdx.y * pstride + col0;
+    const int tot = len * W;
+    for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+        const int j = e / W, c = e % W;
+        if (c < nc) tile[e] = g[(int64_t)j * jstride + c];
+    }
+    __syncthreads();
+    fftdev::block_fft<C, fftdev::CT<T>::kPPT, INV, false, W>(tile, len, W, W, 1, rd, tw, twmul);
+    for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+        const int j = e / W, c = e % W;
+        if (c < nc) g[(int64_t)j * jstride + c] = tile[e];
+    }
+}
+
+// Row transforms along the contiguous axis.
+//   MODE 0 (r2c): real rows of n -> main rows of n/2 + nyq element
+//   MODE 1 (c2r): main rows + nyq -> real rows of n (times `scale`)
+//   MODE 2/3    : complex rows of n, forward / inverse, in place
+template <typename T, int MODE>
+__global__ void __launch_bounds__(1024, 1)
+fft_rows_kernel(const void *in, void *out_main, typename fftdev::CT<T>::t *nyq, int n, int64_t nrows,
+                int rpc, int64_t ccomp_in, int64_t ccomp_out, Radices rd,
+                const typename fftdev::CT<T>::t *__restrict__ tw, const double *__restrict__ d_sub,
+                double scale)
+{
+    using C = typename fftdev::CT<T>::t;
+    constexpr bool INV = (MODE == 1 || MODE == 3);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *tile = reinterpret_cast<C *>(smem_raw);
+    const int len = (MODE <= 1) ? n / 2 : n;
+    const int64_t row0 = (int64_t)blockIdx.x * rpc;
+    const int nr = (int)min((int64_t)rpc, nrows - row0);
+    const int tot = nr * len;
+    const int M = n / 2;
+    const int64_t comp = blockIdx.y;
+
+    if (MODE == 0) {
+        const C *src = reinterpret_cast<const C *>(static_cast<const T *>(in) + comp * ccomp_in) + row0 * M;
+        const T sub = d_sub ? (T)(*d_sub) : (T)0;
+        for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+            C v = src[e];
+            v.x -= sub;
+            v.y -= sub;
+            tile[e] = v;
+        }
+    } else if (MODE == 1) {
+        const C *srcm = static_cast<const C *>(in) + comp * ccomp_in + row0 * M;
+        const C *srcn = nyq + comp * (ccomp_in / M) + row0;  // nyq plane is N*N per component
+        for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+            const int r = e / M, k = e % M;
+            C xk = srcm[(int64_t)r * M + k];
+            C xm = (k == 0) ? srcn[r] : srcm[(int64_t)r * M + (M - k)];
+            if (k == 0) {  // imaginary parts of DC and Nyquist are ignored
+                xk.y = 0;
+                xm.y = 0;
+            }
+            // Z'[k] = X[k] + conj(X[M-k]) + i e^{+2 pi i k/n} (X[k] - conj(X[M-k]))
+            const C a = C{xk.x + xm.x, xk.y - xm.y};
+            const C b = C{xk.x - xm.x, xk.y + xm.y};
+            C wv = __ldg(tw + k);
+            wv.y = -wv.y;
+            const C ib = fftdev::rot<C, true>(fftdev::cmul(wv, b));
+            tile[e] = fftdev::cadd(a, ib);
+        }
+    } else {
+        const C *src = static_cast<const C *>(in) + comp * ccomp_in + row0 * n;
+        for (int e = threadIdx.x; e < tot; e += blockDim.x) tile[e] = src[e];
+    }
+    __syncthreads();
+    fftdev::block_fft<C, fftdev::CT<T>::kPPT, INV, true, 0>(tile, len, nr, 1, len, rd, tw, (MODE <= 1) ? 2 : 1);
+
+    if (MODE == 0) {
+        C *dm = static_cast<C *>(out_main) + comp * ccomp_out + row0 * M;
+        C *dn = nyq + comp * (ccomp_out / M) + row0;
+        const int tot2 = nr * (M + 1);
+        for (int e = threadIdx.x; e < tot2; e += blockDim.x) {
+            const int r = e / (M + 1), k = e % (M + 1);
+            const C zk = tile[r * M + (k % M)];
+            const C zc0 = tile[r * M + ((M - k) % M)];
+            const C zc = C{zc0.x, -zc0.y};
+            // X[k] = (Z[k] + conj Z[M-k])/2 - i/2 e^{-2 pi i k/n} (Z[k] - conj Z[M-k])
+            const C s = fftdev::cadd(zk, zc), d = fftdev::csub(zk, zc);
+            const C wd = fftdev::cmul(__ldg(tw + k), d);
+            const C xk = C{(T)0.5 * (s.x + wd.y), (T)0.5 * (s.y - wd.x)};
+            if (k < M) dm[(int64_t)r * M + k] = xk;
+            else dn[r] = xk;
+        }
+    } else if (MODE == 1) {
+        T *dst = static_cast<T *>(out_main) + comp * ccomp_out + row0 * n;
+        const T sc = (T)scale;
+        for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+            const C v = tile[e];
+            reinterpret_cast<C *>(dst)[e] = C{v.x * sc, v.y * sc};
+        }
+    } else {
+        C *dst = static_cast<C *>(out_main) + comp * ccomp_out + row0 * n;
+        for (int e = threadIdx.x; e < tot; e += blockDim.x) dst[e] = tile[e];
+    }
+}
+
+template <typename T>
+__global__ void split_to_fftw_kernel(const typename fftdev::CT<T>::t *__restrict__ main,
+                                     const typename fftdev::CT<T>::t *__restrict__ nyq,
+                                     typename fftdev::CT<T>::t *__restrict__ dst, int64_t nrows, int M)
+{
+    const int64_t tot = nrows * (M + 1);
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = e / (M + 1);
+        const int k = (int)(e % (M + 1));
+        dst[e] = k < M ? main[r * M + k] : nyq[r];
+    }
+}
+
+template <typename T>
+__global__ void fftw_to_split_kernel(const typename fftdev::CT<T>::t *__restrict__ src,
+                                     typename fftdev::CT<T>::t *__restrict__ main,
+                                     typename fftdev::CT<T>::t *__restrict__ nyq, int64_t nrows, int M)
+{
+    const int64_t tot = nrows * (M + 1);
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = e / (M + 1);
+        const int k = (int)(e % (M + 1));
+        if (k < M) main[r * M + k] = src[e];
+        else nyq[r] = src[e];
+    }
+}
+
+int threads_for(int points, int ppt)
+{
+    int t = (points + ppt - 1) / ppt;
+    t = ((t + 31) / 32) * 32;
+    return std::max(32, std::min(1024, t));
+}
+
+template <typename T>
+void cols_impl(cam_ctx *ctx, FftPlan *p, void *base, int64_t len, int64_t ncols, int64_t jstride,
+               int64_t nplanes, int64_t pstride, int ncomp, int64_t ccomp, bool inv)
+{
+    using C = typename fftdev::CT<T>::t;
+    constexpr int W = fftdev::CT<T>::kCols;
+    const Radices &rd = (len == p->n) ? p->rad_n : p->rad_m;
+    const int twmul = (int)(p->n / len);
+    const int nthr = threads_for((int)len * W, fftdev::CT<T>::kPPT);
+    const size_t smem = (size_t)len * W * sizeof(C);
+    dim3 grid((unsigned)((ncols + W - 1) / W), (unsigned)nplanes, (unsigned)ncomp);
+    auto kern = inv ? fft_cols_kernel<T, true> : fft_cols_kernel<T, false>;
+    CAM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CAM_LAUNCH_NAMED(ctx, "fft_cols", kern, grid, nthr, smem, static_cast<C *>(base), (int)len, (int)ncols, jstride,
+               pstride, ccomp, rd, static_cast<const C *>(p->tw), twmul);
+}
+
+template <typename T, int MODE>
+void rows_impl(cam_ctx *ctx, FftPlan *p, const void *in, void *out, void *nyq, int64_t nrows,
+               int ncomp, int64_t ccomp_in, int64_t ccomp_out, const double *d_sub, double scale)
+{
+    using C = typename fftdev::CT<T>::t;
+    const int n = (int)p->n;
+    const int len = MODE <= 1 ? n / 2 : n;
+    const Radices &rd = MODE <= 1 ? p->rad_m : p->rad_n;
+    const int rpc = std::max(1, (sizeof(T) == 4 ? 4096 : 2048) / len);
+    const int nthr = threads_for(rpc * len, fftdev::CT<T>::kPPT);
+    const size_t smem = (size_t)rpc * len * sizeof(C);
+    dim3 grid((unsigned)((nrows + rpc - 1) / rpc), (unsigned)ncomp);
+    auto kern = fft_rows_kernel<T, MODE>;
+    CAM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CAM_LAUNCH_NAMED(ctx, MODE == 0 ? "fft_rows_r2c" : MODE == 1 ? "fft_rows_c2r" : "fft_rows_c2c", kern, grid, nthr, smem, in, out, static_cast<C *>(nyq), n, nrows, rpc,
+               ccomp_in, ccomp_out, rd, static_cast<const C *>(p->tw), d_sub, scale);
+}
+
+template <typename T>
+void r2c_impl(cam_ctx *ctx, FftPlan *p, const void *in, const double *d_sub, Spectrum &s)
+{
+    const int64_t n = p->n, M = n / 2;
+    rows_impl<T, 0>(ctx, p, in, s.main, s.nyq, n * n, 1, 0, 0, d_sub, 1.0);
+    cols_impl<T>(ctx, p, s.main, n, M, M, n, n * M, 1, 0, false);        // y
+    rows_impl<T, 2>(ctx, p, s.nyq, s.nyq, nullptr, n, 1, 0, 0, nullptr, 1.0);  // nyq, y
+    cols_impl<T>(ctx, p, s.main, n, M, n * M, n, M, 1, 0, false);        // x
+    cols_impl<T>(ctx, p, s.nyq, n, n, n, 1, 0, 1, 0, false);             // nyq, x
+}
+
+template <typename T>
+void c2r_impl(cam_ctx *ctx, FftPlan *p, Spectrum &s, void *out, double scale)
+{
+    const int64_t n = p->n, M = n / 2;
+    cols_impl<T>(ctx, p, s.main, n, M, n * M, n, M, 1, 0, true);         // x
+    cols_impl<T>(ctx, p, s.nyq, n, n, n, 1, 0, 1, 0, true);              // nyq, x
+    cols_impl<T>(ctx, p, s.main, n, M, M, n, n * M, 1, 0, true);         // y
+    rows_impl<T, 3>(ctx, p, s.nyq, s.nyq, nullptr, n, 1, 0, 0, nullptr, 1.0);  // nyq, y
+    rows_impl<T, 1>(ctx, p, s.main, out, s.nyq, n * n, 1, 0, 0, nullptr, scale);
+}
+
+}  // namespace
+
+const void *plan_twiddles(FftPlan *plan) { return plan->tw; }
+
+FftPlan *get_plan(cam_ctx *ctx, int64_t n, int precision)
+{
+    const int64_t key = n * 2 + precision;
+    auto it = ctx->plans.find(key);
+    if (it != ctx->plans.end()) return it->second;
+    CAM_REQUIRE(n >= 8 && n <= 1024 && n % 2 == 0, CAM_E_UNSUPPORTED, "FFT size must be even, 8 <= N <= 1024");
+    auto *p = new FftPlan;
+    p->n = n;
+    p->precision = precision;
+    p->rad_n = factor_radices(n);
+    p->rad_m = factor_radices(n / 2);
+    if (p->rad_n.n < 0 || p->rad_m.n < 0) {
+        delete p;
+        throw Error{CAM_E_UNSUPPORTED, "FFT size must be 2^a 3^b"};
+    }
+    // Roots of unity from long double, correctly rounded to the element type.
+    std::vector<double> re(n), im(n);
+    const long double pi2 = 6.283185307179586476925286766559L;
+    for (int64_t m = 0; m < n; ++m) {
+        const long double a = pi2 * (long double)m / (long double)n;
+        re[m] = (double)cosl(a);
+        im[m] = (double)-sinl(a);
+    }
+    if (precision == CAM_F32) {
+        std::vector<float2> h(n);
+        for (int64_t m = 0; m < n; ++m) h[m] = make_float2((float)re[m], (float)im[m]);
+        p->tw = scratch(ctx, ("fft.tw." + std::to_string(key)).c_str(), n * sizeof(float2));
+        CAM_CUDA_TRY(cudaMemcpy(p->tw, h.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
+    } else {
+        std::vector<double2> h(n);
+        for (int64_t m = 0; m < n; ++m) h[m] = make_double2(re[m], im[m]);
+        p->tw = scratch(ctx, ("fft.tw." + std::to_string(key)).c_str(), n * sizeof(double2));
+        CAM_CUDA_TRY(cudaMemcpy(p->tw, h.data(), n * sizeof(double2), cudaMemcpyHostToDevice));
+    }
+    ctx->plans[key] = p;
+    return p;
+}
+
+void fft_r2c_split(cam_ctx *ctx, FftPlan *plan, const void *real_in, const double *d_sub, Spectrum &out)
+{
+    if (plan->precision == CAM_F32) r2c_impl<float>(ctx, plan, real_in, d_sub, out);
+    else r2c_impl<double>(ctx, plan, real_in, d_sub, out);
+}
+
+void fft_c2r_split(cam_ctx *ctx, FftPlan *plan, Spectrum &spec, void *real_out, double scale)
+{
+    if (plan->precision == CAM_F32) c2r_impl<float>(ctx, plan, spec, real_out, scale);
+    else c2r_impl<double>(ctx, plan, spec, real_out, scale);
+}
+
+void fft_columns(cam_ctx *ctx, FftPlan *plan, void *base, int64_t len, int64_t ncols, int64_t jstride,
+                 int64_t nplanes, int64_t pstride, int ncomp, int64_t ccomp, bool inverse)
+{
+    if (plan->precision == CAM_F32) cols_impl<float>(ctx, plan, base, len, ncols, jstride, nplanes, pstride, ncomp, ccomp, inverse);
+    else cols_impl<double>(ctx, plan, base, len, ncols, jstride, nplanes, pstride, ncomp, ccomp, inverse);
+}
+
+void fft_rows_c2c(cam_ctx *ctx, FftPlan *plan, void *base, int64_t len, int64_t nrows, int ncomp,
+                  int64_t ccomp, bool inverse)
+{
+    (void)len;
+    if (plan->precision == CAM_F32) {
+        if (inverse) rows_impl<float, 3>(ctx, plan, base, base, nullptr, nrows, ncomp, ccomp, ccomp, nullptr, 1.0);
+        else rows_impl<float, 2>(ctx, plan, base, base, nullptr, nrows, ncomp, ccomp, ccomp, nullptr, 1.0);
+    } else {
+        if (inverse) rows_impl<double, 3>(ctx, plan, base, base, nullptr, nrows, ncomp, ccomp, ccomp, nullptr, 1.0);
+        else rows_impl<double, 2>(ctx, plan, base, base, nullptr, nrows, ncomp, ccomp, ccomp, nullptr, 1.0);
+    }
+}
+
+void split_to_fftw(cam_ctx *ctx, const Spectrum &s, void *dst)
+{
+    const int64_t n = s.n, M = n / 2, rows = n * n;
+    const int blocks = (int)std::min<int64_t>((rows * (M + 1) + 255) / 256, kNumSMs * 16);
+    if (s.precision == CAM_F32)
+        CAM_LAUNCH(ctx, split_to_fftw_kernel<float>, blocks, 256, 0, (const float2 *)s.main,
+                   (const float2 *)s.nyq, (float2 *)dst, rows, (int)M);
+    else
+        CAM_LAUNCH(ctx, split_to_fftw_kernel<double>, blocks, 256, 0, (const double2 *)s.main,
+                   (const double2 *)s.nyq, (double2 *)dst, rows, (int)M);
+}
+
+void fftw_to_split(cam_ctx *ctx, const void *src, Spectrum &s)
+{
+    const int64_t n = s.n, M = n / 2, rows = n * n;
+    const int blocks = (int)std::min<int64_t>((rows * (M + 1) + 255) / 256, kNumSMs * 16);
+    if (s.precision == CAM_F32)
+        CAM_LAUNCH(ctx, fftw_to_split_kernel<float>, blocks, 256, 0, (const float2 *)src,
+                   (float2 *)s.main, (float2 *)s.nyq, rows, (int)M);
+    else
+        CAM_LAUNCH(ctx, fftw_to_split_kernel<double>, blocks, 256, 0, (const double2 *)src,
+                   (double2 *)s.main, (double2 *)s.nyq, rows, (int)M);
+}
+
+}  // namespace cam

@@ -1,0 +1,209 @@
+// Device-side FFT building blocks shared by the FFT and T-web kernels:
+// complex helpers, radix-2/3/4/8 butterflies and a Stockham stage that runs
+// over many independent transforms held in shared memory.
+//
+// Stage (Stockham autosort, radix R, Ns = product of the radices already
+// applied): butterfly j of a transform of length len reads elements
+// j + r*len/R, multiplies by exp(-+2 pi i r (j mod Ns) / (Ns R)), applies the
+// R-point DFT and writes to (j / Ns) * Ns * R + (j mod Ns) + r * Ns.  After
+// the last stage the output is in natural order.  Every thread keeps the
+// inputs of its butterflies in registers across a barrier, so one buffer is
+// read and rewritten in place.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace cam {
+
+// Stage list of one transform length.  Integer divisions by the stage's
+// butterfly count nq = len/R and by Ns are done with precomputed
+// multipliers: floor(x / d) = umulhi(x, ceil(2^32 / d)), exact for
+// x, d < 2^16 (all lengths here are <= 1024).
+struct Radices {
+    int n = 0;
+    int r[16];
+    unsigned mq[16];   // ceil(2^32 / (len / r[s]))
+    unsigned mns[16];  // ceil(2^32 / Ns[s]), Ns[s] = r[0] * ... * r[s-1]
+};
+
+inline unsigned div_magic(int64_t d) { return (unsigned)(((1ull << 32) + (uint64_t)d - 1) / (uint64_t)d); }
+
+// len = 8^a 3^b {1, 2, 4}: radix-8 stages first, then 3s, then one 8/4/2.
+inline Radices factor_radices(int64_t len)
+{
+    Radices rd;
+    int64_t m = len;
+    while (m % 8 == 0 && m > 8) { rd.r[rd.n++] = 8; m /= 8; }
+    while (m % 3 == 0) { rd.r[rd.n++] = 3; m /= 3; }
+    if (m == 8) { rd.r[rd.n++] = 8; m = 1; }
+    if (m == 4) { rd.r[rd.n++] = 4; m = 1; }
+    if (m == 2) { rd.r[rd.n++] = 2; m = 1; }
+    if (m != 1 || len > 4096) {
+        rd.n = -1;
+        return rd;
+    }
+    int64_t ns = 1;
+    for (int s = 0; s < rd.n; ++s) {
+        rd.mq[s] = div_magic(len / rd.r[s]);
+        rd.mns[s] = div_magic(ns);
+        ns *= rd.r[s];
+    }
+    return rd;
+}
+
+namespace fftdev {
+
+template <typename T>
+struct CT;
+template <>
+struct CT<float> {
+    using t = float2;
+    static constexpr int kCols = 16;  // 128-byte column tiles
+    static constexpr int kPPT = 16;   // complex points per thread
+};
+template <>
+struct CT<double> {
+    using t = double2;
+    static constexpr int kCols = 8;
+    static constexpr int kPPT = 8;
+};
+
+template <typename C>
+__device__ __forceinline__ C cadd(C a, C b) { return C{a.x + b.x, a.y + b.y}; }
+template <typename C>
+__device__ __forceinline__ C csub(C a, C b) { return C{a.x - b.x, a.y - b.y}; }
+template <typename C>
+__device__ __forceinline__ C cmul(C a, C b) { return C{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x}; }
+// multiply by -i (forward) or +i (inverse)
+template <typename C, bool INV>
+__device__ __forceinline__ C rot(C a) { return INV ? C{-a.y, a.x} : C{a.y, -a.x}; }
+
+template <typename C, bool INV>
+__device__ __forceinline__ void dft2(C &a, C &b)
+{
+    const C t = a;
+    a = cadd(t, b);
+    b = csub(t, b);
+}
+
+template <typename C, int R, bool INV>
+__device__ __forceinline__ void dft(C *v)
+{
+    using T = decltype(v[0].x);
+    if (R == 2) {
+        dft2<C, INV>(v[0], v[1]);
+    } else if (R == 3) {
+        const T s3 = (T)0.86602540378443864676;  // sin(pi/3)
+        const C t1 = cadd(v[1], v[2]);
+        const C t2 = C{v[0].x - (T)0.5 * t1.x, v[0].y - (T)0.5 * t1.y};
+        const C d = csub(v[1], v[2]);
+        const C t3 = rot<C, INV>(C{s3 * d.x, s3 * d.y});
+        v[0] = cadd(v[0], t1);
+        v[1] = cadd(t2, t3);
+        v[2] = csub(t2, t3);
+    } else if (R == 4) {
+        const C a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+        const C b0 = cadd(v[1], v[3]), b1 = rot<C, INV>(csub(v[1], v[3]));
+        v[0] = cadd(a0, b0);
+        v[2] = csub(a0, b0);
+        v[1] = cadd(a1, b1);
+        v[3] = csub(a1, b1);
+    } else if (R == 8) {
+        const T h = (T)0.70710678118654752440;
+        C e[4] = {v[0], v[2], v[4], v[6]};
+        C o[4] = {v[1], v[3], v[5], v[7]};
+        dft<C, 4, INV>(e);
+        dft<C, 4, INV>(o);
+        // o[k] *= W8^k
+        o[1] = INV ? C{h * (o[1].x - o[1].y), h * (o[1].x + o[1].y)}
+                   : C{h * (o[1].x + o[1].y), h * (o[1].y - o[1].x)};
+        o[2] = rot<C, INV>(o[2]);
+        o[3] = INV ? C{-h * (o[3].x + o[3].y), h * (o[3].x - o[3].y)}
+                   : C{h * (o[3].y - o[3].x), -h * (o[3].x + o[3].y)};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            v[k] = cadd(e[k], o[k]);
+            v[k + 4] = csub(e[k], o[k]);
+        }
+    }
+}
+
+// One Stockham stage over `ncol` independent transforms of length `len`
+// stored in shared memory at col*cstride + j*jstride.  JFAST: butterflies
+// of one transform are consecutive (row layout); otherwise consecutive
+// butterflies walk the NCOL columns (column-tile layout).
+template <typename C, int R, int PPT, bool INV, bool JFAST, int NCOL>
+__device__ __forceinline__ void stage(C *buf, int len, int ncol, int jstride, int cstride, int Ns,
+                                      unsigned mq, unsigned mns, const C *__restrict__ tw, int twmul)
+{
+    constexpr int MAXIT = (PPT + R - 1) / R;
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int nq = len / R;
+    const int nbf = nq * (JFAST ? ncol : NCOL);
+    const int twstep = (len / (Ns * R)) * twmul;
+    C v[MAXIT][R];
+    int dsto[MAXIT];
+#pragma unroll
+    for (int it = 0; it < MAXIT; ++it) {
+        const int bi = tid + it * nthr;
+        dsto[it] = -1;
+        if (bi < nbf) {
+            int j, col;
+            if (JFAST) {
+                col = (int)__umulhi((unsigned)bi, mq);
+                j = bi - col * nq;
+            } else {
+                col = bi % NCOL;
+                j = bi / NCOL;
+            }
+            const C *src = buf + col * cstride + j * jstride;
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[it][r] = src[r * nq * jstride];
+            const int q = (int)__umulhi((unsigned)j, mns);
+            const int k = j - q * Ns;
+            if (Ns > 1) {
+                const int step = k * twstep;
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    C w = __ldg(tw + r * step);
+                    if (INV) w.y = -w.y;
+                    v[it][r] = cmul(v[it][r], w);
+                }
+            }
+            dft<C, R, INV>(v[it]);
+            dsto[it] = col * cstride + (j + q * Ns * (R - 1)) * jstride;
+        }
+    }
+    __syncthreads();
+    const int ostride = Ns * jstride;
+#pragma unroll
+    for (int it = 0; it < MAXIT; ++it) {
+        if (dsto[it] >= 0) {
+            C *dst = buf + dsto[it];
+#pragma unroll
+            for (int r = 0; r < R; ++r) dst[r * ostride] = v[it][r];
+        }
+    }
+    __syncthreads();
+}
+
+template <typename C, int PPT, bool INV, bool JFAST, int NCOL>
+__device__ __forceinline__ void block_fft(C *buf, int len, int ncol, int jstride, int cstride,
+                                          const Radices &rd, const C *__restrict__ tw, int twmul)
+{
+    int Ns = 1;
+    for (int s = 0; s < rd.n; ++s) {
+        const unsigned mq = rd.mq[s], mns = rd.mns[s];
+        switch (rd.r[s]) {
+        case 8: stage<C, 8, PPT, INV, JFAST, NCOL>(buf, len, ncol, jstride, cstride, Ns, mq, mns, tw, twmul); break;
+        case 4: stage<C, 4, PPT, INV, JFAST, NCOL>(buf, len, ncol, jstride, cstride, Ns, mq, mns, tw, twmul); break;
+        case 3: stage<C, 3, PPT, INV, JFAST, NCOL>(buf, len, ncol, jstride, cstride, Ns, mq, mns, tw, twmul); break;
+        default: stage<C, 2, PPT, INV, JFAST, NCOL>(buf, len, ncol, jstride, cstride, Ns, mq, mns, tw, twmul); break;
+        }
+        Ns *= rd.r[s];
+    }
+}
+
+}  // namespace fftdev
+}  // namespace cam

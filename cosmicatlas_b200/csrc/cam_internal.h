@@ -1,0 +1,174 @@
+// Internal declarations shared by the CUDA translation units of libcam.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/cam.h"
+
+namespace cam {
+
+constexpr int kNumSMs = 148;  // B200: 2 dies x 74 SMs
+
+// ---------------------------------------------------------------- errors
+struct Error {
+    int code;
+    std::string msg;
+};
+
+#define CAM_CUDA_TRY(expr)                                                          \
+    do {                                                                            \
+        cudaError_t _e = (expr);                                                    \
+        if (_e != cudaSuccess)                                                      \
+            throw ::cam::Error{CAM_E_CUDA, std::string(#expr) + ": " +              \
+                                               cudaGetErrorString(_e)};             \
+    } while (0)
+
+#define CAM_REQUIRE(cond, code, msg)                                                \
+    do {                                                                            \
+        if (!(cond)) throw ::cam::Error{(code), (msg)};                             \
+    } while (0)
+
+// Kernel launch with error check, launch accounting and (when enabled)
+// CUDA-event timing per kernel name.
+#define CAM_LAUNCH_NAMED(ctx, name, kernel, grid, block, smem, ...)                 \
+    do {                                                                            \
+        ::cam::prof_begin((ctx), (name));                                           \
+        kernel<<<(grid), (block), (smem), (ctx)->stream>>>(__VA_ARGS__);            \
+        CAM_CUDA_TRY(cudaGetLastError());                                           \
+        ::cam::prof_end(ctx);                                                       \
+        (ctx)->launches++;                                                          \
+    } while (0)
+#define CAM_LAUNCH(ctx, kernel, grid, block, smem, ...) \
+    CAM_LAUNCH_NAMED(ctx, #kernel, kernel, grid, block, smem, __VA_ARGS__)
+
+// ------------------------------------------------------ device buffers
+// Grow-only device allocation owned by a context, charged to its budget.
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t cap = 0;
+};
+
+struct FftPlan;  // cam_fft.cu
+
+struct ProfRecord {
+    const char *name;
+    cudaEvent_t start, stop;
+};
+
+}  // namespace cam
+
+struct cam_ctx {
+    int device = 0;
+    size_t budget = 0;  // 0 = unlimited
+    size_t used = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    std::recursive_mutex mu;
+    int64_t launches = 0;
+    std::map<std::string, cam::DevBuf> bufs;
+    std::map<int64_t, cam::FftPlan *> plans;  // key: n * 2 + precision
+    // per-kernel timing (cam_profile_enable)
+    bool prof_on = false;
+    std::vector<cam::ProfRecord> prof_pending;
+    std::vector<cudaEvent_t> prof_pool;
+    std::map<std::string, std::pair<int64_t, double>> prof_acc;  // name -> (launches, ms)
+};
+
+namespace cam {
+
+void prof_begin(cam_ctx *ctx, const char *name);
+void prof_end(cam_ctx *ctx);
+
+// Returns a device buffer of at least `bytes`, reallocating (and
+// synchronising the stream) if the cached one is too small.
+void *scratch(cam_ctx *ctx, const char *name, size_t bytes);
+void release_all(cam_ctx *ctx);
+
+// Host <-> device staging helpers for the C ABI.
+template <typename T>
+inline T *stage_in(cam_ctx *ctx, const char *name, const T *p, size_t count, int mem)
+{
+    if (mem == CAM_MEM_DEVICE || p == nullptr) return const_cast<T *>(p);
+    T *d = static_cast<T *>(scratch(ctx, name, count * sizeof(T)));
+    CAM_CUDA_TRY(cudaMemcpyAsync(d, p, count * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+    return d;
+}
+
+// ------------------------------------------------------ assignment
+struct AssignGeom {
+    int n[3];
+    float L[3], d[3], mn[3];
+    int b[3];   // brick extent (cells)
+    int nb[3];  // bricks per axis
+};
+
+struct AssignOut {
+    int precision;      // CAM_F32 / CAM_F64, or -1 for uint32 counts
+    void *mesh;         // device
+    double *d_sum;      // device scalar: sum of the mesh (FP64)
+    int64_t n_in = 0, n_lost = 0;
+};
+
+// Runs the assignment pipeline on device particle arrays.  Writes the mesh
+// and, on the device, the FP64 mesh sum.  Synchronises once (payload size).
+void assign_device(cam_ctx *ctx, const float *x, const float *y, const float *z,
+                   const float *w, int64_t np, const cam_grid &grid, int scheme,
+                   AssignOut &out);
+void cell_keys_device(cam_ctx *ctx, const float *x, const float *y, const float *z,
+                      int64_t np, const cam_grid &grid, int scheme, int64_t *keys);
+AssignGeom make_geom(const cam_grid &g, int scheme, int64_t np);
+
+// ------------------------------------------------------ FFT
+// Internal spectrum layout ("split"): main[N][N][N/2] complex plus the
+// Nyquist plane nyq[N][N] (k = N/2).  Row strides are multiples of 16 bytes.
+struct Spectrum {
+    void *main = nullptr;
+    void *nyq = nullptr;
+    int64_t n = 0;
+    int precision = CAM_F32;
+};
+
+FftPlan *get_plan(cam_ctx *ctx, int64_t n, int precision);
+// Forward r2c of a real N^3 mesh; `sub` (device scalar, may be null) is
+// subtracted from every element on load.
+void fft_r2c_split(cam_ctx *ctx, FftPlan *plan, const void *real_in, const double *d_sub,
+                   Spectrum &out);
+// Inverse c2r (in place on the spectrum), result scaled by `scale`.
+void fft_c2r_split(cam_ctx *ctx, FftPlan *plan, Spectrum &spec, void *real_out, double scale);
+void split_to_fftw(cam_ctx *ctx, const Spectrum &s, void *dst);
+void fftw_to_split(cam_ctx *ctx, const void *src, Spectrum &s);
+
+// Strided complex column FFTs over a batch (used by the T-web passes).
+void fft_columns(cam_ctx *ctx, FftPlan *plan, void *base, int64_t len, int64_t ncols,
+                 int64_t jstride, int64_t nplanes, int64_t pstride, int ncomp,
+                 int64_t cstride_comp, bool inverse);
+void fft_rows_c2c(cam_ctx *ctx, FftPlan *plan, void *base, int64_t len, int64_t nrows,
+                  int ncomp, int64_t cstride_comp, bool inverse);
+const void *plan_twiddles(FftPlan *plan);
+
+// ------------------------------------------------------ power spectrum
+struct PkDevice {
+    double *sums;   // [nbins][2] FP64: sum |F|^2/W^2, sum C/W^2
+    int64_t *modes; // [nbins]
+};
+void power_bin(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins,
+               double *h_sum_raw, double *h_sum_sn, int64_t *h_modes);
+
+// ------------------------------------------------------ T-web
+void tweb_device(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const double *d_mean,
+                 int input_type, const cam_tweb_opts &o, uint8_t *d_labels, float *d_lambdas,
+                 cam_tweb_stats *stats);
+
+// Deterministic FP64 sum of a device array into a device scalar.
+void reduce_sum_f64(cam_ctx *ctx, const double *in, int64_t n, double *out);
+// Mean of a device mesh of precision `prec` into a device scalar (FP64).
+void mesh_mean(cam_ctx *ctx, const void *mesh, int precision, int64_t ncell, double *d_mean);
+
+}  // namespace cam

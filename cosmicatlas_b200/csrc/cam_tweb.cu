@@ -1,0 +1,327 @@
+// T-web cosmic-web classification for sm_100a.
+//
+// Replaces Cwclass::get_CWC, Source/Cwclass.cpp:235-890, with the FFT tidal
+// tensor of EigenValuesTweb, Source/Miscelanious.cpp:1772-1883, and
+// calc_LapPhiv, Source/NumericalMethods.cpp:2609-2680:
+//   T_ab(x) = c2r( k_a k_b / k^2 * exp(-k^2 R^2 / 2) * delta_k ) / N^3
+// with k_a = k_f * (i <= N/2 ? i : i - N) and T = 0 at k = 0; then per cell
+// the eigenvalues lambda1 >= lambda2 >= lambda3 and the label
+// 4 - #{lambda_a > lambda_th} (Source/Cwclass.cpp:875-890).
+//
+// Only the six distinct components are transformed (the reference does
+// nine).  Three kernels:
+//   tidal_x    : inverse FFT along x fused with the multiplier; the six
+//                components of one delta_k tile are made by six consecutive
+//                CTAs, so the tile is read from HBM once and from L2 after;
+//   (columns)  : inverse FFT along y for the six components (generic);
+//   tidal_z    : c2r along z of the six components of a few rows, then the
+//                eigenvalues (FP32 trigonometric solution plus one FP64
+//                Newton step) and the label of every cell, written as uint8.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "cam_fft_device.cuh"
+#include "cam_internal.h"
+
+namespace cam {
+namespace {
+
+template <typename T>
+using CTw = fftdev::CT<T>;
+
+// Component c -> (a, b): xx, yy, zz, xy, xz, yz
+__device__ __forceinline__ void comp_axes(int c, int &a, int &b)
+{
+    const int A[6] = {0, 1, 2, 0, 0, 1};
+    const int B[6] = {0, 1, 2, 1, 2, 2};
+    a = A[c];
+    b = B[c];
+}
+
+}  // namespace
+
+
+namespace {
+
+// Tidal multiplier for signed frequencies (fi, fj, fk) of component c.
+template <typename T>
+__device__ __forceinline__ T tidal_mult(int c, int fi, int fj, int fk, T gauss_coef, T norm)
+{
+    const int64_t q = (int64_t)fi * fi + (int64_t)fj * fj + (int64_t)fk * fk;
+    if (q == 0) return (T)0;
+    int a, b;
+    comp_axes(c, a, b);
+    const int f[3] = {fi, fj, fk};
+    const T ratio = (T)((double)((int64_t)f[a] * f[b]) / (double)q);
+    const T g = gauss_coef != (T)0 ? exp(-gauss_coef * (T)q) : (T)1;
+    return ratio * g * norm;
+}
+
+// Inverse FFT along x of the six tidal components of one tile of delta_k.
+// NYQ = false: main tiles (plane = j, columns = k < N/2, FFT index i with
+// stride N*M).  NYQ = true: the Nyquist plane (columns = j, FFT index i with
+// stride N, k = N/2).
+template <typename T, bool NYQ>
+__global__ void __launch_bounds__(1024, 1)
+tidal_x_kernel(const typename CTw<T>::t *__restrict__ src, typename CTw<T>::t *__restrict__ dst,
+               int n, int ncols, int64_t jstride, int64_t pstride, int64_t ccomp, Radices rd,
+               const typename CTw<T>::t *__restrict__ tw, double gauss_coef, const double *__restrict__ d_mean,
+               int density_input, double scale)
+{
+    using C = typename CTw<T>::t;
+    constexpr int W = CTw<T>::kCols;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *tile = reinterpret_cast<C *>(smem_raw);
+    const int comp = blockIdx.x;  // fastest: the six CTAs of a tile run together
+    const int col0 = blockIdx.y * W;
+    const int plane = blockIdx.z;
+    const int nc = min(W, ncols - col0);
+    const int h = n / 2;
+    const C *g = src + (int64_t)plane * pstride + col0;
+    C *o = dst + (int64_t)comp * ccomp + (int64_t)plane * pstride + col0;
+    double normd = scale;
+    if (density_input) normd /= *d_mean;  // delta_k = F(rho - mean) / mean
+    const T norm = (T)normd, gc = (T)gauss_coef;
+    const int tot = n * W;
+    for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+        const int i = e / W, cc = e % W;
+        if (cc < nc) {
+            const C v = g[(int64_t)i * jstride + cc];
+            const int fi = i <= h ? i : i - n;
+            int fj, fk;
+            if (NYQ) {
+                const int j = col0 + cc;
+                fj = j <= h ? j : j - n;
+                fk = h;
+            } else {
+                fj = plane <= h ? plane : plane - n;
+                fk = col0 + cc;
+            }
+            const T m = tidal_mult<T>(comp, fi, fj, fk, gc, norm);
+            tile[e] = C{v.x * m, v.y * m};
+        }
+    }
+    __syncthreads();
+    fftdev::block_fft<C, CTw<T>::kPPT, true, false, W>(tile, n, W, W, 1, rd, tw, 1);
+    for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+        const int i = e / W, cc = e % W;
+        if (cc < nc) o[(int64_t)i * jstride + cc] = tile[e];
+    }
+}
+
+// FP32 trigonometric eigenvalues of a symmetric 3x3 matrix (O.K. Smith,
+// CACM 4(4):168, 1961), each refined by one Newton step on the FP64
+// characteristic polynomial; returned in descending order.
+__device__ __forceinline__ void eig3(float a00, float a11, float a22, float a01, float a02, float a12,
+                                     double lam[3])
+{
+    const float p1 = a01 * a01 + a02 * a02 + a12 * a12;
+    const float q = (a00 + a11 + a22) * (1.0f / 3.0f);
+    const float b00 = a00 - q, b11 = a11 - q, b22 = a22 - q;
+    const float p2 = b00 * b00 + b11 * b11 + b22 * b22 + 2.0f * p1;
+    float l[3];
+    if (!(p2 > 0.0f)) {
+        l[0] = l[1] = l[2] = q;
+    } else {
+        const float pp = sqrtf(p2 * (1.0f / 6.0f));
+        const float det = b00 * (b11 * b22 - a12 * a12) - a01 * (a01 * b22 - a12 * a02) +
+                          a02 * (a01 * a12 - b11 * a02);
+        float r = det / (2.0f * pp * pp * pp);
+        r = fminf(1.0f, fmaxf(-1.0f, r));
+        const float phi = acosf(r) * (1.0f / 3.0f);
+        l[0] = q + 2.0f * pp * cosf(phi);
+        l[2] = q + 2.0f * pp * cosf(phi + 2.0943951023931954923f);
+        l[1] = 3.0f * q - l[0] - l[2];
+    }
+    // det(x I - A) = x^3 - c2 x^2 + c1 x - c0, coefficients in FP64 from the
+    // FP32 entries (products of two floats are exact in double).
+    const double A00 = a00, A11 = a11, A22 = a22, A01 = a01, A02 = a02, A12 = a12;
+    const double c2 = A00 + A11 + A22;
+    const double c1 = A00 * A11 + A00 * A22 + A11 * A22 - A01 * A01 - A02 * A02 - A12 * A12;
+    const double c0 = A00 * (A11 * A22 - A12 * A12) - A01 * (A01 * A22 - A12 * A02) + A02 * (A01 * A12 - A11 * A02);
+    const double sc = fmax(fabs((double)l[0]), fabs((double)l[2])) + 1e-30;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        double x = l[k];
+        const double f = ((x - c2) * x + c1) * x - c0;
+        const double fp = (3.0 * x - 2.0 * c2) * x + c1;
+        if (fabs(fp) > 1e-6 * sc * sc) {
+            const double dx = f / fp;
+            if (fabs(dx) < 1e-4 * sc) x -= dx;
+        }
+        lam[k] = x;
+    }
+    // keep descending order after refinement
+    if (lam[0] < lam[1]) { const double t = lam[0]; lam[0] = lam[1]; lam[1] = t; }
+    if (lam[1] < lam[2]) { const double t = lam[1]; lam[1] = lam[2]; lam[2] = t; }
+    if (lam[0] < lam[1]) { const double t = lam[0]; lam[0] = lam[1]; lam[1] = t; }
+}
+
+// c2r along z of the six components for `rpc` rows, then eigenvalues and
+// labels.  Component c of row r: main at src + c*ccomp + r*M, Nyquist at
+// nyq + c*N*N + r.
+template <typename T>
+__global__ void __launch_bounds__(512, 1)
+tidal_z_kernel(const typename CTw<T>::t *__restrict__ src, const typename CTw<T>::t *__restrict__ nyq,
+               int n, int64_t nrows, int rpc, int64_t ccomp, Radices rd,
+               const typename CTw<T>::t *__restrict__ tw, double lth, double band,
+               uint8_t *__restrict__ labels, float *__restrict__ lambdas,
+               unsigned long long *__restrict__ counts /* [5] */)
+{
+    using C = typename CTw<T>::t;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *tile = reinterpret_cast<C *>(smem_raw);  // [6][rpc][M]
+    __shared__ unsigned int cnt_s[5];
+    const int M = n / 2;
+    const int64_t row0 = (int64_t)blockIdx.x * rpc;
+    const int nr = (int)min((int64_t)rpc, nrows - row0);
+    const int64_t nn = (int64_t)n * n;
+    if (threadIdx.x < 5) cnt_s[threadIdx.x] = 0;
+    // Load + c2r untangling (see fft_rows_kernel, mode c2r).
+    const int per = rpc * M;
+    for (int e = threadIdx.x; e < 6 * per; e += blockDim.x) {
+        const int c = e / per, rem = e % per;
+        const int r = rem / M, k = rem % M;
+        if (r >= nr) continue;
+        const C *sm = src + (int64_t)c * ccomp + (row0 + r) * M;
+        C xk = sm[k];
+        C xm = k == 0 ? nyq[(int64_t)c * nn + row0 + r] : sm[M - k];
+        if (k == 0) {
+            xk.y = 0;
+            xm.y = 0;
+        }
+        const C a = C{xk.x + xm.x, xk.y - xm.y};
+        const C b = C{xk.x - xm.x, xk.y + xm.y};
+        C wv = __ldg(tw + k);
+        wv.y = -wv.y;
+        const C ib = fftdev::rot<C, true>(fftdev::cmul(wv, b));
+        tile[e] = fftdev::cadd(a, ib);
+    }
+    __syncthreads();
+    fftdev::block_fft<C, CTw<T>::kPPT, true, true, 0>(tile, M, 6 * rpc, 1, M, rd, tw, 2);
+    // Per cell: 6 components -> eigenvalues -> label.
+    unsigned int lc[5] = {0, 0, 0, 0, 0};
+    const T *re = reinterpret_cast<const T *>(tile);  // real row r of comp c at (c*rpc + r)*n
+    const int64_t ncell = nn * n;
+    for (int e = threadIdx.x; e < nr * n; e += blockDim.x) {
+        const int r = e / n, z = e % n;
+        float t6[6];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) t6[c] = (float)re[((int64_t)c * rpc + r) * n + z];
+        double lam[3];
+        eig3(t6[0], t6[1], t6[2], t6[3], t6[4], t6[5], lam);
+        int v = 0, tie = 0;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            v += lam[a] > lth;
+            tie |= fabs(lam[a] - lth) <= band;
+        }
+        const int64_t cell = (row0 + r) * n + z;
+        if (labels) labels[cell] = (uint8_t)(4 - v);
+        if (lambdas) {
+            lambdas[cell] = (float)lam[0];
+            lambdas[ncell + cell] = (float)lam[1];
+            lambdas[2 * ncell + cell] = (float)lam[2];
+        }
+        lc[3 - v]++;
+        lc[4] += tie;
+    }
+#pragma unroll
+    for (int a = 0; a < 5; ++a) {
+        unsigned int v = lc[a];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if ((threadIdx.x & 31) == 0 && v) atomicAdd(&cnt_s[a], v);
+    }
+    __syncthreads();
+    if (threadIdx.x < 5 && cnt_s[threadIdx.x]) atomicAdd(&counts[threadIdx.x], (unsigned long long)cnt_s[threadIdx.x]);
+}
+
+int threads_for(int points, int ppt, int cap)
+{
+    int t = (points + ppt - 1) / ppt;
+    t = ((t + 31) / 32) * 32;
+    return std::max(32, std::min(cap, t));
+}
+
+template <typename T>
+void tweb_impl(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const double *d_mean,
+               int input_type, const cam_tweb_opts &o, uint8_t *d_labels, float *d_lambdas,
+               cam_tweb_stats *stats)
+{
+    using C = typename CTw<T>::t;
+    constexpr int W = CTw<T>::kCols;
+    const int64_t n = dk.n, M = n / 2, nn = n * n;
+    const Radices rn = factor_radices(n), rm = factor_radices(M);
+    CAM_REQUIRE(rn.n > 0 && rm.n > 0, CAM_E_UNSUPPORTED, "T-web size must be 2^a 3^b");
+    const C *tw = static_cast<const C *>(plan_twiddles(plan));
+    const int64_t ccomp = nn * M;
+    C *cm = static_cast<C *>(scratch(ctx, "tw.main", (size_t)6 * ccomp * sizeof(C)));
+    C *cn = static_cast<C *>(scratch(ctx, "tw.nyq", (size_t)6 * nn * sizeof(C)));
+    auto *cnt = static_cast<unsigned long long *>(scratch(ctx, "tw.cnt", 8 * sizeof(unsigned long long)));
+    CAM_CUDA_TRY(cudaMemsetAsync(cnt, 0, 8 * sizeof(unsigned long long), ctx->stream));
+
+    const double kf = 2.0 * M_PI / (double)L;
+    const double R = o.smoothing_R;
+    const double gcoef = R > 0 ? 0.5 * kf * kf * R * R : 0.0;
+    const double scale = 1.0 / ((double)n * (double)n * (double)n);  // c2r divides by N^3
+    const int density = input_type == CAM_INPUT_DENSITY;
+
+    // 1. x: multiplier + inverse FFT along x, six components.
+    {
+        const int nthr = threads_for((int)n * W, CTw<T>::kPPT, 1024);
+        const size_t smem = (size_t)n * W * sizeof(C);
+        auto k0 = tidal_x_kernel<T, false>;
+        auto k1 = tidal_x_kernel<T, true>;
+        CAM_CUDA_TRY(cudaFuncSetAttribute(k0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CAM_CUDA_TRY(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        dim3 g0(6, (unsigned)((M + W - 1) / W), (unsigned)n);
+        CAM_LAUNCH_NAMED(ctx, "tweb_tidal_x", k0, g0, nthr, smem, static_cast<const C *>(dk.main), cm, (int)n, (int)M, n * M,
+                   (int64_t)M, ccomp, rn, tw, gcoef, d_mean, density, scale);
+        dim3 g1(6, (unsigned)((n + W - 1) / W), 1);
+        CAM_LAUNCH_NAMED(ctx, "tweb_tidal_x_nyq", k1, g1, nthr, smem, static_cast<const C *>(dk.nyq), cn, (int)n, (int)n, n,
+                   (int64_t)0, nn, rn, tw, gcoef, d_mean, density, scale);
+    }
+    // 2. y: inverse FFT of the six components.
+    fft_columns(ctx, plan, cm, n, M, M, n, nn * M, 6, ccomp, true);
+    fft_rows_c2c(ctx, plan, cn, n, n, 6, nn, true);
+    // 3. z: c2r + eigenvalues + labels.
+    {
+        const int rpc = std::max(1, (int)((sizeof(T) == 4 ? 8192 : 4096) / (6 * M)));
+        const int nthr = threads_for(6 * rpc * (int)M, CTw<T>::kPPT, 512);
+        CAM_REQUIRE(6 * rpc * M <= (int64_t)nthr * CTw<T>::kPPT, CAM_E_UNSUPPORTED, "T-web row tile too large");
+        const size_t smem = (size_t)6 * rpc * M * sizeof(C);
+        auto kz = tidal_z_kernel<T>;
+        CAM_CUDA_TRY(cudaFuncSetAttribute(kz, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const unsigned grid = (unsigned)((nn + rpc - 1) / rpc);
+        CAM_LAUNCH_NAMED(ctx, "tweb_tidal_z_eigen", kz, grid, nthr, smem, cm, cn, (int)n, nn, rpc, ccomp, rm, tw, o.lambda_th,
+                   o.tie_band, d_labels, d_lambdas, cnt);
+    }
+    if (stats) {
+        unsigned long long h[5];
+        double mean = 0.0;
+        CAM_CUDA_TRY(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+        if (d_mean) CAM_CUDA_TRY(cudaMemcpyAsync(&mean, d_mean, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        for (int a = 0; a < 4; ++a) stats->counts[a] = (int64_t)h[a];
+        stats->ties = (int64_t)h[4];
+        stats->mean = mean;
+    }
+}
+
+}  // namespace
+
+void tweb_device(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const double *d_mean,
+                 int input_type, const cam_tweb_opts &o, uint8_t *d_labels, float *d_lambdas,
+                 cam_tweb_stats *stats)
+{
+    CAM_REQUIRE(std::isfinite(o.lambda_th) && o.tie_band >= 0.0, CAM_E_INVAL, "invalid T-web threshold");
+    CAM_REQUIRE(o.smoothing_R >= 0.f && std::isfinite(o.smoothing_R), CAM_E_INVAL, "invalid smoothing radius");
+    CAM_REQUIRE(input_type == CAM_INPUT_DELTA || d_mean, CAM_E_INVAL, "density input needs the mean");
+    if (dk.precision == CAM_F32) tweb_impl<float>(ctx, plan, dk, L, d_mean, input_type, o, d_labels, d_lambdas, stats);
+    else tweb_impl<double>(ctx, plan, dk, L, d_mean, input_type, o, d_labels, d_lambdas, stats);
+}
+
+}  // namespace cam

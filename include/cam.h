@@ -1,0 +1,207 @@
+/*
+ * cam.h -- C ABI of the B200 mesh hot path of CosmicAtlas/BAM
+ * (particle-to-mesh assignment, 3D r2c/c2r FFT, binned power spectrum, T-web).
+ *
+ * Every function returns CAM_OK (0) or a negative status and never exits.
+ * Pointers are plain host or device pointers; the `mem` field / argument says
+ * which (CAM_MEM_HOST or CAM_MEM_DEVICE).  Device pointers must belong to the
+ * context's device.  Calls on one context are serialised by the context and
+ * run on its stream; results written to host memory are complete when the
+ * call returns, results written to device memory are complete when the
+ * context's stream reaches the point of the call (cam_ctx_sync waits).
+ *
+ * Index convention: mesh cell (i, j, k) lives at k + N3*(j + N2*i) (z fastest),
+ * Source/massFunctions.cpp:74.  Half spectra use the FFTW r2c layout
+ * [i][j][k <= N/2] of complex pairs (re, im).
+ */
+#ifndef CAM_H
+#define CAM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+enum {
+    CAM_OK = 0,
+    CAM_E_INVAL = -1,       /* invalid argument, shape or option          */
+    CAM_E_NOMEM = -2,       /* device allocation failed / over HBM budget */
+    CAM_E_CUDA = -3,        /* CUDA runtime error (see cam_last_error)    */
+    CAM_E_TIMEOUT = -4,     /* a bounded wait ran out                      */
+    CAM_E_BUSY = -5,        /* queue full or job still running            */
+    CAM_E_NOTFOUND = -6,    /* unknown job id                              */
+    CAM_E_UNSUPPORTED = -7, /* size or option not implemented              */
+    CAM_E_NONFINITE = -8    /* a weight was NaN or infinite                */
+};
+
+/* ---- enums ------------------------------------------------------------ */
+enum { CAM_NGP = 0, CAM_CIC = 1, CAM_TSC = 2 };       /* mass assignment  */
+enum { CAM_F32 = 0, CAM_F64 = 1 };                    /* mesh/FFT precision */
+enum { CAM_MEM_HOST = 0, CAM_MEM_DEVICE = 1 };
+enum { CAM_INPUT_DENSITY = 0, CAM_INPUT_DELTA = 1 };  /* P(k)/T-web input  */
+
+typedef struct cam_ctx cam_ctx;
+
+/* Particles in structure-of-arrays form, the reference's xp, yp, zp,
+ * Par_mass vectors (Headers/massFunctions.h:12).  w == NULL means unit mass
+ * (weightmass == false). */
+typedef struct {
+    int64_t n;
+    const float *x, *y, *z, *w;
+    int mem;
+} cam_particles;
+
+/* Mesh geometry: N1..N3, L1..L3, d1..d3 and min1..min3 of getDensity_*
+ * (Headers/massFunctions.h:12-26).  d[a] == 0 means d = L/N computed in
+ * float, as Params::derived_pars does. */
+typedef struct {
+    int64_t n[3];
+    float L[3];
+    float d[3];
+    float min[3];
+} cam_grid;
+
+typedef struct {
+    int64_t n_in;    /* particles assigned                         */
+    int64_t n_lost;  /* particles outside the domain (NLOSS)        */
+    double sum_mesh; /* sum over the mesh, FP64 (get_nobjects)      */
+} cam_assign_stats;
+
+/* Binning and corrections of FftwFunctions::power_spectrum.  Edges are in
+ * units of the fundamental mode k_f = 2 pi / L: kmin = DeltaKmin * k_f,
+ * DeltaK = ndel * k_f (Params::derived_pars, Source/Params.cpp:4099-4104).
+ * nbins == 0 selects the reference default N / (2 ndel). */
+typedef struct {
+    int scheme;         /* window exponent p: NGP 0, CIC 1, TSC 2          */
+    int mas_correction; /* divide by W^2                                  */
+    int sn_correction;  /* subtract aliased Poisson shot noise            */
+    int input_type;     /* CAM_INPUT_DENSITY or CAM_INPUT_DELTA            */
+    int nbins;
+    double DeltaKmin;   /* kmin in units of k_f                            */
+    double ndel;        /* bin width in units of k_f                       */
+} cam_pk_opts;
+
+typedef struct {
+    double n_obj;       /* N_gal = sum of the mesh (density input) or 1    */
+    double shot_noise;  /* V / N_gal                                       */
+    double normal;      /* N_gal^2 / V (density) or N^6 / V (delta)        */
+    double kf;          /* 2 pi / L                                        */
+} cam_pk_info;
+
+/* T-web options (Cwclass::get_CWC, FFT tidal-tensor variant). */
+typedef struct {
+    float smoothing_R;  /* Gaussian exp(-k^2 R^2 / 2); 0 = none            */
+    double lambda_th;   /* label = 4 - #{lambda > lambda_th}               */
+    double tie_band;    /* cells with |lambda - lambda_th| <= band counted */
+    int input_type;     /* CAM_INPUT_DENSITY (rho -> rho/mean - 1) or DELTA */
+} cam_tweb_opts;
+
+typedef struct {
+    int64_t counts[4];  /* cells labelled 1 knot, 2 filament, 3 sheet, 4 void */
+    int64_t ties;       /* cells with an eigenvalue within tie_band of lambda_th */
+    double mean;        /* mean of the input mesh (density input)          */
+} cam_tweb_stats;
+
+/* ---- context ---------------------------------------------------------- */
+
+/* Creates a context on `device` with an HBM budget in bytes (0 = no limit
+ * beyond the device).  Plans, twiddle tables and scratch buffers are owned
+ * by the context and reused across calls. */
+int cam_ctx_create(int device, size_t hbm_budget, cam_ctx **out);
+int cam_ctx_destroy(cam_ctx *ctx);
+/* Sets the CUDA stream (cudaStream_t) the context launches on (NULL = the
+ * context's own stream). */
+int cam_ctx_set_stream(cam_ctx *ctx, void *stream);
+int cam_ctx_sync(cam_ctx *ctx);
+/* Message of the last failure on this context ("" if none). */
+const char *cam_last_error(cam_ctx *ctx);
+/* Number of kernels this context has launched so far. */
+int64_t cam_kernel_launches(cam_ctx *ctx);
+/* Per-kernel timing with CUDA events on the context's stream (no
+ * reference counterpart; the reference prints wall-clock banners,
+ * Source/ScreenOutput.cpp:466).  cam_profile_read writes lines
+ * "kernel,launches,total_ms" and optionally resets the totals. */
+int cam_profile_enable(cam_ctx *ctx, int on);
+int cam_profile_read(cam_ctx *ctx, char *buf, size_t len, int reset);
+const char *cam_version(void);
+
+/* ---- mass assignment --------------------------------------------------
+ * Replaces getDensity_NGP / getDensity_CIC / getDensity_TSC,
+ * Source/massFunctions.cpp:35, :678, :1050 (declared in
+ * Headers/massFunctions.h:12,18,26).  mesh_out (N1*N2*N3 values of the
+ * chosen precision) is overwritten (the reference zeroes delta first).
+ * Deterministic: integer keys, counting sort into mesh bricks, exact
+ * fixed-point accumulation per cell; no float atomics. */
+int cam_assign(cam_ctx *ctx, const cam_particles *parts, const cam_grid *grid,
+               int scheme, int precision, void *mesh_out, int out_mem,
+               cam_assign_stats *stats);
+
+/* Integer NGP counts per cell (uint32), bit-exact with the reference's
+ * float cell arithmetic (getDensity_NGP with weightmass == false). */
+int cam_count_ngp(cam_ctx *ctx, const cam_particles *parts, const cam_grid *grid,
+                  uint32_t *counts_out, int out_mem, cam_assign_stats *stats);
+
+/* Home-cell sort key of every particle: k + N3*(j + N2*i) of the cell the
+ * reference indexes for `scheme`, or N1*N2*N3 for a lost particle. */
+int cam_cell_keys(cam_ctx *ctx, const cam_particles *parts, const cam_grid *grid,
+                  int scheme, int64_t *keys_out, int out_mem);
+
+/* ---- FFT ---------------------------------------------------------------
+ * Replace do_fftw_r2c / do_fftw_c2r, Source/NumericalMethods.cpp:1718, :1818.
+ * Cubic N^3, N = 2^a 3^b, 8 <= N <= 1024.  r2c is unnormalised; c2r divides
+ * by N^3 as the reference does.  `precision` selects float or double
+ * elements.  Plans (twiddles) are built once per (N, precision) and cached. */
+int cam_fft_r2c(cam_ctx *ctx, int64_t n, int precision, const void *in, void *out, int mem);
+int cam_fft_c2r(cam_ctx *ctx, int64_t n, int precision, const void *in, void *out, int mem);
+
+/* ---- power spectrum ----------------------------------------------------
+ * Replaces PowerSpectrumF::compute_power_spectrum_grid(const vector&, bool),
+ * Source/PowerSpectrumF.cpp:1739, and FftwFunctions::power_spectrum,
+ * Source/FftwFunctions.cpp:1660.  mesh is N^3 (cubic) of `precision`.
+ * Outputs per bin (host arrays of nbins; any may be NULL): pk, modes,
+ * kvector (bin centres kmin + (b + 1/2) DeltaK, PowerSpectrumF.cpp:1792). */
+int cam_power(cam_ctx *ctx, const cam_grid *grid, const void *mesh, int precision,
+              int mem, const cam_pk_opts *opts, double *pk, int64_t *modes,
+              double *kvector, cam_pk_info *info);
+
+/* ---- T-web -------------------------------------------------------------
+ * Replaces Cwclass::get_CWC, Source/Cwclass.cpp:235, with the FFT tidal
+ * tensor of EigenValuesTweb, Source/Miscelanious.cpp:1772.  labels (N^3
+ * uint8, values 1..4) and lambdas (3 x N^3 float, planes lambda1, lambda2,
+ * lambda3, descending) may be NULL; out_mem says where they live. */
+int cam_tweb(cam_ctx *ctx, const cam_grid *grid, const void *mesh, int precision,
+             int mem, const cam_tweb_opts *opts, uint8_t *labels, float *lambdas,
+             int out_mem, cam_tweb_stats *stats);
+
+/* ---- one mesh job: particles -> mesh -> FFT -> P(k) [-> T-web] ----------
+ * The plain per-call GPU path of one BAM iteration: the mesh and its
+ * spectrum stay resident on the device between the stages. */
+typedef struct {
+    cam_particles parts;
+    cam_grid grid;
+    int scheme;
+    int precision;
+    cam_pk_opts pk;     /* pk.nbins > 0 to compute P(k)            */
+    int want_tweb;
+    cam_tweb_opts tweb;
+} cam_job_desc;
+
+typedef struct {
+    double *pk;          /* nbins (host), may be NULL              */
+    int64_t *modes;      /* nbins (host), may be NULL              */
+    double *kvector;     /* nbins (host), may be NULL              */
+    uint8_t *labels;     /* N^3 (host), may be NULL                */
+    cam_pk_info pk_info;
+    cam_assign_stats assign;
+    cam_tweb_stats tweb;
+} cam_job_result;
+
+int cam_job_run(cam_ctx *ctx, const cam_job_desc *job, cam_job_result *res);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CAM_H */

@@ -1,0 +1,271 @@
+"""CPU oracle for the CosmicAtlas/BAM mesh hot path -- TEST INFRASTRUCTURE ONLY.
+
+Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` import this module; the product library never does.
+
+Parity status: UNPINNED.  The reference cannot be compiled here (FFTW3, GSL,
+boost, HEALPix, CFITSIO and some of its own headers are missing) and ships no
+golden vectors, so this module restates the reference source text:
+
+* mass assignment, keys, P(k) binning, eigenvalues: ``oracle/cam_oracle.c``
+  (each function cites the reference lines it follows);
+* FFTs: numpy's pocketfft in FP64 stands in for FFTW3 (unpinned third-party
+  boundary: the reference links an unversioned system FFTW,
+  Main/Makefile:42-43);
+* the tidal tensor follows calc_LapPhiv, Source/NumericalMethods.cpp:2609-2680,
+  and the Gaussian filter kernelcomp, Source/NumericalMethods.cpp:2272-2273.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+NGP, CIC, TSC = 0, 1, 2
+SCHEME_P = {NGP: 0, CIC: 1, TSC: 2}  # window exponent p (Source/Params.cpp:3531-3542)
+
+
+def build() -> str:
+    """Compile ``cam_oracle.c`` with the committed Makefile; returns the .so path."""
+    so = os.path.join(_HERE, "_build", "liboracle.so")
+    src = os.path.join(_HERE, "cam_oracle.c")
+    if not os.path.exists(so) or os.path.getmtime(so) < os.path.getmtime(src):
+        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return so
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        _LIB = ctypes.CDLL(build())
+        P = ctypes.c_void_p
+        i64, i32, f64, f32 = ctypes.c_int64, ctypes.c_int, ctypes.c_double, ctypes.c_float
+        _LIB.orc_keys.argtypes = [i32, i64, P, P, P, P, P, P, P, P]
+        _LIB.orc_keys.restype = None
+        _LIB.orc_assign_f64.argtypes = [i32, i64, P, P, P, P, P, P, P, P, P]
+        _LIB.orc_assign_f64.restype = i64
+        _LIB.orc_assign_ref.argtypes = [i32, i64, P, P, P, P, i64, i64, i64,
+                                        f32, f32, f32, f32, f32, f32, f32, f32, f32, P]
+        _LIB.orc_assign_ref.restype = i64
+        _LIB.orc_power_f64.argtypes = [i64, P, i32, i32, i32, f64, f64, f64, f64, i32, P, P, P, P]
+        _LIB.orc_power_f64.restype = None
+        _LIB.orc_power_ref.argtypes = [i64, P, i32, i32, i32, f32, f32, f32, f32, f32, i32, i32, P, P]
+        _LIB.orc_power_ref.restype = None
+        _LIB.orc_bin.argtypes = [f64, f64, f64, i32]
+        _LIB.orc_bin.restype = i64
+        _LIB.orc_eig3_f64.argtypes = [i64, P, P]
+        _LIB.orc_eig3_f64.restype = None
+        _LIB.orc_classify.argtypes = [i64, P, f64, f64, P, P, P]
+        _LIB.orc_classify.restype = None
+    return _LIB
+
+
+def _p(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+@dataclass
+class Grid:
+    """Mesh geometry: cells per axis, box sides, spacing and origin (float32),
+    the fields of s_params_box_mas, Headers/Type_structures_def.h:1141-1152."""
+    n: tuple
+    L: tuple
+    d: tuple
+    mn: tuple
+
+    @staticmethod
+    def cubic(n: int, L: float, mn: float = 0.0) -> "Grid":
+        d = float(np.float32(np.float32(L) / np.float32(n)))
+        return Grid((n, n, n), (L, L, L), (d, d, d), (mn, mn, mn))
+
+    def arrays(self):
+        return (np.asarray(self.n, np.int64), np.asarray(self.L, np.float32),
+                np.asarray(self.d, np.float32), np.asarray(self.mn, np.float32))
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def keys(scheme, x, y, z, grid: Grid) -> np.ndarray:
+    x, y, z = _f32(x), _f32(y), _f32(z)
+    n, L, d, mn = grid.arrays()
+    out = np.empty(x.size, np.int64)
+    lib().orc_keys(scheme, x.size, _p(x), _p(y), _p(z), _p(n), _p(L), _p(d), _p(mn), _p(out))
+    return out
+
+
+def assign_f64(scheme, x, y, z, w, grid: Grid):
+    """FP64 mesh with the pinned semantics; returns (mesh[N1,N2,N3], n_lost)."""
+    x, y, z = _f32(x), _f32(y), _f32(z)
+    w = None if w is None else _f32(w)
+    n, L, d, mn = grid.arrays()
+    mesh = np.empty(tuple(int(v) for v in n), np.float64)
+    lost = lib().orc_assign_f64(scheme, x.size, _p(x), _p(y), _p(z), _p(w),
+                                _p(n), _p(L), _p(d), _p(mn), _p(mesh))
+    return mesh, int(lost)
+
+
+def assign_ref(scheme, x, y, z, w, grid: Grid):
+    """The reference's FP32 serial loop as written (CPU baseline)."""
+    x, y, z = _f32(x), _f32(y), _f32(z)
+    w = None if w is None else _f32(w)
+    n, L, d, mn = grid.n, grid.L, grid.d, grid.mn
+    mesh = np.empty(tuple(n), np.float32)
+    lost = lib().orc_assign_ref(scheme, x.size, _p(x), _p(y), _p(z), _p(w), n[0], n[1], n[2],
+                                L[0], L[1], L[2], d[0], d[1], d[2], mn[0], mn[1], mn[2], _p(mesh))
+    return mesh, int(lost)
+
+
+def rfft3_f64(mesh: np.ndarray) -> np.ndarray:
+    """Unnormalised forward r2c (FFTW layout [i][j][k<=N/2]); stands in for
+    do_fftw_r2c, Source/NumericalMethods.cpp:1718-1753."""
+    return np.fft.rfftn(np.asarray(mesh, np.float64))
+
+
+def irfft3_f64(spec: np.ndarray, n: int) -> np.ndarray:
+    """c2r divided by N^3 as do_fftw_c2r does, Source/NumericalMethods.cpp:1818-1856
+    (numpy's irfftn already divides by N^3)."""
+    return np.fft.irfftn(spec, s=(n, n, n))
+
+
+@dataclass
+class PkResult:
+    pk: np.ndarray
+    modes: np.ndarray
+    sum_raw: np.ndarray
+    sum_sn: np.ndarray
+    kcent: np.ndarray
+    shot_noise: float
+    normal: float
+    n_obj: float
+
+
+def power_from_spectrum(spec, n, L, scheme, nbins, shot_noise, normal,
+                        kmin_u=0.0, dk_u=1.0, mas_corr=True, sn_corr=True) -> PkResult:
+    spec = np.ascontiguousarray(spec, dtype=np.complex128)
+    pk = np.empty(nbins); modes = np.empty(nbins, np.int64)
+    sr = np.empty(nbins); ss = np.empty(nbins)
+    lib().orc_power_f64(n, _p(spec), SCHEME_P[scheme], int(mas_corr), int(sn_corr),
+                        float(shot_noise), float(normal), float(kmin_u), float(dk_u), nbins,
+                        _p(pk), _p(modes), _p(sr), _p(ss))
+    kf = 2.0 * np.pi / L
+    kcent = kf * (kmin_u + (np.arange(nbins) + 0.5) * dk_u)
+    return PkResult(pk, modes, sr, ss, kcent, shot_noise, normal, float("nan"))
+
+
+def power_grid(mesh, L, scheme, nbins, kmin_u=0.0, dk_u=1.0, input_type="density",
+               mas_corr=True, sn_corr=True) -> PkResult:
+    """PowerSpectrumF::compute_power_spectrum_grid, Source/PowerSpectrumF.cpp:1739-1800,
+    in FP64: density input -> data = rho - N_gal/N^3, normal = N_gal^2/V,
+    SN = V/N_gal; delta input -> normal = N^6/V, N_gal = 1."""
+    n = mesh.shape[0]
+    vol = float(L) ** 3
+    mesh = np.asarray(mesh, np.float64)
+    if input_type == "density":
+        ngal = float(mesh.sum())
+        data = mesh - ngal / mesh.size
+        normal = ngal * ngal / vol
+    else:
+        ngal = 1.0
+        data = mesh
+        normal = float(mesh.size) ** 2 / vol
+    sn = vol / ngal
+    spec = rfft3_f64(data)
+    r = power_from_spectrum(spec, n, L, scheme, nbins, sn, normal, kmin_u, dk_u, mas_corr, sn_corr)
+    r.n_obj = ngal
+    return r
+
+
+def signed_freq(n: int) -> np.ndarray:
+    """coords[i] / deltak = i if i <= N/2 else i - N (NumericalMethods.cpp:2625-2626)."""
+    i = np.arange(n)
+    return np.where(i <= n // 2, i, i - n).astype(np.float64)
+
+
+def tidal_components(delta_k, n, L, R):
+    """T_ab = c2r(k_a k_b / k^2 * exp(-k^2 R^2 / 2) * delta_k) / N^3 for the six
+    symmetric pairs (xx, yy, zz, xy, xz, yz).  calc_LapPhiv computes all nine,
+    Source/Miscelanious.cpp:1792-1828."""
+    kf = 2.0 * np.pi / L
+    fx = signed_freq(n)[:, None, None] * kf
+    fy = signed_freq(n)[None, :, None] * kf
+    fz = np.arange(n // 2 + 1, dtype=np.float64)[None, None, :] * kf
+    k2 = fx * fx + fy * fy + fz * fz
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ik2 = np.where(k2 > 0, 1.0 / k2, 0.0)
+    g = np.exp(-0.5 * k2 * R * R) if R > 0 else 1.0
+    base = delta_k * ik2 * g
+    pairs = [(fx, fx), (fy, fy), (fz, fz), (fx, fy), (fx, fz), (fy, fz)]
+    out = np.empty((n, n, n, 6))
+    for c, (a, b) in enumerate(pairs):
+        out[..., c] = irfft3_f64(base * (a * b), n)
+    return out
+
+
+def eig3_f64(t6: np.ndarray) -> np.ndarray:
+    """Descending eigenvalues of the (…,6) tensors via LAPACK (numpy eigvalsh)."""
+    m = np.empty(t6.shape[:-1] + (3, 3))
+    m[..., 0, 0] = t6[..., 0]; m[..., 1, 1] = t6[..., 1]; m[..., 2, 2] = t6[..., 2]
+    m[..., 0, 1] = m[..., 1, 0] = t6[..., 3]
+    m[..., 0, 2] = m[..., 2, 0] = t6[..., 4]
+    m[..., 1, 2] = m[..., 2, 1] = t6[..., 5]
+    return np.linalg.eigvalsh(m)[..., ::-1].copy()
+
+
+def eig3_closed(t6: np.ndarray) -> np.ndarray:
+    t6 = np.ascontiguousarray(t6.reshape(-1, 6), np.float64)
+    lam = np.empty((t6.shape[0], 3))
+    lib().orc_eig3_f64(t6.shape[0], _p(t6), _p(lam))
+    return lam
+
+
+@dataclass
+class TwebResult:
+    labels: np.ndarray
+    lam: np.ndarray
+    counts: np.ndarray
+    ties: int
+
+
+def classify(lam, lth, band=1e-5):
+    """CWClass = 4 - #{lambda > lambda_th}, Source/Cwclass.cpp:875-890."""
+    lam = np.ascontiguousarray(lam.reshape(-1, 3), np.float64)
+    labels = np.empty(lam.shape[0], np.uint8)
+    counts = np.zeros(4, np.int64)
+    ties = np.zeros(1, np.int64)
+    lib().orc_classify(lam.shape[0], _p(lam), float(lth), float(band), _p(labels), _p(counts), _p(ties))
+    return labels, counts, int(ties[0])
+
+
+def tweb_from_spectrum(delta_k, n, L, R, lth, band=1e-5) -> TwebResult:
+    t6 = tidal_components(delta_k, n, L, R)
+    lam = eig3_f64(t6).reshape(n, n, n, 3)
+    labels, counts, ties = classify(lam, lth, band)
+    return TwebResult(labels.reshape(n, n, n), lam, counts, ties)
+
+
+def tweb_density(mesh, L, R, lth, band=1e-5) -> TwebResult:
+    """Cwclass::get_CWC on delta = rho/mean - 1 (Source/Cwclass.cpp:235-890,
+    FFT tidal-tensor variant EigenValuesTweb, Source/Miscelanious.cpp:1772)."""
+    n = mesh.shape[0]
+    mesh = np.asarray(mesh, np.float64)
+    nbar = mesh.sum() / mesh.size
+    delta_k = rfft3_f64(mesh / nbar - 1.0)
+    return tweb_from_spectrum(delta_k, n, L, R, lth, band)
+
+
+def power_ref(spec_c64, n, L, scheme, nbins, shot_noise, normal, ndel=1.0, fix_octant4=True):
+    """The reference's FP32 loop as written (CPU baseline)."""
+    spec = np.ascontiguousarray(spec_c64, dtype=np.complex64)
+    pk = np.empty(nbins, np.float32); md = np.empty(nbins, np.int32)
+    dk = np.float32(2.0 * np.pi / L)
+    lib().orc_power_ref(n, _p(spec), SCHEME_P[scheme], 1, 1, float(shot_noise), float(normal),
+                        float(dk), 0.0, float(ndel * dk), nbins, int(fix_octant4), _p(pk), _p(md))
+    return pk, md

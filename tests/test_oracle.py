@@ -1,0 +1,186 @@
+"""Pins the CPU oracle (no GPU).
+
+The reference ships no golden vectors, so the oracle is pinned against
+known answers derived by hand from the reference source:
+  * cell keys at chosen positions, following the float arithmetic of
+    getDensity_NGP/CIC/TSC (Source/massFunctions.cpp:57-69, :700-737, :1076-1089);
+  * single-particle CIC/TSC weights (massFunctions.cpp:743-769, :1098-1162);
+  * the power spectrum of a plane wave (FftwFunctions.cpp:1660-1876);
+  * eigenvalues of matrices with known spectra and the label rule
+    (Cwclass.cpp:875-890);
+and against the reference loops as written (the FP32 restatement).
+"""
+import numpy as np
+import pytest
+
+import oracle as orc
+
+
+def grid(n, box=1000.0):
+    return orc.Grid.cubic(n, box)
+
+
+# ---------------------------------------------------------------- keys
+def test_ngp_keys_known_positions():
+    # N = 8, L = 1000, d = 125 (exact in float)
+    g = grid(8)
+    x = np.array([0.0, 124.99999, 125.0, np.nextafter(np.float32(1000), 0), 1000.0, -1e-3, 500.0], np.float32)
+    y = np.full_like(x, 250.0)   # cell 2
+    z = np.full_like(x, 0.0)     # cell 0
+    k = orc.keys(orc.NGP, x, y, z, g)
+    lost = 8 ** 3
+    # x: 0 -> 0; 124.99999 -> 0; 125 -> 1; 999.99994 -> 7; 1000 -> lost (x < L);
+    # -0.001 -> lost; 500 -> 4.  key = k + N*(j + N*i) with j = 2, k = 0.
+    expect = [0 * 64 + 16, 16, 64 + 16, 7 * 64 + 16, lost, lost, 4 * 64 + 16]
+    assert k.tolist() == expect
+
+
+def test_cic_and_tsc_keys_known_positions():
+    g = grid(8)
+    # CIC: xpos = x - d/2 wrapped once: x = 10 -> -52.5 + 1000 = 947.5 -> cell 7;
+    # x = 62.5 -> 0 -> cell 0; x = 1000 -> 937.5 -> cell 7 (accepted after wrap).
+    x = np.array([10.0, 62.5, 1000.0, 187.5], np.float32)
+    y = np.full_like(x, 62.5)
+    z = np.full_like(x, 62.5)
+    k = orc.keys(orc.CIC, x, y, z, g)
+    assert k.tolist() == [7 * 64, 0, 7 * 64, 1 * 64]
+    # TSC accepts x == L (closed interval) and wraps its cell 8 to 0.
+    x = np.array([1000.0, 999.0, 0.0], np.float32)
+    k = orc.keys(orc.TSC, x, np.zeros_like(x), np.zeros_like(x), g)
+    assert k.tolist() == [0, 7 * 64, 0]
+    k = orc.keys(orc.TSC, np.array([1000.5], np.float32), np.zeros(1, np.float32), np.zeros(1, np.float32), g)
+    assert k.tolist() == [8 ** 3]
+
+
+def test_keys_follow_float_division_not_double():
+    # d = L / N rounded to float (1000/384 is not representable).  Scan many
+    # positions and check the key against an explicit float32 recomputation.
+    g = orc.Grid.cubic(384, 1000.0)
+    rng = np.random.default_rng(7)
+    x = rng.uniform(0, 1000, 200_000).astype(np.float32)
+    d = np.float32(g.d[0])
+    i = np.floor((x - np.float32(0)) / d).astype(np.int64) % 384
+    k = orc.keys(orc.NGP, x, np.zeros_like(x), np.zeros_like(x), g)
+    assert np.array_equal(k, i * 384 * 384)
+
+
+# ---------------------------------------------------------------- weights
+@pytest.mark.parametrize("t", [0.0, 0.25, 0.5, 0.9375])
+def test_single_particle_cic_weights(t):
+    n, box = 8, 1000.0
+    g = grid(n, box)
+    d = box / n
+    # node i sits at (i + 1/2) d; a particle at (3 + 1/2 + t) d
+    xv = np.float32((3.5 + t) * d)
+    mesh, lost = orc.assign_f64(orc.CIC, np.array([xv]), np.array([xv]), np.array([xv]), np.array([2.0], np.float32), g)
+    assert lost == 0
+    w1 = np.array([1 - t, t])
+    expect = np.zeros((n, n, n))
+    for a in range(2):
+        for b in range(2):
+            for c in range(2):
+                expect[3 + a, 3 + b, 3 + c] = 2.0 * w1[a] * w1[b] * w1[c]
+    np.testing.assert_allclose(mesh, expect, atol=1e-12)
+
+
+@pytest.mark.parametrize("t", [-0.5, -0.2, 0.0, 0.3])
+def test_single_particle_tsc_weights(t):
+    n, box = 8, 1000.0
+    g = grid(n, box)
+    d = box / n
+    xv = np.float32((4.5 + t) * d)   # cell 4, offset t from its centre
+    mesh, lost = orc.assign_f64(orc.TSC, np.array([xv]), np.array([xv]), np.array([xv]), None, g)
+    w1 = np.array([0.5 * (0.5 - t) ** 2, 0.75 - t * t, 0.5 * (0.5 + t) ** 2])
+    expect = np.zeros((n, n, n))
+    for a in range(3):
+        for b in range(3):
+            for c in range(3):
+                expect[3 + a, 3 + b, 3 + c] = w1[a] * w1[b] * w1[c]
+    np.testing.assert_allclose(mesh, expect, atol=1e-12)
+    assert abs(mesh.sum() - 1.0) < 1e-12
+
+
+def test_periodic_wrap_mass_conserved():
+    g = grid(4, 100.0)
+    x = np.array([0.1, 99.9, 50.0], np.float32)
+    for s in (orc.NGP, orc.CIC, orc.TSC):
+        mesh, lost = orc.assign_f64(s, x, x, x, None, g)
+        assert lost == 0
+        assert abs(mesh.sum() - 3.0) < 1e-12
+
+
+def test_oracle_matches_reference_loop_as_written():
+    # The FP32 reference loop computes dx = (xpos - min)/d - i in float, an
+    # absolute error of ~ulp(N) ~ 2e-6 cells per weight; so the two agree to
+    # that absolute level (relative to the largest cell), not per cell.
+    rng = np.random.default_rng(3)
+    g = grid(32, 1000.0)
+    x, y, z = (rng.uniform(1, 999, 20_000).astype(np.float32) for _ in range(3))
+    w = rng.uniform(0.5, 2.0, 20_000).astype(np.float32)
+    for s in (orc.NGP, orc.CIC, orc.TSC):
+        m64, l64 = orc.assign_f64(s, x, y, z, w, g)
+        m32, l32 = orc.assign_ref(s, x, y, z, w, g)
+        assert l64 == l32
+        err = np.max(np.abs(m64 - m32)) / np.abs(m64).max()
+        assert err < 1e-5, (s, err)
+        assert abs(m64.sum() - m32.sum()) / m64.sum() < 1e-5
+
+
+# ---------------------------------------------------------------- P(k)
+def test_plane_wave_power():
+    # delta(x) = A cos(2 pi m.x / N): |F(m)|^2 = (A N^3 / 2)^2, delta input
+    # normal = N^6 / V, so P = A^2 V / 4 in the bin of |m| with one mode.
+    n, box, A = 16, 100.0, 0.3
+    i = np.arange(n)
+    X, Y, Z = np.meshgrid(i, i, i, indexing="ij")
+    m = (2, 1, 2)  # |m| = 3
+    delta = A * np.cos(2 * np.pi * (m[0] * X + m[1] * Y + m[2] * Z) / n)
+    r = orc.power_grid(delta, box, orc.NGP, nbins=8, input_type="delta", mas_corr=False, sn_corr=False)
+    expect = np.zeros(8)
+    expect[3] = A * A * box ** 3 / 4.0 / r.modes[3]
+    np.testing.assert_allclose(r.pk, expect, atol=1e-9 * A * A * box ** 3)
+
+
+def test_bins_edges_go_up():
+    # |k| = 3 k_f exactly (a perfect square) lands in bin 3 with unit bins,
+    # and in bin 2 with 1.5 k_f bins (edges 0, 1.5, 3, 4.5 -> 3 is edge of bin 2).
+    assert orc.lib().orc_bin(9.0, 0.0, 1.0, 10) == 3
+    assert orc.lib().orc_bin(9.0, 0.0, 1.5, 10) == 2
+    assert orc.lib().orc_bin(8.99, 0.0, 1.5, 10) == 1
+    assert orc.lib().orc_bin(0.25, 1.0, 1.0, 10) == -1
+    assert orc.lib().orc_bin(1e6, 0.0, 1.0, 10) == -1
+
+
+def test_mode_count_is_independent_modes():
+    # default binning: every conjugate pair with 0 < |k| < k_Nyq counted once
+    n = 16
+    spec = np.zeros((n, n, n // 2 + 1), np.complex128)
+    r = orc.power_from_spectrum(spec, n, 100.0, orc.NGP, n // 2, 1.0, 1.0)
+    f = np.fft.fftfreq(n, 1.0 / n)
+    K = np.sqrt(f[:, None, None] ** 2 + f[None, :, None] ** 2 + f[None, None, :] ** 2)
+    full = np.bincount(np.floor(K[K > 0]).astype(int), minlength=64)[: n // 2]
+    assert np.array_equal(r.modes * 2, full)
+
+
+# ---------------------------------------------------------------- eigen / labels
+def test_eigen_known_spectra():
+    rng = np.random.default_rng(11)
+    lam_true = np.array([[3.0, 1.0, -2.0], [0.5, 0.5, 0.5], [1e-3, -1e-3, -5.0], [2.0, 2.0, -1.0]])
+    t6 = []
+    for l in lam_true:
+        q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+        m = q @ np.diag(l) @ q.T
+        t6.append([m[0, 0], m[1, 1], m[2, 2], m[0, 1], m[0, 2], m[1, 2]])
+    t6 = np.array(t6)
+    want = np.sort(lam_true, axis=1)[:, ::-1]
+    np.testing.assert_allclose(orc.eig3_f64(t6), want, atol=1e-12)
+    np.testing.assert_allclose(orc.eig3_closed(t6), want, atol=1e-7)
+
+
+def test_label_truth_table():
+    lam = np.array([[1.0, 0.5, 0.2], [1.0, 0.5, -0.2], [1.0, -0.5, -0.2], [-1.0, -0.5, -0.2],
+                    [0.0, 0.0, 0.0], [0.1 + 1e-6, 0.1, 0.0]])
+    labels, counts, ties = orc.classify(lam, 0.0, 1e-5)
+    assert labels.tolist() == [1, 2, 3, 4, 4, 2]
+    labels, counts, ties = orc.classify(lam[5:], 0.1, 1e-5)
+    assert labels.tolist() == [3] and ties == 1
