@@ -125,12 +125,12 @@ __global__ void final_sum_kernel(const double *__restrict__ part, int np, double
 
 }  // namespace
 
-// out[0] = sum, out[1] = sum / n (FP64, fixed order).
-void reduce_sum_f64(cam_ctx *ctx, const double *in, int64_t n, double *out)
+// out[0] = sum, out[1] = sum / divisor (FP64, fixed order).
+void reduce_sum_f64(cam_ctx *ctx, const double *in, int64_t n, double *out, double divisor)
 {
     auto *part = static_cast<double *>(scratch(ctx, "red.part", kRedBlocks * sizeof(double)));
     CAM_LAUNCH(ctx, partial_sum_kernel<double>, kRedBlocks, 256, 0, in, n, part);
-    CAM_LAUNCH(ctx, final_sum_kernel, 1, 32, 0, part, kRedBlocks, out, (double)n);
+    CAM_LAUNCH(ctx, final_sum_kernel, 1, 32, 0, part, kRedBlocks, out, divisor);
 }
 
 void mesh_mean(cam_ctx *ctx, const void *mesh, int precision, int64_t ncell, double *d_out)

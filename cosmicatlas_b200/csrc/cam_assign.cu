@@ -197,9 +197,13 @@ bin_kernel(const float *__restrict__ x, const float *__restrict__ y, const float
                         uint32_t word[3];
 #pragma unroll
                         for (int a = 0; a < 3; ++a) {
+                            // Home cell relative to the brick origin: the
+                            // periodic image in [-1, e], e = brick extent,
+                            // which holds whenever the stencil touches it.
+                            const int e = min(g.b[a], g.n[a] - o[a]);
                             int cl = c[a] - o[a];
-                            if (cl > (g.n[a] >> 1)) cl -= g.n[a];
-                            if (cl < -(g.n[a] >> 1)) cl += g.n[a];
+                            if (cl < -1) cl += g.n[a];
+                            else if (cl > e) cl -= g.n[a];
                             word[a] = pack_axis(cl, t[a]);
                         }
                         payload[slot] = make_uint4(word[0], word[1], word[2], __float_as_uint(wt));
@@ -517,7 +521,8 @@ static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const floa
         launch_dep(deposit_kernel<SCHEME, double>, static_cast<double *>(out.mesh));
     else
         launch_dep(deposit_kernel<SCHEME, uint32_t>, static_cast<uint32_t *>(out.mesh));
-    if (out.d_sum) reduce_sum_f64(ctx, bsum, nb, out.d_sum);
+    // out.d_sum[0] = sum of the mesh, out.d_sum[1] = mean per cell
+    if (out.d_sum) reduce_sum_f64(ctx, bsum, nb, out.d_sum, (double)g.n[0] * g.n[1] * g.n[2]);
 }
 
 void assign_device(cam_ctx *ctx, const float *x, const float *y, const float *z,

@@ -19,7 +19,8 @@ namespace cam {
 // Stage list of one transform length.  Integer divisions by the stage's
 // butterfly count nq = len/R and by Ns are done with precomputed
 // multipliers: floor(x / d) = umulhi(x, ceil(2^32 / d)), exact for
-// x, d < 2^16 (all lengths here are <= 1024).
+// x, d < 2^16 (all lengths here are <= 1024).  d = 1 has no 32-bit
+// multiplier (2^32); the stage handles it separately.
 struct Radices {
     int n = 0;
     int r[16];
@@ -151,7 +152,7 @@ __device__ __forceinline__ void stage(C *buf, int len, int ncol, int jstride, in
         if (bi < nbf) {
             int j, col;
             if (JFAST) {
-                col = (int)__umulhi((unsigned)bi, mq);
+                col = nq == 1 ? bi : (int)__umulhi((unsigned)bi, mq);
                 j = bi - col * nq;
             } else {
                 col = bi % NCOL;
@@ -160,7 +161,7 @@ __device__ __forceinline__ void stage(C *buf, int len, int ncol, int jstride, in
             const C *src = buf + col * cstride + j * jstride;
 #pragma unroll
             for (int r = 0; r < R; ++r) v[it][r] = src[r * nq * jstride];
-            const int q = (int)__umulhi((unsigned)j, mns);
+            const int q = Ns == 1 ? j : (int)__umulhi((unsigned)j, mns);
             const int k = j - q * Ns;
             if (Ns > 1) {
                 const int step = k * twstep;

@@ -166,8 +166,8 @@ void tweb_device(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const
                  int input_type, const cam_tweb_opts &o, uint8_t *d_labels, float *d_lambdas,
                  cam_tweb_stats *stats);
 
-// Deterministic FP64 sum of a device array into a device scalar.
-void reduce_sum_f64(cam_ctx *ctx, const double *in, int64_t n, double *out);
+// Deterministic FP64 sum of a device array: out[0] = sum, out[1] = sum / divisor.
+void reduce_sum_f64(cam_ctx *ctx, const double *in, int64_t n, double *out, double divisor);
 // Mean of a device mesh of precision `prec` into a device scalar (FP64).
 void mesh_mean(cam_ctx *ctx, const void *mesh, int precision, int64_t ncell, double *d_mean);
 

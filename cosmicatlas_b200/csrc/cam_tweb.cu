@@ -285,7 +285,7 @@ void tweb_impl(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const d
                    (int64_t)0, nn, rn, tw, gcoef, d_mean, density, scale);
     }
     // 2. y: inverse FFT of the six components.
-    fft_columns(ctx, plan, cm, n, M, M, n, nn * M, 6, ccomp, true);
+    fft_columns(ctx, plan, cm, n, M, M, n, n * M, 6, ccomp, true);
     fft_rows_c2c(ctx, plan, cn, n, n, 6, nn, true);
     // 3. z: c2r + eigenvalues + labels.
     {

@@ -21,15 +21,17 @@ def ctx():
     c.close()
 
 
-def rel_err_cells(a, b, eps=1e-6):
-    """max over cells |a - b| / (|b| + eps * max|b|): per-cell relative error
-    with a floor at eps of the largest cell (cells that receive only a tiny
-    stencil tail are judged against the mesh scale)."""
+def rel_err_cells(a, b, unit):
+    """max over cells |a - b| / max(|b|, unit): per-cell relative error, where
+    a cell holding less than one particle's mass (`unit` = mean particle
+    weight, 1 for unit masses) is judged against one particle's mass.  Cells
+    that only receive a stencil tail of ~1e-8 of a particle cannot carry a
+    relative error: the fractional offsets themselves are exact only to
+    ~1e-7 cells in FP32."""
     import numpy as np
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
-    scale = eps * max(float(np.abs(b).max()), 1e-300)
-    return float(np.max(np.abs(a - b) / (np.abs(b) + scale)))
+    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), unit)))
 
 
 def pk_rel_err(pk, pk_ref, floor):

@@ -1,8 +1,9 @@
 """GPU mass assignment vs the oracle (through the C ABI).
 
 Bar: sort keys and NGP counts bit-exact; CIC/TSC (and weighted NGP) meshes
-within 1e-5 per cell relative to the FP64 oracle (floor 1e-6 of the largest
-cell); bitwise determinism across runs.
+within 1e-5 per cell relative to the FP64 oracle (cells below one
+particle's mass judged against one particle's mass); bitwise determinism
+across runs and particle orders.
 """
 import numpy as np
 import pytest
@@ -83,7 +84,7 @@ def test_mesh_vs_oracle(ctx, scheme, weighted, precision):
     r = ctx.assign(x, y, z, w, g, scheme, precision)
     ref, lost = orc.assign_f64(scheme, x, y, z, w, orc.Grid.cubic(n, box))
     assert r.n_lost == lost
-    err = rel_err_cells(r.mesh, ref)
+    err = rel_err_cells(r.mesh, ref, 1.0 if w is None else float(np.mean(w)))
     assert err <= 1e-5, err
     assert abs(r.sum_mesh - ref.sum()) <= 1e-9 * ref.sum()
 
@@ -98,7 +99,7 @@ def test_small_and_ragged_meshes(ctx, scheme, n):
     r = ctx.assign(x, y, z, None, g, scheme, F64)
     ref, lost = orc.assign_f64(scheme, x, y, z, None, orc.Grid.cubic(n, box))
     assert r.n_lost == lost
-    assert rel_err_cells(r.mesh, ref) <= 1e-5
+    assert rel_err_cells(r.mesh, ref, 1.0) <= 1e-5
 
 
 def test_non_cubic_mesh(ctx):
@@ -111,7 +112,7 @@ def test_non_cubic_mesh(ctx):
     for s in SCHEMES:
         r = ctx.assign(x, y, z, None, g, s, F32)
         ref, lost = orc.assign_f64(s, x, y, z, None, orc.Grid(n, L, tuple(g.d), mn))
-        assert rel_err_cells(r.mesh, ref) <= 1e-5
+        assert rel_err_cells(r.mesh, ref, 1.0) <= 1e-5
 
 
 def test_empty_and_all_lost(ctx):

@@ -93,7 +93,9 @@ def test_job_equals_stages(ctx):
     mesh = ctx.assign(x, y, z, w, g, TSC, F32).mesh
     pk = ctx.power(mesh, box, Context.pk_opts(TSC, nbins=32))
     tw = ctx.tweb(mesh, box, Context.tweb_opts(8.0, 0.0, BAND))
-    np.testing.assert_allclose(res["pk"].pk, pk.pk, rtol=1e-12)
+    # the job subtracts the mean from the exact per-brick sums, the stage
+    # path from an FP64 sum over the FP32 cells: equal to ~1e-10
+    np.testing.assert_allclose(res["pk"].pk, pk.pk, rtol=1e-8)
     assert np.array_equal(res["tweb"].labels, tw.labels)
 
 
@@ -105,4 +107,5 @@ def test_job_fp64_mesh_c1_shape(ctx):
     res = ctx.job(x, y, z, None, g, CIC, F64, pk=Context.pk_opts(CIC, nbins=64))
     mesh, lost, pk, _ = oracle_job(x, y, z, None, n, box, CIC, 64, None, 0.0, F64)
     floor = pk.shot_noise * pk.sum_sn / np.maximum(pk.modes, 1)
-    assert pk_rel_err(res["pk"].pk, pk.pk, floor) <= 1e-9
+    # FP64 mesh and FFT; the stencil weights are FP32 products (~1e-7)
+    assert pk_rel_err(res["pk"].pk, pk.pk, floor) <= 1e-6
