@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--particles", type=int, default=N_PARTICLES)
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="profiler runs: the device-resident pass only (no e2e pass, no CPU baseline)")
     return ap.parse_args()
 
 
@@ -192,7 +194,8 @@ def run_ours(args):
 
     for _ in range(args.warmup):
         step(dev)
-        step(pinned)
+        if not args.kernels_only:
+            step(pinned)
     # device-resident inputs: the headline `value`
     lat = []
     launches0 = ctx.kernel_launches
@@ -205,7 +208,7 @@ def run_ours(args):
     launches = ctx.kernel_launches - launches0
     job_ms = sorted(a.elapsed_time(b) for a, b in lat)
     # end to end: pinned host particles in, P(k) out
-    ms_e2e = timed(pinned, args.steps)
+    ms_e2e = timed(pinned, args.steps) if not args.kernels_only else float("nan")
 
     jobs = len(SCHEMES) * args.steps * world
     value = jobs / (ms / 1e3)
@@ -335,7 +338,7 @@ def main():
     if out is None:
         return
     rank, local, world = dist_env()
-    if world == 1:
+    if world == 1 and not args.kernels_only:
         cores = os.cpu_count() or 1
         nsample = min(args.particles, 1 << 20)
         v, per_job = cpu_baseline_sample(*parts, nsample, cores)

@@ -4,20 +4,24 @@
 // Source/massFunctions.cpp:35-98, :678-790, :1050-1165.
 //
 // Pipeline (no float atomics, bitwise deterministic):
-//   1. bin_count   : per particle, the reference's FP32 home cell (bit-exact
-//                    key), the mesh bricks its stencil touches, and a count
-//                    per brick (integer atomics).  Also lost particles and
-//                    max |w|.
-//   2. scan        : exclusive scan of the brick counts.
-//   3. bin_scatter : per particle, one 16-byte payload per touched brick:
-//                    home cell relative to the brick, the exact fractional
-//                    offset in fixed point, the weight.
+//   1. bin_count   : each CTA takes a contiguous chunk of particles and
+//                    computes, per particle, the reference's FP32 home cell
+//                    (bit-exact key) and the mesh bricks its stencil
+//                    touches; a shared-memory histogram per CTA gives the
+//                    table count[brick][cta].  Also lost particles, max |w|.
+//   2. scan        : exclusive scan of the table in brick-major order, so
+//                    every (brick, cta) pair owns a contiguous payload range.
+//   3. bin_scatter : the same CTAs re-read their chunks and write one
+//                    16-byte payload per touched brick at their own cursors
+//                    (shared-memory atomics only): home cell relative to the
+//                    brick, exact fractional offset in fixed point, weight.
 //   4. deposit     : one CTA per brick accumulates its payloads into a
-//                    shared-memory tile of int64 fixed-point cell sums.
-//                    Integer sums do not depend on the order the payloads
-//                    arrived in, so the gather is deterministic; the tile is
-//                    then written once, coalesced, as FP32/FP64 (or uint32
-//                    counts for NGP).
+//                    shared-memory tile of 64-bit fixed-point cell sums kept
+//                    as two 32-bit words (32-bit shared atomics, the carry
+//                    detected from the returned old value).  Integer sums do
+//                    not depend on arrival order, so the result is
+//                    deterministic; the tile is written once, coalesced, as
+//                    FP32/FP64 (or uint32 counts for NGP).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -28,8 +32,9 @@
 namespace cam {
 namespace {
 
-constexpr int kBinThreads = 256;
-constexpr int kDepositThreads = 256;
+constexpr int kBinThreads = 1024;
+constexpr int kDepositThreads = 512;
+constexpr int kSmemBricks = 16384;  // per-CTA brick histogram in shared memory (64 KB)
 
 __device__ __forceinline__ int wrapi(int v, int n)
 {
@@ -66,29 +71,42 @@ __device__ __forceinline__ bool home_cell(const float p[3], const AssignGeom &g,
     if (!ok) return false;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        const float u = __fdiv_rn(__fsub_rn(q[a], g.mn[a]), g.d[a]);
-        int i = (int)floorf(u);
-        c[a] = i % g.n[a];  // fmod(float(i), float(N)) for 0 <= i < 2^24
+        // floor of the IEEE quotient fl(t / d).  The product with 1/d is
+        // within 2^-22 u of it; unless that product is this close to an
+        // integer both have the same floor, otherwise divide exactly.
+        const float t = __fsub_rn(q[a], g.mn[a]);
+        float u = __fmul_rn(t, g.inv_d[a]);
+        if (fabsf(u - rintf(u)) <= fmaxf(u, 1.0f) * 4.0e-7f) u = __fdiv_rn(t, g.d[a]);
+        const int i = (int)floorf(u);
+        // fmod(float(i), float(N)): i <= N whenever d = L/N; any i >= 0 otherwise
+        c[a] = i < g.n[a] ? i : (i == g.n[a] ? 0 : i % g.n[a]);
     }
     return true;
+}
+
+// cell / b for the brick extent b (exact for cell < 2^21, b <= 2^11).
+__device__ __forceinline__ int brick_of(int cell, int b, unsigned magic)
+{
+    return b == 1 ? cell : (int)__umulhi((unsigned)cell, magic);
 }
 
 // Exact offset t = (x - min)/d - 1/2 - c in cells, nearest periodic image,
 // in FP32 with error-free transformations: TwoSum for x - min and a fused
 // multiply-add for the subtraction of (c + 1/2) d (the product is exact
-// inside the FMA).  |error| ~ 2e-7 cells.
-__device__ __forceinline__ float exact_offset(float x, float mn, float d, int c, int n)
+// inside the FMA); the residual (|r| <= 1.5 d) is scaled by 1/d.
+// |error| <= ~2e-7 cells.
+__device__ __forceinline__ float exact_offset(float x, float mn, float d, float inv_d, int c, int n)
 {
     const float hi = __fsub_rn(x, mn);
     const float bb = __fsub_rn(hi, x);
     const float lo = __fadd_rn(__fsub_rn(x, __fsub_rn(hi, bb)), __fsub_rn(-mn, bb));
-    const float u = __fdiv_rn(hi, d);
+    const float u = hi * inv_d;
     float ci = (float)c + 0.5f;
     const float diff = u - ci;
     if (diff > 0.5f * (float)n) ci += (float)n;
     else if (diff < -0.5f * (float)n) ci -= (float)n;
     const float r = __fadd_rn(__fmaf_rn(-ci, d, hi), lo);
-    return __fdiv_rn(r, d);
+    return r * inv_d;
 }
 
 template <int SCHEME>
@@ -116,102 +134,111 @@ __device__ __forceinline__ int brick_linear(const AssignGeom &g, int b0, int b1,
     return (b0 * g.nb[1] + b1) * g.nb[2] + b2;
 }
 
-// Passes 1 and 3.  COUNT: count per brick, lost particles, max |w|.
-// SCATTER: write one payload per touched brick at cursor[brick]++.
-template <int SCHEME, bool SCATTER>
-__global__ void __launch_bounds__(kBinThreads)
-bin_kernel(const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z,
-           const float *__restrict__ w, int64_t np, AssignGeom g, uint32_t *__restrict__ counter,
-           uint4 *__restrict__ payload, unsigned long long *__restrict__ lost,
-           unsigned int *__restrict__ wmax_bits)
+// One particle of passes 1 and 3 (see bin_kernel).
+template <int SCHEME, bool SCATTER, bool SMEM>
+__device__ __forceinline__ void bin_one(float px, float py, float pz, float wt, bool weighted,
+                                        const AssignGeom &g, int G, int blk, uint32_t *hist,
+                                        uint32_t *__restrict__ table, uint4 *__restrict__ payload,
+                                        unsigned long long &my_lost, unsigned int &my_wmax)
 {
     using St = Stencil<SCHEME>;
-    const int lane = threadIdx.x & 31;
-    unsigned long long my_lost = 0;
-    unsigned int my_wmax = 0;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < np; base += stride) {
-        const int64_t p = base + threadIdx.x;
-        const bool inrange = p < np;
-        float pos[3] = {0.f, 0.f, 0.f};
-        float wt = 1.0f;
-        if (inrange) {
-            pos[0] = __ldcs(x + p);
-            pos[1] = __ldcs(y + p);
-            pos[2] = __ldcs(z + p);
-            if (w) wt = __ldcs(w + p);
-        }
-        int c[3] = {0, 0, 0};
-        const bool valid = inrange && home_cell<SCHEME>(pos, g, c);
-        if (!SCATTER) {
-            if (inrange && !valid) ++my_lost;
-            if (valid && w) my_wmax = max(my_wmax, __float_as_uint(fabsf(wt)));
-        }
-        // Bricks touched along each axis: 1 or 2.
-        int bl[3], nbx[3];
-        float t[3] = {0.f, 0.f, 0.f};
+    const float pos[3] = {px, py, pz};
+    int c[3] = {0, 0, 0};
+    if (!home_cell<SCHEME>(pos, g, c)) {
+        ++my_lost;
+        return;
+    }
+    if (!SCATTER && weighted) my_wmax = max(my_wmax, __float_as_uint(fabsf(wt)));
+    // Bricks touched along each axis: 1 or 2.
+    int bl[3], nbx[3];
+    float t[3] = {0.f, 0.f, 0.f};
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            const int lo = wrapi(c[a] + St::FIRST, g.n[a]);
-            const int hi = wrapi(c[a] + St::FIRST + St::W - 1, g.n[a]);
-            bl[a] = lo / g.b[a];
-            const int bh = hi / g.b[a];
-            nbx[a] = (bh == bl[a]) ? 1 : 2;
-            if (SCHEME != CAM_NGP && SCATTER && valid)
-                t[a] = exact_offset(pos[a], g.mn[a], g.d[a], c[a], g.n[a]);
-        }
-        // First target (lowest brick on every axis) with warp aggregation.
-        const int key0 = valid ? brick_linear(g, bl[0], bl[1], bl[2]) : -1;
-        const unsigned vmask = __ballot_sync(0xffffffffu, valid);
-        uint32_t slot0 = 0;
-        if (valid) {
-            const unsigned peers = __match_any_sync(vmask, key0);
-            const int leader = __ffs(peers) - 1;
-            const int rank = __popc(peers & ((1u << lane) - 1));
-            uint32_t base_slot = 0;
-            if (lane == leader) base_slot = atomicAdd(counter + key0, (uint32_t)__popc(peers));
-            base_slot = __shfl_sync(peers, base_slot, leader);
-            slot0 = base_slot + rank;
-        }
-        if (!valid) continue;
-        // Payloads / counts for every touched brick.
+    for (int a = 0; a < 3; ++a) {
+        const int lo = wrapi(c[a] + St::FIRST, g.n[a]);
+        const int hi = wrapi(c[a] + St::FIRST + St::W - 1, g.n[a]);
+        bl[a] = brick_of(lo, g.b[a], g.bmagic[a]);
+        nbx[a] = (brick_of(hi, g.b[a], g.bmagic[a]) == bl[a]) ? 1 : 2;
+        if (SCHEME != CAM_NGP && SCATTER) t[a] = exact_offset(pos[a], g.mn[a], g.d[a], g.inv_d[a], c[a], g.n[a]);
+    }
 #pragma unroll
-        for (int i0 = 0; i0 < 2; ++i0) {
-            if (i0 >= nbx[0]) break;
-            const int b0 = (bl[0] + i0) % g.nb[0];
+    for (int i0 = 0; i0 < 2; ++i0) {
+        if (i0 >= nbx[0]) break;
+        const int b0 = (bl[0] + i0 == g.nb[0]) ? 0 : bl[0] + i0;
 #pragma unroll
-            for (int i1 = 0; i1 < 2; ++i1) {
-                if (i1 >= nbx[1]) break;
-                const int b1 = (bl[1] + i1) % g.nb[1];
+        for (int i1 = 0; i1 < 2; ++i1) {
+            if (i1 >= nbx[1]) break;
+            const int b1 = (bl[1] + i1 == g.nb[1]) ? 0 : bl[1] + i1;
 #pragma unroll
-                for (int i2 = 0; i2 < 2; ++i2) {
-                    if (i2 >= nbx[2]) break;
-                    const int b2 = (bl[2] + i2) % g.nb[2];
-                    const bool first = (i0 | i1 | i2) == 0;
-                    const int key = brick_linear(g, b0, b1, b2);
-                    uint32_t slot;
-                    if (first) slot = slot0;
-                    else slot = atomicAdd(counter + key, 1u);
-                    if (SCATTER) {
-                        const int o[3] = {b0 * g.b[0], b1 * g.b[1], b2 * g.b[2]};
-                        uint32_t word[3];
+            for (int i2 = 0; i2 < 2; ++i2) {
+                if (i2 >= nbx[2]) break;
+                const int b2 = (bl[2] + i2 == g.nb[2]) ? 0 : bl[2] + i2;
+                const int key = brick_linear(g, b0, b1, b2);
+                const uint32_t slot = SMEM ? atomicAdd(hist + key, 1u)
+                                           : atomicAdd(table + (int64_t)key * G + blk, 1u);
+                if (SCATTER) {
+                    const int o[3] = {b0 * g.b[0], b1 * g.b[1], b2 * g.b[2]};
+                    uint32_t word[3];
 #pragma unroll
-                        for (int a = 0; a < 3; ++a) {
-                            // Home cell relative to the brick origin: the
-                            // periodic image in [-1, e], e = brick extent,
-                            // which holds whenever the stencil touches it.
-                            const int e = min(g.b[a], g.n[a] - o[a]);
-                            int cl = c[a] - o[a];
-                            if (cl < -1) cl += g.n[a];
-                            else if (cl > e) cl -= g.n[a];
-                            word[a] = pack_axis(cl, t[a]);
-                        }
-                        payload[slot] = make_uint4(word[0], word[1], word[2], __float_as_uint(wt));
+                    for (int a = 0; a < 3; ++a) {
+                        // Home cell relative to the brick origin: the periodic
+                        // image in [-1, e], e = brick extent, which holds
+                        // whenever the stencil touches the brick.
+                        const int e = min(g.b[a], g.n[a] - o[a]);
+                        int cl = c[a] - o[a];
+                        if (cl < -1) cl += g.n[a];
+                        else if (cl > e) cl -= g.n[a];
+                        word[a] = pack_axis(cl, t[a]);
                     }
+                    payload[slot] = make_uint4(word[0], word[1], word[2], __float_as_uint(wt));
                 }
             }
         }
     }
+}
+
+// Passes 1 and 3.  Block `blk` handles particles [blk * chunk, (blk+1) * chunk)
+// (chunk a multiple of 4).  COUNT: table[brick * G + blk] = number of
+// payloads for `brick`, plus lost particles and max |w|.  SCATTER: table
+// holds the exclusive scan; payloads are written at table[brick * G + blk]++.
+// SMEM: the per-CTA counters live in shared memory (nb <= kSmemBricks),
+// otherwise in the table itself.  VEC: 16-byte aligned arrays, four
+// particles per thread per iteration (float4 loads).
+template <int SCHEME, bool SCATTER, bool SMEM, bool VEC>
+__global__ void __launch_bounds__(kBinThreads)
+bin_kernel(const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z,
+           const float *__restrict__ w, int64_t np, int64_t chunk, AssignGeom g, int nb,
+           uint32_t *__restrict__ table, uint4 *__restrict__ payload, unsigned long long *__restrict__ lost,
+           unsigned int *__restrict__ wmax_bits)
+{
+    extern __shared__ uint32_t hist[];
+    const int G = gridDim.x, blk = blockIdx.x;
+    const int lane = threadIdx.x & 31;
+    if (SMEM) {
+        for (int i = threadIdx.x; i < nb; i += blockDim.x) hist[i] = SCATTER ? table[(int64_t)i * G + blk] : 0u;
+        __syncthreads();
+    }
+    unsigned long long my_lost = 0;
+    unsigned int my_wmax = 0;
+    const bool weighted = w != nullptr;
+    const int64_t p0 = (int64_t)blk * chunk, p1 = min(np, p0 + chunk);
+    int64_t ptail = p0;
+    if (VEC) {
+        const int64_t q1 = p0 + ((p1 - p0) & ~(int64_t)3);
+        for (int64_t p = p0 + 4 * (int64_t)threadIdx.x; p < q1; p += 4 * (int64_t)blockDim.x) {
+            const float4 X = __ldcs(reinterpret_cast<const float4 *>(x + p));
+            const float4 Y = __ldcs(reinterpret_cast<const float4 *>(y + p));
+            const float4 Z = __ldcs(reinterpret_cast<const float4 *>(z + p));
+            const float4 Wt = weighted ? __ldcs(reinterpret_cast<const float4 *>(w + p)) : make_float4(1.f, 1.f, 1.f, 1.f);
+            bin_one<SCHEME, SCATTER, SMEM>(X.x, Y.x, Z.x, Wt.x, weighted, g, G, blk, hist, table, payload, my_lost, my_wmax);
+            bin_one<SCHEME, SCATTER, SMEM>(X.y, Y.y, Z.y, Wt.y, weighted, g, G, blk, hist, table, payload, my_lost, my_wmax);
+            bin_one<SCHEME, SCATTER, SMEM>(X.z, Y.z, Z.z, Wt.z, weighted, g, G, blk, hist, table, payload, my_lost, my_wmax);
+            bin_one<SCHEME, SCATTER, SMEM>(X.w, Y.w, Z.w, Wt.w, weighted, g, G, blk, hist, table, payload, my_lost, my_wmax);
+        }
+        ptail = q1;
+    }
+    for (int64_t p = ptail + threadIdx.x; p < p1; p += blockDim.x)
+        bin_one<SCHEME, SCATTER, SMEM>(__ldcs(x + p), __ldcs(y + p), __ldcs(z + p), weighted ? __ldcs(w + p) : 1.0f,
+                                       weighted, g, G, blk, hist, table, payload, my_lost, my_wmax);
     if (!SCATTER) {
         // Warp reductions, one atomic per warp.
 #pragma unroll
@@ -223,64 +250,20 @@ bin_kernel(const float *__restrict__ x, const float *__restrict__ y, const float
             if (my_lost) atomicAdd(lost, my_lost);
             if (my_wmax) atomicMax(wmax_bits, my_wmax);
         }
+        if (SMEM) {
+            __syncthreads();
+            for (int i = threadIdx.x; i < nb; i += blockDim.x) table[(int64_t)i * G + blk] = hist[i];
+        }
     }
 }
 
-// Exclusive scan of the brick counts (single CTA, 1024 threads x 8 items per
-// round).  start[nb] = total.  cursor := start for the scatter pass.
-__global__ void __launch_bounds__(1024)
-scan_kernel(const uint32_t *__restrict__ count, uint32_t *__restrict__ start,
-            uint32_t *__restrict__ cursor, int nb)
+// start[b] = scanned table[b * G] (first CTA's cursor of brick b);
+// start[nb] = total payload count.
+__global__ void brick_starts_kernel(const uint32_t *__restrict__ table, int nb, int G,
+                                    const uint32_t *__restrict__ total, uint32_t *__restrict__ start)
 {
-    __shared__ uint32_t warp_sums[32];
-    __shared__ uint32_t carry_s;
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    if (tid == 0) carry_s = 0;
-    __syncthreads();
-    constexpr int ITEMS = 8;
-    for (int base = 0; base < nb; base += 1024 * ITEMS) {
-        uint32_t v[ITEMS];
-        uint32_t sum = 0;
-#pragma unroll
-        for (int i = 0; i < ITEMS; ++i) {
-            const int idx = base + tid * ITEMS + i;
-            v[i] = idx < nb ? count[idx] : 0u;
-            sum += v[i];
-        }
-        uint32_t incl = sum;
-#pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-            const uint32_t o = __shfl_up_sync(0xffffffffu, incl, off);
-            if (lane >= off) incl += o;
-        }
-        if (lane == 31) warp_sums[wid] = incl;
-        __syncthreads();
-        if (wid == 0) {
-            uint32_t ws = warp_sums[lane];
-            uint32_t wi = ws;
-#pragma unroll
-            for (int off = 1; off < 32; off <<= 1) {
-                const uint32_t o = __shfl_up_sync(0xffffffffu, wi, off);
-                if (lane >= off) wi += o;
-            }
-            warp_sums[lane] = wi - ws;  // exclusive
-        }
-        __syncthreads();
-        uint32_t run = carry_s + warp_sums[wid] + incl - sum;
-#pragma unroll
-        for (int i = 0; i < ITEMS; ++i) {
-            const int idx = base + tid * ITEMS + i;
-            if (idx < nb) {
-                start[idx] = run;
-                cursor[idx] = run;
-            }
-            run += v[i];
-        }
-        __syncthreads();
-        if (tid == 1023) carry_s = run;
-        __syncthreads();
-    }
-    if (tid == 0) start[nb] = carry_s;
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= nb; b += gridDim.x * blockDim.x)
+        start[b] = b < nb ? table[(int64_t)b * G] : *total;
 }
 
 template <typename OutT>
@@ -301,7 +284,24 @@ __device__ __forceinline__ uint32_t convert_out<uint32_t>(long long q, int s)
     return (uint32_t)(q >> s);
 }
 
-// Pass 4: one CTA per brick.
+// Adds round(v) (|v| < 2^32) to the 64-bit fixed-point cell (lo, hi) with
+// 32-bit shared atomics: the low word's old value tells whether the add
+// carried; a negative v adds its two's complement (high word all ones).
+__device__ __forceinline__ void add_fixed(uint32_t *lo, uint32_t *hi, float v)
+{
+    const bool neg = v < 0.0f;
+    const uint32_t m = __float2uint_rn(fabsf(v));
+    const uint32_t ql = neg ? 0u - m : m;
+    const uint32_t old = atomicAdd(lo, ql);
+    const uint32_t carry = (uint32_t)(old + ql) < old ? 1u : 0u;
+    const uint32_t hadd = (neg && m != 0u ? 0xffffffffu : 0u) + carry;
+    if (hadd) atomicAdd(hi, hadd);
+}
+
+// Pass 4: one CTA per brick.  Scale 2^s with max|w| * 2^s < 2^31, so every
+// contribution of a particle (stencil weight <= 1) fits in the low word and
+// the high word only takes carries (and the sign of rare negative weights).
+// Quantum = max|w| / 2^31 per contribution; a cell sum may use all 64 bits.
 template <int SCHEME, typename OutT>
 __global__ void __launch_bounds__(kDepositThreads)
 deposit_kernel(const uint4 *__restrict__ payload, const uint32_t *__restrict__ start,
@@ -309,7 +309,7 @@ deposit_kernel(const uint4 *__restrict__ payload, const uint32_t *__restrict__ s
                OutT *__restrict__ mesh, double *__restrict__ brick_sum)
 {
     using St = Stencil<SCHEME>;
-    extern __shared__ long long tile[];
+    extern __shared__ uint32_t tile32[];
     __shared__ long long red[kDepositThreads / 32];
     const int B = blockIdx.x;
     const int B2 = B % g.nb[2];
@@ -319,26 +319,38 @@ deposit_kernel(const uint4 *__restrict__ payload, const uint32_t *__restrict__ s
     const int e[3] = {min(g.b[0], g.n[0] - o[0]), min(g.b[1], g.n[1] - o[1]),
                       min(g.b[2], g.n[2] - o[2])};
     const int ncell = e[0] * e[1] * e[2];
-    for (int i = threadIdx.x; i < ncell; i += blockDim.x) tile[i] = 0;
+    uint32_t *lo = tile32;
+    uint32_t *hi = tile32 + g.b[0] * g.b[1] * g.b[2];
+    for (int i = threadIdx.x; i < ncell; i += blockDim.x) {
+        lo[i] = 0u;
+        hi[i] = 0u;
+    }
     __syncthreads();
 
     const uint32_t beg = start[B], end = start[B + 1];
-    const uint32_t P = end - beg;
-    // Fixed-point scale 2^s with P * max|w| * 2^s < 2^61: no cell sum can
-    // overflow int64, whatever the order of accumulation.
     const float wmax = weighted ? __uint_as_float(*wmax_bits) : 1.0f;
     int ex = 0;
-    frexp((double)max(P, 1u) * (double)(wmax > 0.f ? wmax : 1.0f), &ex);
-    const int s = 61 - ex;
+    frexpf(wmax > 0.f ? wmax : 1.0f, &ex);
+    const int s = 31 - ex;
+    // 2^s as two exact factors (s may exceed the float exponent range)
+    const float f1 = scalbnf(1.0f, s / 2), f2 = scalbnf(1.0f, s - s / 2);
 
-    for (uint32_t p = beg + threadIdx.x; p < end; p += blockDim.x) {
-        const uint4 v = payload[p];
+    // Two payloads per thread per iteration: both loads are in flight
+    // before the shared-memory atomics of the first one.
+    for (uint32_t p = beg + threadIdx.x; p < end; p += 2 * blockDim.x) {
+        const uint4 va = payload[p];
+        const bool has_b = p + blockDim.x < end;
+        const uint4 vb = has_b ? payload[p + blockDim.x] : make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+        if (u == 1 && !has_b) break;
+        const uint4 v = u == 0 ? va : vb;
         int cl[3];
         float t[3];
         unpack_axis(v.x, cl[0], t[0]);
         unpack_axis(v.y, cl[1], t[1]);
         unpack_axis(v.z, cl[2], t[2]);
-        const float ws = scalbnf(__uint_as_float(v.w), s);
+        const float ws = (__uint_as_float(v.w) * f1) * f2;
         float wa[3][St::W];
         int li[3][St::W];
 #pragma unroll
@@ -374,11 +386,11 @@ deposit_kernel(const uint4 *__restrict__ payload, const uint32_t *__restrict__ s
 #pragma unroll
                 for (int ka = 0; ka < St::W; ++ka) {
                     if (li[2][ka] < 0) continue;
-                    const long long q = __float2ll_rn(wij * wa[2][ka]);
-                    atomicAdd(reinterpret_cast<unsigned long long *>(tile + row + li[2][ka]),
-                              (unsigned long long)q);
+                    const int c = row + li[2][ka];
+                    add_fixed(lo + c, hi + c, wij * wa[2][ka]);
                 }
             }
+        }
         }
     }
     __syncthreads();
@@ -388,7 +400,7 @@ deposit_kernel(const uint4 *__restrict__ payload, const uint32_t *__restrict__ s
         const int lk = i % e[2];
         const int lj = (i / e[2]) % e[1];
         const int lii = i / (e[2] * e[1]);
-        const long long q = tile[i];
+        const long long q = (long long)(((unsigned long long)hi[i] << 32) | lo[i]);
         acc += q;
         const int64_t gidx = ((int64_t)(o[0] + lii) * g.n[1] + (o[1] + lj)) * g.n[2] + (o[2] + lk);
         mesh[gidx] = convert_out<OutT>(q, s);
@@ -465,6 +477,8 @@ AssignGeom make_geom(const cam_grid &gr, int scheme, int64_t np)
     for (int a = 0; a < 3; ++a) {
         while (g.b[a] < g.n[a] && g.n[a] % g.b[a] != 0 && g.n[a] % g.b[a] < 2 && g.b[a] > 3) --g.b[a];
         g.nb[a] = (g.n[a] + g.b[a] - 1) / g.b[a];
+        g.bmagic[a] = (unsigned)(((1ull << 32) + (uint64_t)g.b[a] - 1) / (uint64_t)g.b[a]);
+        g.inv_d[a] = 1.0f / g.d[a];
     }
     (void)scheme;
     return g;
@@ -476,44 +490,62 @@ static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const floa
 {
     const int64_t nb = (int64_t)g.nb[0] * g.nb[1] * g.nb[2];
     CAM_REQUIRE(nb < (1ll << 31), CAM_E_UNSUPPORTED, "too many mesh bricks");
-    auto *counter = static_cast<uint32_t *>(scratch(ctx, "asg.count", nb * sizeof(uint32_t)));
+    // CTAs of the binning passes: one per SM (contiguous chunks of >= 4096
+    // particles).  Few CTAs keep the set of partly written payload sectors
+    // (CTAs x bricks x 128 B) inside L2, so sectors are complete before they
+    // are written back.
+    const int G = (int)std::max<int64_t>(1, std::min<int64_t>(kNumSMs, (np + 4095) / 4096));
+    const int64_t chunk = std::max<int64_t>(4, ((np + G - 1) / G + 3) & ~(int64_t)3);
+    auto aligned = [](const void *p) { return p == nullptr || ((uintptr_t)p & 15u) == 0; };
+    const bool vec = aligned(x) && aligned(y) && aligned(z) && aligned(w);
+    const bool smem_hist = nb <= kSmemBricks;
+    const int64_t tn = nb * G;
+    auto *table = static_cast<uint32_t *>(scratch(ctx, "asg.table", (size_t)tn * sizeof(uint32_t)));
     auto *start = static_cast<uint32_t *>(scratch(ctx, "asg.start", (nb + 1) * sizeof(uint32_t)));
     auto *stats = static_cast<unsigned long long *>(scratch(ctx, "asg.stats", 64));
     auto *bsum = static_cast<double *>(scratch(ctx, "asg.bsum", nb * sizeof(double)));
     unsigned long long *d_lost = stats;
     unsigned int *d_wmax = reinterpret_cast<unsigned int *>(stats + 1);
-    CAM_CUDA_TRY(cudaMemsetAsync(counter, 0, nb * sizeof(uint32_t), ctx->stream));
+    uint32_t *d_total = reinterpret_cast<uint32_t *>(stats + 2);
+    if (!smem_hist) CAM_CUDA_TRY(cudaMemsetAsync(table, 0, (size_t)tn * sizeof(uint32_t), ctx->stream));
     CAM_CUDA_TRY(cudaMemsetAsync(stats, 0, 64, ctx->stream));
 
-    const int gb = grid_for(np, kBinThreads);
-    if (np > 0)
-        CAM_LAUNCH_NAMED(ctx, "assign_bin_count", (bin_kernel<SCHEME, false>), gb, kBinThreads, 0, x, y, z, w, np, g,
-                   counter, (uint4 *)nullptr, d_lost, d_wmax);
-    CAM_LAUNCH_NAMED(ctx, "assign_scan", scan_kernel, 1, 1024, 0, counter, start, counter, (int)nb);
+    const size_t hsmem = smem_hist ? (size_t)nb * sizeof(uint32_t) : 0;
+    auto count_k = smem_hist ? (vec ? bin_kernel<SCHEME, false, true, true> : bin_kernel<SCHEME, false, true, false>)
+                             : (vec ? bin_kernel<SCHEME, false, false, true> : bin_kernel<SCHEME, false, false, false>);
+    auto scatter_k = smem_hist ? (vec ? bin_kernel<SCHEME, true, true, true> : bin_kernel<SCHEME, true, true, false>)
+                               : (vec ? bin_kernel<SCHEME, true, false, true> : bin_kernel<SCHEME, true, false, false>);
+    if (hsmem > 48 * 1024) {
+        CAM_CUDA_TRY(cudaFuncSetAttribute(count_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem));
+        CAM_CUDA_TRY(cudaFuncSetAttribute(scatter_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem));
+    }
+    CAM_LAUNCH_NAMED(ctx, "assign_bin_count", count_k, G, kBinThreads, hsmem, x, y, z, w, np, chunk, g, (int)nb,
+                     table, (uint4 *)nullptr, d_lost, d_wmax);
+    exclusive_scan_u32(ctx, table, tn, d_total);
+    CAM_LAUNCH_NAMED(ctx, "assign_starts", brick_starts_kernel, (unsigned)std::min<int64_t>((nb + 256) / 256, 1024),
+                     256, 0, table, (int)nb, G, d_total, start);
 
     // Payload size and diagnostics back to the host (one synchronisation).
-    uint32_t total = 0;
-    unsigned long long hstats[2] = {0, 0};
-    CAM_CUDA_TRY(cudaMemcpyAsync(&total, start + nb, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
-    CAM_CUDA_TRY(cudaMemcpyAsync(hstats, stats, 16, cudaMemcpyDeviceToHost, ctx->stream));
+    unsigned long long hstats[3] = {0, 0, 0};
+    CAM_CUDA_TRY(cudaMemcpyAsync(hstats, stats, sizeof(hstats), cudaMemcpyDeviceToHost, ctx->stream));
     CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    const uint32_t total = (uint32_t)(hstats[2] & 0xffffffffu);
     const unsigned int wmax_bits = (unsigned int)(hstats[1] & 0xffffffffu);
     CAM_REQUIRE(!w || wmax_bits < 0x7f800000u, CAM_E_NONFINITE, "a particle weight is NaN or infinite");
     out.n_lost = (int64_t)hstats[0];
     out.n_in = np - out.n_lost;
 
     uint4 *payload = static_cast<uint4 *>(scratch(ctx, "asg.payload", std::max<size_t>(total, 1) * sizeof(uint4)));
-    if (np > 0)
-        CAM_LAUNCH_NAMED(ctx, "assign_bin_scatter", (bin_kernel<SCHEME, true>), gb, kBinThreads, 0, x, y, z, w, np, g,
-                   counter, payload, d_lost, d_wmax);
+    CAM_LAUNCH_NAMED(ctx, "assign_bin_scatter", scatter_k, G, kBinThreads, hsmem, x, y, z, w, np, chunk, g,
+                     (int)nb, table, payload, d_lost, d_wmax);
 
-    const size_t smem = (size_t)g.b[0] * g.b[1] * g.b[2] * sizeof(long long);
+    const size_t smem = (size_t)g.b[0] * g.b[1] * g.b[2] * 2 * sizeof(uint32_t);
     CAM_REQUIRE(smem <= 200 * 1024, CAM_E_UNSUPPORTED, "brick tile too large");
     const int weighted = w != nullptr;
     auto launch_dep = [&](auto kern, auto *mesh) {
         CAM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         CAM_LAUNCH_NAMED(ctx, "assign_deposit", kern, (unsigned)nb, kDepositThreads, smem, payload, start, g, d_wmax,
-                   weighted, mesh, bsum);
+                         weighted, mesh, bsum);
     };
     if (out.precision == CAM_F32)
         launch_dep(deposit_kernel<SCHEME, float>, static_cast<float *>(out.mesh));

@@ -105,8 +105,10 @@ inline T *stage_in(cam_ctx *ctx, const char *name, const T *p, size_t count, int
 struct AssignGeom {
     int n[3];
     float L[3], d[3], mn[3];
-    int b[3];   // brick extent (cells)
-    int nb[3];  // bricks per axis
+    float inv_d[3];      // 1/d rounded (offsets only; keys divide exactly)
+    int b[3];            // brick extent (cells)
+    int nb[3];           // bricks per axis
+    unsigned bmagic[3];  // ceil(2^32 / b): cell / b = umulhi(cell, bmagic)
 };
 
 struct AssignOut {
@@ -166,6 +168,9 @@ void tweb_device(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const
                  int input_type, const cam_tweb_opts &o, uint8_t *d_labels, float *d_lambdas,
                  cam_tweb_stats *stats);
 
+// In-place exclusive prefix sum of uint32 values; *total (device, may be
+// null) receives the sum of all inputs.
+void exclusive_scan_u32(cam_ctx *ctx, uint32_t *data, int64_t n, uint32_t *total);
 // Deterministic FP64 sum of a device array: out[0] = sum, out[1] = sum / divisor.
 void reduce_sum_f64(cam_ctx *ctx, const double *in, int64_t n, double *out, double divisor);
 // Mean of a device mesh of precision `prec` into a device scalar (FP64).

@@ -144,22 +144,39 @@ pk_bin_kernel(const C *__restrict__ main, const C *__restrict__ nyq, int n,
     }
 }
 
-__global__ void pk_final_kernel(const double *__restrict__ part, const unsigned long long *__restrict__ pm,
-                                int nparts, int nbins, double *__restrict__ out /* [nbins][2] */,
-                                unsigned long long *__restrict__ modes)
+// One CTA per bin: strided partial sums per thread, then a fixed-shape tree
+// (deterministic for a given grid size).
+__global__ void __launch_bounds__(256)
+pk_final_kernel(const double *__restrict__ part, const unsigned long long *__restrict__ pm, int nparts,
+                int nbins, double *__restrict__ out /* [nbins][2] */, unsigned long long *__restrict__ modes)
 {
-    const int bn = blockIdx.x * blockDim.x + threadIdx.x;
-    if (bn >= nbins) return;
+    __shared__ double r0[256], r1[256];
+    __shared__ unsigned long long rc[256];
+    const int bn = blockIdx.x;
     double s0 = 0.0, s1 = 0.0;
     unsigned long long cn = 0;
-    for (int p = 0; p < nparts; ++p) {
+    for (int p = threadIdx.x; p < nparts; p += blockDim.x) {
         s0 += part[((size_t)p * nbins + bn) * 2];
         s1 += part[((size_t)p * nbins + bn) * 2 + 1];
         cn += pm[(size_t)p * nbins + bn];
     }
-    out[2 * bn] = s0;
-    out[2 * bn + 1] = s1;
-    modes[bn] = cn;
+    r0[threadIdx.x] = s0;
+    r1[threadIdx.x] = s1;
+    rc[threadIdx.x] = cn;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) {
+            r0[threadIdx.x] += r0[threadIdx.x + h];
+            r1[threadIdx.x] += r1[threadIdx.x + h];
+            rc[threadIdx.x] += rc[threadIdx.x + h];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[2 * bn] = r0[0];
+        out[2 * bn + 1] = r1[0];
+        modes[bn] = rc[0];
+    }
 }
 
 double sq_factor(int p, double s)
@@ -225,7 +242,7 @@ void power_bin(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins,
         CAM_LAUNCH_NAMED(ctx, "pk_bin", kern, grid, kPkThreads, smem, (const double2 *)s.main, (const double2 *)s.nyq, n,
                    d_tab, nbins, m_u, inv_s, rpc, part, pm);
     }
-    CAM_LAUNCH(ctx, pk_final_kernel, (nbins + 127) / 128, 128, 0, part, pm, grid, nbins, res, resm);
+    CAM_LAUNCH(ctx, pk_final_kernel, nbins, 256, 0, part, pm, grid, nbins, res, resm);
     std::vector<double> hres(2 * nbins);
     std::vector<unsigned long long> hm(nbins);
     CAM_CUDA_TRY(cudaMemcpyAsync(hres.data(), res, 2 * nbins * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
