@@ -201,6 +201,26 @@ typedef struct {
 
 int cam_job_run(cam_ctx *ctx, const cam_job_desc *job, cam_job_result *res);
 
+/* ---- power spectrum without device allocation --------------------------
+ * No counterpart in the reference.  For callers that may not allocate
+ * device memory -- code running inside a memory pool or arena it does not
+ * own, or a latency-critical loop that must never reach cudaMalloc -- this
+ * bins a spectrum the caller already holds on the current device, using
+ * only a fixed scratch array (about 1.9 MB) built into the library.
+ *   spec    device pointer, FFTW r2c layout [i][j][k <= N/2] of an N^3
+ *           mesh, complex float (CAM_F32) or complex double (CAM_F64)
+ *   n_obj   sum of the density mesh (CAM_INPUT_DENSITY); ignored for delta
+ *   pk, modes  host arrays of nbins (modes may be NULL)
+ *   stream  cudaStream_t to run on (NULL = the legacy default stream);
+ *           the call returns after that stream has finished its work.
+ * Results equal cam_power's binning of the same spectrum.  Limits: N <= 2048
+ * and nbins <= 512; larger inputs return CAM_E_UNSUPPORTED.  The first call
+ * on a device looks up the scratch array's device address.  All calls share
+ * that array and each call overwrites what it uses; calls that overlap on
+ * the GPU (other streams, other host threads) race on it, so serialise them. */
+int cam_power_noalloc(const void *spec, int64_t n, int precision, float box, double n_obj,
+                      const cam_pk_opts *opts, double *pk, int64_t *modes, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
