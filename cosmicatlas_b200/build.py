@@ -75,5 +75,25 @@ def build(verbose: bool = False) -> str:
     return LIB
 
 
+SHIM_SRC = os.path.join(HERE, "shim", "cam_reference_api.cpp")
+SHIM_LIB = os.path.join(HERE, "libcam_refapi.so")
+
+
+def build_shim() -> str:
+    """libcam_refapi.so: the reference's C++ signatures over libcam.so."""
+    lib = build()
+    deps = [SHIM_SRC, lib, os.path.join(HERE, "..", "include", "cam_reference_api.h")]
+    if os.path.exists(SHIM_LIB) and os.path.getmtime(SHIM_LIB) >= max(os.path.getmtime(d) for d in deps):
+        return SHIM_LIB
+    gxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+    cmd = [gxx, "-O2", "-std=c++17", "-fPIC", "-shared", "-o", SHIM_LIB, SHIM_SRC, "-L" + HERE, "-lcam",
+           "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"shim build failed:\n{r.stdout}\n{r.stderr}")
+    return SHIM_LIB
+
+
 if __name__ == "__main__":
     print(build(verbose="--verbose" in sys.argv))
+    print(build_shim())

@@ -8,15 +8,10 @@ from cosmicatlas_b200 import _lib as L
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def declared_functions():
-    names = set()
-    for h in os.listdir(os.path.join(ROOT, "include")):
-        if not h.endswith(".h"):
-            continue
-        src = open(os.path.join(ROOT, "include", h)).read()
-        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-        names |= set(re.findall(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b(cam_\w+)\s*\(", src, flags=re.M))
-    return names
+def declared_functions(header="cam.h", prefix="cam_"):
+    src = open(os.path.join(ROOT, "include", header)).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return set(re.findall(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*:<>]*?\b(" + prefix + r"\w*)\s*\(", src, flags=re.M))
 
 
 def test_library_exports_every_declared_symbol():
@@ -29,6 +24,21 @@ def test_library_exports_every_declared_symbol():
 
 def test_binding_covers_header():
     assert declared_functions() <= set(L.SIGNATURES)
+
+
+def test_reference_shim_exports_reference_signatures():
+    import subprocess
+    from cosmicatlas_b200 import build as B
+    so = B.SHIM_LIB
+    if not os.path.exists(so):
+        B.build_shim()
+    out = subprocess.run(["nm", "-DC", so], capture_output=True, text=True, check=True).stdout
+    names = declared_functions("cam_reference_api.h", "")
+    names = {n for n in names if n in ("getDensity_NGP", "getDensity_CIC", "getDensity_TSC", "do_fftw_r2c",
+                                       "do_fftw_c2r", "EigenValuesTweb", "cam_refapi_last_status")}
+    assert len(names) == 7
+    for n in names:
+        assert any((" T " + n + "(") in line for line in out.splitlines()), n
 
 
 def test_version_string():
