@@ -8,9 +8,10 @@ log10 M ~ N(12.5, 0.5) truncated to [11, 15].  One step = three mesh jobs
 128 bins with window deconvolution and shot-noise subtraction.
 
 value : jobs/s with the particles resident in HBM (device pointers).
-e2e   : jobs/s through cam_job_run with pinned host particle buffers: the
-        host->device copy of the particles and the device->host copy of
-        the P(k) results are inside the timed region.
+e2e   : jobs/s through the C ABI with pinned host particle buffers: every
+        step uploads the step's particles once (cam_particles_stage) and runs
+        the three jobs on them; the host->device copy and the device->host
+        copies of the P(k) results are inside the timed region.
 Multi-GPU: one process per GPU, each runs its own jobs (independent meshes,
 "weak" scaling, no collective in the data path); time is the max over ranks.
 
@@ -48,6 +49,9 @@ def parse():
     ap.add_argument("--particles", type=int, default=N_PARTICLES)
     ap.add_argument("--kernels-only", action="store_true",
                     help="profiler runs: the device-resident pass only (no e2e pass, no CPU baseline)")
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "single512", "large768"],
+                    help="sweep: the benchmark line (default); single512 / large768: one-job latency lines")
+    ap.add_argument("--mesh", type=int, default=0, help="single512 only: override N (profiler runs)")
     return ap.parse_args()
 
 
@@ -159,12 +163,17 @@ def run_ours(args):
     opts = {s: Context.pk_opts(s, nbins=NBINS) for s in SCHEMES}
 
     def step(arrs, lat=None):
+        # host arrays: one upload per step serves the three schemes
+        src = arrs if arrs[0].is_cuda else [ctx.stage(*arrs)]
         for s in SCHEMES:
             if lat is not None:
                 e0 = torch.cuda.Event(enable_timing=True)
                 e1 = torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
-            r = ctx.job(arrs[0], arrs[1], arrs[2], arrs[3], grid, s, 0, pk=opts[s])
+            if len(src) == 1:
+                r = ctx.job(src[0], grid=grid, scheme=s, precision=0, pk=opts[s])
+            else:
+                r = ctx.job(src[0], src[1], src[2], src[3], grid, s, 0, pk=opts[s])
             if lat is not None:
                 e1.record(stream)
                 lat.append((e0, e1))
@@ -213,7 +222,7 @@ def run_ours(args):
     jobs = len(SCHEMES) * args.steps * world
     value = jobs / (ms / 1e3)
     e2e = jobs / (ms_e2e / 1e3)
-    h2d = len(SCHEMES) * npart * 16
+    h2d = npart * 16
     d2h = len(SCHEMES) * NBINS * 24
 
     out = None
@@ -327,8 +336,83 @@ def run_reference(args):
     }
 
 
+def run_single(args):
+    """One-job latency lines (not the benchmark line): single512 = 512^3 CIC,
+    134,217,728 clumped unit-mass particles, L = 1000, P(k) 256 bins, T-web
+    R = 2 cells, lambda_th = 0; large768 = 768^3 TSC of a Zel'dovich-displaced
+    lattice (452,984,832 particles, L = 1500), P(k) 256 bins of 1.5 k_f,
+    T-web R = 3, lambda_th = 0.1."""
+    import torch
+
+    from cosmicatlas_b200 import synth
+    from cosmicatlas_b200.api import CIC, TSC, Context, make_grid
+
+    torch.cuda.set_device(0)
+    if args.workload == "single512":
+        n = args.mesh or 512
+        box, scheme, nb, ndel, R, lth = 1000.0, CIC, n // 2, 1.0, 2.0 * 1000.0 / n, 0.0
+        x, y, z = synth.clumped(n ** 3, box, max(1, 2_000_000 * n ** 3 // 512 ** 3), 1.5, 0.8, seed=7)
+        arrs = [torch.from_numpy(v).cuda() for v in (x, y, z)]
+        del x, y, z
+    else:
+        n, box, scheme, nb, ndel, R, lth = 768, 1500.0, TSC, 256, 1.5, 3.0, 0.1
+        gx, gy, gz, _ = synth.zeldovich_lattice(n, box, device="cuda")
+        arrs = [gx, gy, gz]
+    npart = int(arrs[0].numel())
+    grid = make_grid(n, box)
+    ctx = Context(0)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    pko = Context.pk_opts(scheme, nbins=nb, ndel=ndel)
+    two = Context.tweb_opts(R, lth, 1e-5)
+    for _ in range(args.warmup):
+        ctx.job(arrs[0], arrs[1], arrs[2], None, grid, scheme, 0, pk=pko, tweb=two)
+    ctx.profile(True)
+    ctx.profile_read(reset=True)
+    times = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = ctx.job(arrs[0], arrs[1], arrs[2], None, grid, scheme, 0, pk=pko, tweb=two)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    prof = ctx.profile_read(reset=True)
+    hbm, kind = peaks()
+    nh = n * n * (n // 2 + 1)
+    stage_bytes = {"assign": npart * 12 + 4 * n ** 3, "fft_r2c": 4 * n ** 3 + 8 * nh, "power": 8 * nh,
+                   "tweb": 8 * nh + n ** 3}
+    stage_kernels = {
+        "assign": ["assign_bin_count", "assign_scan", "assign_bin_scatter", "assign_deposit",
+                   "partial_sum_kernel<double>", "final_sum_kernel", "assign_starts", "tile_sum_kernel",
+                   "tile_offsets_kernel", "tile_scan_kernel"],
+        "fft_r2c": ["fft_rows_r2c", "fft_cols", "fft_rows_c2c"],
+        "power": ["pk_bin", "pk_final_kernel"],
+        "tweb": ["tweb_tidal_x", "tweb_tidal_x_nyq", "tweb_tidal_z_eigen"],
+    }
+    k = args.steps
+    stages = {}
+    for st, names in stage_kernels.items():
+        t = sum(prof.get(nm, (0, 0.0))[1] for nm in names) / k
+        stages[st] = {"ms": round(t, 3), "algorithmic_bytes": stage_bytes[st],
+                      "achieved_gbs": round(stage_bytes[st] / (t / 1e3) / 1e9, 1) if t > 0 else None}
+    # the T-web's y-pass runs through fft_cols too: attribute by launch counts is not possible
+    # from totals, so report the raw kernel table alongside
+    out = {"workload": args.workload, "mesh": n, "particles": npart, "ms_per_job": round(float(np.median(times)), 3),
+           "ms_min": round(min(times), 3), "steps": k, "warmup": args.warmup, "peak_gbs": hbm, "peak_kind": kind,
+           "stages": stages, "kernels": {a: {"launches": b[0], "ms_total": round(b[1], 3)} for a, b in sorted(prof.items())},
+           "tweb_counts": [int(v) for v in r["tweb"].counts], "n_lost": r["assign"].n_lost}
+    ctx.close()
+    return out
+
+
 def main():
     args = parse()
+    if args.workload != "sweep":
+        print(json.dumps(run_single(args)), flush=True)
+        return
     if args.impl == "reference":
         out = run_reference(args)
         if out is not None:

@@ -103,6 +103,7 @@ SIGNATURES = {
     "cam_tweb": ([_P, ctypes.POINTER(Grid), _P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(TwebOpts), _P, _P,
                   ctypes.c_int, ctypes.POINTER(TwebStats)], ctypes.c_int),
     "cam_job_run": ([_P, ctypes.POINTER(JobDesc), ctypes.POINTER(JobResult)], ctypes.c_int),
+    "cam_particles_stage": ([_P, ctypes.POINTER(Particles), ctypes.POINTER(Particles)], ctypes.c_int),
     "cam_power_noalloc": ([_P, ctypes.c_int64, ctypes.c_int, ctypes.c_float, ctypes.c_double,
                            ctypes.POINTER(PkOpts), _P, _P, _P], ctypes.c_int),
 }

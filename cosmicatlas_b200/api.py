@@ -247,9 +247,21 @@ class Context:
         return TwebResult(labels, lam, np.array(st.counts[:], np.int64), int(st.ties), st.mean)
 
     # ---------------------------------------------------------------- job
-    def job(self, x, y, z, w, grid: L.Grid, scheme: int, precision=F32, pk: L.PkOpts | None = None,
-            tweb: L.TwebOpts | None = None, want_labels=False):
+    def stage(self, x, y, z, w=None) -> "StagedParticles":
+        """One host->device upload of a particle set, reusable by several jobs
+        (cam_particles_stage); valid until the next stage() on this context."""
         p, keep, dev = self._particles(x, y, z, w)
+        d = L.Particles()
+        self._check(self._lib.cam_particles_stage(self.h, ctypes.byref(p), ctypes.byref(d)))
+        return StagedParticles(d, keep)
+
+    def job(self, x, y=None, z=None, w=None, grid: L.Grid = None, scheme: int = CIC, precision=F32,
+            pk: L.PkOpts | None = None, tweb: L.TwebOpts | None = None, want_labels=False):
+        """One mesh job.  `x` may be a StagedParticles (then y, z, w are unused)."""
+        if isinstance(x, StagedParticles):
+            p = x.parts
+        else:
+            p, keep, dev = self._particles(x, y, z, w)
         d = L.JobDesc()
         d.parts, d.grid, d.scheme, d.precision = p, grid, scheme, precision
         if pk is not None:
@@ -272,6 +284,12 @@ class Context:
             "tweb": TwebResult(labels, None, np.array(r.tweb.counts[:], np.int64), int(r.tweb.ties), r.tweb.mean)
             if tweb is not None else None,
         }
+
+
+@dataclass
+class StagedParticles:
+    parts: L.Particles
+    keep: tuple
 
 
 _default: dict[int, Context] = {}

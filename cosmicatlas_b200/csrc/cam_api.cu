@@ -550,6 +550,36 @@ int cam_tweb(cam_ctx *ctx, const cam_grid *grid, const void *mesh, int precision
     });
 }
 
+int cam_particles_stage(cam_ctx *ctx, const cam_particles *host, cam_particles *device_out)
+{
+    return guarded(ctx, [&] {
+        CAM_REQUIRE(host && device_out, CAM_E_INVAL, "null particles");
+        CAM_REQUIRE(host->n >= 0, CAM_E_INVAL, "negative particle count");
+        CAM_REQUIRE(host->n == 0 || (host->x && host->y && host->z), CAM_E_INVAL, "null particle coordinates");
+        check_mem(host->mem);
+        cam_particles d = *host;
+        if (host->mem == CAM_MEM_HOST) {
+            const size_t bytes = std::max<size_t>((size_t)host->n, 1) * sizeof(float);
+            const float *src[4] = {host->x, host->y, host->z, host->w};
+            const char *names[4] = {"stage.x", "stage.y", "stage.z", "stage.w"};
+            float *dst[4] = {nullptr, nullptr, nullptr, nullptr};
+            for (int a = 0; a < 4; ++a) {
+                if (!src[a]) continue;
+                dst[a] = static_cast<float *>(scratch(ctx, names[a], bytes));
+                if (host->n > 0)
+                    CAM_CUDA_TRY(cudaMemcpyAsync(dst[a], src[a], (size_t)host->n * sizeof(float),
+                                                 cudaMemcpyHostToDevice, ctx->stream));
+            }
+            d.x = dst[0];
+            d.y = dst[1];
+            d.z = dst[2];
+            d.w = dst[3];
+            d.mem = CAM_MEM_DEVICE;
+        }
+        *device_out = d;
+    });
+}
+
 int cam_job_run(cam_ctx *ctx, const cam_job_desc *job, cam_job_result *res)
 {
     return guarded(ctx, [&] {

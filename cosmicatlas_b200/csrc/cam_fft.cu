@@ -37,9 +37,16 @@ struct FftPlan {
 
 namespace {
 
+// Rows per CTA of the row kernels: about 4096 (float) / 2048 (double) points.
+template <typename T>
+constexpr int rows_rpc(int len)
+{
+    return (sizeof(T) == 4 ? 4096 : 2048) / len > 1 ? (sizeof(T) == 4 ? 4096 : 2048) / len : 1;
+}
+
 // Column transforms: element (comp, plane, j, col) at
 // base + comp*ccomp + plane*pstride + j*jstride + col, col < ncols.
-template <typename T, bool INV>
+template <typename T, bool INV, int LEN>
 __global__ void __launch_bounds__(1024, 1)
 fft_cols_kernel(typename fftdev::CT<T>::t *base, int len, int ncols, int64_t jstride, int64_t pstride,
                 int64_t ccomp, Radices rd, const typename fftdev::CT<T>::t *__restrict__ tw, int twmul)
@@ -57,7 +64,11 @@ fft_cols_kernel(typename fftdev::CT<T>::t *base, int len, int ncols, int64_t jst
         if (c < nc) tile[e] = g[(int64_t)j * jstride + c];
     }
     __syncthreads();
-    fftdev::block_fft<C, fftdev::CT<T>::kPPT, INV, false, W>(tile, len, W, W, 1, rd, tw, twmul);
+    if constexpr (LEN > 0)
+        fftdev::block_fft_fixed<C, INV, false, W, LEN, fftdev::ct_threads(LEN, W, fftdev::CT<T>::kPPT), W, 1, 1>(
+            tile, tw);
+    else
+        fftdev::block_fft<C, fftdev::CT<T>::kPPT, INV, false, W>(tile, len, W, W, 1, rd, tw, twmul);
     for (int e = threadIdx.x; e < tot; e += blockDim.x) {
         const int j = e / W, c = e % W;
         if (c < nc) g[(int64_t)j * jstride + c] = tile[e];
@@ -68,7 +79,7 @@ fft_cols_kernel(typename fftdev::CT<T>::t *base, int len, int ncols, int64_t jst
 //   MODE 0 (r2c): real rows of n -> main rows of n/2 + nyq element
 //   MODE 1 (c2r): main rows + nyq -> real rows of n (times `scale`)
 //   MODE 2/3    : complex rows of n, forward / inverse, in place
-template <typename T, int MODE>
+template <typename T, int MODE, int LEN>
 __global__ void __launch_bounds__(1024, 1)
 fft_rows_kernel(const void *in, void *out_main, typename fftdev::CT<T>::t *nyq, int n, int64_t nrows,
                 int rpc, int64_t ccomp_in, int64_t ccomp_out, Radices rd,
@@ -119,7 +130,14 @@ fft_rows_kernel(const void *in, void *out_main, typename fftdev::CT<T>::t *nyq, 
         for (int e = threadIdx.x; e < tot; e += blockDim.x) tile[e] = src[e];
     }
     __syncthreads();
-    fftdev::block_fft<C, fftdev::CT<T>::kPPT, INV, true, 0>(tile, len, nr, 1, len, rd, tw, (MODE <= 1) ? 2 : 1);
+    if constexpr (LEN > 0) {
+        // all rpc rows (the unused ones of the last CTA hold garbage and are not stored)
+        constexpr int RPC = rows_rpc<T>(LEN);
+        fftdev::block_fft_fixed<C, INV, true, RPC, LEN, fftdev::ct_threads(LEN, RPC, fftdev::CT<T>::kPPT), 1, LEN,
+                                (MODE <= 1) ? 2 : 1>(tile, tw);
+    } else {
+        fftdev::block_fft<C, fftdev::CT<T>::kPPT, INV, true, 0>(tile, len, nr, 1, len, rd, tw, (MODE <= 1) ? 2 : 1);
+    }
 
     if (MODE == 0) {
         C *dm = static_cast<C *>(out_main) + comp * ccomp_out + row0 * M;
@@ -194,13 +212,16 @@ void cols_impl(cam_ctx *ctx, FftPlan *p, void *base, int64_t len, int64_t ncols,
     constexpr int W = fftdev::CT<T>::kCols;
     const Radices &rd = (len == p->n) ? p->rad_n : p->rad_m;
     const int twmul = (int)(p->n / len);
-    const int nthr = threads_for((int)len * W, fftdev::CT<T>::kPPT);
+    const int nthr = threads_for((int)len * W, fftdev::CT<T>::kPPT);  // == ct_threads for compiled lengths
     const size_t smem = (size_t)len * W * sizeof(C);
     dim3 grid((unsigned)((ncols + W - 1) / W), (unsigned)nplanes, (unsigned)ncomp);
-    auto kern = inv ? fft_cols_kernel<T, true> : fft_cols_kernel<T, false>;
-    CAM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    CAM_LAUNCH_NAMED(ctx, "fft_cols", kern, grid, nthr, smem, static_cast<C *>(base), (int)len, (int)ncols, jstride,
-               pstride, ccomp, rd, static_cast<const C *>(p->tw), twmul);
+    dispatch_fft_len(len, [&](auto lc) {
+        constexpr int LEN = decltype(lc)::value;
+        auto kern = inv ? fft_cols_kernel<T, true, LEN> : fft_cols_kernel<T, false, LEN>;
+        CAM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CAM_LAUNCH_NAMED(ctx, "fft_cols", kern, grid, nthr, smem, static_cast<C *>(base), (int)len, (int)ncols,
+                         jstride, pstride, ccomp, rd, static_cast<const C *>(p->tw), twmul);
+    });
 }
 
 template <typename T, int MODE>
@@ -211,14 +232,17 @@ void rows_impl(cam_ctx *ctx, FftPlan *p, const void *in, void *out, void *nyq, i
     const int n = (int)p->n;
     const int len = MODE <= 1 ? n / 2 : n;
     const Radices &rd = MODE <= 1 ? p->rad_m : p->rad_n;
-    const int rpc = std::max(1, (sizeof(T) == 4 ? 4096 : 2048) / len);
-    const int nthr = threads_for(rpc * len, fftdev::CT<T>::kPPT);
+    const int rpc = rows_rpc<T>(len);
+    const int nthr = threads_for(rpc * len, fftdev::CT<T>::kPPT);  // == ct_threads for compiled lengths
     const size_t smem = (size_t)rpc * len * sizeof(C);
     dim3 grid((unsigned)((nrows + rpc - 1) / rpc), (unsigned)ncomp);
-    auto kern = fft_rows_kernel<T, MODE>;
+    dispatch_fft_len(len, [&](auto lc) {
+    constexpr int LEN = decltype(lc)::value;
+    auto kern = fft_rows_kernel<T, MODE, LEN>;
     CAM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     CAM_LAUNCH_NAMED(ctx, MODE == 0 ? "fft_rows_r2c" : MODE == 1 ? "fft_rows_c2r" : "fft_rows_c2c", kern, grid, nthr, smem, in, out, static_cast<C *>(nyq), n, nrows, rpc,
                ccomp_in, ccomp_out, rd, static_cast<const C *>(p->tw), d_sub, scale);
+    });
 }
 
 template <typename T>

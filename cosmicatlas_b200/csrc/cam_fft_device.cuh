@@ -14,6 +14,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 namespace cam {
 
 // Stage list of one transform length.  Integer divisions by the stage's
@@ -206,5 +208,139 @@ __device__ __forceinline__ void block_fft(C *buf, int len, int ncol, int jstride
     }
 }
 
+// ---- compile-time stage lists -------------------------------------------
+// Same factorisation as factor_radices, evaluated at compile time, so that
+// each stage of a known length is inlined with constant Ns and len; the
+// register allocator then sees one stage at a time (the runtime stage loop
+// above spills on sm_100a).
+constexpr int ct_num_stages(int len)
+{
+    int n = 0, m = len;
+    while (m % 8 == 0 && m > 8) { ++n; m /= 8; }
+    while (m % 3 == 0) { ++n; m /= 3; }
+    if (m == 8 || m == 4 || m == 2) ++n;
+    return n;
+}
+constexpr int ct_radix(int len, int s)
+{
+    int k = 0, m = len;
+    while (m % 8 == 0 && m > 8) { if (k == s) return 8; ++k; m /= 8; }
+    while (m % 3 == 0) { if (k == s) return 3; ++k; m /= 3; }
+    return m;  // the final 8, 4 or 2
+}
+constexpr unsigned ct_magic(int d) { return d <= 1 ? 0u : (unsigned)(((1ull << 32) + (unsigned long long)d - 1) / (unsigned long long)d); }
+
+// Threads a CTA runs for NCOL transforms of length LEN at PPT points each
+// (a multiple of 32); host and device use the same formula.
+constexpr int ct_threads(int len, int ncol, int ppt)
+{
+    return ((len * ncol + ppt - 1) / ppt + 31) / 32 * 32;
+}
+
+// One Stockham stage with every shape parameter known at compile time:
+// NCOL transforms of length LEN, element (col, j) at col*CSTRIDE + j*JSTRIDE,
+// NTHR threads; JFAST as in stage().  Index arithmetic reduces to shifts,
+// constant multiplies and (for lengths with a factor 3) a constant divide.
+template <typename C, int R, bool INV, bool JFAST, int NCOL, int LEN, int NS, int NTHR, int JSTRIDE,
+          int CSTRIDE, int TWMUL>
+__device__ __forceinline__ void stage_ct(C *buf, const C *__restrict__ tw)
+{
+    constexpr int NQ = LEN / R;
+    constexpr int NBF = NQ * NCOL;
+    constexpr int MAXIT = (NBF + NTHR - 1) / NTHR;
+    constexpr bool EXACT = NBF % NTHR == 0;
+    constexpr int TWSTEP = (LEN / (NS * R)) * TWMUL;
+    const int tid = threadIdx.x;
+    C v[MAXIT][R];
+    int dsto[MAXIT];
+#pragma unroll
+    for (int it = 0; it < MAXIT; ++it) {
+        const int bi = tid + it * NTHR;
+        dsto[it] = -1;
+        if (EXACT || bi < NBF) {
+            const int col = JFAST ? bi / NQ : bi % NCOL;
+            const int j = JFAST ? bi % NQ : bi / NCOL;
+            const C *src = buf + col * CSTRIDE + j * JSTRIDE;
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[it][r] = src[r * NQ * JSTRIDE];
+            const int q = j / NS;
+            const int k = j - q * NS;
+            if (NS > 1) {
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    C w = __ldg(tw + r * k * TWSTEP);
+                    if (INV) w.y = -w.y;
+                    v[it][r] = cmul(v[it][r], w);
+                }
+            }
+            dft<C, R, INV>(v[it]);
+            dsto[it] = col * CSTRIDE + (j + q * NS * (R - 1)) * JSTRIDE;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < MAXIT; ++it) {
+        if (EXACT || dsto[it] >= 0) {
+            C *dst = buf + dsto[it];
+#pragma unroll
+            for (int r = 0; r < R; ++r) dst[r * NS * JSTRIDE] = v[it][r];
+        }
+    }
+    __syncthreads();
+}
+
+// All stages of a length-LEN transform, layout and thread count fixed at
+// compile time (the CTA must run exactly NTHR threads).
+template <typename C, bool INV, bool JFAST, int NCOL, int LEN, int NTHR, int JSTRIDE, int CSTRIDE, int TWMUL,
+          int S = 0, int NS = 1>
+__device__ __forceinline__ void block_fft_fixed(C *buf, const C *__restrict__ tw)
+{
+    if constexpr (S < ct_num_stages(LEN)) {
+        constexpr int R = ct_radix(LEN, S);
+        stage_ct<C, R, INV, JFAST, NCOL, LEN, NS, NTHR, JSTRIDE, CSTRIDE, TWMUL>(buf, tw);
+        block_fft_fixed<C, INV, JFAST, NCOL, LEN, NTHR, JSTRIDE, CSTRIDE, TWMUL, S + 1, NS * R>(buf, tw);
+    }
+}
+
+template <typename C, int PPT, bool INV, bool JFAST, int NCOL, int LEN, int S = 0, int NS = 1>
+__device__ __forceinline__ void block_fft_ct(C *buf, int ncol, int jstride, int cstride, const C *__restrict__ tw,
+                                             int twmul)
+{
+    if constexpr (S < ct_num_stages(LEN)) {
+        constexpr int R = ct_radix(LEN, S);
+        stage<C, R, PPT, INV, JFAST, NCOL>(buf, LEN, ncol, jstride, cstride, NS, ct_magic(LEN / R), ct_magic(NS), tw,
+                                           twmul);
+        block_fft_ct<C, PPT, INV, JFAST, NCOL, LEN, S + 1, NS * R>(buf, ncol, jstride, cstride, tw, twmul);
+    }
+}
+
+// Lengths with a compile-time stage list; any other 2^a 3^b length uses the
+// runtime stage loop.
+#define CAM_FFT_CT_LENGTHS(X) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512) X(768) X(1024)
+
+// Transform of length LEN (LEN = 0: runtime length `len` with stage list rd).
+template <typename C, int PPT, bool INV, bool JFAST, int NCOL, int LEN>
+__device__ __forceinline__ void block_fft_any(C *buf, int len, int ncol, int jstride, int cstride, const Radices &rd,
+                                              const C *__restrict__ tw, int twmul)
+{
+    if constexpr (LEN > 0) block_fft_ct<C, PPT, INV, JFAST, NCOL, LEN>(buf, ncol, jstride, cstride, tw, twmul);
+    else block_fft<C, PPT, INV, JFAST, NCOL>(buf, len, ncol, jstride, cstride, rd, tw, twmul);
+}
+
 }  // namespace fftdev
+
+// Host side: calls f(std::integral_constant<int, LEN>) for a length with a
+// compile-time stage list, or with LEN = 0 for any other length.
+template <typename F>
+inline void dispatch_fft_len(int64_t len, F &&f)
+{
+    switch (len) {
+#define CAM_FFT_CASE(L) \
+    case L: f(std::integral_constant<int, L>{}); return;
+        CAM_FFT_CT_LENGTHS(CAM_FFT_CASE)
+#undef CAM_FFT_CASE
+    default: f(std::integral_constant<int, 0>{}); return;
+    }
+}
+
 }  // namespace cam

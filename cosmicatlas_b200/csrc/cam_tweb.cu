@@ -31,13 +31,26 @@ namespace {
 template <typename T>
 using CTw = fftdev::CT<T>;
 
-// Component c -> (a, b): xx, yy, zz, xy, xz, yz
-__device__ __forceinline__ void comp_axes(int c, int &a, int &b)
+// Rows per CTA of the c2r + eigen pass (6 components of each row):
+// about 4096 (float) / 2048 (double) points per CTA.
+template <typename T>
+constexpr int tweb_rpc(int m)
 {
-    const int A[6] = {0, 1, 2, 0, 0, 1};
-    const int B[6] = {0, 1, 2, 1, 2, 2};
-    a = A[c];
-    b = B[c];
+    return (sizeof(T) == 4 ? 4096 : 2048) / (6 * m) > 1 ? (sizeof(T) == 4 ? 4096 : 2048) / (6 * m) : 1;
+}
+
+// Product of the two signed frequencies of component c (xx, yy, zz, xy,
+// xz, yz), without a runtime-indexed local array.
+__device__ __forceinline__ int comp_product(int c, int fi, int fj, int fk)
+{
+    switch (c) {
+    case 0: return fi * fi;
+    case 1: return fj * fj;
+    case 2: return fk * fk;
+    case 3: return fi * fj;
+    case 4: return fi * fk;
+    default: return fj * fk;
+    }
 }
 
 }  // namespace
@@ -49,12 +62,10 @@ namespace {
 template <typename T>
 __device__ __forceinline__ T tidal_mult(int c, int fi, int fj, int fk, T gauss_coef, T norm)
 {
-    const int64_t q = (int64_t)fi * fi + (int64_t)fj * fj + (int64_t)fk * fk;
+    const int q = fi * fi + fj * fj + fk * fk;
     if (q == 0) return (T)0;
-    int a, b;
-    comp_axes(c, a, b);
-    const int f[3] = {fi, fj, fk};
-    const T ratio = (T)((double)((int64_t)f[a] * f[b]) / (double)q);
+    // f_a f_b and q are exact in float up to N = 2048; one rounding each
+    const T ratio = (T)((float)comp_product(c, fi, fj, fk) * (1.0f / (float)q));
     const T g = gauss_coef != (T)0 ? exp(-gauss_coef * (T)q) : (T)1;
     return ratio * g * norm;
 }
@@ -63,7 +74,7 @@ __device__ __forceinline__ T tidal_mult(int c, int fi, int fj, int fk, T gauss_c
 // NYQ = false: main tiles (plane = j, columns = k < N/2, FFT index i with
 // stride N*M).  NYQ = true: the Nyquist plane (columns = j, FFT index i with
 // stride N, k = N/2).
-template <typename T, bool NYQ>
+template <typename T, bool NYQ, int LEN>
 __global__ void __launch_bounds__(1024, 1)
 tidal_x_kernel(const typename CTw<T>::t *__restrict__ src, typename CTw<T>::t *__restrict__ dst,
                int n, int ncols, int64_t jstride, int64_t pstride, int64_t ccomp, Radices rd,
@@ -104,7 +115,10 @@ tidal_x_kernel(const typename CTw<T>::t *__restrict__ src, typename CTw<T>::t *_
         }
     }
     __syncthreads();
-    fftdev::block_fft<C, CTw<T>::kPPT, true, false, W>(tile, n, W, W, 1, rd, tw, 1);
+    if constexpr (LEN > 0)
+        fftdev::block_fft_fixed<C, true, false, W, LEN, fftdev::ct_threads(LEN, W, CTw<T>::kPPT), W, 1, 1>(tile, tw);
+    else
+        fftdev::block_fft<C, CTw<T>::kPPT, true, false, W>(tile, n, W, W, 1, rd, tw, 1);
     for (int e = threadIdx.x; e < tot; e += blockDim.x) {
         const int i = e / W, cc = e % W;
         if (cc < nc) o[(int64_t)i * jstride + cc] = tile[e];
@@ -130,9 +144,9 @@ __device__ __forceinline__ void eig3(float a00, float a11, float a22, float a01,
                           a02 * (a01 * a12 - b11 * a02);
         float r = det / (2.0f * pp * pp * pp);
         r = fminf(1.0f, fmaxf(-1.0f, r));
-        const float phi = acosf(r) * (1.0f / 3.0f);
-        l[0] = q + 2.0f * pp * cosf(phi);
-        l[2] = q + 2.0f * pp * cosf(phi + 2.0943951023931954923f);
+        const float phi = acosf(r) * (1.0f / 3.0f);  // in [0, pi/3]
+        l[0] = q + 2.0f * pp * __cosf(phi);
+        l[2] = q + 2.0f * pp * __cosf(phi + 2.0943951023931954923f);
         l[1] = 3.0f * q - l[0] - l[2];
     }
     // det(x I - A) = x^3 - c2 x^2 + c1 x - c0, coefficients in FP64 from the
@@ -148,7 +162,9 @@ __device__ __forceinline__ void eig3(float a00, float a11, float a22, float a01,
         const double f = ((x - c2) * x + c1) * x - c0;
         const double fp = (3.0 * x - 2.0 * c2) * x + c1;
         if (fabs(fp) > 1e-6 * sc * sc) {
-            const double dx = f / fp;
+            // f is O(eps_f32) relative, so a float reciprocal of f' keeps the
+            // correction accurate to ~1e-7 of itself
+            const double dx = f * (double)__frcp_rn((float)fp);
             if (fabs(dx) < 1e-4 * sc) x -= dx;
         }
         lam[k] = x;
@@ -162,8 +178,8 @@ __device__ __forceinline__ void eig3(float a00, float a11, float a22, float a01,
 // c2r along z of the six components for `rpc` rows, then eigenvalues and
 // labels.  Component c of row r: main at src + c*ccomp + r*M, Nyquist at
 // nyq + c*N*N + r.
-template <typename T>
-__global__ void __launch_bounds__(512, 1)
+template <typename T, int LEN>
+__global__ void __launch_bounds__(256, 2)
 tidal_z_kernel(const typename CTw<T>::t *__restrict__ src, const typename CTw<T>::t *__restrict__ nyq,
                int n, int64_t nrows, int rpc, int64_t ccomp, Radices rd,
                const typename CTw<T>::t *__restrict__ tw, double lth, double band,
@@ -200,9 +216,15 @@ tidal_z_kernel(const typename CTw<T>::t *__restrict__ src, const typename CTw<T>
         tile[e] = fftdev::cadd(a, ib);
     }
     __syncthreads();
-    fftdev::block_fft<C, CTw<T>::kPPT, true, true, 0>(tile, M, 6 * rpc, 1, M, rd, tw, 2);
+    if constexpr (LEN > 0) {
+        constexpr int RPCZ = tweb_rpc<T>(LEN);
+        fftdev::block_fft_fixed<C, true, true, 6 * RPCZ, LEN, fftdev::ct_threads(LEN, 6 * RPCZ, CTw<T>::kPPT), 1, LEN, 2>(
+            tile, tw);
+    } else {
+        fftdev::block_fft<C, CTw<T>::kPPT, true, true, 0>(tile, M, 6 * rpc, 1, M, rd, tw, 2);
+    }
     // Per cell: 6 components -> eigenvalues -> label.
-    unsigned int lc[5] = {0, 0, 0, 0, 0};
+    unsigned int lc0 = 0, lc1 = 0, lc2 = 0, lc3 = 0, lties = 0;
     const T *re = reinterpret_cast<const T *>(tile);  // real row r of comp c at (c*rpc + r)*n
     const int64_t ncell = nn * n;
     for (int e = threadIdx.x; e < nr * n; e += blockDim.x) {
@@ -225,12 +247,15 @@ tidal_z_kernel(const typename CTw<T>::t *__restrict__ src, const typename CTw<T>
             lambdas[ncell + cell] = (float)lam[1];
             lambdas[2 * ncell + cell] = (float)lam[2];
         }
-        lc[3 - v]++;
-        lc[4] += tie;
+        lc0 += v == 3;  // label 1, knot
+        lc1 += v == 2;
+        lc2 += v == 1;
+        lc3 += v == 0;  // label 4, void
+        lties += tie;
     }
 #pragma unroll
     for (int a = 0; a < 5; ++a) {
-        unsigned int v = lc[a];
+        unsigned int v = a == 0 ? lc0 : a == 1 ? lc1 : a == 2 ? lc2 : a == 3 ? lc3 : lties;
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
         if ((threadIdx.x & 31) == 0 && v) atomicAdd(&cnt_s[a], v);
@@ -273,8 +298,10 @@ void tweb_impl(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const d
     {
         const int nthr = threads_for((int)n * W, CTw<T>::kPPT, 1024);
         const size_t smem = (size_t)n * W * sizeof(C);
-        auto k0 = tidal_x_kernel<T, false>;
-        auto k1 = tidal_x_kernel<T, true>;
+        dispatch_fft_len(n, [&](auto lc) {
+        constexpr int LEN = decltype(lc)::value;
+        auto k0 = tidal_x_kernel<T, false, LEN>;
+        auto k1 = tidal_x_kernel<T, true, LEN>;
         CAM_CUDA_TRY(cudaFuncSetAttribute(k0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         CAM_CUDA_TRY(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         dim3 g0(6, (unsigned)((M + W - 1) / W), (unsigned)n);
@@ -283,21 +310,28 @@ void tweb_impl(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const d
         dim3 g1(6, (unsigned)((n + W - 1) / W), 1);
         CAM_LAUNCH_NAMED(ctx, "tweb_tidal_x_nyq", k1, g1, nthr, smem, static_cast<const C *>(dk.nyq), cn, (int)n, (int)n, n,
                    (int64_t)0, nn, rn, tw, gcoef, d_mean, density, scale);
+        });
     }
     // 2. y: inverse FFT of the six components.
     fft_columns(ctx, plan, cm, n, M, M, n, n * M, 6, ccomp, true);
     fft_rows_c2c(ctx, plan, cn, n, n, 6, nn, true);
     // 3. z: c2r + eigenvalues + labels.
     {
-        const int rpc = std::max(1, (int)((sizeof(T) == 4 ? 8192 : 4096) / (6 * M)));
-        const int nthr = threads_for(6 * rpc * (int)M, CTw<T>::kPPT, 512);
+        // Small tiles (<= 4096 complex, 256 threads) so that several CTAs
+        // share an SM: one CTA's loads overlap another's transform and
+        // eigen-solve.
+        const int rpc = tweb_rpc<T>((int)M);
+        const int nthr = threads_for(6 * rpc * (int)M, CTw<T>::kPPT, 256);
         CAM_REQUIRE(6 * rpc * M <= (int64_t)nthr * CTw<T>::kPPT, CAM_E_UNSUPPORTED, "T-web row tile too large");
         const size_t smem = (size_t)6 * rpc * M * sizeof(C);
-        auto kz = tidal_z_kernel<T>;
+        dispatch_fft_len(M, [&](auto lc) {
+        constexpr int LEN = decltype(lc)::value;
+        auto kz = tidal_z_kernel<T, LEN>;
         CAM_CUDA_TRY(cudaFuncSetAttribute(kz, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         const unsigned grid = (unsigned)((nn + rpc - 1) / rpc);
         CAM_LAUNCH_NAMED(ctx, "tweb_tidal_z_eigen", kz, grid, nthr, smem, cm, cn, (int)n, nn, rpc, ccomp, rm, tw, o.lambda_th,
                    o.tie_band, d_labels, d_lambdas, cnt);
+        });
     }
     if (stats) {
         unsigned long long h[5];

@@ -201,6 +201,14 @@ typedef struct {
 
 int cam_job_run(cam_ctx *ctx, const cam_job_desc *job, cam_job_result *res);
 
+/* Copies host particles into device buffers owned by the context (one
+ * cudaMemcpyAsync per array on the context's stream) and returns them as a
+ * CAM_MEM_DEVICE particle set, valid until the next cam_particles_stage on
+ * this context.  Lets one upload serve several jobs on the same particles
+ * (the reference calls getDensity_* once per scheme on the same vectors,
+ * e.g. Source/Catalog.cpp:662-683). */
+int cam_particles_stage(cam_ctx *ctx, const cam_particles *host, cam_particles *device_out);
+
 /* ---- power spectrum without device allocation --------------------------
  * No counterpart in the reference.  For callers that may not allocate
  * device memory -- code running inside a memory pool or arena it does not
