@@ -49,8 +49,11 @@ def parse():
     ap.add_argument("--particles", type=int, default=N_PARTICLES)
     ap.add_argument("--kernels-only", action="store_true",
                     help="profiler runs: the device-resident pass only (no e2e pass, no CPU baseline)")
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "single512", "large768"],
-                    help="sweep: the benchmark line (default); single512 / large768: one-job latency lines")
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "single512", "large768", "calib", "stream"],
+                    help="sweep: the benchmark line (default); single512 / large768: one-job latency lines; "
+                         "calib / stream: served vs plain per-call jobs/s and latency")
+    ap.add_argument("--jobs", type=int, default=0, help="calib / stream: number of jobs (0 = the config's)")
+    ap.add_argument("--rates", default="50,200,800", help="stream: Poisson arrival rates (jobs/s)")
     ap.add_argument("--mesh", type=int, default=0, help="single512 only: override N (profiler runs)")
     return ap.parse_args()
 
@@ -408,8 +411,204 @@ def run_single(args):
     return out
 
 
+# ------------------------------------------------------------------ serving
+def _latency(v):
+    v = np.sort(np.asarray(v, np.float64))
+    return {"p50": round(float(np.percentile(v, 50)), 3), "p99": round(float(np.percentile(v, 99)), 3),
+            "mean": round(float(v.mean()), 3), "max": round(float(v.max()), 3)}
+
+
+def calib_jobs(njobs):
+    """The calibration batch: njobs independent seeds, 262,144 clumped
+    particles each (clump fraction U[0.5, 0.9], sigma U[1, 4], 2,000
+    clumps), L = 500, CIC onto 64^3 FP32, P(k) in 32 bins, T-web label
+    counts with R = 8, lambda_th = 0.  Particles are drawn on the GPU."""
+    from cosmicatlas_b200 import synth
+    from cosmicatlas_b200.api import CIC, Context, JobSpec, make_grid
+    grid = make_grid(64, 500.0)
+    pk = Context.pk_opts(CIC, nbins=32)
+    tw = Context.tweb_opts(8.0, 0.0, 1e-5)
+    parts = []
+    for j in range(njobs):
+        rng = np.random.default_rng(5 + j)
+        frac, sig = rng.uniform(0.5, 0.9), rng.uniform(1.0, 4.0)
+        parts.append(synth.clumped_torch(262_144, 500.0, 2_000, sig, frac, seed=100_000 + j))
+
+    def specs():
+        return [JobSpec(x, y, z, None, grid=grid, scheme=CIC, precision=0, pk=pk, tweb=tw) for x, y, z in parts]
+    return parts, grid, pk, tw, specs
+
+
+def _events_ms(fn, stream):
+    import torch
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    out = fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1), out
+
+
+def run_calib(args):
+    """Served vs plain per-call throughput on the calibration batch."""
+    import torch
+
+    from cosmicatlas_b200.api import CIC, Context, Server
+    torch.cuda.set_device(0)
+    njobs = args.jobs or 4096
+    parts, grid, pk, tw, specs = calib_jobs(njobs)
+    stream = torch.cuda.current_stream()
+    ctx = Context(0)
+    ctx.set_stream(stream.cuda_stream)
+
+    # plain per-call path: one cam_job_run per job
+    def plain(k):
+        lat = []
+        for x, y, z in parts[:k]:
+            t0 = time.perf_counter()
+            ctx.job(x, y, z, None, grid, CIC, 0, pk=pk, tweb=tw)
+            lat.append(1e3 * (time.perf_counter() - t0))
+        return lat
+    plain(min(njobs, 64))
+    ms_plain, lat_plain = _events_ms(lambda: plain(njobs), stream)
+
+    # graph-packed batches through cam_batch_run
+    ctx.batch(specs()[:64])
+    sp = specs()
+    ms_batch, _ = _events_ms(lambda: ctx.batch(sp), stream)
+
+    # the continuous-batching server: every job submitted at t = 0
+    with Server(0, workers=4, max_batch=32) as srv:
+        warm = specs()[:256]
+        for i in [srv.submit(s) for s in warm]:
+            srv.wait(i)
+        srv.stats(reset=True)
+        sp = specs()
+
+        def serve():
+            ids = [srv.submit(s) for s in sp]
+            for i in ids:
+                srv.wait(i)
+        with ClockSampler(0) as clk:
+            ms_srv, _ = _events_ms(serve, stream)
+        st = srv.stats()
+    ctx.close()
+    return {
+        "workload": f"calibration batch: {njobs} jobs x 262,144 clumped particles, L=500, CIC 64^3 FP32, "
+                    "P(k) 32 bins, T-web counts R=8",
+        "metric": "mesh-jobs/s", "unit": "jobs/s",
+        "plain": {"value": round(njobs / (ms_plain / 1e3), 1), "latency_ms": _latency(lat_plain),
+                  "path": "cam_job_run per job, one context"},
+        "batch": {"value": round(njobs / (ms_batch / 1e3), 1), "path": "cam_batch_run, 32 jobs per graph"},
+        "served": {"value": round(njobs / (ms_srv / 1e3), 1), "path": "cam_server: 4 workers, batches of 32",
+                   "latency_ms": {"p50": round(st["p50_ms"], 3), "p99": round(st["p99_ms"], 3),
+                                  "note": "submit -> result with all jobs submitted at t = 0"},
+                   "batches": st["batches"], "graph_replays": st["graph_replays"]},
+        "speedup_served_vs_plain": round(ms_plain / ms_srv, 2),
+        "speedup_batch_vs_plain": round(ms_plain / ms_batch, 2),
+        "clocks": clk.summary(),
+    }
+
+
+def stream_jobs(njobs, seed=4):
+    """The served mixed stream: N from {64..512} (weights .30/.25/.15/.15/.10
+    /.05), N_p log-uniform [1e5, 5e7], L log-uniform [250, 2000], scheme
+    uniform, half the jobs want the T-web (R = 2 cells, lambda_th = 0);
+    P(k) in N/2 bins of width k_f."""
+    rng = np.random.default_rng(seed)
+    ns = rng.choice([64, 128, 192, 256, 384, 512], size=njobs, p=[0.30, 0.25, 0.15, 0.15, 0.10, 0.05])
+    nps = np.exp(rng.uniform(np.log(1e5), np.log(5e7), size=njobs)).astype(np.int64)
+    boxes = np.exp(rng.uniform(np.log(250.0), np.log(2000.0), size=njobs))
+    schemes = rng.integers(0, 3, size=njobs)
+    tweb = rng.uniform(size=njobs) < 0.5
+    return [dict(n=int(a), np=int(b), box=float(c), scheme=int(d), tweb=bool(e))
+            for a, b, c, d, e in zip(ns, nps, boxes, schemes, tweb)]
+
+
+def run_stream(args):
+    """Served vs plain per-call path on the mixed stream, open-loop Poisson
+    arrivals at each rate plus a closed-loop saturation pass.  Particles
+    come from four shuffled 5e7-particle pools of the clumped process in the
+    unit box (200,000 clumps, sigma = 1.5e-3), scaled by each job's L on the
+    GPU just before submission."""
+    import torch
+
+    from cosmicatlas_b200 import synth
+    from cosmicatlas_b200.api import Context, JobSpec, Server, make_grid
+    torch.cuda.set_device(0)
+    njobs = args.jobs or 2000
+    jobs = stream_jobs(njobs)
+    pools = []
+    for p in range(4):
+        x, y, z = synth.clumped_torch(50_000_000, 1.0, 200_000, 1.5e-3, 0.8, seed=40 + p)
+        perm = torch.randperm(x.numel(), device="cuda", generator=torch.Generator("cuda").manual_seed(p))
+        pools.append(torch.stack([x[perm], y[perm], z[perm]]))
+        del x, y, z, perm
+    prep = torch.cuda.Stream()
+    budget = 150 << 30
+
+    def make(j, i):
+        with torch.cuda.stream(prep):
+            xyz = pools[i % 4][:, :j["np"]] * j["box"]
+            xyz = torch.where(xyz >= j["box"], torch.zeros_like(xyz), xyz)
+        prep.synchronize()
+        n = j["n"]
+        return JobSpec(xyz[0], xyz[1], xyz[2], None, grid=make_grid(n, j["box"]), scheme=j["scheme"], precision=0,
+                       pk=Context.pk_opts(j["scheme"], nbins=n // 2),
+                       tweb=Context.tweb_opts(2.0 * j["box"] / n, 0.0, 1e-5) if j["tweb"] else None)
+
+    def one_pass(workers, max_batch, rate, held_gb=24.0):
+        rng = np.random.default_rng(99)
+        gaps = rng.exponential(1.0 / rate, size=njobs) if rate else np.zeros(njobs)
+        with Server(0, hbm_budget=budget, workers=workers, max_batch=max_batch) as srv:
+            for i in [srv.submit(make(j, k)) for k, j in enumerate(jobs[:8])]:
+                srv.wait(i)
+            srv.stats(reset=True)
+            pending = []  # (id, bytes): inputs the client holds until done
+            held = 0.0
+            t_start = time.perf_counter()
+            t_next = t_start
+            for k, j in enumerate(jobs):
+                t_next += gaps[k]
+                now = time.perf_counter()
+                if t_next > now:
+                    time.sleep(t_next - now)
+                while pending and held > held_gb * 1e9:  # client back-pressure
+                    jid, b = pending.pop(0)
+                    srv.wait(jid)
+                    held -= b
+                jid = srv.submit(make(j, k))
+                pending.append((jid, 12.0 * j["np"]))
+                held += 12.0 * j["np"]
+            for jid, _ in pending:
+                srv.wait(jid)
+            wall = time.perf_counter() - t_start
+            st = srv.stats()
+        return {"jobs_per_s": round(njobs / wall, 1), "p50_ms": round(st["p50_ms"], 2),
+                "p99_ms": round(st["p99_ms"], 2), "batches": st["batches"], "batched_jobs": st["batched_jobs"],
+                "graph_replays": st["graph_replays"], "peak_reserved_gb": round(st["peak_bytes_reserved"] / 1e9, 1)}
+
+    rates = [float(r) for r in args.rates.split(",") if r]
+    out = {"workload": f"served mixed stream: {njobs} jobs, N in 64..512, N_p log-uniform [1e5, 5e7], "
+                       "L log-uniform [250, 2000], NGP/CIC/TSC, half with T-web; HBM budget 150 GB",
+           "metric": "mesh-jobs/s", "unit": "jobs/s", "rates": {}}
+    with ClockSampler(0) as clk:
+        out["saturation"] = {"served": one_pass(4, 16, 0), "plain": one_pass(1, 1, 0)}
+        for r in rates:
+            out["rates"][str(r)] = {"served": one_pass(4, 16, r), "plain": one_pass(1, 1, r)}
+    s, p = out["saturation"]["served"], out["saturation"]["plain"]
+    out["speedup_served_vs_plain"] = round(s["jobs_per_s"] / p["jobs_per_s"], 2)
+    out["clocks"] = clk.summary()
+    return out
+
+
 def main():
     args = parse()
+    if args.workload in ("calib", "stream"):
+        print(json.dumps(run_calib(args) if args.workload == "calib" else run_stream(args)), flush=True)
+        return
     if args.workload != "sweep":
         print(json.dumps(run_single(args)), flush=True)
         return

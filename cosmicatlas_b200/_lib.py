@@ -77,6 +77,15 @@ class JobResult(ctypes.Structure):
                 ("tweb", TwebStats)]
 
 
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
+                ("queued", ctypes.c_int64), ("running", ctypes.c_int64), ("batches", ctypes.c_int64),
+                ("batched_jobs", ctypes.c_int64), ("graph_replays", ctypes.c_int64),
+                ("bytes_reserved", ctypes.c_size_t), ("peak_bytes_reserved", ctypes.c_size_t),
+                ("budget", ctypes.c_size_t), ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
+                ("mean_ms", ctypes.c_double), ("max_ms", ctypes.c_double)]
+
+
 # Exported symbols with their signatures; the non-GPU tests check every one
 # of these resolves.
 _P = ctypes.c_void_p
@@ -106,6 +115,15 @@ SIGNATURES = {
     "cam_particles_stage": ([_P, ctypes.POINTER(Particles), ctypes.POINTER(Particles)], ctypes.c_int),
     "cam_power_noalloc": ([_P, ctypes.c_int64, ctypes.c_int, ctypes.c_float, ctypes.c_double,
                            ctypes.POINTER(PkOpts), _P, _P, _P], ctypes.c_int),
+    "cam_batch_run": ([_P, ctypes.POINTER(JobDesc), ctypes.c_int, ctypes.POINTER(JobResult)], ctypes.c_int),
+    "cam_server_create": ([ctypes.c_int, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_P)],
+                          ctypes.c_int),
+    "cam_server_submit": ([_P, ctypes.POINTER(JobDesc), ctypes.POINTER(JobResult), ctypes.POINTER(ctypes.c_uint64)],
+                          ctypes.c_int),
+    "cam_server_poll": ([_P, ctypes.c_uint64], ctypes.c_int),
+    "cam_server_wait": ([_P, ctypes.c_uint64, ctypes.c_int64], ctypes.c_int),
+    "cam_server_stats_get": ([_P, ctypes.POINTER(ServerStats), ctypes.c_int], ctypes.c_int),
+    "cam_server_destroy": ([_P], ctypes.c_int),
 }
 
 _lib = None

@@ -257,11 +257,43 @@ class Context:
 
     def job(self, x, y=None, z=None, w=None, grid: L.Grid = None, scheme: int = CIC, precision=F32,
             pk: L.PkOpts | None = None, tweb: L.TwebOpts | None = None, want_labels=False):
-        """One mesh job.  `x` may be a StagedParticles (then y, z, w are unused)."""
+        """One mesh job (cam_job_run).  `x` may be a StagedParticles (then y, z,
+        w are unused)."""
+        j = JobSpec(x, y, z, w, grid=grid, scheme=scheme, precision=precision, pk=pk, tweb=tweb,
+                    want_labels=want_labels)
+        self._check(self._lib.cam_job_run(self.h, ctypes.byref(j.desc), ctypes.byref(j.res)))
+        return j.result()
+
+    def batch(self, jobs: list["JobSpec"]) -> list[dict]:
+        """Runs jobs through cam_batch_run: consecutive jobs of one shape are
+        packed into captured-graph batches.  Returns one result per job, as
+        job() does (labels are not available in batches)."""
+        n = len(jobs)
+        descs = (L.JobDesc * n)(*[j.desc for j in jobs])
+        ress = (L.JobResult * n)(*[j.res for j in jobs])
+        rc = self._lib.cam_batch_run(self.h, descs, n, ress)
+        for j, r in zip(jobs, ress):
+            j.res = r  # filled for every job, also when one of them failed
+        self._check(rc)
+        return [j.result() for j in jobs]
+
+
+class JobSpec:
+    """A cam_job_desc with its host result arrays (and the particle arrays
+    kept alive until the job is done)."""
+
+    def __init__(self, x, y=None, z=None, w=None, grid: L.Grid = None, scheme: int = CIC, precision=F32,
+                 pk: L.PkOpts | None = None, tweb: L.TwebOpts | None = None, want_labels=False):
         if isinstance(x, StagedParticles):
-            p = x.parts
+            p, self.keep = x.parts, x.keep
         else:
-            p, keep, dev = self._particles(x, y, z, w)
+            dev = L.is_device(x)
+            xs = tuple(_f32(a) for a in (x, y, z, w))
+            p = L.Particles()
+            p.n = int(xs[0].shape[0])
+            p.x, p.y, p.z, p.w = (L.ptr(a) for a in xs)
+            p.mem = L.MEM_DEVICE if dev else L.MEM_HOST
+            self.keep = xs
         d = L.JobDesc()
         d.parts, d.grid, d.scheme, d.precision = p, grid, scheme, precision
         if pk is not None:
@@ -269,21 +301,100 @@ class Context:
         d.want_tweb = int(tweb is not None)
         if tweb is not None:
             d.tweb = tweb
-        r = L.JobResult()
+        self.desc = d
+        self.want_tweb = tweb is not None
         nb = 0
         if pk is not None:
             nb = pk.nbins if pk.nbins > 0 else int(grid.n[0] / pk.ndel / 2)
-        pkv = np.empty(nb); md = np.empty(nb, np.int64); kv = np.empty(nb)
+        self.nb = nb
+        self.pk = np.empty(nb)
+        self.modes = np.empty(nb, np.int64)
+        self.kvector = np.empty(nb)
         n = grid.n[0]
-        labels = np.empty((n, n, n), np.uint8) if (tweb is not None and want_labels) else None
-        r.pk, r.modes, r.kvector, r.labels = L.ptr(pkv), L.ptr(md), L.ptr(kv), L.ptr(labels)
-        self._check(self._lib.cam_job_run(self.h, ctypes.byref(d), ctypes.byref(r)))
+        self.labels = np.empty((n, n, n), np.uint8) if (tweb is not None and want_labels) else None
+        r = L.JobResult()
+        r.pk, r.modes, r.kvector, r.labels = L.ptr(self.pk), L.ptr(self.modes), L.ptr(self.kvector), \
+            L.ptr(self.labels)
+        self.res = r
+
+    def result(self) -> dict:
+        r = self.res
         return {
-            "pk": PkResult(pkv, md, kv, r.pk_info.n_obj, r.pk_info.shot_noise, r.pk_info.normal) if nb else None,
+            "pk": PkResult(self.pk, self.modes, self.kvector, r.pk_info.n_obj, r.pk_info.shot_noise,
+                           r.pk_info.normal) if self.nb else None,
             "assign": AssignResult(None, r.assign.n_in, r.assign.n_lost, r.assign.sum_mesh),
-            "tweb": TwebResult(labels, None, np.array(r.tweb.counts[:], np.int64), int(r.tweb.ties), r.tweb.mean)
-            if tweb is not None else None,
+            "tweb": TwebResult(self.labels, None, np.array(r.tweb.counts[:], np.int64), int(r.tweb.ties),
+                               r.tweb.mean) if self.want_tweb else None,
         }
+
+
+class Server:
+    """Continuous-batching job server on one device (cam_server_*).
+
+    submit() queues a JobSpec and returns its id; wait(id) returns the job's
+    result dict (raising CamError on a failed job).  Jobs start as soon as a
+    worker and the HBM budget allow; queued small jobs of one shape are
+    packed into captured-graph batches."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0, workers: int = 4, max_batch: int = 16):
+        self._lib = L.lib()
+        h = ctypes.c_void_p()
+        rc = self._lib.cam_server_create(device, hbm_budget, workers, max_batch, ctypes.byref(h))
+        if rc != L.CAM_OK:
+            raise CamError(rc, "cam_server_create failed")
+        self.h = h
+        self._jobs: dict[int, JobSpec] = {}
+
+    def submit(self, job: JobSpec) -> int:
+        jid = ctypes.c_uint64()
+        rc = self._lib.cam_server_submit(self.h, ctypes.byref(job.desc), ctypes.byref(job.res), ctypes.byref(jid))
+        if rc != L.CAM_OK:
+            raise CamError(rc, "cam_server_submit failed")
+        self._jobs[jid.value] = job
+        return jid.value
+
+    def wait(self, jid: int, timeout_s: float | None = None) -> dict:
+        us = -1 if timeout_s is None else int(timeout_s * 1e6)
+        job = self._jobs[jid]
+        rc = job.status if hasattr(job, "status") else self._lib.cam_server_wait(self.h, jid, us)
+        if rc == L.CAM_E_TIMEOUT:
+            raise TimeoutError(f"job {jid} still running")
+        self._jobs.pop(jid)
+        if rc != L.CAM_OK:
+            raise CamError(rc, f"job {jid} failed")
+        return job.result()
+
+    def poll(self, jid: int) -> bool:
+        """True once the job has finished (its status is then kept for wait)."""
+        rc = self._lib.cam_server_poll(self.h, jid)
+        if rc == L.CAM_E_BUSY:
+            return False
+        self._jobs[jid].status = rc
+        return True
+
+    def stats(self, reset: bool = False) -> dict:
+        st = L.ServerStats()
+        rc = self._lib.cam_server_stats_get(self.h, ctypes.byref(st), int(reset))
+        if rc != L.CAM_OK:
+            raise CamError(rc, "cam_server_stats_get failed")
+        return {f: getattr(st, f) for f, _ in L.ServerStats._fields_}
+
+    def close(self):
+        if self.h:
+            self._lib.cam_server_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 @dataclass

@@ -17,9 +17,12 @@ void *scratch(cam_ctx *ctx, const char *name, size_t bytes)
     bytes = std::max<size_t>(bytes, 256);
     DevBuf &b = ctx->bufs[name];
     if (b.cap >= bytes) return b.ptr;
+    CAM_REQUIRE(!ctx->capturing, CAM_E_BUSY, std::string("buffer ") + name + " would grow during stream capture");
     const size_t want = std::max(bytes, b.cap + b.cap / 4);
     if (ctx->budget && ctx->used - b.cap + want > ctx->budget)
         throw Error{CAM_E_NOMEM, std::string("HBM budget exceeded allocating ") + name};
+    std::lock_guard<std::mutex> lk(alloc_mutex());
+    ctx->gen++;
     if (b.ptr) {
         CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
         CAM_CUDA_TRY(cudaFree(b.ptr));
@@ -41,7 +44,7 @@ void *scratch(cam_ctx *ctx, const char *name, size_t bytes)
 
 void prof_begin(cam_ctx *ctx, const char *name)
 {
-    if (!ctx->prof_on) return;
+    if (!ctx->prof_on || ctx->capturing) return;
     auto take = [&]() {
         cudaEvent_t e;
         if (!ctx->prof_pool.empty()) {
@@ -59,7 +62,7 @@ void prof_begin(cam_ctx *ctx, const char *name)
 
 void prof_end(cam_ctx *ctx)
 {
-    if (!ctx->prof_on || ctx->prof_pending.empty()) return;
+    if (!ctx->prof_on || ctx->capturing || ctx->prof_pending.empty()) return;
     CAM_CUDA_TRY(cudaEventRecord(ctx->prof_pending.back().stop, ctx->stream));
 }
 
@@ -80,8 +83,18 @@ static void prof_collect(cam_ctx *ctx)
     ctx->prof_pending.clear();
 }
 
+std::mutex &alloc_mutex()
+{
+    static std::mutex m;
+    return m;
+}
+
 void release_all(cam_ctx *ctx)
 {
+    std::lock_guard<std::mutex> lk(alloc_mutex());
+    ctx->gen++;
+    cudaStreamSynchronize(ctx->stream);
+    free_plans(ctx);  // their twiddles live in the buffers freed below
     for (auto &kv : ctx->bufs)
         if (kv.second.ptr) cudaFree(kv.second.ptr);
     ctx->bufs.clear();
@@ -203,7 +216,11 @@ DevParticles stage_particles(cam_ctx *ctx, const cam_particles *p)
     return d;
 }
 
-cam_grid resolved(const cam_grid &g)
+}  // namespace
+
+namespace cam {
+
+cam_grid resolved_grid(const cam_grid &g)
 {
     cam_grid r = g;
     for (int a = 0; a < 3; ++a)
@@ -211,20 +228,18 @@ cam_grid resolved(const cam_grid &g)
     return r;
 }
 
-int nbins_default(const cam_pk_opts &o, int64_t n)
+int nbins_for(const cam_pk_opts &o, int64_t n)
 {
     if (o.nbins > 0) return o.nbins;
     return (int)((double)n / o.ndel / 2.0);  // Nnp_data = Nft / ndel_data / 2
 }
 
-// Power spectrum of a spectrum already on the device (split layout).
-void power_from_spectrum(cam_ctx *ctx, const Spectrum &s, float L, double n_obj, const cam_pk_opts &o,
-                         double *pk, int64_t *modes, double *kvec, cam_pk_info *info)
+// P(k) per bin from the FP64 bin sums: normalisation and shot noise of
+// PowerSpectrumF::compute_power_spectrum_grid (Source/PowerSpectrumF.cpp:1754-1783)
+// and the final division of FftwFunctions::power_spectrum (:1873-1874).
+void finalize_pk(int64_t n, float L, double n_obj, const cam_pk_opts &o, int nbins, const double *sr,
+                 const double *ss, const int64_t *md, double *pk, int64_t *modes, double *kvec, cam_pk_info *info)
 {
-    const int nbins = nbins_default(o, s.n);
-    std::vector<double> sr(nbins), ss(nbins);
-    std::vector<int64_t> md(nbins);
-    power_bin(ctx, s, o, nbins, sr.data(), ss.data(), md.data());
     const double vol = (double)L * (double)L * (double)L;
     double normal, ngal;
     if (o.input_type == CAM_INPUT_DENSITY) {
@@ -232,7 +247,7 @@ void power_from_spectrum(cam_ctx *ctx, const Spectrum &s, float L, double n_obj,
         normal = ngal * ngal / vol;  // PowerSpectrumF.cpp:1764
     } else {
         ngal = 1.0;
-        const double ng = (double)s.n * s.n * s.n;
+        const double ng = (double)n * n * n;
         normal = ng * ng / vol;      // PowerSpectrumF.cpp:1775
     }
     const double sn = vol / ngal;   // PowerSpectrumF.cpp:1782
@@ -264,6 +279,21 @@ Spectrum alloc_spectrum(cam_ctx *ctx, int64_t n, int precision, const char *tag)
     s.main = scratch(ctx, (std::string(tag) + ".main").c_str(), (size_t)n * n * (n / 2) * cs);
     s.nyq = scratch(ctx, (std::string(tag) + ".nyq").c_str(), (size_t)n * n * cs);
     return s;
+}
+
+}  // namespace cam
+
+namespace {
+
+// Power spectrum of a spectrum already on the device (split layout).
+void power_from_spectrum(cam_ctx *ctx, const Spectrum &s, float L, double n_obj, const cam_pk_opts &o,
+                         double *pk, int64_t *modes, double *kvec, cam_pk_info *info)
+{
+    const int nbins = nbins_for(o, s.n);
+    std::vector<double> sr(nbins), ss(nbins);
+    std::vector<int64_t> md(nbins);
+    power_bin(ctx, s, o, nbins, sr.data(), ss.data(), md.data());
+    finalize_pk(s.n, L, n_obj, o, nbins, sr.data(), ss.data(), md.data(), pk, modes, kvec, info);
 }
 
 void validate_pk(const cam_pk_opts *o)
@@ -312,13 +342,13 @@ int cam_ctx_destroy(cam_ctx *ctx)
         std::lock_guard<std::recursive_mutex> lk(ctx->mu);
         cudaSetDevice(ctx->device);
         cudaStreamSynchronize(ctx->stream);
-        for (auto &kv : ctx->plans) delete kv.second;
         for (auto &r : ctx->prof_pending) {
             cudaEventDestroy(r.start);
             cudaEventDestroy(r.stop);
         }
         for (auto e : ctx->prof_pool) cudaEventDestroy(e);
-        ctx->plans.clear();
+        if (ctx->batch) batch_destroy(ctx->batch);
+        ctx->batch = nullptr;
         release_all(ctx);
         if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     }
@@ -374,7 +404,7 @@ int cam_assign(cam_ctx *ctx, const cam_particles *parts, const cam_grid *grid, i
         check_prec(precision);
         check_mem(out_mem);
         const DevParticles d = stage_particles(ctx, parts);
-        const cam_grid g = resolved(*grid);
+        const cam_grid g = resolved_grid(*grid);
         const int64_t ncell = g.n[0] * g.n[1] * g.n[2];
         AssignOut out;
         out.precision = precision;
@@ -402,7 +432,7 @@ int cam_count_ngp(cam_ctx *ctx, const cam_particles *parts, const cam_grid *grid
         check_mem(out_mem);
         CAM_REQUIRE(parts && parts->w == nullptr, CAM_E_INVAL, "integer counts take unweighted particles");
         const DevParticles d = stage_particles(ctx, parts);
-        const cam_grid g = resolved(*grid);
+        const cam_grid g = resolved_grid(*grid);
         const int64_t ncell = g.n[0] * g.n[1] * g.n[2];
         AssignOut out;
         out.precision = -1;
@@ -430,7 +460,7 @@ int cam_cell_keys(cam_ctx *ctx, const cam_particles *parts, const cam_grid *grid
         check_mem(out_mem);
         CAM_REQUIRE(scheme >= CAM_NGP && scheme <= CAM_TSC, CAM_E_INVAL, "unknown mass assignment scheme");
         const DevParticles d = stage_particles(ctx, parts);
-        const cam_grid g = resolved(*grid);
+        const cam_grid g = resolved_grid(*grid);
         int64_t *dk = out_mem == CAM_MEM_DEVICE ? keys_out
                                                 : static_cast<int64_t *>(scratch(ctx, "keys.out", std::max<int64_t>(d.n, 1) * 8));
         cell_keys_device(ctx, d.x, d.y, d.z, d.n, g, scheme, dk);
@@ -588,7 +618,7 @@ int cam_job_run(cam_ctx *ctx, const cam_job_desc *job, cam_job_result *res)
         check_prec(job->precision);
         const bool want_pk = job->pk.nbins > 0 || job->pk.ndel > 0.0;
         if (want_pk) validate_pk(&job->pk);
-        const cam_grid g = resolved(job->grid);
+        const cam_grid g = resolved_grid(job->grid);
         const int64_t n = g.n[0], ncell = n * n * n;
         const DevParticles d = stage_particles(ctx, &job->parts);
         FftPlan *plan = get_plan(ctx, n, job->precision);

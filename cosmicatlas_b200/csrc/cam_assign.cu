@@ -525,15 +525,29 @@ static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const floa
     CAM_LAUNCH_NAMED(ctx, "assign_starts", brick_starts_kernel, (unsigned)std::min<int64_t>((nb + 256) / 256, 1024),
                      256, 0, table, (int)nb, G, d_total, start);
 
-    // Payload size and diagnostics back to the host (one synchronisation).
-    unsigned long long hstats[3] = {0, 0, 0};
-    CAM_CUDA_TRY(cudaMemcpyAsync(hstats, stats, sizeof(hstats), cudaMemcpyDeviceToHost, ctx->stream));
-    CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    const uint32_t total = (uint32_t)(hstats[2] & 0xffffffffu);
-    const unsigned int wmax_bits = (unsigned int)(hstats[1] & 0xffffffffu);
-    CAM_REQUIRE(!w || wmax_bits < 0x7f800000u, CAM_E_NONFINITE, "a particle weight is NaN or infinite");
-    out.n_lost = (int64_t)hstats[0];
-    out.n_in = np - out.n_lost;
+    uint64_t total = 0;
+    if (ctx->sync_free) {
+        // No host round trip (stream capture): size the payload for the
+        // provable bound, one record per touched brick and at most two
+        // bricks per axis.  Lost count and max |w| stay on the device
+        // (asg.stats) for the caller to read back with the results.
+        int per = 1;
+        for (int a = 0; a < 3; ++a) per *= (SCHEME == CAM_NGP || g.nb[a] == 1) ? 1 : 2;
+        total = (uint64_t)np * per;
+        CAM_REQUIRE(total < (1ull << 32), CAM_E_UNSUPPORTED, "payload bound exceeds 2^32 records");
+        out.n_lost = -1;
+        out.n_in = -1;
+    } else {
+        // Payload size and diagnostics back to the host (one synchronisation).
+        unsigned long long hstats[3] = {0, 0, 0};
+        CAM_CUDA_TRY(cudaMemcpyAsync(hstats, stats, sizeof(hstats), cudaMemcpyDeviceToHost, ctx->stream));
+        CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        total = (uint32_t)(hstats[2] & 0xffffffffu);
+        const unsigned int wmax_bits = (unsigned int)(hstats[1] & 0xffffffffu);
+        CAM_REQUIRE(!w || wmax_bits < 0x7f800000u, CAM_E_NONFINITE, "a particle weight is NaN or infinite");
+        out.n_lost = (int64_t)hstats[0];
+        out.n_in = np - out.n_lost;
+    }
 
     uint4 *payload = static_cast<uint4 *>(scratch(ctx, "asg.payload", std::max<size_t>(total, 1) * sizeof(uint4)));
     CAM_LAUNCH_NAMED(ctx, "assign_bin_scatter", scatter_k, G, kBinThreads, hsmem, x, y, z, w, np, chunk, g,

@@ -271,6 +271,12 @@ void c2r_impl(cam_ctx *ctx, FftPlan *p, Spectrum &s, void *out, double scale)
 
 const void *plan_twiddles(FftPlan *plan) { return plan->tw; }
 
+void free_plans(cam_ctx *ctx)
+{
+    for (auto &kv : ctx->plans) delete kv.second;
+    ctx->plans.clear();
+}
+
 FftPlan *get_plan(cam_ctx *ctx, int64_t n, int precision)
 {
     const int64_t key = n * 2 + precision;

@@ -74,6 +74,14 @@ struct cam_ctx {
     int64_t launches = 0;
     std::map<std::string, cam::DevBuf> bufs;
     std::map<int64_t, cam::FftPlan *> plans;  // key: n * 2 + precision
+    // sync_free: enqueue work only (no host round trips, results left in
+    // device buffers) -- the mode used under stream capture
+    bool sync_free = false;
+    bool capturing = false;  // inside stream capture: no allocation, no events
+    // bumped whenever a scratch buffer is (re)allocated or freed, so that
+    // captured graphs holding its old addresses can be recognised as stale
+    uint64_t gen = 0;
+    void *batch = nullptr;  // cam::BatchRunner of cam_batch_run (cam_serve.cu)
     // per-kernel timing (cam_profile_enable)
     bool prof_on = false;
     std::vector<cam::ProfRecord> prof_pending;
@@ -90,6 +98,9 @@ void prof_end(cam_ctx *ctx);
 // synchronising the stream) if the cached one is too small.
 void *scratch(cam_ctx *ctx, const char *name, size_t bytes);
 void release_all(cam_ctx *ctx);
+// Serialises device allocation/free against stream capture in other threads.
+std::mutex &alloc_mutex();
+void batch_destroy(void *batch);
 
 // Host <-> device staging helpers for the C ABI.
 template <typename T>
@@ -138,6 +149,7 @@ struct Spectrum {
 };
 
 FftPlan *get_plan(cam_ctx *ctx, int64_t n, int precision);
+void free_plans(cam_ctx *ctx);
 // Forward r2c of a real N^3 mesh; `sub` (device scalar, may be null) is
 // subtracted from every element on load.
 void fft_r2c_split(cam_ctx *ctx, FftPlan *plan, const void *real_in, const double *d_sub,
@@ -171,6 +183,12 @@ void tweb_device(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const
 // In-place exclusive prefix sum of uint32 values; *total (device, may be
 // null) receives the sum of all inputs.
 void exclusive_scan_u32(cam_ctx *ctx, uint32_t *data, int64_t n, uint32_t *total);
+cam_grid resolved_grid(const cam_grid &g);
+int nbins_for(const cam_pk_opts &o, int64_t n);
+Spectrum alloc_spectrum(cam_ctx *ctx, int64_t n, int precision, const char *tag);
+void finalize_pk(int64_t n, float L, double n_obj, const cam_pk_opts &o, int nbins, const double *sr,
+                 const double *ss, const int64_t *md, double *pk, int64_t *modes, double *kvec, cam_pk_info *info);
+
 // Deterministic FP64 sum of a device array: out[0] = sum, out[1] = sum / divisor.
 void reduce_sum_f64(cam_ctx *ctx, const double *in, int64_t n, double *out, double divisor);
 // Mean of a device mesh of precision `prec` into a device scalar (FP64).

@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdio>
 #include <cmath>
 #include <vector>
 
@@ -218,8 +219,17 @@ void power_bin(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins,
         tab[2 * (h + 1) + b] = e2;
     }
     const size_t tab_bytes = tab.size() * sizeof(double);
-    auto *d_tab = static_cast<double *>(scratch(ctx, "pk.tab", tab_bytes));
-    CAM_CUDA_TRY(cudaMemcpyAsync(d_tab, tab.data(), tab_bytes, cudaMemcpyHostToDevice, ctx->stream));
+    // One table buffer per (N, scheme, corrections, edges), whose contents
+    // the key determines: it is uploaded once, when created.  A captured
+    // graph keeps reading the buffer it was captured with, and later calls
+    // skip the upload (a pageable copy that would wait for the stream).
+    char key[160];
+    snprintf(key, sizeof(key), "pk.tab.%d.%d.%d.%d.%d.%.17g.%.17g", n, p, o.mas_correction, o.sn_correction, nbins,
+             o.DeltaKmin, o.ndel);
+    const auto found = ctx->bufs.find(key);
+    const bool fresh = found == ctx->bufs.end() || found->second.ptr == nullptr;
+    auto *d_tab = static_cast<double *>(scratch(ctx, key, tab_bytes));
+    if (fresh) CAM_CUDA_TRY(cudaMemcpyAsync(d_tab, tab.data(), tab_bytes, cudaMemcpyHostToDevice, ctx->stream));
 
     const int grid = kNumSMs * 2;
     const int64_t nrows = (int64_t)n * n;
@@ -243,6 +253,7 @@ void power_bin(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins,
                    d_tab, nbins, m_u, inv_s, rpc, part, pm);
     }
     CAM_LAUNCH(ctx, pk_final_kernel, nbins, 256, 0, part, pm, grid, nbins, res, resm);
+    if (ctx->sync_free) return;  // sums stay in pk.res / pk.resm for the caller
     std::vector<double> hres(2 * nbins);
     std::vector<unsigned long long> hm(nbins);
     CAM_CUDA_TRY(cudaMemcpyAsync(hres.data(), res, 2 * nbins * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));

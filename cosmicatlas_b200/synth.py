@@ -42,6 +42,27 @@ def clumped(n: int, box: float, n_clumps: int, sigma: float, clump_frac: float =
     return pos[0].copy(), pos[1].copy(), pos[2].copy()
 
 
+def clumped_torch(n: int, box: float, n_clumps: int, sigma: float, clump_frac: float = 0.8, seed: int = 0,
+                  device: str = "cuda"):
+    """The clumped process of ``clumped`` drawn with torch on `device` (a
+    different random stream than the numpy version, same distribution):
+    returns float32 tensors x, y, z wrapped into [0, box)."""
+    import torch
+    g = torch.Generator(device=device).manual_seed(seed)
+    n_cl = int(round(n * clump_frac))
+    n_un = n - n_cl
+    pos = torch.empty((3, n), dtype=torch.float64, device=device)
+    pos[:, :n_un] = torch.rand((3, n_un), generator=g, device=device, dtype=torch.float64) * box
+    if n_cl:
+        centres = torch.rand((3, n_clumps), generator=g, device=device, dtype=torch.float64) * box
+        which = torch.randint(0, n_clumps, (n_cl,), generator=g, device=device)
+        pos[:, n_un:] = centres[:, which] + sigma * torch.randn((3, n_cl), generator=g, device=device,
+                                                               dtype=torch.float64)
+    f = torch.remainder(pos, box).to(torch.float32)
+    f[f >= box] = 0.0
+    return f[0].contiguous(), f[1].contiguous(), f[2].contiguous()
+
+
 def halo_masses(n: int, mu: float = 12.5, sigma: float = 0.5, lo: float = 11.0, hi: float = 15.0, seed: int = 0):
     rng = np.random.default_rng(seed)
     out = np.empty(n, np.float64)

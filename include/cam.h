@@ -209,6 +209,62 @@ int cam_job_run(cam_ctx *ctx, const cam_job_desc *job, cam_job_result *res);
  * e.g. Source/Catalog.cpp:662-683). */
 int cam_particles_stage(cam_ctx *ctx, const cam_particles *host, cam_particles *device_out);
 
+/* ---- many jobs: graph-packed batches and a continuous-batching server ---
+ * No single counterpart in the reference: BAM issues its mesh jobs one
+ * after another from the calibration loop (Source/Bam.cpp:13424,
+ * Bam::bamrunner), one cam_job_run each.  Both entry points below return,
+ * per job, exactly what cam_job_run returns for it (same kernels, every job
+ * on its own buffers), except that labels are not returned by batches.
+ *
+ * cam_batch_run: consecutive jobs of one shape (mesh, particle count,
+ * weights or not, scheme, precision, box and all P(k)/T-web options equal)
+ * run as batches of up to 32 concurrent jobs.  The first batch of a shape
+ * sizes every buffer; its work is then captured into one CUDA graph, and
+ * later batches of that shape copy their particles in and replay it: one
+ * host synchronisation per batch instead of several per job.
+ * res[i].labels must be NULL.  Returns CAM_OK or the first failing job's
+ * status (the other jobs' results are still filled in). */
+int cam_batch_run(cam_ctx *ctx, const cam_job_desc *jobs, int njobs, cam_job_result *res);
+
+typedef struct cam_server cam_server;
+
+typedef struct {
+    int64_t submitted, completed, failed;
+    int64_t queued, running;          /* at the time of the call            */
+    int64_t batches, batched_jobs;    /* graph-packed batches and their jobs */
+    int64_t graph_replays;            /* batches that replayed a graph      */
+    size_t bytes_reserved;            /* HBM held or reserved by the workers */
+    size_t peak_bytes_reserved;
+    size_t budget;
+    double p50_ms, p99_ms, mean_ms, max_ms;  /* submit -> result latency    */
+} cam_server_stats;
+
+/* Starts a server on `device` with `nworkers` worker threads (each runs
+ * jobs on its own stream, so their work overlaps on the GPU).  A queued job
+ * starts as soon as a worker is free and the server's device memory (held
+ * caches plus the reservations of running jobs) stays within hbm_budget
+ * (0 = 80% of the free memory); jobs are admitted in submission order.
+ * When several queued jobs share a small shape (N <= 128, no labels), a
+ * worker takes up to max_batch of them and runs them as one graph-packed
+ * batch, as cam_batch_run does. */
+int cam_server_create(int device, size_t hbm_budget, int nworkers, int max_batch, cam_server **out);
+/* Queues a job.  The descriptor is copied; the particle arrays and the
+ * result's output arrays must stay valid until the job completes.
+ * CAM_E_NOMEM if the job alone exceeds the budget, CAM_E_INVAL for an
+ * invalid job, CAM_E_BUSY if 2^20 jobs are queued. */
+int cam_server_submit(cam_server *s, const cam_job_desc *job, cam_job_result *res, uint64_t *id);
+/* CAM_E_BUSY while queued or running, else the job's final status (once:
+ * later calls for the same id return CAM_E_NOTFOUND). */
+int cam_server_poll(cam_server *s, uint64_t id);
+/* Waits up to timeout_us (< 0: no limit); CAM_E_TIMEOUT if still running,
+ * else as cam_server_poll. */
+int cam_server_wait(cam_server *s, uint64_t id, int64_t timeout_us);
+/* Counters and latency percentiles; reset != 0 clears the latency record
+ * and the counters after reading them. */
+int cam_server_stats_get(cam_server *s, cam_server_stats *st, int reset);
+/* Finishes the queued and running jobs, then stops the workers. */
+int cam_server_destroy(cam_server *s);
+
 /* ---- power spectrum without device allocation --------------------------
  * No counterpart in the reference.  For callers that may not allocate
  * device memory -- code running inside a memory pool or arena it does not

@@ -55,3 +55,20 @@ def test_no_device_means_invalid_context():
         assert L.lib().cam_ctx_destroy(h) == L.CAM_OK
     else:
         assert rc in (L.CAM_E_INVAL, L.CAM_E_CUDA)
+
+
+def test_server_and_batch_reject_bad_arguments_without_device():
+    # Host-side argument checks of the serving entry points; no device work.
+    import ctypes
+    lib = L.lib()
+    h = ctypes.c_void_p()
+    assert lib.cam_server_create(0, 0, 0, 8, ctypes.byref(h)) == L.CAM_E_INVAL   # no workers
+    assert lib.cam_server_create(0, 0, 2, 0, ctypes.byref(h)) == L.CAM_E_INVAL   # no batch
+    assert lib.cam_server_create(0, 0, 2, 33, ctypes.byref(h)) == L.CAM_E_INVAL  # batch > 32
+    assert lib.cam_server_create(-1, 0, 2, 8, ctypes.byref(h)) == L.CAM_E_INVAL  # no such device
+    assert lib.cam_batch_run(None, None, 0, None) == L.CAM_E_INVAL
+    assert lib.cam_server_submit(None, None, None, None) == L.CAM_E_INVAL
+    assert lib.cam_server_poll(None, 1) == L.CAM_E_INVAL
+    assert lib.cam_server_wait(None, 1, 0) == L.CAM_E_INVAL
+    assert lib.cam_server_stats_get(None, None, 0) == L.CAM_E_INVAL
+    assert lib.cam_server_destroy(None) == L.CAM_E_INVAL
