@@ -586,9 +586,26 @@ def run_stream(args):
                 srv.wait(jid)
             wall = time.perf_counter() - t_start
             st = srv.stats()
+            tr = srv.trace()
+        tr = tr[-njobs:]
+        wait = tr["start_ms"] - tr["submit_ms"]
+        run = tr["end_ms"] - tr["start_ms"]
+        big = tr["big"] == 1
+        free_gb = torch.cuda.mem_get_info()[0] / 1e9
+
+        def pct(v):
+            return [round(float(np.percentile(v, q)), 2) for q in (50, 99)] if len(v) else None
         return {"jobs_per_s": round(njobs / wall, 1), "p50_ms": round(st["p50_ms"], 2),
                 "p99_ms": round(st["p99_ms"], 2), "batches": st["batches"], "batched_jobs": st["batched_jobs"],
-                "graph_replays": st["graph_replays"], "peak_reserved_gb": round(st["peak_bytes_reserved"] / 1e9, 1)}
+                "graph_replays": st["graph_replays"], "peak_reserved_gb": round(st["peak_bytes_reserved"] / 1e9, 1),
+                "trace": {"queue_wait_p50_p99": pct(wait), "run_big_p50_p99": pct(run[big]),
+                          "run_small_p50_p99": pct(run[~big]), "big_jobs": int(big.sum()),
+                          "worker_busy_s": round(float(np.sum(np.unique(np.stack([tr["worker"], tr["start_ms"],
+                                                                                  tr["end_ms"]], 1), axis=0)[:, 2]
+                                                             - np.unique(np.stack([tr["worker"], tr["start_ms"],
+                                                                                   tr["end_ms"]], 1), axis=0)[:, 1])
+                                                  / 1e3), 2),
+                          "device_free_gb_after": round(free_gb, 1)}}
 
     rates = [float(r) for r in args.rates.split(",") if r]
     out = {"workload": f"served mixed stream: {njobs} jobs, N in 64..512, N_p log-uniform [1e5, 5e7], "

@@ -86,6 +86,12 @@ class ServerStats(ctypes.Structure):
                 ("mean_ms", ctypes.c_double), ("max_ms", ctypes.c_double)]
 
 
+class JobTrace(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_uint64), ("submit_ms", ctypes.c_double), ("start_ms", ctypes.c_double),
+                ("end_ms", ctypes.c_double), ("worker", ctypes.c_int), ("batch", ctypes.c_int),
+                ("status", ctypes.c_int), ("big", ctypes.c_int)]
+
+
 # Exported symbols with their signatures; the non-GPU tests check every one
 # of these resolves.
 _P = ctypes.c_void_p
@@ -123,6 +129,8 @@ SIGNATURES = {
     "cam_server_poll": ([_P, ctypes.c_uint64], ctypes.c_int),
     "cam_server_wait": ([_P, ctypes.c_uint64, ctypes.c_int64], ctypes.c_int),
     "cam_server_stats_get": ([_P, ctypes.POINTER(ServerStats), ctypes.c_int], ctypes.c_int),
+    "cam_server_last_error": ([_P], ctypes.c_char_p),
+    "cam_server_trace": ([_P, ctypes.POINTER(JobTrace), ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "cam_server_destroy": ([_P], ctypes.c_int),
 }
 

@@ -361,7 +361,7 @@ class Server:
             raise TimeoutError(f"job {jid} still running")
         self._jobs.pop(jid)
         if rc != L.CAM_OK:
-            raise CamError(rc, f"job {jid} failed")
+            raise CamError(rc, f"job {jid} failed ({self._lib.cam_server_last_error(self.h).decode()})")
         return job.result()
 
     def poll(self, jid: int) -> bool:
@@ -378,6 +378,18 @@ class Server:
         if rc != L.CAM_OK:
             raise CamError(rc, "cam_server_stats_get failed")
         return {f: getattr(st, f) for f, _ in L.ServerStats._fields_}
+
+    def trace(self, max_records: int = 1 << 20) -> np.ndarray:
+        """Completed jobs since the last call: structured array with id,
+        submit_ms, start_ms, end_ms, worker, batch, status, big."""
+        buf = (L.JobTrace * max_records)()
+        cnt = ctypes.c_int()
+        rc = self._lib.cam_server_trace(self.h, buf, max_records, ctypes.byref(cnt))
+        if rc != L.CAM_OK:
+            raise CamError(rc, "cam_server_trace failed")
+        dt = np.dtype([(f, np.uint64 if f == "id" else (np.float64 if f.endswith("_ms") else np.int32))
+                       for f, _ in L.JobTrace._fields_])
+        return np.array([tuple(getattr(r, f) for f, _ in L.JobTrace._fields_) for r in buf[:cnt.value]], dtype=dt)
 
     def close(self):
         if self.h:

@@ -12,29 +12,61 @@
 
 namespace cam {
 
+// Library-owned stream-ordered memory pool per device.  Scratch buffers
+// grow and shrink without cudaMalloc/cudaFree, whose implicit device-wide
+// synchronisation would stall every other context's work (the serving
+// workers run concurrently).  Freed blocks are kept for reuse (release
+// threshold: unlimited) and are only handed out again once their free has
+// completed on the GPU (no reuse through stream dependencies), so a buffer
+// allocated on one stream is safe to use from any stream.
+cudaMemPool_t device_pool(int device)
+{
+    static std::mutex m;
+    static cudaMemPool_t pools[64] = {};
+    CAM_REQUIRE(device >= 0 && device < 64, CAM_E_INVAL, "device index out of range");
+    std::lock_guard<std::mutex> lk(m);
+    if (!pools[device]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t p = nullptr;
+        CAM_CUDA_TRY(cudaMemPoolCreate(&p, &props));
+        uint64_t keep = ~0ull;
+        int no = 0;
+        CAM_CUDA_TRY(cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep));
+        CAM_CUDA_TRY(cudaMemPoolSetAttribute(p, cudaMemPoolReuseFollowEventDependencies, &no));
+        CAM_CUDA_TRY(cudaMemPoolSetAttribute(p, cudaMemPoolReuseAllowInternalDependencies, &no));
+        pools[device] = p;
+    }
+    return pools[device];
+}
+
 void *scratch(cam_ctx *ctx, const char *name, size_t bytes)
 {
     bytes = std::max<size_t>(bytes, 256);
     DevBuf &b = ctx->bufs[name];
     if (b.cap >= bytes) return b.ptr;
     CAM_REQUIRE(!ctx->capturing, CAM_E_BUSY, std::string("buffer ") + name + " would grow during stream capture");
-    const size_t want = std::max(bytes, b.cap + b.cap / 4);
+    const size_t want = std::max(bytes, b.cap + b.cap / 2);
     if (ctx->budget && ctx->used - b.cap + want > ctx->budget)
         throw Error{CAM_E_NOMEM, std::string("HBM budget exceeded allocating ") + name};
+    cudaMemPool_t pool = device_pool(ctx->device);
     std::lock_guard<std::mutex> lk(alloc_mutex());
     ctx->gen++;
     if (b.ptr) {
-        CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-        CAM_CUDA_TRY(cudaFree(b.ptr));
+        // stream-ordered: the work already queued on this stream that reads
+        // the old buffer completes before the memory is released
+        CAM_CUDA_TRY(cudaFreeAsync(b.ptr, ctx->stream));
         ctx->used -= b.cap;
         b.ptr = nullptr;
         b.cap = 0;
     }
     void *p = nullptr;
-    cudaError_t e = cudaMalloc(&p, want);
+    cudaError_t e = cudaMallocFromPoolAsync(&p, want, pool, ctx->stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        throw Error{CAM_E_NOMEM, std::string("cudaMalloc failed for ") + name + ": " + cudaGetErrorString(e)};
+        throw Error{CAM_E_NOMEM, std::string("device allocation failed for ") + name + ": " + cudaGetErrorString(e)};
     }
     b.ptr = p;
     b.cap = want;
@@ -83,6 +115,20 @@ static void prof_collect(cam_ctx *ctx)
     ctx->prof_pending.clear();
 }
 
+void smem_limit(const void *func, size_t bytes)
+{
+    static std::mutex m;
+    static std::map<std::pair<int, const void *>, size_t> cur;
+    if (bytes <= 48 * 1024) return;  // within the default limit
+    int dev = 0;
+    CAM_CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(m);
+    size_t &c = cur[{dev, func}];
+    if (c >= bytes) return;
+    CAM_CUDA_TRY(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    c = bytes;
+}
+
 std::mutex &alloc_mutex()
 {
     static std::mutex m;
@@ -93,12 +139,20 @@ void release_all(cam_ctx *ctx)
 {
     std::lock_guard<std::mutex> lk(alloc_mutex());
     ctx->gen++;
-    cudaStreamSynchronize(ctx->stream);
     free_plans(ctx);  // their twiddles live in the buffers freed below
     for (auto &kv : ctx->bufs)
-        if (kv.second.ptr) cudaFree(kv.second.ptr);
+        if (kv.second.ptr) cudaFreeAsync(kv.second.ptr, ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
     ctx->bufs.clear();
     ctx->used = 0;
+    // hand the pool's idle memory back to the device
+    if (ctx->device >= 0 && ctx->device < 64) {
+        try {
+            cudaMemPoolTrimTo(device_pool(ctx->device), 0);
+        } catch (const Error &) {
+        }
+    }
+    cudaGetLastError();
 }
 
 namespace {

@@ -516,8 +516,8 @@ static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const floa
     auto scatter_k = smem_hist ? (vec ? bin_kernel<SCHEME, true, true, true> : bin_kernel<SCHEME, true, true, false>)
                                : (vec ? bin_kernel<SCHEME, true, false, true> : bin_kernel<SCHEME, true, false, false>);
     if (hsmem > 48 * 1024) {
-        CAM_CUDA_TRY(cudaFuncSetAttribute(count_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem));
-        CAM_CUDA_TRY(cudaFuncSetAttribute(scatter_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem));
+        smem_at_least(count_k, hsmem);
+        smem_at_least(scatter_k, hsmem);
     }
     CAM_LAUNCH_NAMED(ctx, "assign_bin_count", count_k, G, kBinThreads, hsmem, x, y, z, w, np, chunk, g, (int)nb,
                      table, (uint4 *)nullptr, d_lost, d_wmax);
@@ -557,7 +557,7 @@ static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const floa
     CAM_REQUIRE(smem <= 200 * 1024, CAM_E_UNSUPPORTED, "brick tile too large");
     const int weighted = w != nullptr;
     auto launch_dep = [&](auto kern, auto *mesh) {
-        CAM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        smem_at_least(kern, smem);
         CAM_LAUNCH_NAMED(ctx, "assign_deposit", kern, (unsigned)nb, kDepositThreads, smem, payload, start, g, d_wmax,
                          weighted, mesh, bsum);
     };

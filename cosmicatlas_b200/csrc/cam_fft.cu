@@ -218,7 +218,7 @@ void cols_impl(cam_ctx *ctx, FftPlan *p, void *base, int64_t len, int64_t ncols,
     dispatch_fft_len(len, [&](auto lc) {
         constexpr int LEN = decltype(lc)::value;
         auto kern = inv ? fft_cols_kernel<T, true, LEN> : fft_cols_kernel<T, false, LEN>;
-        CAM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        smem_at_least(kern, smem);
         CAM_LAUNCH_NAMED(ctx, "fft_cols", kern, grid, nthr, smem, static_cast<C *>(base), (int)len, (int)ncols,
                          jstride, pstride, ccomp, rd, static_cast<const C *>(p->tw), twmul);
     });
@@ -239,7 +239,7 @@ void rows_impl(cam_ctx *ctx, FftPlan *p, const void *in, void *out, void *nyq, i
     dispatch_fft_len(len, [&](auto lc) {
     constexpr int LEN = decltype(lc)::value;
     auto kern = fft_rows_kernel<T, MODE, LEN>;
-    CAM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    smem_at_least(kern, smem);
     CAM_LAUNCH_NAMED(ctx, MODE == 0 ? "fft_rows_r2c" : MODE == 1 ? "fft_rows_c2r" : "fft_rows_c2c", kern, grid, nthr, smem, in, out, static_cast<C *>(nyq), n, nrows, rpc,
                ccomp_in, ccomp_out, rd, static_cast<const C *>(p->tw), d_sub, scale);
     });

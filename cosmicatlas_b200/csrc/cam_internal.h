@@ -100,6 +100,15 @@ void *scratch(cam_ctx *ctx, const char *name, size_t bytes);
 void release_all(cam_ctx *ctx);
 // Serialises device allocation/free against stream capture in other threads.
 std::mutex &alloc_mutex();
+// Raises a kernel's dynamic shared-memory limit on the current device to at
+// least `bytes`, never lowering it: another thread may be about to launch
+// the same kernel with a larger size.
+void smem_limit(const void *func, size_t bytes);
+template <typename K>
+inline void smem_at_least(K *kern, size_t bytes)
+{
+    smem_limit(reinterpret_cast<const void *>(kern), bytes);
+}
 void batch_destroy(void *batch);
 
 // Host <-> device staging helpers for the C ABI.

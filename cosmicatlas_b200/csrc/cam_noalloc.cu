@@ -216,6 +216,25 @@ int na_scratch(int dev, void **out)
     return CAM_OK;
 }
 
+// The kernels' dynamic shared-memory limit on the current device is only
+// ever raised: a concurrent call on another stream or thread may be about to
+// launch with a larger size than this one.
+cudaError_t raise_smem_limit(int precision, size_t smem)
+{
+    static std::mutex m;
+    static size_t cur[2][64];
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= 64) return e != cudaSuccess ? e : cudaErrorInvalidDevice;
+    const int p = precision == CAM_F32 ? 0 : 1;
+    std::lock_guard<std::mutex> lk(m);
+    if (cur[p][dev] >= smem) return cudaSuccess;
+    e = p == 0 ? cudaFuncSetAttribute(na_bin_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+               : cudaFuncSetAttribute(na_bin_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) cur[p][dev] = smem;
+    return e;
+}
+
 }  // namespace
 
 extern "C" int cam_power_noalloc(const void *spec, int64_t n, int precision, float box, double n_obj,
@@ -273,16 +292,13 @@ extern "C" int cam_power_noalloc(const void *spec, int64_t n, int precision, flo
     const int64_t rpc = ((int64_t)n * n + kNaCtas - 1) / kNaCtas;
     const float m_u = (float)opts->DeltaKmin, inv_s = (float)(1.0 / opts->ndel);
     cudaError_t e = cudaMemcpyAsync(tab, htab, tab_bytes, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = raise_smem_limit(precision, smem);
     if (e == cudaSuccess) {
         if (precision == CAM_F32) {
-            e = cudaFuncSetAttribute(na_bin_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e == cudaSuccess)
-                na_bin_kernel<float2><<<kNaCtas, kNaThreads, smem, st>>>(static_cast<const float2 *>(spec), (int)n, tab,
+            na_bin_kernel<float2><<<kNaCtas, kNaThreads, smem, st>>>(static_cast<const float2 *>(spec), (int)n, tab,
                                                                          nbins, m_u, inv_s, rpc, part, pm);
         } else {
-            e = cudaFuncSetAttribute(na_bin_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e == cudaSuccess)
-                na_bin_kernel<double2><<<kNaCtas, kNaThreads, smem, st>>>(static_cast<const double2 *>(spec), (int)n,
+            na_bin_kernel<double2><<<kNaCtas, kNaThreads, smem, st>>>(static_cast<const double2 *>(spec), (int)n,
                                                                           tab, nbins, m_u, inv_s, rpc, part, pm);
         }
     }

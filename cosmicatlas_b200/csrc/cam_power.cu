@@ -243,12 +243,12 @@ void power_bin(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins,
     const float m_u = (float)o.DeltaKmin, inv_s = (float)(1.0 / o.ndel);
     if (s.precision == CAM_F32) {
         auto kern = pk_bin_kernel<float2>;
-        CAM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        smem_at_least(kern, smem);
         CAM_LAUNCH_NAMED(ctx, "pk_bin", kern, grid, kPkThreads, smem, (const float2 *)s.main, (const float2 *)s.nyq, n,
                    d_tab, nbins, m_u, inv_s, rpc, part, pm);
     } else {
         auto kern = pk_bin_kernel<double2>;
-        CAM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        smem_at_least(kern, smem);
         CAM_LAUNCH_NAMED(ctx, "pk_bin", kern, grid, kPkThreads, smem, (const double2 *)s.main, (const double2 *)s.nyq, n,
                    d_tab, nbins, m_u, inv_s, rpc, part, pm);
     }

@@ -58,21 +58,18 @@ struct Slot {
     cam_ctx *c = nullptr;
     unsigned char *pin = nullptr;
     size_t pin_bytes = 0;
-    float *in[4] = {nullptr, nullptr, nullptr, nullptr};
-    size_t in_cap = 0;
-    uint64_t local_gen = 0;  // bumped when `in` or `pin` is reallocated
+    float *in[4] = {nullptr, nullptr, nullptr, nullptr};  // scratch of c
+    uint64_t local_gen = 0;  // bumped when `pin` is reallocated
     uint64_t gen() const { return c->gen + local_gen; }
-    size_t device_bytes() const { return c->used + 4 * in_cap * sizeof(float); }
+    size_t device_bytes() const { return c->used; }
     ~Slot()
     {
         if (!c) return;
         cudaSetDevice(c->device);
         cudaStreamSynchronize(c->stream);
-        {
+        if (pin) {
             std::lock_guard<std::mutex> lk(alloc_mutex());
-            for (auto *p : in)
-                if (p) cudaFree(p);
-            if (pin) cudaFreeHost(pin);
+            cudaFreeHost(pin);
         }
         cam_ctx_destroy(c);  // takes the allocation mutex itself
     }
@@ -129,18 +126,12 @@ Slot *make_slot(int device)
 void ensure_slot(Slot &s, const cam_job_desc &d)
 {
     const size_t np = (size_t)std::max<int64_t>(d.parts.n, 1);
-    if (s.in_cap < np) {
-        std::lock_guard<std::mutex> lk(alloc_mutex());
-        CAM_CUDA_TRY(cudaStreamSynchronize(s.c->stream));
-        s.local_gen++;
-        for (auto *&p : s.in) {
-            if (p) cudaFree(p);
-            p = nullptr;
-        }
-        s.in_cap = 0;
-        for (auto *&p : s.in) CAM_CUDA_TRY(cudaMalloc(&p, np * sizeof(float)));
-        s.in_cap = np;
-    }
+    static const char *names[4] = {"slot.x", "slot.y", "slot.z", "slot.w"};
+    const uint64_t g0 = s.c->gen;
+    for (int a = 0; a < 4; ++a) s.in[a] = static_cast<float *>(scratch(s.c, names[a], np * sizeof(float)));
+    // inputs are written on the batch's main stream: let a fresh allocation
+    // (ordered on the slot's stream) complete first
+    if (s.c->gen != g0) CAM_CUDA_TRY(cudaStreamSynchronize(s.c->stream));
     const int nb = want_pk(d) ? nbins_for(d.pk, d.grid.n[0]) : 0;
     const size_t need = sizeof(MirrorHead) + (size_t)nb * 3 * 8;
     if (s.pin_bytes < need) {
@@ -330,18 +321,22 @@ struct BatchRunner {
         return g;
     }
 
-    // Runs B same-shaped jobs and fills res[] and rc[] (per-job status).
-    // capture_after: uncaptured runs of a batch key before it is captured
-    // (0 = never capture).
+    // Runs B jobs concurrently (one slot each) and fills res[] and rc[]
+    // (per-job status).  Jobs of one shape are captured into a graph after
+    // `capture_after` uncaptured runs of that batch (0 = never) and replayed
+    // from then on; jobs of mixed shapes always run uncaptured.
     void run(const cam_job_desc *jobs, int B, cam_job_result *res, int *rc, int capture_after)
     {
         ensure_slots(B);
         for (int j = 0; j < B; ++j) ensure_slot(*slots[j], jobs[j]);
+        const std::string key = std::to_string(B) + "#" + shape_key(jobs[0]);
+        bool same = true;
+        for (int j = 1; j < B && same; ++j) same = shape_key(jobs[j]) == shape_key(jobs[0]);
+        if (!same) capture_after = 0;
         // A graph holds the addresses of the slot buffers it was captured
         // with: if any of them was reallocated since, drop the graph.
-        const std::string key = std::to_string(B) + "#" + shape_key(jobs[0]);
         GraphEntry *ge = nullptr;
-        for (auto it = graphs.begin(); it != graphs.end(); ++it) {
+        for (auto it = graphs.begin(); same && it != graphs.end(); ++it) {
             if (it->key != key) continue;
             if (it->gens == gens(B)) {
                 ge = &*it;
@@ -417,9 +412,11 @@ struct cam_server {
         std::chrono::steady_clock::time_point t_submit;
         size_t footprint;
         std::string shape;
-        bool batchable;
+        bool batchable;  // small mesh, no labels: may share a batch
+        bool big;        // fills the GPU alone: at most max_big run at once
     };
     struct Worker {
+        int index = 0;
         cam_ctx *ctx = nullptr;
         std::unique_ptr<BatchRunner> br;
         size_t held = 0;      // device bytes cached between jobs
@@ -429,7 +426,13 @@ struct cam_server {
     int device = 0;
     size_t budget = 0;
     int max_batch = 16;
-    int64_t small_n = 128;  // meshes up to 128^3 are packed into graph batches
+    int64_t small_n = 128;  // meshes up to 128^3 are packed into batches
+    int max_big = 1;        // large jobs running at once (they contend for L2)
+    int big_running = 0;
+    // Large jobs run on one shared context (max_big == 1), so their
+    // multi-GB buffers exist once instead of once per worker.
+    cam_ctx *big_ctx = nullptr;
+    size_t big_held = 0;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<Job> queue;
@@ -439,13 +442,16 @@ struct cam_server {
     uint64_t next_id = 1;
     size_t peak_reserved = 0;
     int64_t submitted = 0, completed = 0, failed = 0, batches = 0, batched_jobs = 0, replays = 0;
-    bool trim = false;  // the queue head does not fit: idle workers drop caches
+    std::string last_err;  // message of the most recent failed job
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    std::vector<cam_server_job_trace> trace;  // completed jobs, oldest first
+    bool trim = false;     // the queue head does not fit: idle workers drop caches
     bool stop = false;
     std::vector<std::unique_ptr<Worker>> workers;
 
     size_t reserved() const
     {
-        size_t r = 0;
+        size_t r = big_held;
         for (auto &w : workers) r += w->held + w->inflight;
         return r;
     }
@@ -457,15 +463,29 @@ struct cam_server {
         w.held = 0;
     }
 
-    // Under `mu`: takes the queue head (and, for a small shape, queued jobs
-    // of the same shape) if it fits the budget.
+    // Under `mu`: picks the oldest queued job that may start (a large job
+    // waits while max_big large jobs run; smaller jobs may pass it) and, if
+    // it is batchable, more batchable queued jobs -- of its own shape when
+    // there are several (a graph can be replayed), else of any shape -- up
+    // to max_batch, as far as the HBM budget allows.
     bool admit(Worker &w, std::vector<Job> &take)
     {
-        const Job &h = queue.front();
-        std::vector<size_t> pick{0};
-        if (h.batchable)
-            for (size_t i = 1; i < queue.size() && (int)pick.size() < max_batch; ++i)
-                if (queue[i].batchable && queue[i].shape == h.shape) pick.push_back(i);
+        size_t h = queue.size();
+        for (size_t i = 0; i < queue.size() && i < 1024; ++i)
+            if (!queue[i].big || big_running < max_big) {
+                h = i;
+                break;
+            }
+        if (h == queue.size()) return false;
+        const Job &hd = queue[h];
+        std::vector<size_t> pick{h};
+        if (hd.batchable) {
+            for (size_t i = h + 1; i < queue.size() && (int)pick.size() < max_batch; ++i)
+                if (queue[i].batchable && queue[i].shape == hd.shape) pick.push_back(i);
+            if (pick.size() == 1)
+                for (size_t i = h + 1; i < queue.size() && i < h + 1024 && (int)pick.size() < max_batch; ++i)
+                    if (queue[i].batchable) pick.push_back(i);
+        }
         size_t need = 0;
         for (size_t i : pick) need += queue[i].footprint;
         const size_t r = reserved();
@@ -473,6 +493,8 @@ struct cam_server {
             need -= queue[pick.back()].footprint;
             pick.pop_back();
         }
+        // a large job reuses the shared context's cached buffers
+        if (hd.big) need = need > big_held ? need - big_held : 0;
         if (r + need > budget) {
             if (w.held > 0 && r - w.held + need <= budget) {
                 drop_cache(w);
@@ -489,6 +511,7 @@ struct cam_server {
             queue.erase(queue.begin() + (long)*it);
         }
         std::reverse(take.begin(), take.end());
+        for (auto &j : take) big_running += j.big;
         w.inflight = need;
         n_running += (int64_t)take.size();
         peak_reserved = std::max(peak_reserved, reserved());
@@ -505,6 +528,10 @@ struct cam_server {
                 std::unique_lock<std::mutex> lk(mu);
                 for (;;) {
                     if (trim && w.held > 0) drop_cache(w);
+                    if (trim && big_running == 0 && big_held > 0) {
+                        release_all(big_ctx);
+                        big_held = 0;
+                    }
                     if (!queue.empty() && admit(w, take)) break;
                     if (stop && queue.empty()) break;
                     cv_work.wait(lk);
@@ -513,9 +540,13 @@ struct cam_server {
             }
             std::vector<int> rcs(take.size(), CAM_OK);
             int64_t rp = 0;
+            std::string msg;
+            const auto t_start = std::chrono::steady_clock::now();
             try {
                 if (take.size() == 1) {
-                    rcs[0] = cam_job_run(w.ctx, &take[0].desc, take[0].res);
+                    cam_ctx *c = take[0].big ? big_ctx : w.ctx;
+                    rcs[0] = cam_job_run(c, &take[0].desc, take[0].res);
+                    if (rcs[0] != CAM_OK) msg = cam_last_error(c);
                 } else {
                     if (!w.br) w.br.reset(new BatchRunner(device));
                     std::vector<cam_job_desc> d(take.size());
@@ -526,24 +557,38 @@ struct cam_server {
                     }
                     const int64_t before = w.br->replays;
                     w.br->run(d.data(), (int)take.size(), r.data(), rcs.data(),
-                              (int)take.size() == max_batch ? 1 : 2);
+                              (int)take.size() == max_batch ? 1 : 2);  // mixed shapes: never captured
                     rp = w.br->replays - before;
-                    for (size_t i = 0; i < take.size(); ++i) *take[i].res = r[i];
+                    for (size_t i = 0; i < take.size(); ++i) {
+                        *take[i].res = r[i];
+                        if (rcs[i] != CAM_OK) msg = "a particle weight is NaN or infinite";
+                    }
                 }
             } catch (const Error &e) {
                 for (auto &rc : rcs) rc = e.code;
+                msg = e.msg;
             } catch (...) {
                 for (auto &rc : rcs) rc = CAM_E_CUDA;
+                msg = "unexpected exception";
             }
             const auto now = std::chrono::steady_clock::now();
             {
                 std::lock_guard<std::mutex> lk(mu);
                 w.inflight = 0;
                 w.held = w.ctx->used + (w.br ? w.br->device_bytes() : 0);
+                if (take.size() == 1 && take[0].big) big_held = big_ctx->used;
                 n_running -= (int64_t)take.size();
+                for (auto &j : take) big_running -= j.big;
+                if (!msg.empty()) last_err = msg;
+                auto since = [&](std::chrono::steady_clock::time_point t) {
+                    return std::chrono::duration<double, std::milli>(t - t0).count();
+                };
                 for (size_t i = 0; i < take.size(); ++i) {
                     const double ms = std::chrono::duration<double, std::milli>(now - take[i].t_submit).count();
                     done[take[i].id] = rcs[i];
+                    if (trace.size() >= (1u << 20)) trace.erase(trace.begin(), trace.begin() + (1u << 19));
+                    trace.push_back(cam_server_job_trace{take[i].id, since(take[i].t_submit), since(t_start), since(now),
+                                                         w.index, (int)take.size(), rcs[i], take[i].big ? 1 : 0});
                     if (lat_ms.size() >= (1u << 22)) lat_ms.erase(lat_ms.begin(), lat_ms.begin() + (1u << 21));
                     lat_ms.push_back(ms);
                     ++completed;
@@ -620,11 +665,17 @@ int cam_server_create(int device, size_t hbm_budget, int nworkers, int max_batch
     }
     s->budget = hbm_budget;
     s->max_batch = max_batch;
+    {
+        const int rc = cam_ctx_create(device, 0, &s->big_ctx);
+        if (rc != CAM_OK) return rc;
+    }
     for (int i = 0; i < nworkers; ++i) {
         std::unique_ptr<cam_server::Worker> w(new cam_server::Worker);
+        w->index = i;
         const int rc = cam_ctx_create(device, 0, &w->ctx);
         if (rc != CAM_OK) {
             for (auto &x : s->workers) cam_ctx_destroy(x->ctx);
+            cam_ctx_destroy(s->big_ctx);
             return rc;
         }
         s->workers.push_back(std::move(w));
@@ -651,7 +702,10 @@ int cam_server_submit(cam_server *s, const cam_job_desc *job, cam_job_result *re
     j.res = res;
     j.footprint = job_footprint(*job);
     j.shape = shape_key(*job);
-    j.batchable = job->grid.n[0] <= s->small_n && res->labels == nullptr && s->max_batch > 1;
+    // a job that moves more than ~0.75 GB through HBM fills the GPU by itself
+    const double ncell = (double)job->grid.n[0] * (double)job->grid.n[1] * (double)job->grid.n[2];
+    j.big = (double)job->parts.n * 64.0 + ncell * 48.0 > 768.0 * (1 << 20);
+    j.batchable = !j.big && job->grid.n[0] <= s->small_n && res->labels == nullptr && s->max_batch > 1;
     j.t_submit = std::chrono::steady_clock::now();
     {
         std::lock_guard<std::mutex> lk(s->mu);
@@ -748,6 +802,26 @@ int cam_server_stats_get(cam_server *s, cam_server_stats *st, int reset)
     return CAM_OK;
 }
 
+int cam_server_trace(cam_server *s, cam_server_job_trace *out, int max, int *count)
+{
+    if (!s || !count || max < 0 || (max > 0 && !out)) return CAM_E_INVAL;
+    std::lock_guard<std::mutex> lk(s->mu);
+    const size_t k = std::min(s->trace.size(), (size_t)max);
+    std::copy(s->trace.begin(), s->trace.begin() + (long)k, out);
+    s->trace.erase(s->trace.begin(), s->trace.begin() + (long)k);
+    *count = (int)k;
+    return CAM_OK;
+}
+
+const char *cam_server_last_error(cam_server *s)
+{
+    if (!s) return "null server";
+    std::lock_guard<std::mutex> lk(s->mu);
+    thread_local std::string copy;
+    copy = s->last_err;
+    return copy.c_str();
+}
+
 int cam_server_destroy(cam_server *s)
 {
     if (!s) return CAM_E_INVAL;
@@ -762,6 +836,7 @@ int cam_server_destroy(cam_server *s)
         w->br.reset();
         cam_ctx_destroy(w->ctx);
     }
+    cam_ctx_destroy(s->big_ctx);
     delete s;
     return CAM_OK;
 }

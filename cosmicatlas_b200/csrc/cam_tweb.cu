@@ -302,8 +302,8 @@ void tweb_impl(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const d
         constexpr int LEN = decltype(lc)::value;
         auto k0 = tidal_x_kernel<T, false, LEN>;
         auto k1 = tidal_x_kernel<T, true, LEN>;
-        CAM_CUDA_TRY(cudaFuncSetAttribute(k0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        CAM_CUDA_TRY(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        smem_at_least(k0, smem);
+        smem_at_least(k1, smem);
         dim3 g0(6, (unsigned)((M + W - 1) / W), (unsigned)n);
         CAM_LAUNCH_NAMED(ctx, "tweb_tidal_x", k0, g0, nthr, smem, static_cast<const C *>(dk.main), cm, (int)n, (int)M, n * M,
                    (int64_t)M, ccomp, rn, tw, gcoef, d_mean, density, scale);
@@ -327,7 +327,7 @@ void tweb_impl(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const d
         dispatch_fft_len(M, [&](auto lc) {
         constexpr int LEN = decltype(lc)::value;
         auto kz = tidal_z_kernel<T, LEN>;
-        CAM_CUDA_TRY(cudaFuncSetAttribute(kz, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        smem_at_least(kz, smem);
         const unsigned grid = (unsigned)((nn + rpc - 1) / rpc);
         CAM_LAUNCH_NAMED(ctx, "tweb_tidal_z_eigen", kz, grid, nthr, smem, cm, cn, (int)n, nn, rpc, ccomp, rm, tw, o.lambda_th,
                    o.tie_band, d_labels, d_lambdas, cnt);

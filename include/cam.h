@@ -262,6 +262,21 @@ int cam_server_wait(cam_server *s, uint64_t id, int64_t timeout_us);
 /* Counters and latency percentiles; reset != 0 clears the latency record
  * and the counters after reading them. */
 int cam_server_stats_get(cam_server *s, cam_server_stats *st, int reset);
+/* Per-job trace (no reference counterpart: BAM prints wall-clock banners
+ * only, Source/ScreenOutput.cpp:466).  Times in ms since the server started. */
+typedef struct {
+    uint64_t id;
+    double submit_ms, start_ms, end_ms;
+    int worker;  /* worker thread that ran the job                    */
+    int batch;   /* jobs in the batch it ran in (1 = alone)           */
+    int status;
+    int big;     /* counted as a large job (at most one runs at once) */
+} cam_server_job_trace;
+/* Moves up to `max` records of completed jobs (oldest first) into out. */
+int cam_server_trace(cam_server *s, cam_server_job_trace *out, int max, int *count);
+/* Message of the most recent failed job ("" if none); valid until the next
+ * call from this thread. */
+const char *cam_server_last_error(cam_server *s);
 /* Finishes the queued and running jobs, then stops the workers. */
 int cam_server_destroy(cam_server *s);
 

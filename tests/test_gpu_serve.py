@@ -136,9 +136,15 @@ def test_server_replays_graphs_for_packed_jobs(ctx):
         ids = [srv.submit(spec(j)) for j in jobs]
         got = [srv.wait(i, timeout_s=300) for i in ids]
         st = srv.stats()
+        tr = srv.trace()
     for g, a in zip(got, alone):
         assert_same(g, a)
     assert st["batches"] >= 3 and st["graph_replays"] >= 1, st
+    # per-job trace: every job once, times ordered, batch sizes add up
+    assert sorted(tr["id"].tolist()) == sorted(ids)
+    assert np.all(tr["start_ms"] >= tr["submit_ms"]) and np.all(tr["end_ms"] >= tr["start_ms"])
+    assert np.all(tr["status"] == 0) and np.all(tr["worker"] == 0)
+    assert int((tr["batch"] > 1).sum()) == st["batched_jobs"]
 
 
 def test_server_budget_admission(ctx):
