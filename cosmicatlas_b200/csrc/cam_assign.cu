@@ -34,7 +34,12 @@ namespace {
 
 constexpr int kBinThreads = 1024;
 constexpr int kDepositThreads = 512;
+constexpr int kScatterThreads = 512;  // scatter pass: two CTAs per SM
 constexpr int kSmemBricks = 16384;  // per-CTA brick histogram in shared memory (64 KB)
+// Global per-brick counters and append cursors sit one per 128-byte line:
+// atomics on one line are serialised in its L2 slice, so packed counters
+// would funnel all bricks through a few slices.
+constexpr int kCursorStride = 32;
 
 __device__ __forceinline__ int wrapi(int v, int n)
 {
@@ -173,8 +178,10 @@ __device__ __forceinline__ void bin_one(float px, float py, float pz, float wt, 
                 if (i2 >= nbx[2]) break;
                 const int b2 = (bl[2] + i2 == g.nb[2]) ? 0 : bl[2] + i2;
                 const int key = brick_linear(g, b0, b1, b2);
-                const uint32_t slot = SMEM ? atomicAdd(hist + key, 1u)
-                                           : atomicAdd(table + (int64_t)key * G + blk, 1u);
+                // count: per-CTA shared histogram, or the global counts;
+                // scatter: the brick's global append cursor
+                const uint32_t slot = (SMEM && !SCATTER) ? atomicAdd(hist + key, 1u)
+                                                         : atomicAdd(table + (int64_t)key * kCursorStride, 1u);
                 if (SCATTER) {
                     const int o[3] = {b0 * g.b[0], b1 * g.b[1], b2 * g.b[2]};
                     uint32_t word[3];
@@ -197,12 +204,20 @@ __device__ __forceinline__ void bin_one(float px, float py, float pz, float wt, 
 }
 
 // Passes 1 and 3.  Block `blk` handles particles [blk * chunk, (blk+1) * chunk)
-// (chunk a multiple of 4).  COUNT: table[brick * G + blk] = number of
-// payloads for `brick`, plus lost particles and max |w|.  SCATTER: table
-// holds the exclusive scan; payloads are written at table[brick * G + blk]++.
-// SMEM: the per-CTA counters live in shared memory (nb <= kSmemBricks),
-// otherwise in the table itself.  VEC: 16-byte aligned arrays, four
-// particles per thread per iteration (float4 loads).
+// (chunk a multiple of 4).
+//   COUNT   : table[brick * kCursorStride] += number of payloads for the
+//             brick (through a per-CTA shared-memory histogram when SMEM,
+//             nb <= kSmemBricks), plus lost particles and max |w|.
+//   SCATTER : table[brick * kCursorStride] is the brick's append cursor (the
+//             exclusive scan of the counts); every payload takes the next
+//             slot of its brick with one global atomic, and its words are
+//             packed while the atomic is in flight.  A brick's records are appended
+//             contiguously by all CTAs, so its few open 128-byte lines fill
+//             in L2 and are written back whole.  The order of records inside
+//             a brick varies from run to run; the deposit's integer sums do
+//             not depend on it.
+// VEC: 16-byte aligned arrays, four particles per thread per iteration
+// (float4 loads).
 template <int SCHEME, bool SCATTER, bool SMEM, bool VEC>
 __global__ void __launch_bounds__(kBinThreads)
 bin_kernel(const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z,
@@ -211,10 +226,11 @@ bin_kernel(const float *__restrict__ x, const float *__restrict__ y, const float
            unsigned int *__restrict__ wmax_bits)
 {
     extern __shared__ uint32_t hist[];
+    constexpr bool kHist = SMEM && !SCATTER;
     const int G = gridDim.x, blk = blockIdx.x;
     const int lane = threadIdx.x & 31;
-    if (SMEM) {
-        for (int i = threadIdx.x; i < nb; i += blockDim.x) hist[i] = SCATTER ? table[(int64_t)i * G + blk] : 0u;
+    if (kHist) {
+        for (int i = threadIdx.x; i < nb; i += blockDim.x) hist[i] = 0u;
         __syncthreads();
     }
     unsigned long long my_lost = 0;
@@ -229,16 +245,16 @@ bin_kernel(const float *__restrict__ x, const float *__restrict__ y, const float
             const float4 Y = __ldcs(reinterpret_cast<const float4 *>(y + p));
             const float4 Z = __ldcs(reinterpret_cast<const float4 *>(z + p));
             const float4 Wt = weighted ? __ldcs(reinterpret_cast<const float4 *>(w + p)) : make_float4(1.f, 1.f, 1.f, 1.f);
-            bin_one<SCHEME, SCATTER, SMEM>(X.x, Y.x, Z.x, Wt.x, weighted, g, G, blk, hist, table, payload, my_lost, my_wmax);
-            bin_one<SCHEME, SCATTER, SMEM>(X.y, Y.y, Z.y, Wt.y, weighted, g, G, blk, hist, table, payload, my_lost, my_wmax);
-            bin_one<SCHEME, SCATTER, SMEM>(X.z, Y.z, Z.z, Wt.z, weighted, g, G, blk, hist, table, payload, my_lost, my_wmax);
-            bin_one<SCHEME, SCATTER, SMEM>(X.w, Y.w, Z.w, Wt.w, weighted, g, G, blk, hist, table, payload, my_lost, my_wmax);
+            bin_one<SCHEME, SCATTER, kHist>(X.x, Y.x, Z.x, Wt.x, weighted, g, G, blk, hist, table, payload, my_lost, my_wmax);
+            bin_one<SCHEME, SCATTER, kHist>(X.y, Y.y, Z.y, Wt.y, weighted, g, G, blk, hist, table, payload, my_lost, my_wmax);
+            bin_one<SCHEME, SCATTER, kHist>(X.z, Y.z, Z.z, Wt.z, weighted, g, G, blk, hist, table, payload, my_lost, my_wmax);
+            bin_one<SCHEME, SCATTER, kHist>(X.w, Y.w, Z.w, Wt.w, weighted, g, G, blk, hist, table, payload, my_lost, my_wmax);
         }
         ptail = q1;
     }
     for (int64_t p = ptail + threadIdx.x; p < p1; p += blockDim.x)
-        bin_one<SCHEME, SCATTER, SMEM>(__ldcs(x + p), __ldcs(y + p), __ldcs(z + p), weighted ? __ldcs(w + p) : 1.0f,
-                                       weighted, g, G, blk, hist, table, payload, my_lost, my_wmax);
+        bin_one<SCHEME, SCATTER, kHist>(__ldcs(x + p), __ldcs(y + p), __ldcs(z + p), weighted ? __ldcs(w + p) : 1.0f,
+                                        weighted, g, G, blk, hist, table, payload, my_lost, my_wmax);
     if (!SCATTER) {
         // Warp reductions, one atomic per warp.
 #pragma unroll
@@ -250,20 +266,32 @@ bin_kernel(const float *__restrict__ x, const float *__restrict__ y, const float
             if (my_lost) atomicAdd(lost, my_lost);
             if (my_wmax) atomicMax(wmax_bits, my_wmax);
         }
-        if (SMEM) {
+        if (kHist) {
             __syncthreads();
-            for (int i = threadIdx.x; i < nb; i += blockDim.x) table[(int64_t)i * G + blk] = hist[i];
+            for (int i = threadIdx.x; i < nb; i += blockDim.x)
+                if (hist[i]) atomicAdd(table + (int64_t)i * kCursorStride, hist[i]);
         }
     }
 }
 
-// start[b] = scanned table[b * G] (first CTA's cursor of brick b);
-// start[nb] = total payload count.
-__global__ void brick_starts_kernel(const uint32_t *__restrict__ table, int nb, int G,
-                                    const uint32_t *__restrict__ total, uint32_t *__restrict__ start)
+// counts[b] = padded[b * kCursorStride] (contiguous, for the scan).
+__global__ void compact_counts_kernel(const uint32_t *__restrict__ padded, int nb, uint32_t *__restrict__ counts)
 {
-    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= nb; b += gridDim.x * blockDim.x)
-        start[b] = b < nb ? table[(int64_t)b * G] : *total;
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x)
+        counts[b] = padded[(int64_t)b * kCursorStride];
+}
+
+// start[b] = scanned count of brick b (its first payload), start[nb] = total;
+// the padded cursors start there.
+__global__ void brick_starts_kernel(const uint32_t *__restrict__ scanned, int nb,
+                                    const uint32_t *__restrict__ total, uint32_t *__restrict__ start,
+                                    uint32_t *__restrict__ cursor)
+{
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= nb; b += gridDim.x * blockDim.x) {
+        const uint32_t v = b < nb ? scanned[b] : *total;
+        start[b] = v;
+        if (b < nb) cursor[(int64_t)b * kCursorStride] = v;
+    }
 }
 
 template <typename OutT>
@@ -494,36 +522,39 @@ static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const floa
     // particles).  Few CTAs keep the set of partly written payload sectors
     // (CTAs x bricks x 128 B) inside L2, so sectors are complete before they
     // are written back.
+    // Count pass: one CTA of 1024 threads per SM (its brick histogram in
+    // shared memory); scatter pass: two CTAs of 512 threads per SM.  Both
+    // take contiguous chunks of >= 4096 particles.
     const int G = (int)std::max<int64_t>(1, std::min<int64_t>(kNumSMs, (np + 4095) / 4096));
     const int64_t chunk = std::max<int64_t>(4, ((np + G - 1) / G + 3) & ~(int64_t)3);
+    const int G2 = (int)std::max<int64_t>(1, std::min<int64_t>(2 * kNumSMs, (np + 4095) / 4096));
+    const int64_t chunk2 = std::max<int64_t>(4, ((np + G2 - 1) / G2 + 3) & ~(int64_t)3);
     auto aligned = [](const void *p) { return p == nullptr || ((uintptr_t)p & 15u) == 0; };
     const bool vec = aligned(x) && aligned(y) && aligned(z) && aligned(w);
     const bool smem_hist = nb <= kSmemBricks;
-    const int64_t tn = nb * G;
-    auto *table = static_cast<uint32_t *>(scratch(ctx, "asg.table", (size_t)tn * sizeof(uint32_t)));
+    // per-brick counters, one per 128-byte line (counts, then cursors)
+    auto *table = static_cast<uint32_t *>(scratch(ctx, "asg.cursor", (size_t)nb * kCursorStride * sizeof(uint32_t)));
+    auto *counts = static_cast<uint32_t *>(scratch(ctx, "asg.counts", (size_t)nb * sizeof(uint32_t)));
     auto *start = static_cast<uint32_t *>(scratch(ctx, "asg.start", (nb + 1) * sizeof(uint32_t)));
     auto *stats = static_cast<unsigned long long *>(scratch(ctx, "asg.stats", 64));
     auto *bsum = static_cast<double *>(scratch(ctx, "asg.bsum", nb * sizeof(double)));
     unsigned long long *d_lost = stats;
     unsigned int *d_wmax = reinterpret_cast<unsigned int *>(stats + 1);
     uint32_t *d_total = reinterpret_cast<uint32_t *>(stats + 2);
-    if (!smem_hist) CAM_CUDA_TRY(cudaMemsetAsync(table, 0, (size_t)tn * sizeof(uint32_t), ctx->stream));
+    CAM_CUDA_TRY(cudaMemsetAsync(table, 0, (size_t)nb * kCursorStride * sizeof(uint32_t), ctx->stream));
     CAM_CUDA_TRY(cudaMemsetAsync(stats, 0, 64, ctx->stream));
 
     const size_t hsmem = smem_hist ? (size_t)nb * sizeof(uint32_t) : 0;
     auto count_k = smem_hist ? (vec ? bin_kernel<SCHEME, false, true, true> : bin_kernel<SCHEME, false, true, false>)
                              : (vec ? bin_kernel<SCHEME, false, false, true> : bin_kernel<SCHEME, false, false, false>);
-    auto scatter_k = smem_hist ? (vec ? bin_kernel<SCHEME, true, true, true> : bin_kernel<SCHEME, true, true, false>)
-                               : (vec ? bin_kernel<SCHEME, true, false, true> : bin_kernel<SCHEME, true, false, false>);
-    if (hsmem > 48 * 1024) {
-        smem_at_least(count_k, hsmem);
-        smem_at_least(scatter_k, hsmem);
-    }
+    auto scatter_k = vec ? bin_kernel<SCHEME, true, false, true> : bin_kernel<SCHEME, true, false, false>;
+    if (hsmem > 48 * 1024) smem_at_least(count_k, hsmem);
     CAM_LAUNCH_NAMED(ctx, "assign_bin_count", count_k, G, kBinThreads, hsmem, x, y, z, w, np, chunk, g, (int)nb,
                      table, (uint4 *)nullptr, d_lost, d_wmax);
-    exclusive_scan_u32(ctx, table, tn, d_total);
-    CAM_LAUNCH_NAMED(ctx, "assign_starts", brick_starts_kernel, (unsigned)std::min<int64_t>((nb + 256) / 256, 1024),
-                     256, 0, table, (int)nb, G, d_total, start);
+    const unsigned sg = (unsigned)std::min<int64_t>((nb + 256) / 256, 1024);
+    CAM_LAUNCH_NAMED(ctx, "assign_starts", compact_counts_kernel, sg, 256, 0, table, (int)nb, counts);
+    exclusive_scan_u32(ctx, counts, nb, d_total);
+    CAM_LAUNCH_NAMED(ctx, "assign_starts", brick_starts_kernel, sg, 256, 0, counts, (int)nb, d_total, start, table);
 
     uint64_t total = 0;
     if (ctx->sync_free) {
@@ -550,7 +581,7 @@ static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const floa
     }
 
     uint4 *payload = static_cast<uint4 *>(scratch(ctx, "asg.payload", std::max<size_t>(total, 1) * sizeof(uint4)));
-    CAM_LAUNCH_NAMED(ctx, "assign_bin_scatter", scatter_k, G, kBinThreads, hsmem, x, y, z, w, np, chunk, g,
+    CAM_LAUNCH_NAMED(ctx, "assign_bin_scatter", scatter_k, G2, kScatterThreads, 0, x, y, z, w, np, chunk2, g,
                      (int)nb, table, payload, d_lost, d_wmax);
 
     const size_t smem = (size_t)g.b[0] * g.b[1] * g.b[2] * 2 * sizeof(uint32_t);

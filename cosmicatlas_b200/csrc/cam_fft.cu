@@ -88,13 +88,19 @@ fft_rows_kernel(const void *in, void *out_main, typename fftdev::CT<T>::t *nyq, 
 {
     using C = typename fftdev::CT<T>::t;
     constexpr bool INV = (MODE == 1 || MODE == 3);
+    constexpr bool PAD = LEN > 0;  // row tiles of the compile-time transforms are padded
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    C *tile = reinterpret_cast<C *>(smem_raw);
-    const int len = (MODE <= 1) ? n / 2 : n;
-    const int64_t row0 = (int64_t)blockIdx.x * rpc;
-    const int nr = (int)min((int64_t)rpc, nrows - row0);
+    C *tile = reinterpret_cast<C *>(smem_raw);  // element e at slot sidx<PAD>(e)
+    auto at = [&](int e) -> C & { return tile[fftdev::sidx<PAD>(e)]; };
+    // With a compile-time length, row length, M and rows per CTA are
+    // constants (the host passes the same values): index divisions become
+    // multiplies.
+    const int len = LEN > 0 ? LEN : ((MODE <= 1) ? n / 2 : n);
+    const int M = LEN > 0 ? ((MODE <= 1) ? LEN : LEN / 2) : n / 2;
+    const int rpcv = LEN > 0 ? rows_rpc<T>(LEN) : rpc;
+    const int64_t row0 = (int64_t)blockIdx.x * rpcv;
+    const int nr = (int)min((int64_t)rpcv, nrows - row0);
     const int tot = nr * len;
-    const int M = n / 2;
     const int64_t comp = blockIdx.y;
 
     if (MODE == 0) {
@@ -104,7 +110,7 @@ fft_rows_kernel(const void *in, void *out_main, typename fftdev::CT<T>::t *nyq, 
             C v = src[e];
             v.x -= sub;
             v.y -= sub;
-            tile[e] = v;
+            at(e) = v;
         }
     } else if (MODE == 1) {
         const C *srcm = static_cast<const C *>(in) + comp * ccomp_in + row0 * M;
@@ -123,18 +129,18 @@ fft_rows_kernel(const void *in, void *out_main, typename fftdev::CT<T>::t *nyq, 
             C wv = __ldg(tw + k);
             wv.y = -wv.y;
             const C ib = fftdev::rot<C, true>(fftdev::cmul(wv, b));
-            tile[e] = fftdev::cadd(a, ib);
+            at(e) = fftdev::cadd(a, ib);
         }
     } else {
         const C *src = static_cast<const C *>(in) + comp * ccomp_in + row0 * n;
-        for (int e = threadIdx.x; e < tot; e += blockDim.x) tile[e] = src[e];
+        for (int e = threadIdx.x; e < tot; e += blockDim.x) at(e) = src[e];
     }
     __syncthreads();
     if constexpr (LEN > 0) {
         // all rpc rows (the unused ones of the last CTA hold garbage and are not stored)
         constexpr int RPC = rows_rpc<T>(LEN);
         fftdev::block_fft_fixed<C, INV, true, RPC, LEN, fftdev::ct_threads(LEN, RPC, fftdev::CT<T>::kPPT), 1, LEN,
-                                (MODE <= 1) ? 2 : 1>(tile, tw);
+                                (MODE <= 1) ? 2 : 1, PAD>(tile, tw);
     } else {
         fftdev::block_fft<C, fftdev::CT<T>::kPPT, INV, true, 0>(tile, len, nr, 1, len, rd, tw, (MODE <= 1) ? 2 : 1);
     }
@@ -145,8 +151,8 @@ fft_rows_kernel(const void *in, void *out_main, typename fftdev::CT<T>::t *nyq, 
         const int tot2 = nr * (M + 1);
         for (int e = threadIdx.x; e < tot2; e += blockDim.x) {
             const int r = e / (M + 1), k = e % (M + 1);
-            const C zk = tile[r * M + (k % M)];
-            const C zc0 = tile[r * M + ((M - k) % M)];
+            const C zk = at(r * M + (k % M));
+            const C zc0 = at(r * M + ((M - k) % M));
             const C zc = C{zc0.x, -zc0.y};
             // X[k] = (Z[k] + conj Z[M-k])/2 - i/2 e^{-2 pi i k/n} (Z[k] - conj Z[M-k])
             const C s = fftdev::cadd(zk, zc), d = fftdev::csub(zk, zc);
@@ -159,12 +165,12 @@ fft_rows_kernel(const void *in, void *out_main, typename fftdev::CT<T>::t *nyq, 
         T *dst = static_cast<T *>(out_main) + comp * ccomp_out + row0 * n;
         const T sc = (T)scale;
         for (int e = threadIdx.x; e < tot; e += blockDim.x) {
-            const C v = tile[e];
+            const C v = at(e);
             reinterpret_cast<C *>(dst)[e] = C{v.x * sc, v.y * sc};
         }
     } else {
         C *dst = static_cast<C *>(out_main) + comp * ccomp_out + row0 * n;
-        for (int e = threadIdx.x; e < tot; e += blockDim.x) dst[e] = tile[e];
+        for (int e = threadIdx.x; e < tot; e += blockDim.x) dst[e] = at(e);
     }
 }
 
@@ -234,10 +240,10 @@ void rows_impl(cam_ctx *ctx, FftPlan *p, const void *in, void *out, void *nyq, i
     const Radices &rd = MODE <= 1 ? p->rad_m : p->rad_n;
     const int rpc = rows_rpc<T>(len);
     const int nthr = threads_for(rpc * len, fftdev::CT<T>::kPPT);  // == ct_threads for compiled lengths
-    const size_t smem = (size_t)rpc * len * sizeof(C);
     dim3 grid((unsigned)((nrows + rpc - 1) / rpc), (unsigned)ncomp);
     dispatch_fft_len(len, [&](auto lc) {
     constexpr int LEN = decltype(lc)::value;
+    const size_t smem = (size_t)fftdev::padded_len((int64_t)rpc * len, LEN > 0) * sizeof(C);
     auto kern = fft_rows_kernel<T, MODE, LEN>;
     smem_at_least(kern, smem);
     CAM_LAUNCH_NAMED(ctx, MODE == 0 ? "fft_rows_r2c" : MODE == 1 ? "fft_rows_c2r" : "fft_rows_c2c", kern, grid, nthr, smem, in, out, static_cast<C *>(nyq), n, nrows, rpc,

@@ -237,12 +237,27 @@ constexpr int ct_threads(int len, int ncol, int ppt)
     return ((len * ncol + ppt - 1) / ppt + 31) / 32 * 32;
 }
 
+// Shared-memory slot of tile element i.  With PAD one spare element follows
+// every 32: row transforms (JSTRIDE 1) store their first stages with a
+// stride of R elements, which without padding lands a warp on two banks.
+template <bool PAD>
+__device__ __forceinline__ int sidx(int i)
+{
+    return PAD ? i + (i >> 5) : i;
+}
+// Elements a padded tile of n elements occupies.
+__host__ __device__ constexpr int64_t padded_len(int64_t n, bool pad)
+{
+    return pad ? n + n / 32 + 1 : n;
+}
+
 // One Stockham stage with every shape parameter known at compile time:
-// NCOL transforms of length LEN, element (col, j) at col*CSTRIDE + j*JSTRIDE,
-// NTHR threads; JFAST as in stage().  Index arithmetic reduces to shifts,
-// constant multiplies and (for lengths with a factor 3) a constant divide.
+// NCOL transforms of length LEN, element (col, j) at col*CSTRIDE + j*JSTRIDE
+// (slot sidx<PAD> of that), NTHR threads; JFAST as in stage().  Index
+// arithmetic reduces to shifts, constant multiplies and (for lengths with a
+// factor 3) a constant divide.
 template <typename C, int R, bool INV, bool JFAST, int NCOL, int LEN, int NS, int NTHR, int JSTRIDE,
-          int CSTRIDE, int TWMUL>
+          int CSTRIDE, int TWMUL, bool PAD = false>
 __device__ __forceinline__ void stage_ct(C *buf, const C *__restrict__ tw)
 {
     constexpr int NQ = LEN / R;
@@ -260,9 +275,9 @@ __device__ __forceinline__ void stage_ct(C *buf, const C *__restrict__ tw)
         if (EXACT || bi < NBF) {
             const int col = JFAST ? bi / NQ : bi % NCOL;
             const int j = JFAST ? bi % NQ : bi / NCOL;
-            const C *src = buf + col * CSTRIDE + j * JSTRIDE;
+            const int src = col * CSTRIDE + j * JSTRIDE;
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[it][r] = src[r * NQ * JSTRIDE];
+            for (int r = 0; r < R; ++r) v[it][r] = buf[sidx<PAD>(src + r * NQ * JSTRIDE)];
             const int q = j / NS;
             const int k = j - q * NS;
             if (NS > 1) {
@@ -281,9 +296,8 @@ __device__ __forceinline__ void stage_ct(C *buf, const C *__restrict__ tw)
 #pragma unroll
     for (int it = 0; it < MAXIT; ++it) {
         if (EXACT || dsto[it] >= 0) {
-            C *dst = buf + dsto[it];
 #pragma unroll
-            for (int r = 0; r < R; ++r) dst[r * NS * JSTRIDE] = v[it][r];
+            for (int r = 0; r < R; ++r) buf[sidx<PAD>(dsto[it] + r * NS * JSTRIDE)] = v[it][r];
         }
     }
     __syncthreads();
@@ -292,13 +306,13 @@ __device__ __forceinline__ void stage_ct(C *buf, const C *__restrict__ tw)
 // All stages of a length-LEN transform, layout and thread count fixed at
 // compile time (the CTA must run exactly NTHR threads).
 template <typename C, bool INV, bool JFAST, int NCOL, int LEN, int NTHR, int JSTRIDE, int CSTRIDE, int TWMUL,
-          int S = 0, int NS = 1>
+          bool PAD = false, int S = 0, int NS = 1>
 __device__ __forceinline__ void block_fft_fixed(C *buf, const C *__restrict__ tw)
 {
     if constexpr (S < ct_num_stages(LEN)) {
         constexpr int R = ct_radix(LEN, S);
-        stage_ct<C, R, INV, JFAST, NCOL, LEN, NS, NTHR, JSTRIDE, CSTRIDE, TWMUL>(buf, tw);
-        block_fft_fixed<C, INV, JFAST, NCOL, LEN, NTHR, JSTRIDE, CSTRIDE, TWMUL, S + 1, NS * R>(buf, tw);
+        stage_ct<C, R, INV, JFAST, NCOL, LEN, NS, NTHR, JSTRIDE, CSTRIDE, TWMUL, PAD>(buf, tw);
+        block_fft_fixed<C, INV, JFAST, NCOL, LEN, NTHR, JSTRIDE, CSTRIDE, TWMUL, PAD, S + 1, NS * R>(buf, tw);
     }
 }
 

@@ -8,15 +8,23 @@
 // the eigenvalues lambda1 >= lambda2 >= lambda3 and the label
 // 4 - #{lambda_a > lambda_th} (Source/Cwclass.cpp:875-890).
 //
-// Only the six distinct components are transformed (the reference does
-// nine).  Three kernels:
-//   tidal_x    : inverse FFT along x fused with the multiplier; the six
-//                components of one delta_k tile are made by six consecutive
-//                CTAs, so the tile is read from HBM once and from L2 after;
-//   (columns)  : inverse FFT along y for the six components (generic);
-//   tidal_z    : c2r along z of the six components of a few rows, then the
-//                eigenvalues (FP32 trigonometric solution plus one FP64
-//                Newton step) and the label of every cell, written as uint8.
+// Only the six distinct components are made (the reference transforms
+// nine), and the multiplier is split into its separable factors:
+//   T_ab = IFFT_z[ k_z^r IFFT_y[ k_y^q IFFT_x[ k_x^p phi ] ] ],
+//   phi = delta_k exp(-k^2 R^2 / 2) / k^2,  p + q + r = 2,
+// so the x pass transforms three fields (p = 0, 1, 2) instead of six.
+// Three kernels:
+//   tidal_x    : phi times k_x^p and the inverse FFT along x, p = 0, 1, 2;
+//                the three CTAs of one delta_k tile run together, so the
+//                tile is read from HBM once and from L2 after;
+//   tidal_y    : for input field p, the fields (p, q), q = 0 .. 2-p: times
+//                k_y^q and the inverse FFT along y; (p, 0) overwrites its
+//                input in place, as the last output of the same CTA;
+//   tidal_z    : times k_z^r, c2r along z of the six fields of a few rows,
+//                then the eigenvalues (FP32 trigonometric solution plus one
+//                FP64 Newton step) and the label of every cell (uint8).
+// Field slots: 0 = (0,0) -> T_zz, 1 = (1,0) -> T_xz, 2 = (2,0) -> T_xx,
+// 3 = (0,1) -> T_yz, 4 = (0,2) -> T_yy, 5 = (1,1) -> T_xy.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -39,18 +47,20 @@ constexpr int tweb_rpc(int m)
     return (sizeof(T) == 4 ? 4096 : 2048) / (6 * m) > 1 ? (sizeof(T) == 4 ? 4096 : 2048) / (6 * m) : 1;
 }
 
-// Product of the two signed frequencies of component c (xx, yy, zz, xy,
-// xz, yz), without a runtime-indexed local array.
-__device__ __forceinline__ int comp_product(int c, int fi, int fj, int fk)
+// f^e for e = 0, 1, 2 (exact in float for |f| <= 2048).
+__device__ __forceinline__ float ipow(int f, int e)
 {
-    switch (c) {
-    case 0: return fi * fi;
-    case 1: return fj * fj;
-    case 2: return fk * fk;
-    case 3: return fi * fj;
-    case 4: return fi * fk;
-    default: return fj * fk;
-    }
+    return e == 0 ? 1.0f : (e == 1 ? (float)f : (float)(f * f));
+}
+
+// Field slot of (p, q) and the power r = 2 - p - q of k_z it still needs.
+__host__ __device__ constexpr int slot_of(int p, int q)
+{
+    return q == 0 ? p : (p == 0 ? 2 + q : 5);
+}
+__device__ __forceinline__ int kz_power(int slot)
+{
+    return slot == 0 ? 2 : ((slot == 1 || slot == 3) ? 1 : 0);
 }
 
 }  // namespace
@@ -58,24 +68,40 @@ __device__ __forceinline__ int comp_product(int c, int fi, int fj, int fk)
 
 namespace {
 
-// Tidal multiplier for signed frequencies (fi, fj, fk) of component c.
+// Launch bounds of a column kernel for FFT length LEN: its exact thread
+// count, and as many CTAs per SM as fit 1024 threads (768 for lengths with
+// a factor 3, whose radix-3 stages need up to ~85 registers).
+template <typename T, int LEN>
+constexpr int col_threads()
+{
+    return LEN > 0 ? fftdev::ct_threads(LEN, CTw<T>::kCols, CTw<T>::kPPT) : 1024;
+}
+template <typename T, int LEN>
+constexpr int col_min_blocks()
+{
+    return ((LEN % 3 == 0 ? 768 : 1024) / col_threads<T, LEN>()) > 1
+               ? (LEN % 3 == 0 ? 768 : 1024) / col_threads<T, LEN>()
+               : 1;
+}
+
+// k_x^p phi / delta_k for signed frequencies (fi, fj, fk).
 template <typename T>
-__device__ __forceinline__ T tidal_mult(int c, int fi, int fj, int fk, T gauss_coef, T norm)
+__device__ __forceinline__ T phi_mult(int p, int fi, int fj, int fk, T gauss_coef, T norm)
 {
     const int q = fi * fi + fj * fj + fk * fk;
     if (q == 0) return (T)0;
-    // f_a f_b and q are exact in float up to N = 2048; one rounding each
-    const T ratio = (T)((float)comp_product(c, fi, fj, fk) * (1.0f / (float)q));
+    // f^p and q are exact in float up to N = 2048; one rounding each
+    const T ratio = (T)(ipow(fi, p) * (1.0f / (float)q));
     const T g = gauss_coef != (T)0 ? exp(-gauss_coef * (T)q) : (T)1;
     return ratio * g * norm;
 }
 
-// Inverse FFT along x of the six tidal components of one tile of delta_k.
+// Inverse FFT along x of k_x^p phi, p = blockIdx.x, for one tile of delta_k.
 // NYQ = false: main tiles (plane = j, columns = k < N/2, FFT index i with
 // stride N*M).  NYQ = true: the Nyquist plane (columns = j, FFT index i with
 // stride N, k = N/2).
 template <typename T, bool NYQ, int LEN>
-__global__ void __launch_bounds__(1024, 1)
+__global__ void __launch_bounds__(col_threads<T, LEN>(), col_min_blocks<T, LEN>())
 tidal_x_kernel(const typename CTw<T>::t *__restrict__ src, typename CTw<T>::t *__restrict__ dst,
                int n, int ncols, int64_t jstride, int64_t pstride, int64_t ccomp, Radices rd,
                const typename CTw<T>::t *__restrict__ tw, double gauss_coef, const double *__restrict__ d_mean,
@@ -85,7 +111,7 @@ tidal_x_kernel(const typename CTw<T>::t *__restrict__ src, typename CTw<T>::t *_
     constexpr int W = CTw<T>::kCols;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *tile = reinterpret_cast<C *>(smem_raw);
-    const int comp = blockIdx.x;  // fastest: the six CTAs of a tile run together
+    const int comp = blockIdx.x;  // p; fastest: the three CTAs of a tile run together
     const int col0 = blockIdx.y * W;
     const int plane = blockIdx.z;
     const int nc = min(W, ncols - col0);
@@ -110,7 +136,7 @@ tidal_x_kernel(const typename CTw<T>::t *__restrict__ src, typename CTw<T>::t *_
                 fj = plane <= h ? plane : plane - n;
                 fk = col0 + cc;
             }
-            const T m = tidal_mult<T>(comp, fi, fj, fk, gc, norm);
+            const T m = phi_mult<T>(comp, fi, fj, fk, gc, norm);
             tile[e] = C{v.x * m, v.y * m};
         }
     }
@@ -122,6 +148,50 @@ tidal_x_kernel(const typename CTw<T>::t *__restrict__ src, typename CTw<T>::t *_
     for (int e = threadIdx.x; e < tot; e += blockDim.x) {
         const int i = e / W, cc = e % W;
         if (cc < nc) o[(int64_t)i * jstride + cc] = tile[e];
+    }
+}
+
+// Inverse FFT along y of k_y^q times field p, q = 2-p .. 0, for one tile
+// (p = blockIdx.x, columns blockIdx.y * W.., plane blockIdx.z).  Element
+// (plane, j, col) of field s sits at base + s*ccomp + plane*pstride +
+// j*jstride + col*cstride.  The tile is re-read (from L2) for every q, and
+// (p, 0) -- no factor -- is written last, over its own input.
+template <typename T, int LEN>
+__global__ void __launch_bounds__(col_threads<T, LEN>(), col_min_blocks<T, LEN>())
+tidal_y_kernel(typename CTw<T>::t *__restrict__ base, int n, int ncols, int64_t jstride, int64_t cstride,
+               int64_t pstride, int64_t ccomp, Radices rd, const typename CTw<T>::t *__restrict__ tw)
+{
+    using C = typename CTw<T>::t;
+    constexpr int W = CTw<T>::kCols;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *tile = reinterpret_cast<C *>(smem_raw);
+    const int p = blockIdx.x;
+    const int col0 = blockIdx.y * W;
+    const int nc = min(W, ncols - col0);
+    const int h = n / 2;
+    const int64_t off = (int64_t)blockIdx.z * pstride + (int64_t)col0 * cstride;
+    const C *in = base + (int64_t)p * ccomp + off;
+    const int tot = n * W;
+    for (int q = 2 - p; q >= 0; --q) {
+        for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+            const int j = e / W, cc = e % W;
+            if (cc < nc) {
+                const C v = in[(int64_t)j * jstride + (int64_t)cc * cstride];
+                const T m = (T)ipow(j <= h ? j : j - n, q);
+                tile[e] = C{v.x * m, v.y * m};
+            }
+        }
+        __syncthreads();
+        if constexpr (LEN > 0)
+            fftdev::block_fft_fixed<C, true, false, W, LEN, fftdev::ct_threads(LEN, W, CTw<T>::kPPT), W, 1, 1>(tile, tw);
+        else
+            fftdev::block_fft<C, CTw<T>::kPPT, true, false, W>(tile, n, W, W, 1, rd, tw, 1);
+        C *o = base + (int64_t)slot_of(p, q) * ccomp + off;
+        for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+            const int j = e / W, cc = e % W;
+            if (cc < nc) o[(int64_t)j * jstride + (int64_t)cc * cstride] = tile[e];
+        }
+        __syncthreads();
     }
 }
 
@@ -175,10 +245,46 @@ __device__ __forceinline__ void eig3(float a00, float a11, float a22, float a01,
     if (lam[0] < lam[1]) { const double t = lam[0]; lam[0] = lam[1]; lam[1] = t; }
 }
 
+// Coefficients of det(x I - A) = x^3 - c2 x^2 + c1 x - c0 in FP64 from the
+// FP32 entries (products of two floats are exact in double).
+__device__ __forceinline__ void char_poly(float a00, float a11, float a22, float a01, float a02, float a12,
+                                          double &c2, double &c1, double &c0)
+{
+    const double A00 = a00, A11 = a11, A22 = a22, A01 = a01, A02 = a02, A12 = a12;
+    c2 = A00 + A11 + A22;
+    c1 = A00 * A11 + A00 * A22 + A11 * A22 - A01 * A01 - A02 * A02 - A12 * A12;
+    c0 = A00 * (A11 * A22 - A12 * A12) - A01 * (A01 * A22 - A12 * A02) + A02 * (A01 * A12 - A11 * A02);
+}
+
+// Number of eigenvalues greater than t: the sign changes of the coefficients
+// of p(x + t) = x^3 + (3t - c2) x^2 + (3t^2 - 2 c2 t + c1) x + p(t), zeros
+// skipped.  Descartes' rule of signs is exact here because every root of
+// the characteristic polynomial of a symmetric matrix is real.
+__device__ __forceinline__ int count_above(double c2, double c1, double c0, double t)
+{
+    const double a2 = 3.0 * t - c2;
+    const double a1 = (3.0 * t - 2.0 * c2) * t + c1;
+    const double a0 = ((t - c2) * t + c1) * t - c0;
+    int changes = 0;
+    bool neg = false;  // sign of the last nonzero coefficient (leading 1 > 0)
+    if (a2 != 0.0) {
+        changes += a2 < 0.0;
+        neg = a2 < 0.0;
+    }
+    if (a1 != 0.0) {
+        changes += (a1 < 0.0) != neg;
+        neg = a1 < 0.0;
+    }
+    if (a0 != 0.0) changes += (a0 < 0.0) != neg;
+    return changes;
+}
+
 // c2r along z of the six components for `rpc` rows, then eigenvalues and
-// labels.  Component c of row r: main at src + c*ccomp + r*M, Nyquist at
+// labels.  Without LAMBDAS the eigenvalues are not formed: the label needs
+// only the number of them above lambda_th, and the tie flag whether that
+// number differs between lambda_th - band and lambda_th + band.  Component c of row r: main at src + c*ccomp + r*M, Nyquist at
 // nyq + c*N*N + r.
-template <typename T, int LEN>
+template <typename T, int LEN, bool LAMBDAS>
 __global__ void __launch_bounds__(256, 2)
 tidal_z_kernel(const typename CTw<T>::t *__restrict__ src, const typename CTw<T>::t *__restrict__ nyq,
                int n, int64_t nrows, int rpc, int64_t ccomp, Radices rd,
@@ -187,16 +293,22 @@ tidal_z_kernel(const typename CTw<T>::t *__restrict__ src, const typename CTw<T>
                unsigned long long *__restrict__ counts /* [5] */)
 {
     using C = typename CTw<T>::t;
+    constexpr bool PAD = LEN > 0;  // row tiles of the compile-time transforms are padded
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    C *tile = reinterpret_cast<C *>(smem_raw);  // [6][rpc][M]
+    C *tile = reinterpret_cast<C *>(smem_raw);  // [6][rpc][M], element e at slot sidx<PAD>(e)
     __shared__ unsigned int cnt_s[5];
-    const int M = n / 2;
-    const int64_t row0 = (int64_t)blockIdx.x * rpc;
-    const int nr = (int)min((int64_t)rpc, nrows - row0);
+    // With a compile-time length the row length and rows per CTA are
+    // constants (the host passes the same values), so the index divisions
+    // below become multiplies.
+    const int M = LEN > 0 ? LEN : n / 2;
+    const int nz = LEN > 0 ? 2 * LEN : n;
+    const int rpcv = LEN > 0 ? tweb_rpc<T>(LEN) : rpc;
+    const int64_t row0 = (int64_t)blockIdx.x * rpcv;
+    const int nr = (int)min((int64_t)rpcv, nrows - row0);
     const int64_t nn = (int64_t)n * n;
     if (threadIdx.x < 5) cnt_s[threadIdx.x] = 0;
     // Load + c2r untangling (see fft_rows_kernel, mode c2r).
-    const int per = rpc * M;
+    const int per = rpcv * M;
     for (int e = threadIdx.x; e < 6 * per; e += blockDim.x) {
         const int c = e / per, rem = e % per;
         const int r = rem / M, k = rem % M;
@@ -208,45 +320,58 @@ tidal_z_kernel(const typename CTw<T>::t *__restrict__ src, const typename CTw<T>
             xk.y = 0;
             xm.y = 0;
         }
+        // the remaining factor k_z^r of this field (k_z >= 0 in the half spectrum)
+        const int rz = kz_power(c);
+        const T fa = (T)ipow(k, rz), fb = (T)ipow(k == 0 ? M : M - k, rz);
+        xk = C{xk.x * fa, xk.y * fa};
+        xm = C{xm.x * fb, xm.y * fb};
         const C a = C{xk.x + xm.x, xk.y - xm.y};
         const C b = C{xk.x - xm.x, xk.y + xm.y};
         C wv = __ldg(tw + k);
         wv.y = -wv.y;
         const C ib = fftdev::rot<C, true>(fftdev::cmul(wv, b));
-        tile[e] = fftdev::cadd(a, ib);
+        tile[fftdev::sidx<PAD>(e)] = fftdev::cadd(a, ib);
     }
     __syncthreads();
     if constexpr (LEN > 0) {
         constexpr int RPCZ = tweb_rpc<T>(LEN);
-        fftdev::block_fft_fixed<C, true, true, 6 * RPCZ, LEN, fftdev::ct_threads(LEN, 6 * RPCZ, CTw<T>::kPPT), 1, LEN, 2>(
-            tile, tw);
+        fftdev::block_fft_fixed<C, true, true, 6 * RPCZ, LEN, fftdev::ct_threads(LEN, 6 * RPCZ, CTw<T>::kPPT), 1, LEN, 2,
+                                true>(tile, tw);
     } else {
         fftdev::block_fft<C, CTw<T>::kPPT, true, true, 0>(tile, M, 6 * rpc, 1, M, rd, tw, 2);
     }
     // Per cell: 6 components -> eigenvalues -> label.
     unsigned int lc0 = 0, lc1 = 0, lc2 = 0, lc3 = 0, lties = 0;
-    const T *re = reinterpret_cast<const T *>(tile);  // real row r of comp c at (c*rpc + r)*n
+    // real value z of row r of comp c: half z & 1 of complex element (c*rpc + r)*M + z/2
+    const T *re = reinterpret_cast<const T *>(tile);
     const int64_t ncell = nn * n;
-    for (int e = threadIdx.x; e < nr * n; e += blockDim.x) {
-        const int r = e / n, z = e % n;
+    for (int e = threadIdx.x; e < nr * nz; e += blockDim.x) {
+        const int r = e / nz, z = e % nz;
         float t6[6];
 #pragma unroll
-        for (int c = 0; c < 6; ++c) t6[c] = (float)re[((int64_t)c * rpc + r) * n + z];
-        double lam[3];
-        eig3(t6[0], t6[1], t6[2], t6[3], t6[4], t6[5], lam);
+        for (int c = 0; c < 6; ++c)
+            t6[c] = (float)re[2 * fftdev::sidx<PAD>((c * rpcv + r) * M + (z >> 1)) + (z & 1)];
+        // (xx, yy, zz, xy, xz, yz) from slots (2, 4, 0, 5, 1, 3)
         int v = 0, tie = 0;
+        const int64_t cell = (row0 + r) * nz + z;
+        if constexpr (LAMBDAS) {
+            double lam[3];
+            eig3(t6[2], t6[4], t6[0], t6[5], t6[1], t6[3], lam);
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            v += lam[a] > lth;
-            tie |= fabs(lam[a] - lth) <= band;
-        }
-        const int64_t cell = (row0 + r) * n + z;
-        if (labels) labels[cell] = (uint8_t)(4 - v);
-        if (lambdas) {
+            for (int a = 0; a < 3; ++a) {
+                v += lam[a] > lth;
+                tie |= fabs(lam[a] - lth) <= band;
+            }
             lambdas[cell] = (float)lam[0];
             lambdas[ncell + cell] = (float)lam[1];
             lambdas[2 * ncell + cell] = (float)lam[2];
+        } else {
+            double c2, c1, c0;
+            char_poly(t6[2], t6[4], t6[0], t6[5], t6[1], t6[3], c2, c1, c0);
+            v = count_above(c2, c1, c0, lth);
+            tie = count_above(c2, c1, c0, lth - band) != count_above(c2, c1, c0, lth + band);
         }
+        if (labels) labels[cell] = (uint8_t)(4 - v);
         lc0 += v == 3;  // label 1, knot
         lc1 += v == 2;
         lc2 += v == 1;
@@ -294,7 +419,7 @@ void tweb_impl(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const d
     const double scale = 1.0 / ((double)n * (double)n * (double)n);  // c2r divides by N^3
     const int density = input_type == CAM_INPUT_DENSITY;
 
-    // 1. x: multiplier + inverse FFT along x, six components.
+    // 1. x: k_x^p phi + inverse FFT along x, p = 0, 1, 2 (slots 0..2).
     {
         const int nthr = threads_for((int)n * W, CTw<T>::kPPT, 1024);
         const size_t smem = (size_t)n * W * sizeof(C);
@@ -304,17 +429,32 @@ void tweb_impl(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const d
         auto k1 = tidal_x_kernel<T, true, LEN>;
         smem_at_least(k0, smem);
         smem_at_least(k1, smem);
-        dim3 g0(6, (unsigned)((M + W - 1) / W), (unsigned)n);
+        dim3 g0(3, (unsigned)((M + W - 1) / W), (unsigned)n);
         CAM_LAUNCH_NAMED(ctx, "tweb_tidal_x", k0, g0, nthr, smem, static_cast<const C *>(dk.main), cm, (int)n, (int)M, n * M,
                    (int64_t)M, ccomp, rn, tw, gcoef, d_mean, density, scale);
-        dim3 g1(6, (unsigned)((n + W - 1) / W), 1);
+        dim3 g1(3, (unsigned)((n + W - 1) / W), 1);
         CAM_LAUNCH_NAMED(ctx, "tweb_tidal_x_nyq", k1, g1, nthr, smem, static_cast<const C *>(dk.nyq), cn, (int)n, (int)n, n,
                    (int64_t)0, nn, rn, tw, gcoef, d_mean, density, scale);
         });
     }
-    // 2. y: inverse FFT of the six components.
-    fft_columns(ctx, plan, cm, n, M, M, n, n * M, 6, ccomp, true);
-    fft_rows_c2c(ctx, plan, cn, n, n, 6, nn, true);
+    // 2. y: k_y^q and the inverse FFT along y: three fields in, six out.
+    {
+        const int nthr = threads_for((int)n * W, CTw<T>::kPPT, 1024);
+        const size_t smem = (size_t)n * W * sizeof(C);
+        dispatch_fft_len(n, [&](auto lc) {
+        constexpr int LEN = decltype(lc)::value;
+        auto ky = tidal_y_kernel<T, LEN>;
+        smem_at_least(ky, smem);
+        // main: planes i, FFT index j (stride M), columns k (stride 1)
+        dim3 g0(3, (unsigned)((M + W - 1) / W), (unsigned)n);
+        CAM_LAUNCH_NAMED(ctx, "tweb_tidal_y", ky, g0, nthr, smem, cm, (int)n, (int)M, (int64_t)M, (int64_t)1, n * M,
+                         ccomp, rn, tw);
+        // Nyquist plane: columns i (stride N), FFT index j (stride 1)
+        dim3 g1(3, (unsigned)((n + W - 1) / W), 1);
+        CAM_LAUNCH_NAMED(ctx, "tweb_tidal_y_nyq", ky, g1, nthr, smem, cn, (int)n, (int)n, (int64_t)1, n, (int64_t)0,
+                         nn, rn, tw);
+        });
+    }
     // 3. z: c2r + eigenvalues + labels.
     {
         // Small tiles (<= 4096 complex, 256 threads) so that several CTAs
@@ -323,10 +463,10 @@ void tweb_impl(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const d
         const int rpc = tweb_rpc<T>((int)M);
         const int nthr = threads_for(6 * rpc * (int)M, CTw<T>::kPPT, 256);
         CAM_REQUIRE(6 * rpc * M <= (int64_t)nthr * CTw<T>::kPPT, CAM_E_UNSUPPORTED, "T-web row tile too large");
-        const size_t smem = (size_t)6 * rpc * M * sizeof(C);
         dispatch_fft_len(M, [&](auto lc) {
         constexpr int LEN = decltype(lc)::value;
-        auto kz = tidal_z_kernel<T, LEN>;
+        const size_t smem = (size_t)fftdev::padded_len(6 * rpc * M, LEN > 0) * sizeof(C);
+        auto kz = d_lambdas ? tidal_z_kernel<T, LEN, true> : tidal_z_kernel<T, LEN, false>;
         smem_at_least(kz, smem);
         const unsigned grid = (unsigned)((nn + rpc - 1) / rpc);
         CAM_LAUNCH_NAMED(ctx, "tweb_tidal_z_eigen", kz, grid, nthr, smem, cm, cn, (int)n, nn, rpc, ccomp, rm, tw, o.lambda_th,
