@@ -54,6 +54,8 @@ def parse():
                          "calib / stream: served vs plain per-call jobs/s and latency")
     ap.add_argument("--jobs", type=int, default=0, help="calib / stream: number of jobs (0 = the config's)")
     ap.add_argument("--rates", default="50,200,800", help="stream: Poisson arrival rates (jobs/s)")
+    ap.add_argument("--serving-jobs", type=int, default=1024,
+                    help="sweep: jobs of the calibration batch timed served vs per-call on the same line (0: skip)")
     ap.add_argument("--mesh", type=int, default=0, help="single512 only: override N (profiler runs)")
     return ap.parse_args()
 
@@ -75,52 +77,112 @@ def config_dict(n_particles, extra=None):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clock, max clock and clock-event (throttle) reasons of the GPU,
+    sampled every 5 ms through NVML while the timed region runs (reading
+    only; nvidia-smi -lms 100 if NVML is unavailable)."""
+
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+               "sw_power_cap": 0x4}
 
     def __init__(self, index):
         self.index = index
-        self.samples = []
+        self.samples = []  # (sm_mhz, max_mhz, reasons bitmask)
         self.proc = None
+        self.thread = None
+        self.stop = threading.Event()
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            p = torch.cuda.get_device_properties(self.index)
+            bus = "%08x:%02x:%02x.0" % (p.pci_domain_id, p.pci_bus_id, p.pci_device_id)
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _poll(self, nv, h):
+        get_r = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self.stop.is_set():
+            try:
+                self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)), float(mx), int(get_r(h))))
+            except Exception:
+                pass
+            self.stop.wait(0.005)
+
+    def _sample_now(self):
+        if self.nv is None:
+            return
+        nv, h = self.nv
+        get_r = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        try:
+            self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                                 float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)), int(get_r(h))))
+        except Exception:
+            pass
 
     def __enter__(self):
+        self.nv = None
+        try:
+            nv, h = self._nvml_handle()
+            self.nv = (nv, h)
+            # one sample at the start (short timed regions), then every 5 ms
+            self._sample_now()
+            self.thread = threading.Thread(target=self._poll, args=(nv, h), daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            pass
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread = threading.Thread(target=self._read_smi, daemon=True)
             self.thread.start()
+            t0 = time.time()
+            while not self.samples and time.time() - t0 < 3.0:  # first line before the timed region
+                time.sleep(0.01)
+            self.samples.clear()
         except FileNotFoundError:
             self.proc = None
         return self
 
-    def _read(self):
+    def _read_smi(self):
+        bits = [0x8, 0x40, 0x20, 0x4]
         for line in self.proc.stdout:
-            self.samples.append([v.strip() for v in line.split(",")])
+            f = [v.strip() for v in line.split(",")]
+            try:
+                r = sum(b for i, b in enumerate(bits) if len(f) > 5 + i and f[5 + i].lower().startswith("active"))
+                self.samples.append((float(f[1]), float(f[2]), r))
+            except ValueError:
+                pass
 
     def __exit__(self, *a):
+        self._sample_now()  # and one at the end
+        self.stop.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
 
     def summary(self):
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = set()
-        for s in self.samples:
-            for i, nme in enumerate(names):
-                if len(s) > 5 + i and s[5 + i].lower().startswith("active"):
-                    reasons.add(nme)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.samples)}
+        sm = [s[0] for s in self.samples]
+        reasons = sorted(n for n, b in self.REASONS.items() if any(s[2] & b for s in self.samples))
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(s[1] for s in self.samples), "reasons": reasons,
+                "samples": len(self.samples), "source": "nvml" if self.proc is None else "nvidia-smi"}
 
 
 def peaks():
@@ -211,14 +273,19 @@ def run_ours(args):
     # device-resident inputs: the headline `value`
     lat = []
     launches0 = ctx.kernel_launches
-    ctx.profile(True)
-    ctx.profile_read(reset=True)
     with ClockSampler(local) as clk:
         ms = timed(dev, args.steps, lat)
-    prof = ctx.profile_read(reset=True)
-    ctx.profile(False)
     launches = ctx.kernel_launches - launches0
     job_ms = sorted(a.elapsed_time(b) for a, b in lat)
+    # per-kernel CUDA-event times from a separate, untimed pass
+    prof_steps = min(args.steps, 10)
+    ctx.profile(True)
+    ctx.profile_read(reset=True)
+    for _ in range(prof_steps):
+        step(dev)
+    torch.cuda.synchronize()
+    prof = ctx.profile_read(reset=True)
+    ctx.profile(False)
     # end to end: pinned host particles in, P(k) out
     ms_e2e = timed(pinned, args.steps) if not args.kernels_only else float("nan")
 
@@ -231,7 +298,7 @@ def run_ours(args):
     out = None
     if rank == 0:
         hbm, peak_kind = peaks()
-        jobs_rank = len(SCHEMES) * args.steps
+        jobs_rank = len(SCHEMES) * prof_steps  # jobs of the profiled pass
         # stage roofline: algorithmic bytes per job (unit = one mesh job)
         nh = NMESH * NMESH * (NMESH // 2 + 1)
         stage_bytes = {
@@ -240,8 +307,9 @@ def run_ours(args):
             "power": 8 * nh,
         }
         stage_kernels = {
-            "assign": ["assign_bin_count", "assign_scan", "assign_bin_scatter", "assign_deposit",
-                       "partial_sum_kernel<double>", "final_sum_kernel"],
+            "assign": ["assign_bin_count", "assign_starts", "tile_sum_kernel", "tile_offsets_kernel",
+                       "tile_scan_kernel", "assign_bin_scatter", "assign_deposit", "partial_sum_kernel<double>",
+                       "final_sum_kernel"],
             "fft_r2c": ["fft_rows_r2c", "fft_cols", "fft_rows_c2c"],
             "power": ["pk_bin", "pk_final_kernel"],
         }
@@ -254,6 +322,12 @@ def run_ours(args):
         dom = max(stages, key=lambda s: stages[s]["ms_per_job"])
         traffic = ncu_traffic()
         dom_traffic = traffic.get(dom) if isinstance(traffic, dict) else None
+        # the single kernel with the most time, with its ncu DRAM bytes
+        kname, (kl, kms) = max(prof.items(), key=lambda t: t[1][1])
+        kbytes = (traffic or {}).get("kernels", {}).get(kname)
+        dominant_kernel = {"name": kname, "ms_per_launch": round(kms / max(kl, 1), 4),
+                           "dram_bytes_per_launch": kbytes,
+                           "dram_gbs": round(kbytes / (kms / max(kl, 1) / 1e3) / 1e9, 1) if kbytes else None}
         kernels = {k: {"launches": v[0], "ms_total": round(v[1], 3)} for k, v in sorted(prof.items())}
         out = {
             "metric": METRIC, "value": round(value, 3), "unit": "jobs/s", "n_gpus": world,
@@ -268,7 +342,10 @@ def run_ours(args):
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "stage": dom, "achieved": stages[dom]["achieved_gbs"],
                          "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
-                         "frac": stages[dom]["frac"], "traffic": dom_traffic},
+                         "frac": stages[dom]["frac"], "traffic": dom_traffic,
+                         "note": "stage = the kernels that implement one assignment (algorithmic bytes "
+                                 "N_p*16 + 4*N^3 per job); traffic = their ncu DRAM bytes per job",
+                         "dominant_kernel": dominant_kernel},
             "stages": stages,
             "kernels": kernels,
             "clocks": clk.summary(),
@@ -563,9 +640,12 @@ def run_stream(args):
         rng = np.random.default_rng(99)
         gaps = rng.exponential(1.0 / rate, size=njobs) if rate else np.zeros(njobs)
         with Server(0, hbm_budget=budget, workers=workers, max_batch=max_batch) as srv:
-            for i in [srv.submit(make(j, k)) for k, j in enumerate(jobs[:8])]:
+            # warm-up: the first 100 jobs of the stream, all at once, so the
+            # contexts' buffers and plans are sized as a running server's are
+            for i in [srv.submit(make(j, k)) for k, j in enumerate(jobs[:100])]:
                 srv.wait(i)
             srv.stats(reset=True)
+            srv.trace()
             pending = []  # (id, bytes): inputs the client holds until done
             held = 0.0
             t_start = time.perf_counter()
@@ -646,6 +726,11 @@ def main():
                                "sample": f"{nsample} of {args.particles} particles per scheme (serial scatter "
                                          f"scaled by {args.particles / nsample:g}), full 256^3 FFT and P(k), "
                                          f"FFT on {cores} threads"}
+        if args.serving_jobs > 0:
+            # the metric's "vs plain path" part: the same jobs through the
+            # per-call path and through the serving loop, on this GPU
+            args.jobs = args.serving_jobs
+            out["serving"] = run_calib(args)
     print(json.dumps(out), flush=True)
 
 

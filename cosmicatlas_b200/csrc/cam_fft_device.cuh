@@ -238,17 +238,20 @@ constexpr int ct_threads(int len, int ncol, int ppt)
 }
 
 // Shared-memory slot of tile element i.  With PAD one spare element follows
-// every 32: row transforms (JSTRIDE 1) store their first stages with a
-// stride of R elements, which without padding lands a warp on two banks.
+// every 16: row transforms (JSTRIDE 1) store their first stages with a
+// stride of R elements, which without padding lands a warp on a few banks.
+// One slot in 16 makes every radix-8 stage of the power-of-two lengths
+// conflict-free for 8-byte elements (one in 32 still leaves two-way
+// conflicts in the first two stages).
 template <bool PAD>
 __device__ __forceinline__ int sidx(int i)
 {
-    return PAD ? i + (i >> 5) : i;
+    return PAD ? i + (i >> 4) : i;
 }
 // Elements a padded tile of n elements occupies.
 __host__ __device__ constexpr int64_t padded_len(int64_t n, bool pad)
 {
-    return pad ? n + n / 32 + 1 : n;
+    return pad ? n + n / 16 + 1 : n;
 }
 
 // One Stockham stage with every shape parameter known at compile time:

@@ -231,7 +231,10 @@ void power_bin(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins,
     auto *d_tab = static_cast<double *>(scratch(ctx, key, tab_bytes));
     if (fresh) CAM_CUDA_TRY(cudaMemcpyAsync(d_tab, tab.data(), tab_bytes, cudaMemcpyHostToDevice, ctx->stream));
 
-    const int grid = kNumSMs * 2;
+    // four CTAs per SM where their shared bins fit (<= 56 KB each), two
+    // otherwise: the loop is latency-bound, more resident warps hide it
+    const size_t smem_need = tab_bytes + (size_t)kPkWarps * nbins * (2 * sizeof(double) + sizeof(unsigned long long));
+    const int grid = kNumSMs * (smem_need <= 56 * 1024 ? 4 : 2);
     const int64_t nrows = (int64_t)n * n;
     const int64_t rpc = (nrows + grid - 1) / grid;
     auto *part = static_cast<double *>(scratch(ctx, "pk.part", (size_t)grid * nbins * 2 * sizeof(double)));

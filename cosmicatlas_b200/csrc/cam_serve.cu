@@ -141,8 +141,12 @@ void ensure_slot(Slot &s, const cam_job_desc &d)
         if (s.pin) cudaFreeHost(s.pin);
         s.pin = nullptr;
         s.pin_bytes = 0;
-        CAM_CUDA_TRY(cudaMallocHost(&s.pin, need));
-        s.pin_bytes = need;
+        // one allocation in practice: pinned allocation and release can
+        // synchronise the device, so the mirror starts large (64 KB: about
+        // 2,700 P(k) bins) rather than growing with each job's bin count
+        const size_t bytes = std::max<size_t>(need, 64 << 10);
+        CAM_CUDA_TRY(cudaMallocHost(&s.pin, bytes));
+        s.pin_bytes = bytes;
     }
 }
 
@@ -465,9 +469,10 @@ struct cam_server {
 
     // Under `mu`: picks the oldest queued job that may start (a large job
     // waits while max_big large jobs run; smaller jobs may pass it) and, if
-    // it is batchable, more batchable queued jobs -- of its own shape when
-    // there are several (a graph can be replayed), else of any shape -- up
-    // to max_batch, as far as the HBM budget allows.
+    // it is batchable, queued jobs of its own shape up to max_batch (their
+    // graph is replayed), as far as the HBM budget allows.  Jobs of distinct
+    // shapes run one per worker: batched together they would wait for the
+    // slowest of them and gain no graph.
     bool admit(Worker &w, std::vector<Job> &take)
     {
         size_t h = queue.size();
@@ -479,13 +484,9 @@ struct cam_server {
         if (h == queue.size()) return false;
         const Job &hd = queue[h];
         std::vector<size_t> pick{h};
-        if (hd.batchable) {
+        if (hd.batchable)
             for (size_t i = h + 1; i < queue.size() && (int)pick.size() < max_batch; ++i)
                 if (queue[i].batchable && queue[i].shape == hd.shape) pick.push_back(i);
-            if (pick.size() == 1)
-                for (size_t i = h + 1; i < queue.size() && i < h + 1024 && (int)pick.size() < max_batch; ++i)
-                    if (queue[i].batchable) pick.push_back(i);
-        }
         size_t need = 0;
         for (size_t i : pick) need += queue[i].footprint;
         const size_t r = reserved();
@@ -557,7 +558,7 @@ struct cam_server {
                     }
                     const int64_t before = w.br->replays;
                     w.br->run(d.data(), (int)take.size(), r.data(), rcs.data(),
-                              (int)take.size() == max_batch ? 1 : 2);  // mixed shapes: never captured
+                              (int)take.size() == max_batch ? 1 : 2);
                     rp = w.br->replays - before;
                     for (size_t i = 0; i < take.size(); ++i) {
                         *take[i].res = r[i];

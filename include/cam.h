@@ -243,7 +243,10 @@ typedef struct {
  * jobs on its own stream, so their work overlaps on the GPU).  A queued job
  * starts as soon as a worker is free and the server's device memory (held
  * caches plus the reservations of running jobs) stays within hbm_budget
- * (0 = 80% of the free memory); jobs are admitted in submission order.
+ * (0 = 80% of the free memory); jobs are admitted oldest first.  A large
+ * job (one that moves more than ~0.75 GB through HBM, and so fills the GPU
+ * by itself) runs on a context shared by the large jobs, one at a time;
+ * smaller jobs may start ahead of a large job that waits for that lane.
  * When several queued jobs share a small shape (N <= 128, no labels), a
  * worker takes up to max_batch of them and runs them as one graph-packed
  * batch, as cam_batch_run does. */

@@ -140,6 +140,26 @@ def test_bitwise_deterministic(ctx, scheme):
     assert np.array_equal(a.view(np.uint32), c.view(np.uint32))
 
 
+@pytest.mark.parametrize("scheme", SCHEMES)
+@pytest.mark.parametrize("n", [96, 32])
+def test_many_particles_vs_oracle(ctx, scheme, n):
+    # 4.5 M weighted particles (clumped, plus the edge positions).  At n = 32
+    # the bricks shrink to 4 x 4 x 32 cells, so TSC stencils cross brick
+    # faces for most particles (several payload records per particle).
+    box = 1000.0
+    x, y, z = mixed_inputs(n, box, 4_500_000, seed=31 + n)
+    w = synth.halo_masses(x.size, seed=32)
+    g = make_grid(n, box)
+    r = ctx.assign(x, y, z, w, g, scheme, F32)
+    ref, lost = orc.assign_f64(scheme, x, y, z, w, orc.Grid.cubic(n, box))
+    assert r.n_lost == lost
+    err = rel_err_cells(r.mesh, ref, float(np.mean(w)))
+    assert err <= 1e-5, err
+    p = np.random.default_rng(2).permutation(x.size)
+    c = ctx.assign(x[p], y[p], z[p], w[p], g, scheme, F32).mesh
+    assert np.array_equal(r.mesh.view(np.uint32), c.view(np.uint32))
+
+
 def test_device_arrays_roundtrip(ctx):
     import torch
     n, box = 64, 500.0
