@@ -49,8 +49,8 @@ def parse():
     ap.add_argument("--particles", type=int, default=N_PARTICLES)
     ap.add_argument("--kernels-only", action="store_true",
                     help="profiler runs: the device-resident pass only (no e2e pass, no CPU baseline)")
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "single512", "large768", "calib", "stream"],
-                    help="sweep: the benchmark line (default); single512 / large768: one-job latency lines; "
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "single512", "large768", "c1", "calib", "stream"],
+                    help="sweep: the benchmark line (default); single512 / large768 / c1: one-job latency lines; "
                          "calib / stream: served vs plain per-call jobs/s and latency")
     ap.add_argument("--jobs", type=int, default=0, help="calib / stream: number of jobs (0 = the config's)")
     ap.add_argument("--rates", default="50,200,800", help="stream: Poisson arrival rates (jobs/s)")
@@ -428,7 +428,14 @@ def run_single(args):
     from cosmicatlas_b200.api import CIC, TSC, Context, make_grid
 
     torch.cuda.set_device(0)
-    if args.workload == "single512":
+    prec = 0
+    if args.workload == "c1":
+        # config 1: 2,000,000 particles (20% uniform, 80% in 20,000 clumps of
+        # sigma 2), CIC onto 128^3 FP64, P(k) 64 bins, T-web R = 8, lambda_th 0
+        n, box, scheme, nb, ndel, R, lth, prec = 128, 1000.0, CIC, 64, 1.0, 8.0, 0.0, 1
+        x, y, z = synth.clumped(2_000_000, box, 20_000, 2.0, 0.8, seed=1)
+        arrs = [torch.from_numpy(v).cuda() for v in (x, y, z)]
+    elif args.workload == "single512":
         n = args.mesh or 512
         box, scheme, nb, ndel, R, lth = 1000.0, CIC, n // 2, 1.0, 2.0 * 1000.0 / n, 0.0
         x, y, z = synth.clumped(n ** 3, box, max(1, 2_000_000 * n ** 3 // 512 ** 3), 1.5, 0.8, seed=7)
@@ -446,7 +453,7 @@ def run_single(args):
     pko = Context.pk_opts(scheme, nbins=nb, ndel=ndel)
     two = Context.tweb_opts(R, lth, 1e-5)
     for _ in range(args.warmup):
-        ctx.job(arrs[0], arrs[1], arrs[2], None, grid, scheme, 0, pk=pko, tweb=two)
+        ctx.job(arrs[0], arrs[1], arrs[2], None, grid, scheme, prec, pk=pko, tweb=two)
     ctx.profile(True)
     ctx.profile_read(reset=True)
     times = []
@@ -455,7 +462,7 @@ def run_single(args):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        r = ctx.job(arrs[0], arrs[1], arrs[2], None, grid, scheme, 0, pk=pko, tweb=two)
+        r = ctx.job(arrs[0], arrs[1], arrs[2], None, grid, scheme, prec, pk=pko, tweb=two)
         e1.record(stream)
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1))
@@ -470,7 +477,7 @@ def run_single(args):
                    "tile_offsets_kernel", "tile_scan_kernel"],
         "fft_r2c": ["fft_rows_r2c", "fft_cols", "fft_rows_c2c"],
         "power": ["pk_bin", "pk_final_kernel"],
-        "tweb": ["tweb_tidal_x", "tweb_tidal_x_nyq", "tweb_tidal_z_eigen"],
+        "tweb": ["tweb_tidal_x", "tweb_tidal_x_nyq", "tweb_tidal_y", "tweb_tidal_y_nyq", "tweb_tidal_z_eigen"],
     }
     k = args.steps
     stages = {}
@@ -485,7 +492,34 @@ def run_single(args):
            "stages": stages, "kernels": {a: {"launches": b[0], "ms_total": round(b[1], 3)} for a, b in sorted(prof.items())},
            "tweb_counts": [int(v) for v in r["tweb"].counts], "n_lost": r["assign"].n_lost}
     ctx.close()
+    if args.workload == "c1":
+        out["cpu_ref"] = c1_cpu_reference(x, y, z, n, box, scheme, nb, R, lth)
     return out
+
+
+def c1_cpu_reference(x, y, z, n, box, scheme, nbins, R, lth):
+    """Config 1 through the oracle port of the reference path on the host:
+    the serial FP32 scatter as written, scipy rfftn on all cores (standing in
+    for threaded FFTW), the OpenMP P(k) loop, and the T-web (FFT tidal
+    tensor, per-cell eigenvalues)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    import scipy.fft
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    g = orc.Grid.cubic(n, box)
+    t0 = time.perf_counter()
+    mesh, _ = orc.assign_ref(scheme, x, y, z, None, g)
+    t1 = time.perf_counter()
+    ngal = float(mesh.sum(dtype=np.float64))
+    spec = scipy.fft.rfftn(mesh.astype(np.float64) - ngal / mesh.size, workers=cores)
+    orc.power_ref(spec, n, box, scheme, nbins, box ** 3 / ngal, ngal * ngal / box ** 3)
+    t2 = time.perf_counter()
+    orc.tweb_density(mesh.astype(np.float64), box, R, lth)
+    t3 = time.perf_counter()
+    return {"ms_per_job": round(1e3 * (t3 - t0), 1), "assign_ms": round(1e3 * (t1 - t0), 1),
+            "fft_pk_ms": round(1e3 * (t2 - t1), 1), "tweb_ms": round(1e3 * (t3 - t2), 1), "cores": cores,
+            "kind": "port"}
 
 
 # ------------------------------------------------------------------ serving
