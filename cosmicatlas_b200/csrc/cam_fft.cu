@@ -75,6 +75,70 @@ fft_cols_kernel(typename fftdev::CT<T>::t *base, int len, int ncols, int64_t jst
     }
 }
 
+// Column transforms, persistent and double-buffered: each CTA walks the
+// column tiles blockIdx.x, blockIdx.x + gridDim.x, ...; while it transforms
+// one tile in shared memory, the next tile's rows are already on their way
+// (asynchronous 16-byte copies), so the load latency that bounds the
+// one-tile-per-CTA kernel overlaps the butterflies.  Full tiles only
+// (ncols a multiple of W) and 16-byte aligned rows; the host checks.
+// Tile t: column tile t % nct, plane (t / nct) % nplanes, component
+// t / (nct * nplanes).
+// CTAs per SM the pipelined column kernel is built for: as many as fit
+// 1024 threads and two tiles each in 200 KB of shared memory.
+template <typename T, int LEN>
+constexpr int pipe_min_blocks()
+{
+    constexpr int nthr = fftdev::ct_threads(LEN, fftdev::CT<T>::kCols, fftdev::CT<T>::kPPT);
+    constexpr int by_thr = 1024 / nthr;
+    constexpr int by_smem = (200 * 1024) / (2 * LEN * fftdev::CT<T>::kCols * (int)sizeof(typename fftdev::CT<T>::t));
+    constexpr int b = by_thr < by_smem ? by_thr : by_smem;
+    return b > 1 ? b : 1;
+}
+
+template <typename T, bool INV, int LEN>
+__global__ void __launch_bounds__(fftdev::ct_threads(LEN, fftdev::CT<T>::kCols, fftdev::CT<T>::kPPT),
+                                  pipe_min_blocks<T, LEN>())
+fft_cols_pipe_kernel(typename fftdev::CT<T>::t *base, int nct, int nplanes, int64_t ntiles, int64_t jstride,
+                     int64_t pstride, int64_t ccomp, const typename fftdev::CT<T>::t *__restrict__ tw)
+{
+    using C = typename fftdev::CT<T>::t;
+    constexpr int W = fftdev::CT<T>::kCols;
+    constexpr int NTHR = fftdev::ct_threads(LEN, W, fftdev::CT<T>::kPPT);
+    constexpr int CPR = W * (int)sizeof(C) / 16;  // 16-byte chunks per tile row
+    constexpr int EPC = 16 / (int)sizeof(C);      // elements per chunk
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *const buf0 = reinterpret_cast<C *>(smem_raw);  // tiles at buf0 and buf0 + LEN * W
+    auto tile_ptr = [&](int64_t t) {
+        const int64_t ct = t % nct, r = t / nct;
+        return base + (r / nplanes) * ccomp + (r % nplanes) * pstride + ct * W;
+    };
+    auto load = [&](int64_t t, C *dst) {
+        const C *g = tile_ptr(t);
+        for (int e = threadIdx.x; e < LEN * CPR; e += NTHR) {
+            const int j = e / CPR, k = e % CPR;
+            fftdev::cp_async16(dst + j * W + k * EPC, g + (int64_t)j * jstride + k * EPC);
+        }
+    };
+    int cur = 0;
+    int64_t t = blockIdx.x;
+    if (t < ntiles) load(t, buf0);
+    fftdev::cp_async_commit();
+    for (; t < ntiles; t += gridDim.x) {
+        C *const here = buf0 + cur * (LEN * W), *const other = buf0 + (cur ^ 1) * (LEN * W);
+        const int64_t tn = t + gridDim.x;
+        if (tn < ntiles) load(tn, other);
+        fftdev::cp_async_commit();
+        fftdev::cp_async_wait<1>();  // this thread's copies of tile t have landed
+        __syncthreads();     // ... and everyone's
+        fftdev::block_fft_fixed<C, INV, false, W, LEN, NTHR, W, 1, 1>(here, tw);
+        C *g = tile_ptr(t);
+        for (int e = threadIdx.x; e < LEN * W; e += NTHR) g[(int64_t)(e / W) * jstride + (e % W)] = here[e];
+        __syncthreads();  // buf[cur] is refilled by the next iteration's prefetch
+        cur ^= 1;
+    }
+    fftdev::cp_async_wait<0>();
+}
+
 // Row transforms along the contiguous axis.
 //   MODE 0 (r2c): real rows of n -> main rows of n/2 + nyq element
 //   MODE 1 (c2r): main rows + nyq -> real rows of n (times `scale`)
@@ -221,8 +285,27 @@ void cols_impl(cam_ctx *ctx, FftPlan *p, void *base, int64_t len, int64_t ncols,
     const int nthr = threads_for((int)len * W, fftdev::CT<T>::kPPT);  // == ct_threads for compiled lengths
     const size_t smem = (size_t)len * W * sizeof(C);
     dim3 grid((unsigned)((ncols + W - 1) / W), (unsigned)nplanes, (unsigned)ncomp);
+    // persistent double-buffered kernel: compile-time length, full tiles,
+    // 16-byte aligned rows, two tiles within 200 KB of shared memory
+    const size_t es = sizeof(C);
+    const bool pipe_ok = ncols % W == 0 && (jstride * es) % 16 == 0 && (pstride * es) % 16 == 0 &&
+                         (ccomp * es) % 16 == 0 && ((uintptr_t)base % 16) == 0 && 2 * smem <= 200 * 1024 &&
+                         (int64_t)nplanes * ncomp * (ncols / W) < (1ll << 40);
     dispatch_fft_len(len, [&](auto lc) {
         constexpr int LEN = decltype(lc)::value;
+        if constexpr (LEN > 0 && 2 * LEN * W * sizeof(C) <= 200 * 1024) {
+            if (pipe_ok) {
+                auto kp = inv ? fft_cols_pipe_kernel<T, true, LEN> : fft_cols_pipe_kernel<T, false, LEN>;
+                smem_at_least(kp, 2 * smem);
+                int per_sm = 0;
+                CAM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kp, nthr, 2 * smem));
+                const int64_t ntiles = (int64_t)nplanes * ncomp * (ncols / W);
+                const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)kNumSMs * std::max(per_sm, 1)));
+                CAM_LAUNCH_NAMED(ctx, "fft_cols", kp, g, nthr, 2 * smem, static_cast<C *>(base), (int)(ncols / W),
+                                 (int)nplanes, ntiles, jstride, pstride, ccomp, static_cast<const C *>(p->tw));
+                return;
+            }
+        }
         auto kern = inv ? fft_cols_kernel<T, true, LEN> : fft_cols_kernel<T, false, LEN>;
         smem_at_least(kern, smem);
         CAM_LAUNCH_NAMED(ctx, "fft_cols", kern, grid, nthr, smem, static_cast<C *>(base), (int)len, (int)ncols,

@@ -237,6 +237,21 @@ constexpr int ct_threads(int len, int ncol, int ppt)
     return ((len * ncol + ppt - 1) / ppt + 31) / 32 * 32;
 }
 
+// 16-byte asynchronous global -> shared copy (LDGSTS, cached in L2 only)
+// and its group fences; the waits are hardware waits on this thread's own
+// copies.
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // Shared-memory slot of tile element i.  With PAD one spare element follows
 // every 16: row transforms (JSTRIDE 1) store their first stages with a
 // stride of R elements, which without padding lands a warp on a few banks.

@@ -195,6 +195,117 @@ tidal_y_kernel(typename CTw<T>::t *__restrict__ base, int n, int ncols, int64_t 
     }
 }
 
+// CTAs per SM the pipelined T-web column kernel is built for: as many as
+// fit 1024 threads and three tiles each in 200 KB of shared memory.
+template <typename T, int LEN>
+constexpr int tpipe_min_blocks()
+{
+    constexpr int by_thr = 1024 / col_threads<T, LEN>();
+    constexpr int by_smem = (200 * 1024) / (3 * LEN * CTw<T>::kCols * (int)sizeof(typename CTw<T>::t));
+    constexpr int b = by_thr < by_smem ? by_thr : by_smem;
+    return b > 1 ? b : 1;
+}
+
+// Pipelined T-web column passes over the main planes; persistent CTAs walk
+// the work units blockIdx.x, blockIdx.x + gridDim.x, ...  While a unit is
+// worked on, the next unit's input tile is already being copied in
+// (asynchronous 16-byte copies), and a separate work tile lets one loaded
+// input give several outputs.
+//   MODE 0 (x pass): unit = (column tile, plane j) of delta_k; it gives the
+//     fields k_x^p phi, p = 0, 1, 2, each transformed along x into slot p.
+//   MODE 1 (y pass): unit = (p, column tile, plane i); slot p's tile gives
+//     the fields (p, q), q = 2-p .. 0, each times k_y^q and transformed
+//     along y into slot_of(p, q); (p, 0) goes last, over its own input.
+// Element (j, col) of a tile sits at (tile base) + j*jstride + col, the
+// unit's tile base at plane*pstride + column tile*W; full tiles only and
+// 16-byte aligned rows (the host checks).
+template <typename T, int MODE, int LEN>
+__global__ void __launch_bounds__(col_threads<T, LEN>(), tpipe_min_blocks<T, LEN>())
+tidal_pipe_kernel(const typename CTw<T>::t *src, typename CTw<T>::t *dst, int n, int nct, int64_t nunits,
+                  int64_t jstride, int64_t pstride, int64_t ccomp, const typename CTw<T>::t *__restrict__ tw,
+                  double gauss_coef, const double *__restrict__ d_mean, int density_input, double scale)
+{
+    using C = typename CTw<T>::t;
+    constexpr int W = CTw<T>::kCols;
+    constexpr int NTHR = col_threads<T, LEN>();
+    constexpr int CPR = W * (int)sizeof(C) / 16;  // 16-byte chunks per tile row
+    constexpr int EPC = 16 / (int)sizeof(C);
+    constexpr int TILE = LEN * W;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *const in0 = reinterpret_cast<C *>(smem_raw);  // input tiles at in0 and in0 + TILE
+    C *const work = in0 + 2 * TILE;
+    const int h = n / 2;
+    T norm = (T)0, gc = (T)0;
+    if (MODE == 0) {
+        double normd = scale;
+        if (density_input) normd /= *d_mean;  // delta_k = F(rho - mean) / mean
+        norm = (T)normd;
+        gc = (T)gauss_coef;
+    }
+    // unit -> (p, column tile, plane); p = 0 for the x pass (all three made)
+    auto decode = [&](int64_t t, int &p, int &ct, int &plane) {
+        if (MODE == 0) {
+            p = 0;
+            ct = (int)(t % nct);
+            plane = (int)(t / nct);
+        } else {
+            p = (int)(t % 3);
+            const int64_t r = t / 3;
+            ct = (int)(r % nct);
+            plane = (int)(r / nct);
+        }
+    };
+    auto load = [&](int64_t t, C *buf) {
+        int p, ct, plane;
+        decode(t, p, ct, plane);
+        const C *g = src + (MODE == 1 ? (int64_t)p * ccomp : 0) + (int64_t)plane * pstride + (int64_t)ct * W;
+        for (int e = threadIdx.x; e < LEN * CPR; e += NTHR) {
+            const int j = e / CPR, k = e % CPR;
+            fftdev::cp_async16(buf + j * W + k * EPC, g + (int64_t)j * jstride + k * EPC);
+        }
+    };
+    int cur = 0;
+    int64_t t = blockIdx.x;
+    if (t < nunits) load(t, in0);
+    fftdev::cp_async_commit();
+    for (; t < nunits; t += gridDim.x) {
+        C *const in = in0 + cur * TILE;
+        const int64_t tn = t + gridDim.x;
+        if (tn < nunits) load(tn, in0 + (cur ^ 1) * TILE);
+        fftdev::cp_async_commit();
+        fftdev::cp_async_wait<1>();  // this thread's copies of unit t have landed
+        __syncthreads();             // ... and everyone's
+        int p, ct, plane;
+        decode(t, p, ct, plane);
+        const int nout = MODE == 0 ? 3 : 3 - p;
+        for (int o = 0; o < nout; ++o) {
+            const int q = MODE == 0 ? 0 : 2 - p - o;  // y pass: q = 2-p .. 0
+            const int pp = MODE == 0 ? o : p;
+            for (int e = threadIdx.x; e < TILE; e += NTHR) {
+                const int j = e / W, cc = e % W;
+                const int fj = j <= h ? j : j - n;
+                T m;
+                if (MODE == 0) {
+                    const int fy = plane <= h ? plane : plane - n;
+                    m = phi_mult<T>(pp, fj, fy, ct * W + cc, gc, norm);
+                } else {
+                    m = (T)ipow(fj, q);
+                }
+                const C v = in[e];
+                work[e] = C{v.x * m, v.y * m};
+            }
+            __syncthreads();
+            fftdev::block_fft_fixed<C, true, false, W, LEN, NTHR, W, 1, 1>(work, tw);
+            const int slot = MODE == 0 ? pp : slot_of(p, q);
+            C *g = dst + (int64_t)slot * ccomp + (int64_t)plane * pstride + (int64_t)ct * W;
+            for (int e = threadIdx.x; e < TILE; e += NTHR) g[(int64_t)(e / W) * jstride + (e % W)] = work[e];
+            __syncthreads();  // work is refilled by the next output
+        }
+        cur ^= 1;
+    }
+    fftdev::cp_async_wait<0>();
+}
+
 // FP32 trigonometric eigenvalues of a symmetric 3x3 matrix (O.K. Smith,
 // CACM 4(4):168, 1961), each refined by one Newton step on the FP64
 // characteristic polynomial; returned in descending order.
@@ -279,6 +390,58 @@ __device__ __forceinline__ int count_above(double c2, double c1, double c0, doub
     return changes;
 }
 
+// Label of one cell from its six field values (slots 0..5 of t6), written
+// to labels[cell] (and lambdas when LAMBDAS); the label and tie counters
+// of the calling thread are advanced.
+template <bool LAMBDAS>
+__device__ __forceinline__ void label_cell(const float t6[6], double lth, double band, int64_t cell, int64_t ncell,
+                                           uint8_t *__restrict__ labels, float *__restrict__ lambdas,
+                                           unsigned &lc0, unsigned &lc1, unsigned &lc2, unsigned &lc3,
+                                           unsigned &lties)
+{
+    // (xx, yy, zz, xy, xz, yz) from slots (2, 4, 0, 5, 1, 3)
+    int v = 0, tie = 0;
+    if constexpr (LAMBDAS) {
+        double lam[3];
+        eig3(t6[2], t6[4], t6[0], t6[5], t6[1], t6[3], lam);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            v += lam[a] > lth;
+            tie |= fabs(lam[a] - lth) <= band;
+        }
+        lambdas[cell] = (float)lam[0];
+        lambdas[ncell + cell] = (float)lam[1];
+        lambdas[2 * ncell + cell] = (float)lam[2];
+    } else {
+        double c2, c1, c0;
+        char_poly(t6[2], t6[4], t6[0], t6[5], t6[1], t6[3], c2, c1, c0);
+        v = count_above(c2, c1, c0, lth);
+        tie = count_above(c2, c1, c0, lth - band) != count_above(c2, c1, c0, lth + band);
+    }
+    if (labels) labels[cell] = (uint8_t)(4 - v);
+    lc0 += v == 3;  // label 1, knot
+    lc1 += v == 2;
+    lc2 += v == 1;
+    lc3 += v == 0;  // label 4, void
+    lties += tie;
+}
+
+// Adds the CTA's label and tie counters to counts[0..4] (cnt_s: five shared
+// words, zeroed before the first barrier of the kernel).
+__device__ __forceinline__ void flush_counts(unsigned lc0, unsigned lc1, unsigned lc2, unsigned lc3, unsigned lties,
+                                             unsigned *cnt_s, unsigned long long *__restrict__ counts)
+{
+#pragma unroll
+    for (int a = 0; a < 5; ++a) {
+        unsigned v = a == 0 ? lc0 : a == 1 ? lc1 : a == 2 ? lc2 : a == 3 ? lc3 : lties;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if ((threadIdx.x & 31) == 0 && v) atomicAdd(&cnt_s[a], v);
+    }
+    __syncthreads();
+    if (threadIdx.x < 5 && cnt_s[threadIdx.x]) atomicAdd(&counts[threadIdx.x], (unsigned long long)cnt_s[threadIdx.x]);
+}
+
 // c2r along z of the six components for `rpc` rows, then eigenvalues and
 // labels.  Without LAMBDAS the eigenvalues are not formed: the label needs
 // only the number of them above lambda_th, and the tie flag whether that
@@ -341,7 +504,7 @@ tidal_z_kernel(const typename CTw<T>::t *__restrict__ src, const typename CTw<T>
         fftdev::block_fft<C, CTw<T>::kPPT, true, true, 0>(tile, M, 6 * rpc, 1, M, rd, tw, 2);
     }
     // Per cell: 6 components -> eigenvalues -> label.
-    unsigned int lc0 = 0, lc1 = 0, lc2 = 0, lc3 = 0, lties = 0;
+    unsigned lc0 = 0, lc1 = 0, lc2 = 0, lc3 = 0, lties = 0;
     // real value z of row r of comp c: half z & 1 of complex element (c*rpc + r)*M + z/2
     const T *re = reinterpret_cast<const T *>(tile);
     const int64_t ncell = nn * n;
@@ -351,42 +514,110 @@ tidal_z_kernel(const typename CTw<T>::t *__restrict__ src, const typename CTw<T>
 #pragma unroll
         for (int c = 0; c < 6; ++c)
             t6[c] = (float)re[2 * fftdev::sidx<PAD>((c * rpcv + r) * M + (z >> 1)) + (z & 1)];
-        // (xx, yy, zz, xy, xz, yz) from slots (2, 4, 0, 5, 1, 3)
-        int v = 0, tie = 0;
-        const int64_t cell = (row0 + r) * nz + z;
-        if constexpr (LAMBDAS) {
-            double lam[3];
-            eig3(t6[2], t6[4], t6[0], t6[5], t6[1], t6[3], lam);
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                v += lam[a] > lth;
-                tie |= fabs(lam[a] - lth) <= band;
-            }
-            lambdas[cell] = (float)lam[0];
-            lambdas[ncell + cell] = (float)lam[1];
-            lambdas[2 * ncell + cell] = (float)lam[2];
-        } else {
-            double c2, c1, c0;
-            char_poly(t6[2], t6[4], t6[0], t6[5], t6[1], t6[3], c2, c1, c0);
-            v = count_above(c2, c1, c0, lth);
-            tie = count_above(c2, c1, c0, lth - band) != count_above(c2, c1, c0, lth + band);
+        label_cell<LAMBDAS>(t6, lth, band, (row0 + r) * nz + z, ncell, labels, lambdas, lc0, lc1, lc2, lc3, lties);
+    }
+    flush_counts(lc0, lc1, lc2, lc3, lties, cnt_s, counts);
+}
+
+// The z pass, persistent and pipelined (compile-time length LEN = N/2):
+// CTAs walk the groups of RPC rows blockIdx.x, blockIdx.x + gridDim.x, ...
+// A group's raw rows are consumed by the untangling step, so the copy of
+// the next group's rows into the same raw buffer (asynchronous 16-byte
+// copies) starts right after it and runs while the group is transformed
+// and labelled.  Label counts are kept per thread across groups and added
+// once per CTA.
+template <typename T, int LEN>
+constexpr int zpipe_threads()
+{
+    return fftdev::ct_threads(LEN, 6 * tweb_rpc<T>(LEN), CTw<T>::kPPT);
+}
+template <typename T, int LEN>
+constexpr size_t zpipe_smem()
+{
+    return ((size_t)6 * tweb_rpc<T>(LEN) * LEN + (size_t)fftdev::padded_len(6 * tweb_rpc<T>(LEN) * LEN, true)) *
+           sizeof(typename CTw<T>::t);
+}
+template <typename T, int LEN, bool LAMBDAS>
+__global__ void __launch_bounds__(zpipe_threads<T, LEN>(), 2)  // <= 128 registers: no spills
+tidal_z_pipe_kernel(const typename CTw<T>::t *__restrict__ src, const typename CTw<T>::t *__restrict__ nyq, int n,
+                    int64_t nrows, int64_t ccomp, const typename CTw<T>::t *__restrict__ tw, double lth, double band,
+                    uint8_t *__restrict__ labels, float *__restrict__ lambdas,
+                    unsigned long long *__restrict__ counts /* [5] */)
+{
+    using C = typename CTw<T>::t;
+    constexpr int M = LEN;
+    constexpr int RPC = tweb_rpc<T>(LEN);
+    constexpr int PER = RPC * M;    // complex elements of one field in a group
+    constexpr int RAW = 6 * PER;
+    constexpr int NTHR = zpipe_threads<T, LEN>();
+    constexpr int EPC = 16 / (int)sizeof(C);
+    constexpr int CPRow = M / EPC;  // 16-byte chunks per row
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *const raw = reinterpret_cast<C *>(smem_raw);  // the raw rows of one group
+    C *const tile = raw + RAW;                       // padded work tile [6][RPC][M]
+    __shared__ unsigned cnt_s[5];
+    if (threadIdx.x < 5) cnt_s[threadIdx.x] = 0;
+    const int64_t nn = (int64_t)n * n, ncell = nn * n;
+    const int64_t ngroups = (nrows + RPC - 1) / RPC;
+    auto load = [&](int64_t gi, C *buf) {
+        const int64_t row0 = gi * RPC;
+        const int nr = (int)min((int64_t)RPC, nrows - row0);
+        for (int e = threadIdx.x; e < 6 * RPC * CPRow; e += NTHR) {
+            const int c = e / (RPC * CPRow), rem = e % (RPC * CPRow);
+            const int r = rem / CPRow, k = rem % CPRow;
+            if (r < nr)
+                fftdev::cp_async16(buf + c * PER + r * M + k * EPC, src + (int64_t)c * ccomp + (row0 + r) * M + k * EPC);
         }
-        if (labels) labels[cell] = (uint8_t)(4 - v);
-        lc0 += v == 3;  // label 1, knot
-        lc1 += v == 2;
-        lc2 += v == 1;
-        lc3 += v == 0;  // label 4, void
-        lties += tie;
-    }
+    };
+    unsigned lc0 = 0, lc1 = 0, lc2 = 0, lc3 = 0, lties = 0;
+    int64_t gi = blockIdx.x;
+    if (gi < ngroups) load(gi, raw);
+    fftdev::cp_async_commit();
+    for (; gi < ngroups; gi += gridDim.x) {
+        fftdev::cp_async_wait<0>();  // this thread's copies of group gi have landed
+        __syncthreads();             // ... and everyone's
+        const int64_t row0 = gi * RPC;
+        const int nr = (int)min((int64_t)RPC, nrows - row0);
+        // c2r untangling with the remaining factor k_z^r of each field
+        for (int e = threadIdx.x; e < RAW; e += NTHR) {
+            const int c = e / PER, rem = e % PER;
+            const int r = rem / M, k = rem % M;
+            if (r >= nr) continue;
+            C xk = raw[c * PER + r * M + k];
+            C xm = k == 0 ? nyq[(int64_t)c * nn + row0 + r] : raw[c * PER + r * M + (M - k)];
+            if (k == 0) {
+                xk.y = 0;
+                xm.y = 0;
+            }
+            const int rz = kz_power(c);
+            const T fa = (T)ipow(k, rz), fb = (T)ipow(k == 0 ? M : M - k, rz);
+            xk = C{xk.x * fa, xk.y * fa};
+            xm = C{xm.x * fb, xm.y * fb};
+            const C a = C{xk.x + xm.x, xk.y - xm.y};
+            const C b = C{xk.x - xm.x, xk.y + xm.y};
+            C wv = __ldg(tw + k);
+            wv.y = -wv.y;
+            const C ib = fftdev::rot<C, true>(fftdev::cmul(wv, b));
+            tile[fftdev::sidx<true>(e)] = fftdev::cadd(a, ib);
+        }
+        __syncthreads();  // raw is consumed: fetch the next group behind the transform
+        const int64_t gn = gi + gridDim.x;
+        if (gn < ngroups) load(gn, raw);
+        fftdev::cp_async_commit();
+        fftdev::block_fft_fixed<C, true, true, 6 * RPC, LEN, NTHR, 1, LEN, 2, true>(tile, tw);
+        const T *re = reinterpret_cast<const T *>(tile);
+        for (int e = threadIdx.x; e < nr * 2 * M; e += NTHR) {
+            const int r = e / (2 * M), z = e % (2 * M);
+            float t6[6];
 #pragma unroll
-    for (int a = 0; a < 5; ++a) {
-        unsigned int v = a == 0 ? lc0 : a == 1 ? lc1 : a == 2 ? lc2 : a == 3 ? lc3 : lties;
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-        if ((threadIdx.x & 31) == 0 && v) atomicAdd(&cnt_s[a], v);
+            for (int c = 0; c < 6; ++c) t6[c] = (float)re[2 * fftdev::sidx<true>((c * RPC + r) * M + (z >> 1)) + (z & 1)];
+            label_cell<LAMBDAS>(t6, lth, band, (row0 + r) * 2 * M + z, ncell, labels, lambdas, lc0, lc1, lc2, lc3,
+                                lties);
+        }
+        __syncthreads();  // tile is refilled next
     }
-    __syncthreads();
-    if (threadIdx.x < 5 && cnt_s[threadIdx.x]) atomicAdd(&counts[threadIdx.x], (unsigned long long)cnt_s[threadIdx.x]);
+    fftdev::cp_async_wait<0>();
+    flush_counts(lc0, lc1, lc2, lc3, lties, cnt_s, counts);
 }
 
 int threads_for(int points, int ppt, int cap)
@@ -394,6 +625,38 @@ int threads_for(int points, int ppt, int cap)
     int t = (points + ppt - 1) / ppt;
     t = ((t + 31) / 32) * 32;
     return std::max(32, std::min(cap, t));
+}
+
+// Launches the pipelined T-web column kernel for the main planes when it
+// applies (compile-time length, full 16-byte aligned tiles, three tiles
+// within 200 KB of shared memory); returns false otherwise.
+template <typename T, int MODE, int LEN>
+bool pipe_launch(cam_ctx *ctx, const char *name, const typename CTw<T>::t *src, typename CTw<T>::t *dst, int64_t n,
+                 int64_t M, int64_t jstride, int64_t pstride, int64_t ccomp, const typename CTw<T>::t *tw,
+                 double gcoef, const double *d_mean, int density, double scale)
+{
+    using C = typename CTw<T>::t;
+    constexpr int W = CTw<T>::kCols;
+    if constexpr (LEN == 0 || 3 * LEN * W * sizeof(C) > 200 * 1024) {
+        return false;
+    } else {
+        const size_t es = sizeof(C);
+        if (M % W != 0 || (jstride * es) % 16 || (pstride * es) % 16 || (ccomp * es) % 16 ||
+            ((uintptr_t)src % 16) || ((uintptr_t)dst % 16))
+            return false;
+        auto k = tidal_pipe_kernel<T, MODE, LEN>;
+        const size_t smem = 3 * (size_t)LEN * W * sizeof(C);
+        smem_at_least(k, smem);
+        int per_sm = 0;
+        CAM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, col_threads<T, LEN>(), smem));
+        const int nct = (int)(M / W);
+        const int64_t nunits = (int64_t)nct * n * (MODE == 0 ? 1 : 3);
+        const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>(nunits, (int64_t)kNumSMs * std::max(per_sm, 1)));
+        constexpr int nthr = col_threads<T, LEN>();
+        CAM_LAUNCH_NAMED(ctx, name, k, g, nthr, smem, src, dst, (int)n, nct, nunits, jstride, pstride, ccomp, tw, gcoef,
+                         d_mean, density, scale);
+        return true;
+    }
 }
 
 template <typename T>
@@ -427,11 +690,14 @@ void tweb_impl(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const d
         constexpr int LEN = decltype(lc)::value;
         auto k0 = tidal_x_kernel<T, false, LEN>;
         auto k1 = tidal_x_kernel<T, true, LEN>;
-        smem_at_least(k0, smem);
         smem_at_least(k1, smem);
-        dim3 g0(3, (unsigned)((M + W - 1) / W), (unsigned)n);
-        CAM_LAUNCH_NAMED(ctx, "tweb_tidal_x", k0, g0, nthr, smem, static_cast<const C *>(dk.main), cm, (int)n, (int)M, n * M,
-                   (int64_t)M, ccomp, rn, tw, gcoef, d_mean, density, scale);
+        if (!pipe_launch<T, 0, LEN>(ctx, "tweb_tidal_x", static_cast<const C *>(dk.main), cm, n, M, n * M, (int64_t)M,
+                                    ccomp, tw, gcoef, d_mean, density, scale)) {
+            smem_at_least(k0, smem);
+            dim3 g0(3, (unsigned)((M + W - 1) / W), (unsigned)n);
+            CAM_LAUNCH_NAMED(ctx, "tweb_tidal_x", k0, g0, nthr, smem, static_cast<const C *>(dk.main), cm, (int)n,
+                             (int)M, n * M, (int64_t)M, ccomp, rn, tw, gcoef, d_mean, density, scale);
+        }
         dim3 g1(3, (unsigned)((n + W - 1) / W), 1);
         CAM_LAUNCH_NAMED(ctx, "tweb_tidal_x_nyq", k1, g1, nthr, smem, static_cast<const C *>(dk.nyq), cn, (int)n, (int)n, n,
                    (int64_t)0, nn, rn, tw, gcoef, d_mean, density, scale);
@@ -446,9 +712,12 @@ void tweb_impl(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const d
         auto ky = tidal_y_kernel<T, LEN>;
         smem_at_least(ky, smem);
         // main: planes i, FFT index j (stride M), columns k (stride 1)
-        dim3 g0(3, (unsigned)((M + W - 1) / W), (unsigned)n);
-        CAM_LAUNCH_NAMED(ctx, "tweb_tidal_y", ky, g0, nthr, smem, cm, (int)n, (int)M, (int64_t)M, (int64_t)1, n * M,
-                         ccomp, rn, tw);
+        if (!pipe_launch<T, 1, LEN>(ctx, "tweb_tidal_y", cm, cm, n, M, (int64_t)M, n * M, ccomp, tw, 0.0, nullptr, 0,
+                                    1.0)) {
+            dim3 g0(3, (unsigned)((M + W - 1) / W), (unsigned)n);
+            CAM_LAUNCH_NAMED(ctx, "tweb_tidal_y", ky, g0, nthr, smem, cm, (int)n, (int)M, (int64_t)M, (int64_t)1, n * M,
+                             ccomp, rn, tw);
+        }
         // Nyquist plane: columns i (stride N), FFT index j (stride 1)
         dim3 g1(3, (unsigned)((n + W - 1) / W), 1);
         CAM_LAUNCH_NAMED(ctx, "tweb_tidal_y_nyq", ky, g1, nthr, smem, cn, (int)n, (int)n, (int64_t)1, n, (int64_t)0,
@@ -466,6 +735,21 @@ void tweb_impl(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const d
         dispatch_fft_len(M, [&](auto lc) {
         constexpr int LEN = decltype(lc)::value;
         const size_t smem = (size_t)fftdev::padded_len(6 * rpc * M, LEN > 0) * sizeof(C);
+        if constexpr (LEN > 0 && LEN <= 512 && (LEN & (LEN - 1)) == 0 && zpipe_smem<T, LEN>() <= 200 * 1024) {
+            // persistent pipelined z pass, for the power-of-two row lengths
+            // (whose transforms fit the register bound without spilling)
+            auto kp = d_lambdas ? tidal_z_pipe_kernel<T, LEN, true> : tidal_z_pipe_kernel<T, LEN, false>;
+            constexpr size_t psmem = zpipe_smem<T, LEN>();
+            constexpr int pthr = zpipe_threads<T, LEN>();
+            smem_at_least(kp, psmem);
+            int per_sm = 0;
+            CAM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kp, pthr, psmem));
+            const int64_t ngroups = (nn + tweb_rpc<T>(LEN) - 1) / tweb_rpc<T>(LEN);
+            const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ngroups, (int64_t)kNumSMs * std::max(per_sm, 1)));
+            CAM_LAUNCH_NAMED(ctx, "tweb_tidal_z_eigen", kp, g, pthr, psmem, cm, cn, (int)n, nn, ccomp, tw, o.lambda_th,
+                             o.tie_band, d_labels, d_lambdas, cnt);
+            return;
+        }
         auto kz = d_lambdas ? tidal_z_kernel<T, LEN, true> : tidal_z_kernel<T, LEN, false>;
         smem_at_least(kz, smem);
         const unsigned grid = (unsigned)((nn + rpc - 1) / rpc);
