@@ -238,6 +238,74 @@ fft_rows_kernel(const void *in, void *out_main, typename fftdev::CT<T>::t *nyq, 
     }
 }
 
+// r2c rows (mode 0 of fft_rows_kernel), persistent and pipelined, for one
+// component and a compile-time half length LEN: CTAs walk the groups of
+// rows_rpc rows blockIdx.x, blockIdx.x + gridDim.x, ...  A group's raw rows
+// are consumed when they are copied (minus the mean) into the padded work
+// tile, so the next group's copy into the raw buffer starts right after and
+// runs while the group is transformed and untangled.
+template <typename T, int LEN>
+__global__ void __launch_bounds__(fftdev::ct_threads(LEN, rows_rpc<T>(LEN), fftdev::CT<T>::kPPT), 2)
+fft_rows_r2c_pipe_kernel(const T *__restrict__ in, typename fftdev::CT<T>::t *__restrict__ out_main,
+                         typename fftdev::CT<T>::t *__restrict__ nyq, int64_t nrows,
+                         const typename fftdev::CT<T>::t *__restrict__ tw, const double *__restrict__ d_sub)
+{
+    using C = typename fftdev::CT<T>::t;
+    constexpr int M = LEN;
+    constexpr int RPC = rows_rpc<T>(LEN);
+    constexpr int RAW = RPC * M;
+    constexpr int NTHR = fftdev::ct_threads(LEN, RPC, fftdev::CT<T>::kPPT);
+    constexpr int EPC = 16 / (int)sizeof(C);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *const raw = reinterpret_cast<C *>(smem_raw);
+    C *const tile = raw + RAW;  // element e at slot sidx<true>(e)
+    const C *src = reinterpret_cast<const C *>(in);
+    const T sub = d_sub ? (T)(*d_sub) : (T)0;
+    const int64_t ngroups = (nrows + RPC - 1) / RPC;
+    auto load = [&](int64_t gi) {
+        const int64_t row0 = gi * RPC;
+        const int tot = (int)min((int64_t)RPC, nrows - row0) * M;
+        for (int e = threadIdx.x * EPC; e < tot; e += NTHR * EPC) fftdev::cp_async16(raw + e, src + row0 * M + e);
+    };
+    int64_t gi = blockIdx.x;
+    if (gi < ngroups) load(gi);
+    fftdev::cp_async_commit();
+    for (; gi < ngroups; gi += gridDim.x) {
+        fftdev::cp_async_wait<0>();
+        __syncthreads();
+        const int64_t row0 = gi * RPC;
+        const int nr = (int)min((int64_t)RPC, nrows - row0);
+        for (int e = threadIdx.x; e < nr * M; e += NTHR) {
+            C v = raw[e];
+            v.x -= sub;
+            v.y -= sub;
+            tile[fftdev::sidx<true>(e)] = v;
+        }
+        __syncthreads();  // raw is consumed: fetch the next group behind the transform
+        const int64_t gn = gi + gridDim.x;
+        if (gn < ngroups) load(gn);
+        fftdev::cp_async_commit();
+        // all RPC rows (the unused ones of the last group hold stale data and are not stored)
+        fftdev::block_fft_fixed<C, false, true, RPC, LEN, NTHR, 1, LEN, 2, true>(tile, tw);
+        C *dm = out_main + row0 * M;
+        C *dn = nyq + row0;
+        for (int e = threadIdx.x; e < nr * (M + 1); e += NTHR) {
+            const int r = e / (M + 1), k = e % (M + 1);
+            const C zk = tile[fftdev::sidx<true>(r * M + (k % M))];
+            const C zc0 = tile[fftdev::sidx<true>(r * M + ((M - k) % M))];
+            const C zc = C{zc0.x, -zc0.y};
+            // X[k] = (Z[k] + conj Z[M-k])/2 - i/2 e^{-2 pi i k/n} (Z[k] - conj Z[M-k])
+            const C s = fftdev::cadd(zk, zc), d = fftdev::csub(zk, zc);
+            const C wd = fftdev::cmul(__ldg(tw + k), d);
+            const C xk = C{(T)0.5 * (s.x + wd.y), (T)0.5 * (s.y - wd.x)};
+            if (k < M) dm[(int64_t)r * M + k] = xk;
+            else dn[r] = xk;
+        }
+        __syncthreads();  // tile is refilled next
+    }
+    fftdev::cp_async_wait<0>();
+}
+
 template <typename T>
 __global__ void split_to_fftw_kernel(const typename fftdev::CT<T>::t *__restrict__ main,
                                      const typename fftdev::CT<T>::t *__restrict__ nyq,
@@ -327,6 +395,23 @@ void rows_impl(cam_ctx *ctx, FftPlan *p, const void *in, void *out, void *nyq, i
     dispatch_fft_len(len, [&](auto lc) {
     constexpr int LEN = decltype(lc)::value;
     const size_t smem = (size_t)fftdev::padded_len((int64_t)rpc * len, LEN > 0) * sizeof(C);
+    if constexpr (MODE == 0 && LEN >= 16 && LEN <= 512 && (LEN & (LEN - 1)) == 0) {
+        // pipelined r2c rows for the power-of-two half lengths (their
+        // transforms fit the register bound without spilling): one
+        // component, 16-byte aligned input, raw + padded tile within 200 KB
+        const size_t psmem = (size_t)rpc * len * sizeof(C) + smem;
+        if (ncomp == 1 && ((uintptr_t)in % 16) == 0 && (len * sizeof(C)) % 16 == 0 && psmem <= 200 * 1024) {
+            auto kp = fft_rows_r2c_pipe_kernel<T, LEN>;
+            smem_at_least(kp, psmem);
+            int per_sm = 0;
+            CAM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kp, nthr, psmem));
+            const int64_t ngroups = (nrows + rpc - 1) / rpc;
+            const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ngroups, (int64_t)kNumSMs * std::max(per_sm, 1)));
+            CAM_LAUNCH_NAMED(ctx, "fft_rows_r2c", kp, g, nthr, psmem, static_cast<const T *>(in), static_cast<C *>(out),
+                             static_cast<C *>(nyq), nrows, static_cast<const C *>(p->tw), d_sub);
+            return;
+        }
+    }
     auto kern = fft_rows_kernel<T, MODE, LEN>;
     smem_at_least(kern, smem);
     CAM_LAUNCH_NAMED(ctx, MODE == 0 ? "fft_rows_r2c" : MODE == 1 ? "fft_rows_c2r" : "fft_rows_c2c", kern, grid, nthr, smem, in, out, static_cast<C *>(nyq), n, nrows, rpc,
