@@ -144,7 +144,7 @@ template <int SCHEME, bool SCATTER, bool SMEM>
 __device__ __forceinline__ void bin_one(float px, float py, float pz, float wt, bool weighted,
                                         const AssignGeom &g, int G, int blk, uint32_t *hist,
                                         uint32_t *__restrict__ table, uint4 *__restrict__ payload,
-                                        unsigned long long &my_lost, unsigned int &my_wmax)
+                                        unsigned long long &my_lost, unsigned int &my_wmax, unsigned int &my_neg)
 {
     using St = Stencil<SCHEME>;
     const float pos[3] = {px, py, pz};
@@ -153,7 +153,10 @@ __device__ __forceinline__ void bin_one(float px, float py, float pz, float wt, 
         ++my_lost;
         return;
     }
-    if (!SCATTER && weighted) my_wmax = max(my_wmax, __float_as_uint(fabsf(wt)));
+    if (!SCATTER && weighted) {
+        my_wmax = max(my_wmax, __float_as_uint(fabsf(wt)));
+        my_neg |= wt < 0.0f;
+    }
     // Bricks touched along each axis: 1 or 2.
     int bl[3], nbx[3];
     float t[3] = {0.f, 0.f, 0.f};
@@ -234,7 +237,7 @@ bin_kernel(const float *__restrict__ x, const float *__restrict__ y, const float
         __syncthreads();
     }
     unsigned long long my_lost = 0;
-    unsigned int my_wmax = 0;
+    unsigned int my_wmax = 0, my_neg = 0;
     const bool weighted = w != nullptr;
     const int64_t p0 = (int64_t)blk * chunk, p1 = min(np, p0 + chunk);
     int64_t ptail = p0;
@@ -245,26 +248,28 @@ bin_kernel(const float *__restrict__ x, const float *__restrict__ y, const float
             const float4 Y = __ldcs(reinterpret_cast<const float4 *>(y + p));
             const float4 Z = __ldcs(reinterpret_cast<const float4 *>(z + p));
             const float4 Wt = weighted ? __ldcs(reinterpret_cast<const float4 *>(w + p)) : make_float4(1.f, 1.f, 1.f, 1.f);
-            bin_one<SCHEME, SCATTER, kHist>(X.x, Y.x, Z.x, Wt.x, weighted, g, G, blk, hist, table, payload, my_lost, my_wmax);
-            bin_one<SCHEME, SCATTER, kHist>(X.y, Y.y, Z.y, Wt.y, weighted, g, G, blk, hist, table, payload, my_lost, my_wmax);
-            bin_one<SCHEME, SCATTER, kHist>(X.z, Y.z, Z.z, Wt.z, weighted, g, G, blk, hist, table, payload, my_lost, my_wmax);
-            bin_one<SCHEME, SCATTER, kHist>(X.w, Y.w, Z.w, Wt.w, weighted, g, G, blk, hist, table, payload, my_lost, my_wmax);
+            bin_one<SCHEME, SCATTER, kHist>(X.x, Y.x, Z.x, Wt.x, weighted, g, G, blk, hist, table, payload, my_lost, my_wmax, my_neg);
+            bin_one<SCHEME, SCATTER, kHist>(X.y, Y.y, Z.y, Wt.y, weighted, g, G, blk, hist, table, payload, my_lost, my_wmax, my_neg);
+            bin_one<SCHEME, SCATTER, kHist>(X.z, Y.z, Z.z, Wt.z, weighted, g, G, blk, hist, table, payload, my_lost, my_wmax, my_neg);
+            bin_one<SCHEME, SCATTER, kHist>(X.w, Y.w, Z.w, Wt.w, weighted, g, G, blk, hist, table, payload, my_lost, my_wmax, my_neg);
         }
         ptail = q1;
     }
     for (int64_t p = ptail + threadIdx.x; p < p1; p += blockDim.x)
         bin_one<SCHEME, SCATTER, kHist>(__ldcs(x + p), __ldcs(y + p), __ldcs(z + p), weighted ? __ldcs(w + p) : 1.0f,
-                                        weighted, g, G, blk, hist, table, payload, my_lost, my_wmax);
+                                        weighted, g, G, blk, hist, table, payload, my_lost, my_wmax, my_neg);
     if (!SCATTER) {
         // Warp reductions, one atomic per warp.
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) {
             my_lost += __shfl_down_sync(0xffffffffu, my_lost, off);
             my_wmax = max(my_wmax, __shfl_down_sync(0xffffffffu, my_wmax, off));
+            my_neg |= __shfl_down_sync(0xffffffffu, my_neg, off);
         }
         if (lane == 0) {
             if (my_lost) atomicAdd(lost, my_lost);
             if (my_wmax) atomicMax(wmax_bits, my_wmax);
+            if (my_neg) atomicOr(wmax_bits + 1, 1u);  // some weight is negative
         }
         if (kHist) {
             __syncthreads();
@@ -326,17 +331,102 @@ __device__ __forceinline__ void add_fixed(uint32_t *lo, uint32_t *hi, float v)
     if (hadd) atomicAdd(hi, hadd);
 }
 
+// One payload record into the brick's fixed-point tile.  lc = home cell
+// relative to the brick + FIRST + s is the stencil point's local cell; when
+// the brick has neighbours along an axis (nb > 1) a point outside [0, e)
+// belongs to another brick, and when one brick spans the axis the point
+// wraps periodically inside it.  NONNEG: every particle weight is >= 0, so
+// an add of a non-negative contribution is one 32-bit atomic plus a carry
+// only when the low word overflows.
+template <int SCHEME, bool NONNEG>
+__device__ __forceinline__ void deposit_record(const uint4 v, const AssignGeom &g, const int e[3], const bool whole[3],
+                                               float f1, float f2, uint32_t *lo, uint32_t *hi)
+{
+    using St = Stencil<SCHEME>;
+    int cl[3];
+    float t[3];
+    unpack_axis(v.x, cl[0], t[0]);
+    unpack_axis(v.y, cl[1], t[1]);
+    unpack_axis(v.z, cl[2], t[2]);
+    const float ws = (__uint_as_float(v.w) * f1) * f2;
+    float wa[3][St::W];
+    int li[3][St::W];
+    bool ok[3][St::W];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (SCHEME == CAM_NGP) {
+            wa[a][0] = 1.0f;
+        } else if (SCHEME == CAM_CIC) {
+            wa[a][0] = 1.0f - t[a];
+            wa[a][St::W - 1] = t[a];
+        } else {
+            const float hm = 0.5f - t[a], hp = 0.5f + t[a];
+            wa[a][0] = 0.5f * hm * hm;
+            wa[a][1] = 0.75f - t[a] * t[a];
+            wa[a][St::W - 1] = 0.5f * hp * hp;
+        }
+#pragma unroll
+        for (int sidx = 0; sidx < St::W; ++sidx) {
+            int lc = cl[a] + St::FIRST + sidx;
+            if (whole[a]) lc += lc < 0 ? e[a] : (lc >= e[a] ? -e[a] : 0);
+            li[a][sidx] = lc;
+            ok[a][sidx] = (unsigned)lc < (unsigned)e[a];
+        }
+    }
+#pragma unroll
+    for (int ia = 0; ia < St::W; ++ia) {
+#pragma unroll
+        for (int ja = 0; ja < St::W; ++ja) {
+            const float wij = ws * wa[0][ia] * wa[1][ja];
+            const int row = (li[0][ia] * e[1] + li[1][ja]) * e[2];
+            const bool okij = ok[0][ia] && ok[1][ja];
+#pragma unroll
+            for (int ka = 0; ka < St::W; ++ka) {
+                if (!(okij && ok[2][ka])) continue;
+                const int c = row + li[2][ka];
+                const float val = wij * wa[2][ka];
+                // a stencil weight can dip below zero by ~1e-6 (the FP32 key
+                // and the exact offset disagree near a cell edge): such
+                // contributions take the signed path too
+                if (NONNEG && val >= 0.0f) {
+                    const uint32_t m = __float2uint_rn(val);
+                    const uint32_t old = atomicAdd(lo + c, m);
+                    if (old + m < old) atomicAdd(hi + c, 1u);
+                } else {
+                    add_fixed(lo + c, hi + c, val);
+                }
+            }
+        }
+    }
+}
+
+template <int SCHEME, bool NONNEG>
+__device__ __forceinline__ void deposit_range(const uint4 *__restrict__ payload, uint32_t beg, uint32_t end,
+                                              const AssignGeom &g, const int e[3], const bool whole[3], float f1,
+                                              float f2, uint32_t *lo, uint32_t *hi)
+{
+    // Two records per thread per iteration: both loads are in flight before
+    // the shared-memory atomics of the first one.
+    for (uint32_t p = beg + threadIdx.x; p < end; p += 2 * blockDim.x) {
+        const uint4 va = payload[p];
+        const bool has_b = p + blockDim.x < end;
+        const uint4 vb = has_b ? payload[p + blockDim.x] : make_uint4(0u, 0u, 0u, 0u);
+        deposit_record<SCHEME, NONNEG>(va, g, e, whole, f1, f2, lo, hi);
+        if (has_b) deposit_record<SCHEME, NONNEG>(vb, g, e, whole, f1, f2, lo, hi);
+    }
+}
+
 // Pass 4: one CTA per brick.  Scale 2^s with max|w| * 2^s < 2^31, so every
 // contribution of a particle (stencil weight <= 1) fits in the low word and
 // the high word only takes carries (and the sign of rare negative weights).
 // Quantum = max|w| / 2^31 per contribution; a cell sum may use all 64 bits.
+// wstat[0] = bits of max |w|, wstat[1] != 0 if some weight is negative.
 template <int SCHEME, typename OutT>
 __global__ void __launch_bounds__(kDepositThreads)
 deposit_kernel(const uint4 *__restrict__ payload, const uint32_t *__restrict__ start,
-               AssignGeom g, const unsigned int *__restrict__ wmax_bits, int weighted,
+               AssignGeom g, const unsigned int *__restrict__ wstat, int weighted,
                OutT *__restrict__ mesh, double *__restrict__ brick_sum)
 {
-    using St = Stencil<SCHEME>;
     extern __shared__ uint32_t tile32[];
     __shared__ long long red[kDepositThreads / 32];
     const int B = blockIdx.x;
@@ -346,6 +436,7 @@ deposit_kernel(const uint4 *__restrict__ payload, const uint32_t *__restrict__ s
     const int o[3] = {B0 * g.b[0], B1 * g.b[1], B2 * g.b[2]};
     const int e[3] = {min(g.b[0], g.n[0] - o[0]), min(g.b[1], g.n[1] - o[1]),
                       min(g.b[2], g.n[2] - o[2])};
+    const bool whole[3] = {g.nb[0] == 1, g.nb[1] == 1, g.nb[2] == 1};
     const int ncell = e[0] * e[1] * e[2];
     uint32_t *lo = tile32;
     uint32_t *hi = tile32 + g.b[0] * g.b[1] * g.b[2];
@@ -356,71 +447,15 @@ deposit_kernel(const uint4 *__restrict__ payload, const uint32_t *__restrict__ s
     __syncthreads();
 
     const uint32_t beg = start[B], end = start[B + 1];
-    const float wmax = weighted ? __uint_as_float(*wmax_bits) : 1.0f;
+    const float wmax = weighted ? __uint_as_float(wstat[0]) : 1.0f;
+    const bool nonneg = !weighted || wstat[1] == 0u;
     int ex = 0;
     frexpf(wmax > 0.f ? wmax : 1.0f, &ex);
     const int s = 31 - ex;
     // 2^s as two exact factors (s may exceed the float exponent range)
     const float f1 = scalbnf(1.0f, s / 2), f2 = scalbnf(1.0f, s - s / 2);
-
-    // Two payloads per thread per iteration: both loads are in flight
-    // before the shared-memory atomics of the first one.
-    for (uint32_t p = beg + threadIdx.x; p < end; p += 2 * blockDim.x) {
-        const uint4 va = payload[p];
-        const bool has_b = p + blockDim.x < end;
-        const uint4 vb = has_b ? payload[p + blockDim.x] : make_uint4(0u, 0u, 0u, 0u);
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-        if (u == 1 && !has_b) break;
-        const uint4 v = u == 0 ? va : vb;
-        int cl[3];
-        float t[3];
-        unpack_axis(v.x, cl[0], t[0]);
-        unpack_axis(v.y, cl[1], t[1]);
-        unpack_axis(v.z, cl[2], t[2]);
-        const float ws = (__uint_as_float(v.w) * f1) * f2;
-        float wa[3][St::W];
-        int li[3][St::W];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            if (SCHEME == CAM_NGP) {
-                wa[a][0] = 1.0f;
-            } else if (SCHEME == CAM_CIC) {
-                wa[a][0] = 1.0f - t[a];
-                wa[a][St::W - 1] = t[a];
-            } else {
-                const float hm = 0.5f - t[a], hp = 0.5f + t[a];
-                wa[a][0] = 0.5f * hm * hm;
-                wa[a][1] = 0.75f - t[a] * t[a];
-                wa[a][St::W - 1] = 0.5f * hp * hp;
-            }
-#pragma unroll
-            for (int sidx = 0; sidx < St::W; ++sidx) {
-                // Global cell of this stencil point, wrapped, then local
-                // index in the brick or -1 when it belongs to another brick.
-                const int gc = wrapi(o[a] + cl[a] + St::FIRST + sidx, g.n[a]);
-                const int lc = gc - o[a];
-                li[a][sidx] = (lc >= 0 && lc < e[a]) ? lc : -1;
-            }
-        }
-#pragma unroll
-        for (int ia = 0; ia < St::W; ++ia) {
-            if (li[0][ia] < 0) continue;
-#pragma unroll
-            for (int ja = 0; ja < St::W; ++ja) {
-                if (li[1][ja] < 0) continue;
-                const float wij = ws * wa[0][ia] * wa[1][ja];
-                const int row = (li[0][ia] * e[1] + li[1][ja]) * e[2];
-#pragma unroll
-                for (int ka = 0; ka < St::W; ++ka) {
-                    if (li[2][ka] < 0) continue;
-                    const int c = row + li[2][ka];
-                    add_fixed(lo + c, hi + c, wij * wa[2][ka]);
-                }
-            }
-        }
-        }
-    }
+    if (nonneg) deposit_range<SCHEME, true>(payload, beg, end, g, e, whole, f1, f2, lo, hi);
+    else deposit_range<SCHEME, false>(payload, beg, end, g, e, whole, f1, f2, lo, hi);
     __syncthreads();
 
     long long acc = 0;

@@ -141,6 +141,21 @@ def test_bitwise_deterministic(ctx, scheme):
 
 
 @pytest.mark.parametrize("scheme", SCHEMES)
+def test_signed_weights_vs_oracle(ctx, scheme):
+    # some negative weights: the deposit's signed fixed-point path
+    n, box = 64, 1000.0
+    x, y, z = mixed_inputs(n, box, 300_000, seed=41)
+    w = synth.halo_masses(x.size, seed=42)
+    w[np.random.default_rng(43).random(x.size) < 0.2] *= -1.0
+    g = make_grid(n, box)
+    r = ctx.assign(x, y, z, w, g, scheme, F64)
+    ref, lost = orc.assign_f64(scheme, x, y, z, w, orc.Grid.cubic(n, box))
+    assert r.n_lost == lost
+    err = rel_err_cells(r.mesh, ref, float(np.mean(np.abs(w))))
+    assert err <= 1e-5, err
+
+
+@pytest.mark.parametrize("scheme", SCHEMES)
 @pytest.mark.parametrize("n", [96, 32])
 def test_many_particles_vs_oracle(ctx, scheme, n):
     # 4.5 M weighted particles (clumped, plus the edge positions).  At n = 32
