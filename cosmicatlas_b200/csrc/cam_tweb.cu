@@ -370,12 +370,10 @@ __device__ __forceinline__ void char_poly(float a00, float a11, float a22, float
 // Number of eigenvalues greater than t: the sign changes of the coefficients
 // of p(x + t) = x^3 + (3t - c2) x^2 + (3t^2 - 2 c2 t + c1) x + p(t), zeros
 // skipped.  Descartes' rule of signs is exact here because every root of
-// the characteristic polynomial of a symmetric matrix is real.
-__device__ __forceinline__ int count_above(double c2, double c1, double c0, double t)
+// the characteristic polynomial of a symmetric matrix is real.  Takes the
+// three lower coefficients.
+__device__ __forceinline__ int sign_changes(double a2, double a1, double a0)
 {
-    const double a2 = 3.0 * t - c2;
-    const double a1 = (3.0 * t - 2.0 * c2) * t + c1;
-    const double a0 = ((t - c2) * t + c1) * t - c0;
     int changes = 0;
     bool neg = false;  // sign of the last nonzero coefficient (leading 1 > 0)
     if (a2 != 0.0) {
@@ -388,6 +386,20 @@ __device__ __forceinline__ int count_above(double c2, double c1, double c0, doub
     }
     if (a0 != 0.0) changes += (a0 < 0.0) != neg;
     return changes;
+}
+// Taylor coefficients of p at t: p(t + s) = s^3 + a2 s^2 + a1 s + a0.
+__device__ __forceinline__ void shifted_poly(double c2, double c1, double c0, double t, double &a2, double &a1,
+                                             double &a0)
+{
+    a2 = 3.0 * t - c2;
+    a1 = (3.0 * t - 2.0 * c2) * t + c1;
+    a0 = ((t - c2) * t + c1) * t - c0;
+}
+__device__ __forceinline__ int count_above(double c2, double c1, double c0, double t)
+{
+    double a2, a1, a0;
+    shifted_poly(c2, c1, c0, t, a2, a1, a0);
+    return sign_changes(a2, a1, a0);
 }
 
 // Label of one cell from its six field values (slots 0..5 of t6), written
@@ -413,10 +425,15 @@ __device__ __forceinline__ void label_cell(const float t6[6], double lth, double
         lambdas[ncell + cell] = (float)lam[1];
         lambdas[2 * ncell + cell] = (float)lam[2];
     } else {
-        double c2, c1, c0;
+        double c2, c1, c0, a2, a1, a0;
         char_poly(t6[2], t6[4], t6[0], t6[5], t6[1], t6[3], c2, c1, c0);
-        v = count_above(c2, c1, c0, lth);
-        tie = count_above(c2, c1, c0, lth - band) != count_above(c2, c1, c0, lth + band);
+        shifted_poly(c2, c1, c0, lth, a2, a1, a0);
+        v = sign_changes(a2, a1, a0);
+        // |p(lth + s) - p(lth)| <= band (|a1| + band (|a2| + band)) for
+        // |s| <= band: above that bound p has no root in the band, and the
+        // counts at its two ends agree.  Only the other cells count again.
+        if (!(fabs(a0) > band * (fabs(a1) + band * (fabs(a2) + band))))
+            tie = count_above(c2, c1, c0, lth - band) != count_above(c2, c1, c0, lth + band);
     }
     if (labels) labels[cell] = (uint8_t)(4 - v);
     lc0 += v == 3;  // label 1, knot
@@ -537,8 +554,21 @@ constexpr size_t zpipe_smem()
     return ((size_t)6 * tweb_rpc<T>(LEN) * LEN + (size_t)fftdev::padded_len(6 * tweb_rpc<T>(LEN) * LEN, true)) *
            sizeof(typename CTw<T>::t);
 }
+// CTAs per SM.  Several CTAs per SM hide the latencies of the transform
+// stages, barriers and FP64 label arithmetic; the register bound that comes
+// with them is one the instantiation fits without spilling (ptxas -v):
+// float LEN 256 and double LEN 128/256 in 80 registers (4 CTAs of 192
+// threads), float LEN 512 in 96 (3 CTAs); the others need the 2-CTA bound.
+// Capped by the shared memory of the CTAs.
+template <typename T, int LEN>
+constexpr int zpipe_min_blocks()
+{
+    const int want = sizeof(T) == 4 ? (LEN == 256 ? 4 : (LEN == 512 ? 3 : 2))
+                                     : ((LEN == 128 || LEN == 256) ? 4 : 2);
+    return (int)std::min<size_t>(want, std::max<size_t>(1, (220 * 1024) / (zpipe_smem<T, LEN>() + 1024)));
+}
 template <typename T, int LEN, bool LAMBDAS>
-__global__ void __launch_bounds__(zpipe_threads<T, LEN>(), 2)  // <= 128 registers: no spills
+__global__ void __launch_bounds__(zpipe_threads<T, LEN>(), zpipe_min_blocks<T, LEN>())
 tidal_z_pipe_kernel(const typename CTw<T>::t *__restrict__ src, const typename CTw<T>::t *__restrict__ nyq, int n,
                     int64_t nrows, int64_t ccomp, const typename CTw<T>::t *__restrict__ tw, double lth, double band,
                     uint8_t *__restrict__ labels, float *__restrict__ lambdas,
