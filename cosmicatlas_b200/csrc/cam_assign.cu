@@ -299,22 +299,31 @@ __global__ void brick_starts_kernel(const uint32_t *__restrict__ scanned, int nb
     }
 }
 
+// Cell sum q (units of 2^-s) as the output type; sc = 2^-s, so q * sc is
+// exact in double (|q| < 2^63, -97 <= s <= 180) and the float output is one
+// rounding of the exact value.
 template <typename OutT>
-__device__ __forceinline__ OutT convert_out(long long q, int s);
+__device__ __forceinline__ OutT convert_out(long long q, int s, double sc);
 template <>
-__device__ __forceinline__ float convert_out<float>(long long q, int s)
+__device__ __forceinline__ float convert_out<float>(long long q, int, double sc)
 {
-    return __double2float_rn(ldexp((double)q, -s));
+    return __double2float_rn((double)q * sc);
 }
 template <>
-__device__ __forceinline__ double convert_out<double>(long long q, int s)
+__device__ __forceinline__ double convert_out<double>(long long q, int, double sc)
 {
-    return ldexp((double)q, -s);
+    return (double)q * sc;
 }
 template <>
-__device__ __forceinline__ uint32_t convert_out<uint32_t>(long long q, int s)
+__device__ __forceinline__ uint32_t convert_out<uint32_t>(long long q, int s, double)
 {
     return (uint32_t)(q >> s);
+}
+
+// floor(i / d) for i, d < 2^16: multiply-high by m = ceil(2^32 / d) (d > 1).
+__device__ __forceinline__ unsigned div_small(unsigned i, unsigned d, unsigned m)
+{
+    return d == 1u ? i : __umulhi(i, m);
 }
 
 // Adds round(v) (|v| < 2^32) to the 64-bit fixed-point cell (lo, hi) with
@@ -438,11 +447,15 @@ deposit_kernel(const uint4 *__restrict__ payload, const uint32_t *__restrict__ s
                       min(g.b[2], g.n[2] - o[2])};
     const bool whole[3] = {g.nb[0] == 1, g.nb[1] == 1, g.nb[2] == 1};
     const int ncell = e[0] * e[1] * e[2];
+    const int cap = g.b[0] * g.b[1] * g.b[2];
     uint32_t *lo = tile32;
-    uint32_t *hi = tile32 + g.b[0] * g.b[1] * g.b[2];
-    for (int i = threadIdx.x; i < ncell; i += blockDim.x) {
-        lo[i] = 0u;
-        hi[i] = 0u;
+    uint32_t *hi = tile32 + cap;
+    {
+        // both words of all cap cells, 16 bytes a store
+        const int nw = 2 * cap;
+        uint4 *t4 = reinterpret_cast<uint4 *>(tile32);
+        for (int i = threadIdx.x; i < nw / 4; i += blockDim.x) t4[i] = make_uint4(0u, 0u, 0u, 0u);
+        for (int i = (nw & ~3) + threadIdx.x; i < nw; i += blockDim.x) tile32[i] = 0u;
     }
     __syncthreads();
 
@@ -459,14 +472,21 @@ deposit_kernel(const uint4 *__restrict__ payload, const uint32_t *__restrict__ s
     __syncthreads();
 
     long long acc = 0;
+    const double sc = ldexp(1.0, -s);
+    // cell i = (li * e1 + lj) * e2 + lk; a tile holds < 2^16 cells
+    const unsigned e2 = (unsigned)e[2], e12 = (unsigned)(e[1] * e[2]);
+    const unsigned m2 = e2 > 1u ? (unsigned)((0x100000000ull + e2 - 1) / e2) : 0u;
+    const unsigned m12 = e12 > 1u ? (unsigned)((0x100000000ull + e12 - 1) / e12) : 0u;
+    const unsigned e1 = (unsigned)e[1];
     for (int i = threadIdx.x; i < ncell; i += blockDim.x) {
-        const int lk = i % e[2];
-        const int lj = (i / e[2]) % e[1];
-        const int lii = i / (e[2] * e[1]);
+        const unsigned row = div_small((unsigned)i, e2, m2);  // li * e1 + lj
+        const unsigned lk = (unsigned)i - row * e2;
+        const unsigned lii = div_small((unsigned)i, e12, m12);
+        const unsigned lj = row - lii * e1;
         const long long q = (long long)(((unsigned long long)hi[i] << 32) | lo[i]);
         acc += q;
-        const int64_t gidx = ((int64_t)(o[0] + lii) * g.n[1] + (o[1] + lj)) * g.n[2] + (o[2] + lk);
-        mesh[gidx] = convert_out<OutT>(q, s);
+        const int64_t gidx = ((int64_t)(o[0] + (int)lii) * g.n[1] + (o[1] + (int)lj)) * g.n[2] + (o[2] + (int)lk);
+        mesh[gidx] = convert_out<OutT>(q, s, sc);
     }
     // Deterministic block sum of the integer cell sums.
 #pragma unroll
