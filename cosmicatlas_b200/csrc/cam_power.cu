@@ -83,52 +83,69 @@ pk_bin_kernel(const C *__restrict__ main, const C *__restrict__ nyq, int n,
     const int64_t r_beg = (int64_t)blockIdx.x * rows_per_cta;
     const int64_t r_end = min(nrows, r_beg + rows_per_cta);
     for (int64_t r = r_beg + warp; r < r_end; r += kPkWarps) {
-        const int i = (int)(r / n), j = (int)(r % n);
+        const int i = (int)r / n, j = (int)r - i * n;  // n * n < 2^31 (host check)
         if (i == h || j == h) continue;
         const int a = i <= h ? i : n - i;
         const int b = j <= h ? j : n - j;
         const double tab_ab = tw2[a] * tw2[b];
         const double sn_ab = tsn[a] * tsn[b];
         const int64_t q0 = (int64_t)a * a + (int64_t)b * b;
-        for (int c0 = 0; c0 <= M; c0 += 32) {
+        for (int c0 = 0; c0 < M; c0 += 32) {
             const int c = c0 + lane;
             double vraw = 0.0, vsn = 0.0;
-            unsigned long long vcnt = 0;
+            bool valid = false;
             int bin = nbins;
-            if (c <= M) {
+            if (c < M) {
                 const double q = (double)(q0 + (int64_t)c * c);
                 bin = pk_bin(q, E2, nbins, m_u, inv_s);
                 if (bin >= 0 && bin < nbins && pk_visited(i, j, c, n)) {
-                    const C f = c < M ? main[r * M + c] : nyq[r];
+                    const C f = main[r * M + c];
                     const double re = (double)f.x, im = (double)f.y;
                     vraw = (re * re + im * im) * (tab_ab * tw2[c]);
                     vsn = sn_ab * tsn[c];
-                    vcnt = 1;
+                    valid = true;
                 }
             }
             // Segmented suffix sums over runs of equal bins (bins are
-            // non-decreasing in c, so runs are contiguous lanes).
+            // non-decreasing in c, so runs are contiguous lanes); a run ends
+            // at the next run head.
+            const int prev = __shfl_up_sync(0xffffffffu, bin, 1);
+            const bool head = lane == 0 || prev != bin;
+            const unsigned heads = __ballot_sync(0xffffffffu, head);
+            const unsigned later = heads & ~((2u << lane) - 1u);
+            const int end = later ? __ffs((int)later) - 1 : 32;
 #pragma unroll
             for (int off = 1; off < 32; off <<= 1) {
                 const double or_ = __shfl_down_sync(0xffffffffu, vraw, off);
                 const double os = __shfl_down_sync(0xffffffffu, vsn, off);
-                const unsigned long long oc = __shfl_down_sync(0xffffffffu, vcnt, off);
-                const int ob = __shfl_down_sync(0xffffffffu, bin, off);
-                if (lane + off < 32 && ob == bin) {
+                if (lane + off < end) {
                     vraw += or_;
                     vsn += os;
-                    vcnt += oc;
                 }
             }
-            const int prev = __shfl_up_sync(0xffffffffu, bin, 1);
-            const bool head = lane == 0 || prev != bin;
-            if (head && bin >= 0 && bin < nbins && vcnt) {
+            const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+            const unsigned run = (end == 32 ? 0xffffffffu : ((1u << end) - 1u)) & ~((1u << lane) - 1u);
+            const int cnt = __popc(vmask & run);
+            if (head && bin >= 0 && bin < nbins && cnt) {
                 mysum[2 * bin] += vraw;
                 mysum[2 * bin + 1] += vsn;
-                mycnt[bin] += vcnt;
+                mycnt[bin] += (unsigned long long)cnt;
             }
             __syncwarp();
         }
+        // c = M, the Nyquist plane element of the row: one lane adds it
+        if (lane == 0) {
+            const double q = (double)(q0 + (int64_t)M * M);
+            const int bin = pk_bin(q, E2, nbins, m_u, inv_s);
+            if (bin >= 0 && bin < nbins && pk_visited(i, j, M, n)) {
+                const C f = nyq[r];
+                const double re = (double)f.x, im = (double)f.y;
+                mysum[2 * bin] += (re * re + im * im) * (tab_ab * tw2[M]);
+                mysum[2 * bin + 1] += sn_ab * tsn[M];
+                mycnt[bin] += 1ull;
+            }
+        }
+        __syncwarp();
     }
     __syncthreads();
     for (int bn = threadIdx.x; bn < nbins; bn += blockDim.x) {
@@ -197,6 +214,7 @@ void power_bin(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins,
 {
     const int n = (int)s.n, h = n / 2;
     CAM_REQUIRE(nbins >= 1 && nbins <= 4096, CAM_E_INVAL, "nbins must be in [1, 4096]");
+    CAM_REQUIRE((int64_t)n * n < (1ll << 31), CAM_E_UNSUPPORTED, "mesh too large for P(k)");
     CAM_REQUIRE(o.ndel > 0.0 && std::isfinite(o.ndel) && std::isfinite(o.DeltaKmin), CAM_E_INVAL,
                 "bin width must be > 0");
     CAM_REQUIRE(o.scheme >= 0 && o.scheme <= 2, CAM_E_INVAL, "unknown window scheme");

@@ -277,20 +277,28 @@ tidal_pipe_kernel(const typename CTw<T>::t *src, typename CTw<T>::t *dst, int n,
         __syncthreads();             // ... and everyone's
         int p, ct, plane;
         decode(t, p, ct, plane);
+        if (MODE == 0) {
+            // phi = delta_k exp(-k^2 R^2 / 2) / k^2, once per input element;
+            // each output then only multiplies by k_x^p
+            const int fy = plane <= h ? plane : plane - n;
+            for (int e = threadIdx.x; e < TILE; e += NTHR) {
+                const int j = e / W, cc = e % W;
+                const int fj = j <= h ? j : j - n;
+                const T m = phi_mult<T>(0, fj, fy, ct * W + cc, gc, norm);
+                const C v = in[e];
+                in[e] = C{v.x * m, v.y * m};
+            }
+        }
         const int nout = MODE == 0 ? 3 : 3 - p;
         for (int o = 0; o < nout; ++o) {
             const int q = MODE == 0 ? 0 : 2 - p - o;  // y pass: q = 2-p .. 0
             const int pp = MODE == 0 ? o : p;
+            // the x pass: k_x^o on this thread's own phi elements (no barrier
+            // needed between the two loops)
             for (int e = threadIdx.x; e < TILE; e += NTHR) {
-                const int j = e / W, cc = e % W;
+                const int j = e / W;
                 const int fj = j <= h ? j : j - n;
-                T m;
-                if (MODE == 0) {
-                    const int fy = plane <= h ? plane : plane - n;
-                    m = phi_mult<T>(pp, fj, fy, ct * W + cc, gc, norm);
-                } else {
-                    m = (T)ipow(fj, q);
-                }
+                const T m = (T)ipow(fj, MODE == 0 ? o : q);
                 const C v = in[e];
                 work[e] = C{v.x * m, v.y * m};
             }
