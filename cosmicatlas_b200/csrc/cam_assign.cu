@@ -139,7 +139,61 @@ __device__ __forceinline__ int brick_linear(const AssignGeom &g, int b0, int b1,
     return (b0 * g.nb[1] + b1) * g.nb[2] + b2;
 }
 
-// One particle of passes 1 and 3 (see bin_kernel).
+// One particle of pass 1: the bricks its stencil touches (the brick of its
+// first stencil cell and, along each axis whose stencil crosses a brick
+// face, the next brick, periodically) each get one count.
+template <int SCHEME, bool SMEM>
+__device__ __forceinline__ void count_one(float px, float py, float pz, float wt, bool weighted, const AssignGeom &g,
+                                          uint32_t *hist, uint32_t *__restrict__ table, unsigned long long &my_lost,
+                                          unsigned int &my_wmax, unsigned int &my_neg)
+{
+    using St = Stencil<SCHEME>;
+    const float pos[3] = {px, py, pz};
+    int c[3] = {0, 0, 0};
+    if (!home_cell<SCHEME>(pos, g, c)) {
+        ++my_lost;
+        return;
+    }
+    if (weighted) {
+        my_wmax = max(my_wmax, __float_as_uint(fabsf(wt)));
+        my_neg |= wt < 0.0f;
+    }
+    int bl[3];
+    bool two[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const int lo = wrapi(c[a] + St::FIRST, g.n[a]);
+        const int hi = wrapi(c[a] + St::FIRST + St::W - 1, g.n[a]);
+        bl[a] = brick_of(lo, g.b[a], g.bmagic[a]);
+        two[a] = St::W > 1 && brick_of(hi, g.b[a], g.bmagic[a]) != bl[a];
+    }
+    const int s1 = g.nb[2], s0 = g.nb[1] * g.nb[2];
+    const int k0 = bl[0] * s0 + bl[1] * s1 + bl[2];
+    // key step to the next brick along each axis (periodic)
+    const int d2 = bl[2] + 1 == g.nb[2] ? -bl[2] : 1;
+    const int d1 = (bl[1] + 1 == g.nb[1] ? -bl[1] : 1) * s1;
+    const int d0 = (bl[0] + 1 == g.nb[0] ? -bl[0] : 1) * s0;
+    auto add = [&](int key) {
+        if (SMEM) atomicAdd(hist + key, 1u);
+        else atomicAdd(table + (int64_t)key * kCursorStride, 1u);
+    };
+    add(k0);
+    if (two[2]) add(k0 + d2);
+    if (two[1]) {
+        add(k0 + d1);
+        if (two[2]) add(k0 + d1 + d2);
+    }
+    if (two[0]) {
+        add(k0 + d0);
+        if (two[2]) add(k0 + d0 + d2);
+        if (two[1]) {
+            add(k0 + d0 + d1);
+            if (two[2]) add(k0 + d0 + d1 + d2);
+        }
+    }
+}
+
+// One particle of pass 3 (see bin_kernel).
 template <int SCHEME, bool SCATTER, bool SMEM>
 __device__ __forceinline__ void bin_one(float px, float py, float pz, float wt, bool weighted,
                                         const AssignGeom &g, int G, int blk, uint32_t *hist,
@@ -239,6 +293,13 @@ bin_kernel(const float *__restrict__ x, const float *__restrict__ y, const float
     unsigned long long my_lost = 0;
     unsigned int my_wmax = 0, my_neg = 0;
     const bool weighted = w != nullptr;
+    auto one = [&](float px, float py, float pz, float wt) {
+        if (SCATTER)
+            bin_one<SCHEME, true, false>(px, py, pz, wt, weighted, g, G, blk, hist, table, payload, my_lost, my_wmax,
+                                         my_neg);
+        else
+            count_one<SCHEME, kHist>(px, py, pz, wt, weighted, g, hist, table, my_lost, my_wmax, my_neg);
+    };
     const int64_t p0 = (int64_t)blk * chunk, p1 = min(np, p0 + chunk);
     int64_t ptail = p0;
     if (VEC) {
@@ -248,16 +309,15 @@ bin_kernel(const float *__restrict__ x, const float *__restrict__ y, const float
             const float4 Y = __ldcs(reinterpret_cast<const float4 *>(y + p));
             const float4 Z = __ldcs(reinterpret_cast<const float4 *>(z + p));
             const float4 Wt = weighted ? __ldcs(reinterpret_cast<const float4 *>(w + p)) : make_float4(1.f, 1.f, 1.f, 1.f);
-            bin_one<SCHEME, SCATTER, kHist>(X.x, Y.x, Z.x, Wt.x, weighted, g, G, blk, hist, table, payload, my_lost, my_wmax, my_neg);
-            bin_one<SCHEME, SCATTER, kHist>(X.y, Y.y, Z.y, Wt.y, weighted, g, G, blk, hist, table, payload, my_lost, my_wmax, my_neg);
-            bin_one<SCHEME, SCATTER, kHist>(X.z, Y.z, Z.z, Wt.z, weighted, g, G, blk, hist, table, payload, my_lost, my_wmax, my_neg);
-            bin_one<SCHEME, SCATTER, kHist>(X.w, Y.w, Z.w, Wt.w, weighted, g, G, blk, hist, table, payload, my_lost, my_wmax, my_neg);
+            one(X.x, Y.x, Z.x, Wt.x);
+            one(X.y, Y.y, Z.y, Wt.y);
+            one(X.z, Y.z, Z.z, Wt.z);
+            one(X.w, Y.w, Z.w, Wt.w);
         }
         ptail = q1;
     }
     for (int64_t p = ptail + threadIdx.x; p < p1; p += blockDim.x)
-        bin_one<SCHEME, SCATTER, kHist>(__ldcs(x + p), __ldcs(y + p), __ldcs(z + p), weighted ? __ldcs(w + p) : 1.0f,
-                                        weighted, g, G, blk, hist, table, payload, my_lost, my_wmax, my_neg);
+        one(__ldcs(x + p), __ldcs(y + p), __ldcs(z + p), weighted ? __ldcs(w + p) : 1.0f);
     if (!SCATTER) {
         // Warp reductions, one atomic per warp.
 #pragma unroll
