@@ -18,9 +18,10 @@
 //                the three CTAs of one delta_k tile run together, so the
 //                tile is read from HBM once and from L2 after;
 //   tidal_y    : for input field p, the fields (p, q), q = 0 .. 2-p: times
-//                k_y^q and the inverse FFT along y; (p, 0) overwrites its
-//                input in place, as the last output of the same CTA;
-//   tidal_z    : times k_z^r, c2r along z of the six fields of a few rows,
+//                k_y^q k_z^r (r = 2-p-q; k_z is constant along y) and the
+//                inverse FFT along y; (p, 0) overwrites its input in place,
+//                as the last output of the same CTA;
+//   tidal_z    : c2r along z of the six fields of a few rows,
 //                then the eigenvalues (FP32 trigonometric solution plus one
 //                FP64 Newton step) and the label of every cell (uint8).
 // Field slots: 0 = (0,0) -> T_zz, 1 = (1,0) -> T_xz, 2 = (2,0) -> T_xx,
@@ -53,14 +54,10 @@ __device__ __forceinline__ float ipow(int f, int e)
     return e == 0 ? 1.0f : (e == 1 ? (float)f : (float)(f * f));
 }
 
-// Field slot of (p, q) and the power r = 2 - p - q of k_z it still needs.
+// Field slot of (p, q); the y pass gives it the factor k_z^r, r = 2 - p - q.
 __host__ __device__ constexpr int slot_of(int p, int q)
 {
     return q == 0 ? p : (p == 0 ? 2 + q : 5);
-}
-__device__ __forceinline__ int kz_power(int slot)
-{
-    return slot == 0 ? 2 : ((slot == 1 || slot == 3) ? 1 : 0);
 }
 
 }  // namespace
@@ -151,15 +148,16 @@ tidal_x_kernel(const typename CTw<T>::t *__restrict__ src, typename CTw<T>::t *_
     }
 }
 
-// Inverse FFT along y of k_y^q times field p, q = 2-p .. 0, for one tile
-// (p = blockIdx.x, columns blockIdx.y * W.., plane blockIdx.z).  Element
-// (plane, j, col) of field s sits at base + s*ccomp + plane*pstride +
-// j*jstride + col*cstride.  The tile is re-read (from L2) for every q, and
-// (p, 0) -- no factor -- is written last, over its own input.
+// Inverse FFT along y of k_y^q k_z^r times field p, q = 2-p .. 0,
+// r = 2-p-q, for one tile (p = blockIdx.x, columns blockIdx.y * W.., plane
+// blockIdx.z).  Element (plane, j, col) of field s sits at base + s*ccomp +
+// plane*pstride + j*jstride + col*cstride.  k_z = kz_fixed if >= 0 (the
+// Nyquist plane), else the column.  The tile is re-read (from L2) for every
+// q, and (p, 0) is written last, over its own input.
 template <typename T, int LEN>
 __global__ void __launch_bounds__(col_threads<T, LEN>(), col_min_blocks<T, LEN>())
 tidal_y_kernel(typename CTw<T>::t *__restrict__ base, int n, int ncols, int64_t jstride, int64_t cstride,
-               int64_t pstride, int64_t ccomp, Radices rd, const typename CTw<T>::t *__restrict__ tw)
+               int64_t pstride, int64_t ccomp, Radices rd, const typename CTw<T>::t *__restrict__ tw, int kz_fixed)
 {
     using C = typename CTw<T>::t;
     constexpr int W = CTw<T>::kCols;
@@ -177,7 +175,8 @@ tidal_y_kernel(typename CTw<T>::t *__restrict__ base, int n, int ncols, int64_t 
             const int j = e / W, cc = e % W;
             if (cc < nc) {
                 const C v = in[(int64_t)j * jstride + (int64_t)cc * cstride];
-                const T m = (T)ipow(j <= h ? j : j - n, q);
+                const int kz = kz_fixed >= 0 ? kz_fixed : col0 + cc;
+                const T m = (T)(ipow(j <= h ? j : j - n, q) * ipow(kz, 2 - p - q));
                 tile[e] = C{v.x * m, v.y * m};
             }
         }
@@ -294,7 +293,8 @@ tidal_pipe_kernel(const typename CTw<T>::t *src, typename CTw<T>::t *dst, int n,
             const int q = MODE == 0 ? 0 : 2 - p - o;  // y pass: q = 2-p .. 0
             const int pp = MODE == 0 ? o : p;
             // the x pass: k_x^o on this thread's own phi elements (no barrier
-            // needed between the two loops)
+            // needed between the two loops);
+            // the y pass: k_y^q (k_z^r is applied to the transformed tile)
             for (int e = threadIdx.x; e < TILE; e += NTHR) {
                 const int j = e / W;
                 const int fj = j <= h ? j : j - n;
@@ -306,7 +306,13 @@ tidal_pipe_kernel(const typename CTw<T>::t *src, typename CTw<T>::t *dst, int n,
             fftdev::block_fft_fixed<C, true, false, W, LEN, NTHR, W, 1, 1>(work, tw);
             const int slot = MODE == 0 ? pp : slot_of(p, q);
             C *g = dst + (int64_t)slot * ccomp + (int64_t)plane * pstride + (int64_t)ct * W;
-            for (int e = threadIdx.x; e < TILE; e += NTHR) g[(int64_t)(e / W) * jstride + (e % W)] = work[e];
+            // the y pass: k_z^r, r = 2 - p - q, k_z = the column (constant
+            // along y, so it commutes with the transform)
+            for (int e = threadIdx.x; e < TILE; e += NTHR) {
+                const C v = work[e];
+                const T mz = MODE == 0 ? (T)1 : (T)ipow(ct * W + e % W, 2 - p - q);
+                g[(int64_t)(e / W) * jstride + (e % W)] = MODE == 0 ? v : C{v.x * mz, v.y * mz};
+            }
             __syncthreads();  // work is refilled by the next output
         }
         cur ^= 1;
@@ -508,11 +514,6 @@ tidal_z_kernel(const typename CTw<T>::t *__restrict__ src, const typename CTw<T>
             xk.y = 0;
             xm.y = 0;
         }
-        // the remaining factor k_z^r of this field (k_z >= 0 in the half spectrum)
-        const int rz = kz_power(c);
-        const T fa = (T)ipow(k, rz), fb = (T)ipow(k == 0 ? M : M - k, rz);
-        xk = C{xk.x * fa, xk.y * fa};
-        xm = C{xm.x * fb, xm.y * fb};
         const C a = C{xk.x + xm.x, xk.y - xm.y};
         const C b = C{xk.x - xm.x, xk.y + xm.y};
         C wv = __ldg(tw + k);
@@ -590,6 +591,7 @@ tidal_z_pipe_kernel(const typename CTw<T>::t *__restrict__ src, const typename C
     constexpr int NTHR = zpipe_threads<T, LEN>();
     constexpr int EPC = 16 / (int)sizeof(C);
     constexpr int CPRow = M / EPC;  // 16-byte chunks per row
+    constexpr int HALF = M / 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *const raw = reinterpret_cast<C *>(smem_raw);  // the raw rows of one group
     C *const tile = raw + RAW;                       // padded work tile [6][RPC][M]
@@ -616,41 +618,51 @@ tidal_z_pipe_kernel(const typename CTw<T>::t *__restrict__ src, const typename C
         __syncthreads();             // ... and everyone's
         const int64_t row0 = gi * RPC;
         const int nr = (int)min((int64_t)RPC, nrows - row0);
-        // c2r untangling with the remaining factor k_z^r of each field
-        for (int e = threadIdx.x; e < RAW; e += NTHR) {
-            const int c = e / PER, rem = e % PER;
-            const int r = rem / M, k = rem % M;
+        // c2r untangling.  Elements k and M - k of a row use the same two
+        // inputs X[k], X[M - k]: with a = X[k] + conj(X[M - k]),
+        // u = conj(w^k) (X[k] - conj(X[M - k])) and conj(w^(M-k)) = -w^k,
+        //   Z[k] = a + i u,   Z[M - k] = conj(a) + i conj(u).
+        // Item 0 of a row makes Z[0] (with the Nyquist element X[M]) and
+        // Z[M/2].
+        for (int e = threadIdx.x; e < 6 * RPC * HALF; e += NTHR) {
+            const int row = e / HALF, k = e % HALF;  // row = field * RPC + r
+            const int c = row / RPC, r = row % RPC;
             if (r >= nr) continue;
-            C xk = raw[c * PER + r * M + k];
-            C xm = k == 0 ? nyq[(int64_t)c * nn + row0 + r] : raw[c * PER + r * M + (M - k)];
-            if (k == 0) {
-                xk.y = 0;
-                xm.y = 0;
-            }
-            const int rz = kz_power(c);
-            const T fa = (T)ipow(k, rz), fb = (T)ipow(k == 0 ? M : M - k, rz);
-            xk = C{xk.x * fa, xk.y * fa};
-            xm = C{xm.x * fb, xm.y * fb};
+            const C *rr = raw + row * M;
+            C *zt = tile + fftdev::sidx<true>(row * M);  // rows start on a 16-element boundary
+            const int kk = k == 0 ? HALF : k;
+            const C xk = rr[kk], xm = rr[M - kk];
             const C a = C{xk.x + xm.x, xk.y - xm.y};
             const C b = C{xk.x - xm.x, xk.y + xm.y};
-            C wv = __ldg(tw + k);
+            C wv = __ldg(tw + kk);
             wv.y = -wv.y;
-            const C ib = fftdev::rot<C, true>(fftdev::cmul(wv, b));
-            tile[fftdev::sidx<true>(e)] = fftdev::cadd(a, ib);
+            const C u = fftdev::cmul(wv, b);
+            zt[fftdev::sidx<true>(kk)] = C{a.x - u.y, a.y + u.x};
+            if (k == 0) {
+                const T x0 = rr[0].x, xn = nyq[(int64_t)c * nn + row0 + r].x;
+                zt[0] = C{x0 + xn, x0 - xn};
+            } else {
+                zt[fftdev::sidx<true>(M - k)] = C{a.x + u.y, u.x - a.y};
+            }
         }
         __syncthreads();  // raw is consumed: fetch the next group behind the transform
         const int64_t gn = gi + gridDim.x;
         if (gn < ngroups) load(gn, raw);
         fftdev::cp_async_commit();
         fftdev::block_fft_fixed<C, true, true, 6 * RPC, LEN, NTHR, 1, LEN, 2, true>(tile, tw);
-        const T *re = reinterpret_cast<const T *>(tile);
-        for (int e = threadIdx.x; e < nr * 2 * M; e += NTHR) {
-            const int r = e / (2 * M), z = e % (2 * M);
-            float t6[6];
+        // complex element m of a row holds the real values at z = 2m, 2m + 1
+        for (int e = threadIdx.x; e < nr * M; e += NTHR) {
+            const int r = e / M, m = e % M;
+            float ta[6], tb[6];
 #pragma unroll
-            for (int c = 0; c < 6; ++c) t6[c] = (float)re[2 * fftdev::sidx<true>((c * RPC + r) * M + (z >> 1)) + (z & 1)];
-            label_cell<LAMBDAS>(t6, lth, band, (row0 + r) * 2 * M + z, ncell, labels, lambdas, lc0, lc1, lc2, lc3,
-                                lties);
+            for (int c = 0; c < 6; ++c) {
+                const C v = tile[fftdev::sidx<true>((c * RPC + r) * M + m)];
+                ta[c] = (float)v.x;
+                tb[c] = (float)v.y;
+            }
+            const int64_t cell = (row0 + r) * 2 * M + 2 * m;
+            label_cell<LAMBDAS>(ta, lth, band, cell, ncell, labels, lambdas, lc0, lc1, lc2, lc3, lties);
+            label_cell<LAMBDAS>(tb, lth, band, cell + 1, ncell, labels, lambdas, lc0, lc1, lc2, lc3, lties);
         }
         __syncthreads();  // tile is refilled next
     }
@@ -754,12 +766,12 @@ void tweb_impl(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const d
                                     1.0)) {
             dim3 g0(3, (unsigned)((M + W - 1) / W), (unsigned)n);
             CAM_LAUNCH_NAMED(ctx, "tweb_tidal_y", ky, g0, nthr, smem, cm, (int)n, (int)M, (int64_t)M, (int64_t)1, n * M,
-                             ccomp, rn, tw);
+                             ccomp, rn, tw, -1);
         }
         // Nyquist plane: columns i (stride N), FFT index j (stride 1)
         dim3 g1(3, (unsigned)((n + W - 1) / W), 1);
         CAM_LAUNCH_NAMED(ctx, "tweb_tidal_y_nyq", ky, g1, nthr, smem, cn, (int)n, (int)n, (int64_t)1, n, (int64_t)0,
-                         nn, rn, tw);
+                         nn, rn, tw, (int)M);
         });
     }
     // 3. z: c2r + eigenvalues + labels.
