@@ -404,6 +404,11 @@ int cam_ctx_destroy(cam_ctx *ctx)
         if (ctx->batch) batch_destroy(ctx->batch);
         ctx->batch = nullptr;
         release_all(ctx);
+        if (ctx->job_pin) {
+            std::lock_guard<std::mutex> lk(alloc_mutex());
+            cudaFreeHost(ctx->job_pin);
+            ctx->job_pin = nullptr;
+        }
         if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     }
     delete ctx;
@@ -676,34 +681,77 @@ int cam_job_run(cam_ctx *ctx, const cam_job_desc *job, cam_job_result *res)
         const int64_t n = g.n[0], ncell = n * n * n;
         const DevParticles d = stage_particles(ctx, &job->parts);
         FftPlan *plan = get_plan(ctx, n, job->precision);
-        AssignOut out;
-        out.precision = job->precision;
-        out.mesh = scratch(ctx, "job.mesh", ncell * esize(job->precision));
-        auto *dsum = static_cast<double *>(scratch(ctx, "job.sum", 2 * sizeof(double)));
-        out.d_sum = dsum;
-        assign_device(ctx, d.x, d.y, d.z, d.w, d.n, g, job->scheme, out);
-        // FFT of rho - mean, mean from the deposit's exact per-brick sums.
-        Spectrum s = alloc_spectrum(ctx, n, job->precision, "job.spec");
-        fft_r2c_split(ctx, plan, out.mesh, dsum + 1, s);
-        double hs[2] = {0.0, 0.0};
-        CAM_CUDA_TRY(cudaMemcpyAsync(hs, dsum, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
-        CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-        res->assign.n_in = out.n_in;
-        res->assign.n_lost = out.n_lost;
-        res->assign.sum_mesh = hs[0];
-        if (want_pk) {
-            cam_pk_opts po = job->pk;
-            power_from_spectrum(ctx, s, g.L[0], hs[0], po, res->pk, res->modes, res->kvector, &res->pk_info);
+        const int nb = want_pk ? nbins_for(job->pk, n) : 0;
+        // Readback of one run: assignment statistics [4], mesh sum and mean
+        // [2], P(k) sums [nb][2] and modes [nb], into a pinned buffer.
+        const size_t pin_bytes = 4 * 8 + 2 * 8 + (size_t)nb * 24;
+        if (ctx->job_pin_bytes < pin_bytes) {
+            std::lock_guard<std::mutex> lk(alloc_mutex());
+            if (ctx->job_pin) CAM_CUDA_TRY(cudaFreeHost(ctx->job_pin));
+            ctx->job_pin = nullptr;
+            ctx->job_pin_bytes = 0;
+            CAM_CUDA_TRY(cudaHostAlloc(reinterpret_cast<void **>(&ctx->job_pin), pin_bytes, cudaHostAllocDefault));
+            ctx->job_pin_bytes = pin_bytes;
         }
-        if (job->want_tweb) {
-            uint8_t *dl = res->labels ? static_cast<uint8_t *>(scratch(ctx, "tw.labels", ncell)) : nullptr;
-            cam_tweb_opts to = job->tweb;
-            tweb_device(ctx, plan, s, g.L[0], dsum + 1, to.input_type, to, dl, nullptr, &res->tweb);
-            if (dl) {
-                CAM_CUDA_TRY(cudaMemcpyAsync(res->labels, dl, ncell, cudaMemcpyDeviceToHost, ctx->stream));
-                CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        auto *hstats = reinterpret_cast<unsigned long long *>(ctx->job_pin);
+        auto *hsum = reinterpret_cast<double *>(ctx->job_pin + 32);
+        auto *hpk = reinterpret_cast<double *>(ctx->job_pin + 48);
+        auto *hmd = reinterpret_cast<unsigned long long *>(ctx->job_pin + 48 + (size_t)nb * 16);
+        // One run of the whole job.  defer: the assignment sizes its payload
+        // from an estimate and nothing waits for the host until the single
+        // readback at the end; returns true if the estimate fell short (the
+        // results are then void and the job runs again without defer).
+        auto run = [&](bool defer) -> bool {
+            AssignOut out;
+            out.precision = job->precision;
+            out.mesh = scratch(ctx, "job.mesh", ncell * esize(job->precision));
+            auto *dsum = static_cast<double *>(scratch(ctx, "job.sum", 2 * sizeof(double)));
+            out.d_sum = dsum;
+            out.defer = defer;
+            assign_device(ctx, d.x, d.y, d.z, d.w, d.n, g, job->scheme, out);
+            // FFT of rho - mean, mean from the deposit's exact per-brick sums.
+            Spectrum s = alloc_spectrum(ctx, n, job->precision, "job.spec");
+            fft_r2c_split(ctx, plan, out.mesh, dsum + 1, s);
+            PkDevice pkd{nullptr, nullptr};
+            if (want_pk) pkd = power_bin_device(ctx, s, job->pk, nb);
+            CAM_CUDA_TRY(cudaMemcpyAsync(hstats, assign_stats(ctx), 32, cudaMemcpyDeviceToHost, ctx->stream));
+            CAM_CUDA_TRY(cudaMemcpyAsync(hsum, dsum, 16, cudaMemcpyDeviceToHost, ctx->stream));
+            if (want_pk) {
+                CAM_CUDA_TRY(cudaMemcpyAsync(hpk, pkd.sums, (size_t)nb * 16, cudaMemcpyDeviceToHost, ctx->stream));
+                CAM_CUDA_TRY(cudaMemcpyAsync(hmd, pkd.modes, (size_t)nb * 8, cudaMemcpyDeviceToHost, ctx->stream));
             }
-        }
+            CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+            if (defer && (hstats[3] & 0xffffffffu)) return true;
+            if (d.w) {
+                const unsigned wbits = (unsigned)(hstats[1] & 0xffffffffu);
+                CAM_REQUIRE(wbits < 0x7f800000u, CAM_E_NONFINITE, "a particle weight is NaN or infinite");
+            }
+            res->assign.n_lost = (int64_t)hstats[0];
+            res->assign.n_in = d.n - res->assign.n_lost;
+            res->assign.sum_mesh = hsum[0];
+            if (want_pk) {
+                std::vector<double> sr(nb), ss(nb);
+                std::vector<int64_t> md(nb);
+                for (int b = 0; b < nb; ++b) {
+                    sr[b] = hpk[2 * b];
+                    ss[b] = hpk[2 * b + 1];
+                    md[b] = (int64_t)hmd[b];
+                }
+                finalize_pk(n, g.L[0], hsum[0], job->pk, nb, sr.data(), ss.data(), md.data(), res->pk, res->modes,
+                            res->kvector, &res->pk_info);
+            }
+            if (job->want_tweb) {
+                uint8_t *dl = res->labels ? static_cast<uint8_t *>(scratch(ctx, "tw.labels", ncell)) : nullptr;
+                cam_tweb_opts to = job->tweb;
+                tweb_device(ctx, plan, s, g.L[0], dsum + 1, to.input_type, to, dl, nullptr, &res->tweb);
+                if (dl) {
+                    CAM_CUDA_TRY(cudaMemcpyAsync(res->labels, dl, ncell, cudaMemcpyDeviceToHost, ctx->stream));
+                    CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+                }
+            }
+            return false;
+        };
+        if (run(true)) run(false);
     });
 }
 

@@ -197,8 +197,9 @@ __device__ __forceinline__ void count_one(float px, float py, float pz, float wt
 template <int SCHEME, bool SCATTER, bool SMEM>
 __device__ __forceinline__ void bin_one(float px, float py, float pz, float wt, bool weighted,
                                         const AssignGeom &g, int G, int blk, uint32_t *hist,
-                                        uint32_t *__restrict__ table, uint4 *__restrict__ payload,
-                                        unsigned long long &my_lost, unsigned int &my_wmax, unsigned int &my_neg)
+                                        uint32_t *__restrict__ table, uint4 *__restrict__ payload, uint64_t cap,
+                                        unsigned int *ovf, unsigned long long &my_lost, unsigned int &my_wmax,
+                                        unsigned int &my_neg)
 {
     using St = Stencil<SCHEME>;
     const float pos[3] = {px, py, pz};
@@ -253,7 +254,10 @@ __device__ __forceinline__ void bin_one(float px, float py, float pz, float wt, 
                         else if (cl > e) cl -= g.n[a];
                         word[a] = pack_axis(cl, t[a]);
                     }
-                    payload[slot] = make_uint4(word[0], word[1], word[2], __float_as_uint(wt));
+                    // records past the payload's capacity (a deferred
+                    // estimate that fell short) are flagged, not written
+                    if (slot < cap) payload[slot] = make_uint4(word[0], word[1], word[2], __float_as_uint(wt));
+                    else atomicOr(ovf, 1u);
                 }
             }
         }
@@ -280,7 +284,7 @@ __global__ void __launch_bounds__(kBinThreads)
 bin_kernel(const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z,
            const float *__restrict__ w, int64_t np, int64_t chunk, AssignGeom g, int nb,
            uint32_t *__restrict__ table, uint4 *__restrict__ payload, unsigned long long *__restrict__ lost,
-           unsigned int *__restrict__ wmax_bits)
+           unsigned int *__restrict__ wmax_bits, uint64_t cap, unsigned int *__restrict__ ovf)
 {
     extern __shared__ uint32_t hist[];
     constexpr bool kHist = SMEM && !SCATTER;
@@ -295,8 +299,8 @@ bin_kernel(const float *__restrict__ x, const float *__restrict__ y, const float
     const bool weighted = w != nullptr;
     auto one = [&](float px, float py, float pz, float wt) {
         if (SCATTER)
-            bin_one<SCHEME, true, false>(px, py, pz, wt, weighted, g, G, blk, hist, table, payload, my_lost, my_wmax,
-                                         my_neg);
+            bin_one<SCHEME, true, false>(px, py, pz, wt, weighted, g, G, blk, hist, table, payload, cap, ovf,
+                                         my_lost, my_wmax, my_neg);
         else
             count_one<SCHEME, kHist>(px, py, pz, wt, weighted, g, hist, table, my_lost, my_wmax, my_neg);
     };
@@ -492,7 +496,7 @@ __device__ __forceinline__ void deposit_range(const uint4 *__restrict__ payload,
 // wstat[0] = bits of max |w|, wstat[1] != 0 if some weight is negative.
 template <int SCHEME, typename OutT>
 __global__ void __launch_bounds__(kDepositThreads)
-deposit_kernel(const uint4 *__restrict__ payload, const uint32_t *__restrict__ start,
+deposit_kernel(const uint4 *__restrict__ payload, const uint32_t *__restrict__ start, uint32_t nrec,
                AssignGeom g, const unsigned int *__restrict__ wstat, int weighted,
                OutT *__restrict__ mesh, double *__restrict__ brick_sum)
 {
@@ -519,7 +523,8 @@ deposit_kernel(const uint4 *__restrict__ payload, const uint32_t *__restrict__ s
     }
     __syncthreads();
 
-    const uint32_t beg = start[B], end = start[B + 1];
+    // records beyond the payload's capacity nrec were not written (overflow flag)
+    const uint32_t beg = min(start[B], nrec), end = min(start[B + 1], nrec);
     const float wmax = weighted ? __uint_as_float(wstat[0]) : 1.0f;
     const bool nonneg = !weighted || wstat[1] == 0u;
     int ex = 0;
@@ -656,6 +661,7 @@ static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const floa
     unsigned long long *d_lost = stats;
     unsigned int *d_wmax = reinterpret_cast<unsigned int *>(stats + 1);
     uint32_t *d_total = reinterpret_cast<uint32_t *>(stats + 2);
+    unsigned int *d_ovf = reinterpret_cast<unsigned int *>(stats + 3);
     CAM_CUDA_TRY(cudaMemsetAsync(table, 0, (size_t)nb * kCursorStride * sizeof(uint32_t), ctx->stream));
     CAM_CUDA_TRY(cudaMemsetAsync(stats, 0, 64, ctx->stream));
 
@@ -665,7 +671,7 @@ static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const floa
     auto scatter_k = vec ? bin_kernel<SCHEME, true, false, true> : bin_kernel<SCHEME, true, false, false>;
     if (hsmem > 48 * 1024) smem_at_least(count_k, hsmem);
     CAM_LAUNCH_NAMED(ctx, "assign_bin_count", count_k, G, kBinThreads, hsmem, x, y, z, w, np, chunk, g, (int)nb,
-                     table, (uint4 *)nullptr, d_lost, d_wmax);
+                     table, (uint4 *)nullptr, d_lost, d_wmax, (uint64_t)0, d_ovf);
     const unsigned sg = (unsigned)std::min<int64_t>((nb + 256) / 256, 1024);
     CAM_LAUNCH_NAMED(ctx, "assign_starts", compact_counts_kernel, sg, 256, 0, table, (int)nb, counts);
     exclusive_scan_u32(ctx, counts, nb, d_total);
@@ -683,12 +689,33 @@ static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const floa
         CAM_REQUIRE(total < (1ull << 32), CAM_E_UNSUPPORTED, "payload bound exceeds 2^32 records");
         out.n_lost = -1;
         out.n_in = -1;
+    } else if (out.defer) {
+        // No host round trip: the expected record count of a uniform
+        // catalogue (a stencil crosses a face of a brick of extent b with
+        // probability (W-1)/b per axis) with a 25% margin, never below what
+        // this context used before nor above the provable bound.  The
+        // scatter flags records past it; the caller then reruns.
+        double f = 1.0;
+        uint64_t per = 1;
+        for (int a = 0; a < 3; ++a) {
+            if (SCHEME == CAM_NGP || g.nb[a] == 1) continue;
+            f *= 1.0 + std::min(1.0, (double)(Stencil<SCHEME>::W - 1) / g.b[a]);
+            per *= 2;
+        }
+        const uint64_t bound = (uint64_t)np * per;
+        uint64_t est = (uint64_t)((double)np * f * 1.25) + 65536;
+        est = std::min(bound, std::max(est, ctx->asg_cap));
+        total = std::min<uint64_t>(est, 0xffffffffull);
+        ctx->asg_cap = std::max(ctx->asg_cap, total);
+        out.n_lost = -1;
+        out.n_in = -1;
     } else {
         // Payload size and diagnostics back to the host (one synchronisation).
         unsigned long long hstats[3] = {0, 0, 0};
         CAM_CUDA_TRY(cudaMemcpyAsync(hstats, stats, sizeof(hstats), cudaMemcpyDeviceToHost, ctx->stream));
         CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
         total = (uint32_t)(hstats[2] & 0xffffffffu);
+        ctx->asg_cap = std::max<uint64_t>(ctx->asg_cap, total);  // deferred runs size from it
         const unsigned int wmax_bits = (unsigned int)(hstats[1] & 0xffffffffu);
         CAM_REQUIRE(!w || wmax_bits < 0x7f800000u, CAM_E_NONFINITE, "a particle weight is NaN or infinite");
         out.n_lost = (int64_t)hstats[0];
@@ -697,15 +724,15 @@ static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const floa
 
     uint4 *payload = static_cast<uint4 *>(scratch(ctx, "asg.payload", std::max<size_t>(total, 1) * sizeof(uint4)));
     CAM_LAUNCH_NAMED(ctx, "assign_bin_scatter", scatter_k, G2, kScatterThreads, 0, x, y, z, w, np, chunk2, g,
-                     (int)nb, table, payload, d_lost, d_wmax);
+                     (int)nb, table, payload, d_lost, d_wmax, total, d_ovf);
 
     const size_t smem = (size_t)g.b[0] * g.b[1] * g.b[2] * 2 * sizeof(uint32_t);
     CAM_REQUIRE(smem <= 200 * 1024, CAM_E_UNSUPPORTED, "brick tile too large");
     const int weighted = w != nullptr;
     auto launch_dep = [&](auto kern, auto *mesh) {
         smem_at_least(kern, smem);
-        CAM_LAUNCH_NAMED(ctx, "assign_deposit", kern, (unsigned)nb, kDepositThreads, smem, payload, start, g, d_wmax,
-                         weighted, mesh, bsum);
+        CAM_LAUNCH_NAMED(ctx, "assign_deposit", kern, (unsigned)nb, kDepositThreads, smem, payload, start,
+                         (uint32_t)std::min<uint64_t>(total, 0xffffffffull), g, d_wmax, weighted, mesh, bsum);
     };
     if (out.precision == CAM_F32)
         launch_dep(deposit_kernel<SCHEME, float>, static_cast<float *>(out.mesh));
@@ -715,6 +742,11 @@ static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const floa
         launch_dep(deposit_kernel<SCHEME, uint32_t>, static_cast<uint32_t *>(out.mesh));
     // out.d_sum[0] = sum of the mesh, out.d_sum[1] = mean per cell
     if (out.d_sum) reduce_sum_f64(ctx, bsum, nb, out.d_sum, (double)g.n[0] * g.n[1] * g.n[2]);
+}
+
+unsigned long long *assign_stats(cam_ctx *ctx)
+{
+    return static_cast<unsigned long long *>(scratch(ctx, "asg.stats", 64));
 }
 
 void assign_device(cam_ctx *ctx, const float *x, const float *y, const float *z,

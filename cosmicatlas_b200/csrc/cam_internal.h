@@ -78,6 +78,9 @@ struct cam_ctx {
     // device buffers) -- the mode used under stream capture
     bool sync_free = false;
     bool capturing = false;  // inside stream capture: no allocation, no events
+    uint64_t asg_cap = 0;    // payload records of deferred assignments (grow-only)
+    unsigned char *job_pin = nullptr;  // pinned readback buffer of cam_job_run
+    size_t job_pin_bytes = 0;
     // bumped whenever a scratch buffer is (re)allocated or freed, so that
     // captured graphs holding its old addresses can be recognised as stale
     uint64_t gen = 0;
@@ -136,10 +139,21 @@ struct AssignOut {
     void *mesh;         // device
     double *d_sum;      // device scalar: sum of the mesh (FP64)
     int64_t n_in = 0, n_lost = 0;
+    // defer: no host round trip.  The payload holds an estimate of the
+    // record count (grow-only per context); records past it are not
+    // written and raise the overflow word of the device statistics, in
+    // which case the caller reruns without defer.  n_in / n_lost are -1.
+    bool defer = false;
 };
 
+// Device statistics of the last assignment of a context (asg.stats):
+// [0] lost particles, [1] low word: bits of max |w|, [2] low word: payload
+// records, [3] low word: nonzero if the deferred payload overflowed.
+unsigned long long *assign_stats(cam_ctx *ctx);
+
 // Runs the assignment pipeline on device particle arrays.  Writes the mesh
-// and, on the device, the FP64 mesh sum.  Synchronises once (payload size).
+// and, on the device, the FP64 mesh sum.  Synchronises once (payload size)
+// unless sync_free or out.defer.
 void assign_device(cam_ctx *ctx, const float *x, const float *y, const float *z,
                    const float *w, int64_t np, const cam_grid &grid, int scheme,
                    AssignOut &out);
@@ -177,10 +191,13 @@ void fft_rows_c2c(cam_ctx *ctx, FftPlan *plan, void *base, int64_t len, int64_t 
 const void *plan_twiddles(FftPlan *plan);
 
 // ------------------------------------------------------ power spectrum
+// Bin sums of a spectrum left on the device: sums [nbins][2] FP64
+// (sum |F|^2/W^2, sum C/W^2), modes [nbins].
 struct PkDevice {
-    double *sums;   // [nbins][2] FP64: sum |F|^2/W^2, sum C/W^2
-    int64_t *modes; // [nbins]
+    double *sums;
+    unsigned long long *modes;
 };
+PkDevice power_bin_device(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins);
 void power_bin(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins,
                double *h_sum_raw, double *h_sum_sn, int64_t *h_modes);
 

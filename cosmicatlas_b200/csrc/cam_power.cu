@@ -209,8 +209,7 @@ double sq_factor(int p, double s)
 
 }  // namespace
 
-void power_bin(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins, double *h_sum_raw,
-               double *h_sum_sn, int64_t *h_modes)
+PkDevice power_bin_device(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins)
 {
     const int n = (int)s.n, h = n / 2;
     CAM_REQUIRE(nbins >= 1 && nbins <= 4096, CAM_E_INVAL, "nbins must be in [1, 4096]");
@@ -274,7 +273,16 @@ void power_bin(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins,
                    d_tab, nbins, m_u, inv_s, rpc, part, pm);
     }
     CAM_LAUNCH(ctx, pk_final_kernel, nbins, 256, 0, part, pm, grid, nbins, res, resm);
+    return PkDevice{res, resm};
+}
+
+void power_bin(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins, double *h_sum_raw,
+               double *h_sum_sn, int64_t *h_modes)
+{
+    const PkDevice d = power_bin_device(ctx, s, o, nbins);
     if (ctx->sync_free) return;  // sums stay in pk.res / pk.resm for the caller
+    double *res = d.sums;
+    unsigned long long *resm = d.modes;
     std::vector<double> hres(2 * nbins);
     std::vector<unsigned long long> hm(nbins);
     CAM_CUDA_TRY(cudaMemcpyAsync(hres.data(), res, 2 * nbins * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));

@@ -109,3 +109,38 @@ def test_job_fp64_mesh_c1_shape(ctx):
     floor = pk.shot_noise * pk.sum_sn / np.maximum(pk.modes, 1)
     # FP64 mesh and FFT; the stencil weights are FP32 products (~1e-7)
     assert pk_rel_err(res["pk"].pk, pk.pk, floor) <= 1e-6
+
+
+def test_job_payload_estimate_overflow_reruns():
+    # Every particle's CIC stencil crosses a brick face along all three axes
+    # (home cell 31 ends a brick for every power-of-two brick extent <= 32),
+    # so each gives 8 records, far above the job's payload estimate: the
+    # first job of a fresh context overflows it and reruns exactly; the
+    # second finds the grown capacity and runs once.
+    n, box, nbins = 64, 64.0, 24
+    rng = np.random.default_rng(41)
+    npart = 60_000
+    x, y, z = (rng.uniform(31.5, 32.5, npart).astype(np.float32) for _ in range(3))
+    w = synth.halo_masses(npart, seed=42)
+    g = make_grid(n, box)
+    opts = Context.pk_opts(CIC, nbins=nbins)
+    c = Context(0)
+    try:
+        l0 = c.kernel_launches
+        r1 = c.job(x, y, z, w, g, CIC, F32, pk=opts)
+        l1 = c.kernel_launches
+        r2 = c.job(x, y, z, w, g, CIC, F32, pk=opts)
+        l2 = c.kernel_launches
+        mesh = c.assign(x, y, z, w, g, CIC, F32).mesh
+        pk = c.power(mesh, box, opts)
+    finally:
+        c.close()
+    assert l1 - l0 > l2 - l1  # the first job ran twice
+    assert r1["assign"].n_lost == 0 and r1["assign"].n_in == npart
+    assert np.array_equal(r1["pk"].pk, r2["pk"].pk)
+    np.testing.assert_allclose(r1["pk"].pk, pk.pk, rtol=1e-8)
+    _, lost, opk, _ = oracle_job(x, y, z, w, n, box, CIC, nbins, None, 0.0, F32)
+    assert lost == 0
+    floor = opk.shot_noise * opk.sum_sn / np.maximum(opk.modes, 1)
+    assert np.array_equal(r1["pk"].modes, opk.modes)
+    assert pk_rel_err(r1["pk"].pk, opk.pk, floor) <= 1e-5
