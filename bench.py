@@ -11,7 +11,9 @@ value : jobs/s with the particles resident in HBM (device pointers).
 e2e   : jobs/s through the C ABI with pinned host particle buffers: every
         step uploads the step's particles once (cam_particles_stage) and runs
         the three jobs on them; the host->device copy and the device->host
-        copies of the P(k) results are inside the timed region.
+        copies of the P(k) results are inside the timed region.  Two contexts
+        on two streams alternate steps, and each step's upload is issued
+        before the previous step's jobs (the copy engine overlaps them).
 Multi-GPU: one process per GPU, each runs its own jobs (independent meshes,
 "weak" scaling, no collective in the data path); time is the max over ranks.
 
@@ -249,6 +251,42 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
+    # second context for the host-fed pass: step i+1's upload (an
+    # asynchronous copy on its stream) runs under step i's jobs
+    ctx_b = Context(local)
+    stream_b = torch.cuda.Stream()
+    ctx_b.set_stream(stream_b.cuda_stream)
+    ctxs = (ctx, ctx_b)
+
+    def host_fed(k):
+        staged = [None, None]
+        staged[0] = ctxs[0].stage(*pinned)
+        r = None
+        for i in range(k):
+            if i + 1 < k:
+                staged[(i + 1) % 2] = ctxs[(i + 1) % 2].stage(*pinned)
+            c, src = ctxs[i % 2], staged[i % 2]
+            for s in SCHEMES:
+                r = c.job(src, grid=grid, scheme=s, precision=0, pk=opts[s])
+        return r
+
+    def timed_host_fed(k):
+        barrier()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        host_fed(k)
+        # every job has returned its P(k) to the host: all work is done
+        t1.record(stream)
+        torch.cuda.synchronize()
+        ms = t0.elapsed_time(t1)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        barrier()
+        return ms
+
     def timed(arrs, k, lat=None):
         barrier()
         t0 = torch.cuda.Event(enable_timing=True)
@@ -269,7 +307,7 @@ def run_ours(args):
     for _ in range(args.warmup):
         step(dev)
         if not args.kernels_only:
-            step(pinned)
+            host_fed(2)
     # device-resident inputs: the headline `value`
     lat = []
     launches0 = ctx.kernel_launches
@@ -287,7 +325,7 @@ def run_ours(args):
     prof = ctx.profile_read(reset=True)
     ctx.profile(False)
     # end to end: pinned host particles in, P(k) out
-    ms_e2e = timed(pinned, args.steps) if not args.kernels_only else float("nan")
+    ms_e2e = timed_host_fed(args.steps) if not args.kernels_only else float("nan")
 
     jobs = len(SCHEMES) * args.steps * world
     value = jobs / (ms / 1e3)
@@ -338,7 +376,9 @@ def run_ours(args):
             "latency_ms": {"p50": round(float(np.percentile(job_ms, 50)), 3),
                            "p99": round(float(np.percentile(job_ms, 99)), 3)},
             "e2e": {"value": round(e2e, 3), "unit": "jobs/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
+                    "d2h_bytes_per_step": d2h,
+                    "path": "cam_particles_stage + 3 x cam_job_run per step; two contexts alternate steps, "
+                            "each upload issued before the previous step's jobs"},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "stage": dom, "achieved": stages[dom]["achieved_gbs"],
                          "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
