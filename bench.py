@@ -80,14 +80,15 @@ def config_dict(n_particles, extra=None):
 
 class ClockSampler:
     """SM clock, max clock and clock-event (throttle) reasons of the GPU,
-    sampled every 5 ms through NVML while the timed region runs (reading
-    only; nvidia-smi -lms 100 if NVML is unavailable)."""
+    sampled every `period_s` (5 ms) through NVML while the timed region runs
+    (reading only; nvidia-smi -lms 100 if NVML is unavailable)."""
 
     REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
                "sw_power_cap": 0x4}
 
-    def __init__(self, index):
+    def __init__(self, index, period_s=0.005):
         self.index = index
+        self.period_s = period_s
         self.samples = []  # (sm_mhz, max_mhz, reasons bitmask)
         self.proc = None
         self.thread = None
@@ -113,7 +114,7 @@ class ClockSampler:
                 self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)), float(mx), int(get_r(h))))
             except Exception:
                 pass
-            self.stop.wait(0.005)
+            self.stop.wait(self.period_s)
 
     def _sample_now(self):
         if self.nv is None:
@@ -765,7 +766,7 @@ def run_stream(args):
     out = {"workload": f"served mixed stream: {njobs} jobs, N in 64..512, N_p log-uniform [1e5, 5e7], "
                        "L log-uniform [250, 2000], NGP/CIC/TSC, half with T-web; HBM budget 150 GB",
            "metric": "mesh-jobs/s", "unit": "jobs/s", "rates": {}}
-    with ClockSampler(0) as clk:
+    with ClockSampler(0, period_s=0.05) as clk:  # minutes long: 20 samples/s
         out["saturation"] = {"served": one_pass(4, 16, 0), "plain": one_pass(1, 1, 0)}
         for r in rates:
             out["rates"][str(r)] = {"served": one_pass(4, 16, r), "plain": one_pass(1, 1, r)}

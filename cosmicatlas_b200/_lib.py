@@ -103,6 +103,7 @@ SIGNATURES = {
     "cam_ctx_sync": ([_P], ctypes.c_int),
     "cam_last_error": ([_P], ctypes.c_char_p),
     "cam_kernel_launches": ([_P], ctypes.c_int64),
+    "cam_pool_trim": ([ctypes.c_int], ctypes.c_int),
     "cam_profile_enable": ([_P, ctypes.c_int], ctypes.c_int),
     "cam_profile_read": ([_P, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_int], ctypes.c_int),
     "cam_assign": ([_P, ctypes.POINTER(Particles), ctypes.POINTER(Grid), ctypes.c_int, ctypes.c_int, _P,

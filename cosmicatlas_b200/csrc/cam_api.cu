@@ -65,6 +65,14 @@ void *scratch(cam_ctx *ctx, const char *name, size_t bytes)
     void *p = nullptr;
     cudaError_t e = cudaMallocFromPoolAsync(&p, want, pool, ctx->stream);
     if (e != cudaSuccess) {
+        // idle pool memory may be fragmented or held for other sizes: hand
+        // it back to the device and try once more
+        cudaGetLastError();
+        cudaDeviceSynchronize();
+        cudaMemPoolTrimTo(pool, 0);
+        e = cudaMallocFromPoolAsync(&p, want, pool, ctx->stream);
+    }
+    if (e != cudaSuccess) {
         cudaGetLastError();
         throw Error{CAM_E_NOMEM, std::string("device allocation failed for ") + name + ": " + cudaGetErrorString(e)};
     }
@@ -145,13 +153,10 @@ void release_all(cam_ctx *ctx)
     cudaStreamSynchronize(ctx->stream);
     ctx->bufs.clear();
     ctx->used = 0;
-    // hand the pool's idle memory back to the device
-    if (ctx->device >= 0 && ctx->device < 64) {
-        try {
-            cudaMemPoolTrimTo(device_pool(ctx->device), 0);
-        } catch (const Error &) {
-        }
-    }
+    // The freed blocks stay in the device pool: trimming it here made every
+    // later growth map new physical memory while other contexts' jobs ran,
+    // and jobs running at that moment stalled for 0.4-1 s (served stream).
+    // The pool is trimmed on an allocation failure or by cam_pool_trim.
     cudaGetLastError();
 }
 
@@ -428,6 +433,28 @@ int cam_ctx_sync(cam_ctx *ctx)
 const char *cam_last_error(cam_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
 int64_t cam_kernel_launches(cam_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
+int cam_pool_trim(int device)
+{
+    try {
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+            cudaGetLastError();
+            return CAM_E_INVAL;
+        }
+        std::lock_guard<std::mutex> lk(alloc_mutex());
+        cudaMemPool_t pool = device_pool(device);
+        int prev = 0;
+        cudaGetDevice(&prev);
+        cudaSetDevice(device);
+        cudaDeviceSynchronize();  // frees still in flight complete first
+        const cudaError_t e = cudaMemPoolTrimTo(pool, 0);
+        cudaSetDevice(prev);
+        return e == cudaSuccess ? CAM_OK : CAM_E_CUDA;
+    } catch (const Error &e) {
+        return e.code;
+    }
+}
 
 int cam_profile_enable(cam_ctx *ctx, int on)
 {

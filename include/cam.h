@@ -112,6 +112,13 @@ typedef struct {
  * by the context and reused across calls. */
 int cam_ctx_create(int device, size_t hbm_budget, cam_ctx **out);
 int cam_ctx_destroy(cam_ctx *ctx);
+/* Device memory of all contexts comes from one stream-ordered pool per
+ * device.  Memory a context frees (cam_ctx_destroy, a server dropping its
+ * caches) stays in the pool for the next allocation, so a long-running
+ * process does not pay the device's allocation cost again; the pool is
+ * trimmed automatically when an allocation fails.  cam_pool_trim hands the
+ * pool's idle memory back to the device now.  No reference counterpart. */
+int cam_pool_trim(int device);
 /* Sets the CUDA stream (cudaStream_t) the context launches on (NULL = the
  * context's own stream). */
 int cam_ctx_set_stream(cam_ctx *ctx, void *stream);
