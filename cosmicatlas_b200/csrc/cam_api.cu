@@ -184,12 +184,23 @@ __global__ void __launch_bounds__(256) partial_sum_kernel(const T *__restrict__ 
     }
 }
 
-__global__ void final_sum_kernel(const double *__restrict__ part, int np, double *__restrict__ out,
-                                 double divisor)
+// One CTA of kFinalThreads: thread t sums in[t], in[t + kFinalThreads], ...
+// in order, then a fixed shuffle tree per warp and the warp sums in order
+// (FP64, the same order on every run).  out[0] = sum, out[1] = sum / divisor.
+constexpr int kFinalThreads = 1024;
+__global__ void __launch_bounds__(kFinalThreads)
+final_sum_kernel(const double *__restrict__ part, int np, double *__restrict__ out, double divisor)
 {
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
+    __shared__ double red[kFinalThreads / 32];
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < np; i += kFinalThreads) acc += part[i];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
         double t = 0.0;
-        for (int i = 0; i < np; ++i) t += part[i];
+        for (int w = 0; w < kFinalThreads / 32; ++w) t += red[w];
         out[0] = t;
         out[1] = t / divisor;
     }
@@ -197,12 +208,17 @@ __global__ void final_sum_kernel(const double *__restrict__ part, int np, double
 
 }  // namespace
 
-// out[0] = sum, out[1] = sum / divisor (FP64, fixed order).
+// out[0] = sum, out[1] = sum / divisor (FP64, fixed order).  Up to 2^16
+// values are summed by one CTA directly.
 void reduce_sum_f64(cam_ctx *ctx, const double *in, int64_t n, double *out, double divisor)
 {
+    if (n <= 65536) {
+        CAM_LAUNCH(ctx, final_sum_kernel, 1, kFinalThreads, 0, in, (int)n, out, divisor);
+        return;
+    }
     auto *part = static_cast<double *>(scratch(ctx, "red.part", kRedBlocks * sizeof(double)));
     CAM_LAUNCH(ctx, partial_sum_kernel<double>, kRedBlocks, 256, 0, in, n, part);
-    CAM_LAUNCH(ctx, final_sum_kernel, 1, 32, 0, part, kRedBlocks, out, divisor);
+    CAM_LAUNCH(ctx, final_sum_kernel, 1, kFinalThreads, 0, part, kRedBlocks, out, divisor);
 }
 
 void mesh_mean(cam_ctx *ctx, const void *mesh, int precision, int64_t ncell, double *d_out)
@@ -212,7 +228,7 @@ void mesh_mean(cam_ctx *ctx, const void *mesh, int precision, int64_t ncell, dou
         CAM_LAUNCH(ctx, partial_sum_kernel<float>, kRedBlocks, 256, 0, (const float *)mesh, ncell, part);
     else
         CAM_LAUNCH(ctx, partial_sum_kernel<double>, kRedBlocks, 256, 0, (const double *)mesh, ncell, part);
-    CAM_LAUNCH(ctx, final_sum_kernel, 1, 32, 0, part, kRedBlocks, d_out, (double)ncell);
+    CAM_LAUNCH(ctx, final_sum_kernel, 1, kFinalThreads, 0, part, kRedBlocks, d_out, (double)ncell);
 }
 
 }  // namespace cam

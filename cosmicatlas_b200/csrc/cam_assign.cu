@@ -343,6 +343,60 @@ bin_kernel(const float *__restrict__ x, const float *__restrict__ y, const float
     }
 }
 
+// Brick starts in one CTA (nb <= kOffThreads * kOffItems): thread t scans
+// the counts of bricks [t * kOffItems, (t + 1) * kOffItems) in order, the
+// per-thread sums are scanned across the CTA, and every brick's start goes
+// to start[b] and to its padded cursor (which held its count); start[nb] =
+// *total = all records.
+constexpr int kOffThreads = 1024;
+constexpr int kOffItems = 16;
+__global__ void __launch_bounds__(kOffThreads)
+brick_offsets_kernel(uint32_t *__restrict__ padded, int nb, uint32_t *__restrict__ start, uint32_t *__restrict__ total)
+{
+    __shared__ uint32_t warp_sums[kOffThreads / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int base = threadIdx.x * kOffItems;
+    uint32_t v[kOffItems];
+    uint32_t s = 0;
+#pragma unroll
+    for (int i = 0; i < kOffItems; ++i) {
+        v[i] = base + i < nb ? padded[(int64_t)(base + i) * kCursorStride] : 0u;
+        s += v[i];
+    }
+    uint32_t incl = s;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t o = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl += o;
+    }
+    if (lane == 31) warp_sums[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        const uint32_t ws = warp_sums[lane];
+        uint32_t wi = ws;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t o = __shfl_up_sync(0xffffffffu, wi, off);
+            if (lane >= off) wi += o;
+        }
+        warp_sums[lane] = wi - ws;
+        if (lane == 31) {
+            start[nb] = wi;
+            *total = wi;
+        }
+    }
+    __syncthreads();
+    uint32_t run = warp_sums[wid] + incl - s;
+#pragma unroll
+    for (int i = 0; i < kOffItems; ++i) {
+        if (base + i < nb) {
+            start[base + i] = run;
+            padded[(int64_t)(base + i) * kCursorStride] = run;
+        }
+        run += v[i];
+    }
+}
+
 // counts[b] = padded[b * kCursorStride] (contiguous, for the scan).
 __global__ void compact_counts_kernel(const uint32_t *__restrict__ padded, int nb, uint32_t *__restrict__ counts)
 {
@@ -654,7 +708,6 @@ static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const floa
     const bool smem_hist = nb <= kSmemBricks;
     // per-brick counters, one per 128-byte line (counts, then cursors)
     auto *table = static_cast<uint32_t *>(scratch(ctx, "asg.cursor", (size_t)nb * kCursorStride * sizeof(uint32_t)));
-    auto *counts = static_cast<uint32_t *>(scratch(ctx, "asg.counts", (size_t)nb * sizeof(uint32_t)));
     auto *start = static_cast<uint32_t *>(scratch(ctx, "asg.start", (nb + 1) * sizeof(uint32_t)));
     auto *stats = static_cast<unsigned long long *>(scratch(ctx, "asg.stats", 64));
     auto *bsum = static_cast<double *>(scratch(ctx, "asg.bsum", nb * sizeof(double)));
@@ -672,10 +725,16 @@ static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const floa
     if (hsmem > 48 * 1024) smem_at_least(count_k, hsmem);
     CAM_LAUNCH_NAMED(ctx, "assign_bin_count", count_k, G, kBinThreads, hsmem, x, y, z, w, np, chunk, g, (int)nb,
                      table, (uint4 *)nullptr, d_lost, d_wmax, (uint64_t)0, d_ovf);
-    const unsigned sg = (unsigned)std::min<int64_t>((nb + 256) / 256, 1024);
-    CAM_LAUNCH_NAMED(ctx, "assign_starts", compact_counts_kernel, sg, 256, 0, table, (int)nb, counts);
-    exclusive_scan_u32(ctx, counts, nb, d_total);
-    CAM_LAUNCH_NAMED(ctx, "assign_starts", brick_starts_kernel, sg, 256, 0, counts, (int)nb, d_total, start, table);
+    if (nb <= (int64_t)kOffThreads * kOffItems) {
+        CAM_LAUNCH_NAMED(ctx, "assign_starts", brick_offsets_kernel, 1, kOffThreads, 0, table, (int)nb, start, d_total);
+    } else {
+        auto *counts = static_cast<uint32_t *>(scratch(ctx, "asg.counts", (size_t)nb * sizeof(uint32_t)));
+        const unsigned sg = (unsigned)std::min<int64_t>((nb + 256) / 256, 1024);
+        CAM_LAUNCH_NAMED(ctx, "assign_starts", compact_counts_kernel, sg, 256, 0, table, (int)nb, counts);
+        exclusive_scan_u32(ctx, counts, nb, d_total);
+        CAM_LAUNCH_NAMED(ctx, "assign_starts", brick_starts_kernel, sg, 256, 0, counts, (int)nb, d_total, start,
+                         table);
+    }
 
     uint64_t total = 0;
     if (ctx->sync_free) {
