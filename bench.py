@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--particles", type=int, default=N_PARTICLES)
     ap.add_argument("--kernels-only", action="store_true",
                     help="profiler runs: the device-resident pass only (no e2e pass, no CPU baseline)")
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "single512", "large768", "c1", "calib", "stream"],
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "single512", "large768", "c1", "calib", "stream", "bam"],
                     help="sweep: the benchmark line (default); single512 / large768 / c1: one-job latency lines; "
                          "calib / stream: served vs plain per-call jobs/s and latency")
     ap.add_argument("--jobs", type=int, default=0, help="calib / stream: number of jobs (0 = the config's)")
@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--serving-jobs", type=int, default=1024,
                     help="sweep: jobs of the calibration batch timed served vs per-call on the same line (0: skip)")
     ap.add_argument("--mesh", type=int, default=0, help="single512 only: override N (profiler runs)")
+    ap.add_argument("--tweb-method", default="fft", choices=["fft", "fd"],
+                    help="single-job workloads: T-web tidal tensor by FFTs (k_a k_b / k^2) or by the "
+                         "reference's default finite differences")
     return ap.parse_args()
 
 
@@ -492,7 +495,8 @@ def run_single(args):
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
     pko = Context.pk_opts(scheme, nbins=nb, ndel=ndel)
-    two = Context.tweb_opts(R, lth, 1e-5)
+    from cosmicatlas_b200 import _lib as CL
+    two = Context.tweb_opts(R, lth, 1e-5, method=CL.TWEB_FD if args.tweb_method == "fd" else CL.TWEB_FFT)
     for _ in range(args.warmup):
         ctx.job(arrs[0], arrs[1], arrs[2], None, grid, scheme, prec, pk=pko, tweb=two)
     ctx.profile(True)
@@ -518,7 +522,8 @@ def run_single(args):
                    "tile_offsets_kernel", "tile_scan_kernel"],
         "fft_r2c": ["fft_rows_r2c", "fft_cols", "fft_rows_c2c"],
         "power": ["pk_bin", "pk_final_kernel"],
-        "tweb": ["tweb_tidal_x", "tweb_tidal_x_nyq", "tweb_tidal_y", "tweb_tidal_y_nyq", "tweb_tidal_z_eigen"],
+        "tweb": ["tweb_tidal_x", "tweb_tidal_x_nyq", "tweb_tidal_y", "tweb_tidal_y_nyq", "tweb_tidal_z_eigen",
+                 "fd_table_kernel"],
     }
     k = args.steps
     stages = {}
@@ -528,7 +533,8 @@ def run_single(args):
                       "achieved_gbs": round(stage_bytes[st] / (t / 1e3) / 1e9, 1) if t > 0 else None}
     # the T-web's y-pass runs through fft_cols too: attribute by launch counts is not possible
     # from totals, so report the raw kernel table alongside
-    out = {"workload": args.workload, "mesh": n, "particles": npart, "ms_per_job": round(float(np.median(times)), 3),
+    out = {"workload": args.workload, "tweb_method": args.tweb_method, "mesh": n, "particles": npart,
+           "ms_per_job": round(float(np.median(times)), 3),
            "ms_min": round(min(times), 3), "steps": k, "warmup": args.warmup, "peak_gbs": hbm, "peak_kind": kind,
            "stages": stages, "kernels": {a: {"launches": b[0], "ms_total": round(b[1], 3)} for a, b in sorted(prof.items())},
            "tweb_counts": [int(v) for v in r["tweb"].counts], "n_lost": r["assign"].n_lost}
@@ -536,6 +542,62 @@ def run_single(args):
     if args.workload == "c1":
         out["cpu_ref"] = c1_cpu_reference(x, y, z, n, box, scheme, nb, R, lth)
     return out
+
+
+def run_bam(args):
+    """The kernel steps of one BAM calibration iteration at N^3 (default 512):
+    the 3D update of GetKernel (rejection form, kernel *= weight per bin,
+    N/2 bins) and Konvolve of an FP32 N^3 mesh, all resident on the device.
+    Algorithmic bytes: update 8 N^2 (N/2+1) (kernel read and written);
+    Konvolve 4 N^3 (in) + 4 N^2 (N/2+1) (kernel) + 4 N^3 (out)."""
+    import torch
+
+    from cosmicatlas_b200 import _lib as CL
+    from cosmicatlas_b200.api import Context
+
+    torch.cuda.set_device(0)
+    n = args.mesh or 512
+    box = 1000.0
+    nb = n // 2
+    gen = torch.Generator(device="cuda").manual_seed(5)
+    delta = torch.randn((n, n, n), device="cuda", generator=gen)
+    kern = torch.ones((n, n, n // 2 + 1), device="cuda")
+    out = torch.empty_like(delta)
+    w = np.random.default_rng(5).uniform(0.99, 1.01, nb)
+    ctx = Context(0)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    for _ in range(args.warmup):
+        ctx.bam_kernel_update(kern, box, w, CL.KERNEL_SCALE)
+        ctx.konvolve(delta, box, kern, out=out)
+    ctx.profile(True)
+    ctx.profile_read(reset=True)
+    tu, tk = [], []
+    for _ in range(args.steps):
+        for dst, fn in ((tu, lambda: ctx.bam_kernel_update(kern, box, w, CL.KERNEL_SCALE)),
+                        (tk, lambda: ctx.konvolve(delta, box, kern, out=out))):
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            dst.append(e0.elapsed_time(e1))
+    prof = ctx.profile_read(reset=True)
+    ctx.close()
+    hbm, kind = peaks()
+    nh = n * n * (n // 2 + 1)
+    bu, bk = 8 * nh, 8 * n ** 3 + 4 * nh
+    mu, mk = float(np.median(tu)), float(np.median(tk))
+    return {"workload": "bam", "mesh": n, "nbins": nb,
+            "kernel_update": {"ms": round(mu, 3), "algorithmic_bytes": bu, "achieved_gbs": round(bu / mu / 1e6, 1),
+                              "frac": round(bu / mu / 1e6 / hbm, 4)},
+            "konvolve": {"ms": round(mk, 3), "algorithmic_bytes": bk, "achieved_gbs": round(bk / mk / 1e6, 1),
+                         "frac": round(bk / mk / 1e6 / hbm, 4)},
+            "peak_gbs": hbm, "peak_kind": kind, "steps": args.steps, "warmup": args.warmup,
+            "note": "host round trip included: each call reads its bin sums back",
+            "kernels": {a: {"launches": b[0], "ms_total": round(b[1], 3)} for a, b in sorted(prof.items())}}
 
 
 def c1_cpu_reference(x, y, z, n, box, scheme, nbins, R, lth):
@@ -780,6 +842,9 @@ def main():
     args = parse()
     if args.workload in ("calib", "stream"):
         print(json.dumps(run_calib(args) if args.workload == "calib" else run_stream(args)), flush=True)
+        return
+    if args.workload == "bam":
+        print(json.dumps(run_bam(args)), flush=True)
         return
     if args.workload != "sweep":
         print(json.dumps(run_single(args)), flush=True)

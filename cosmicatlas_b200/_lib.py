@@ -19,7 +19,9 @@ CAM_E_TIMEOUT, CAM_E_BUSY, CAM_E_NOTFOUND, CAM_E_UNSUPPORTED, CAM_E_NONFINITE = 
 NGP, CIC, TSC = 0, 1, 2
 F32, F64 = 0, 1
 MEM_HOST, MEM_DEVICE = 0, 1
-INPUT_DENSITY, INPUT_DELTA = 0, 1
+INPUT_DENSITY, INPUT_DELTA, INPUT_POTENTIAL = 0, 1, 2
+TWEB_FFT, TWEB_FD = 0, 1
+KERNEL_SET, KERNEL_SCALE = 0, 1
 
 _STATUS = {CAM_E_INVAL: "CAM_E_INVAL", CAM_E_NOMEM: "CAM_E_NOMEM", CAM_E_CUDA: "CAM_E_CUDA",
            CAM_E_TIMEOUT: "CAM_E_TIMEOUT", CAM_E_BUSY: "CAM_E_BUSY", CAM_E_NOTFOUND: "CAM_E_NOTFOUND",
@@ -59,7 +61,7 @@ class PkInfo(ctypes.Structure):
 
 class TwebOpts(ctypes.Structure):
     _fields_ = [("smoothing_R", ctypes.c_float), ("lambda_th", ctypes.c_double), ("tie_band", ctypes.c_double),
-                ("input_type", ctypes.c_int)]
+                ("input_type", ctypes.c_int), ("method", ctypes.c_int)]
 
 
 class TwebStats(ctypes.Structure):
@@ -118,6 +120,16 @@ SIGNATURES = {
                    ctypes.POINTER(PkInfo)], ctypes.c_int),
     "cam_tweb": ([_P, ctypes.POINTER(Grid), _P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(TwebOpts), _P, _P,
                   ctypes.c_int, ctypes.POINTER(TwebStats)], ctypes.c_int),
+    "cam_cross_power": ([_P, ctypes.POINTER(Grid), _P, _P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(PkOpts),
+                         ctypes.c_int, ctypes.c_int, _P, _P, _P, _P, _P], ctypes.c_int),
+    "cam_poisson": ([_P, ctypes.POINTER(Grid), _P, ctypes.c_int, ctypes.c_int, ctypes.c_float, _P, ctypes.c_int],
+                    ctypes.c_int),
+    "cam_gradfindif": ([_P, ctypes.POINTER(Grid), _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, ctypes.c_int],
+                       ctypes.c_int),
+    "cam_bam_kernel_update": ([_P, ctypes.POINTER(Grid), ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                               _P, ctypes.c_int, _P, ctypes.c_int, _P, _P], ctypes.c_int),
+    "cam_konvolve": ([_P, ctypes.POINTER(Grid), _P, ctypes.c_int, ctypes.c_int, _P, ctypes.c_int, _P, ctypes.c_int],
+                     ctypes.c_int),
     "cam_job_run": ([_P, ctypes.POINTER(JobDesc), ctypes.POINTER(JobResult)], ctypes.c_int),
     "cam_particles_stage": ([_P, ctypes.POINTER(Particles), ctypes.POINTER(Particles)], ctypes.c_int),
     "cam_power_noalloc": ([_P, ctypes.c_int64, ctypes.c_int, ctypes.c_float, ctypes.c_double,

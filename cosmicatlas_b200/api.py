@@ -223,11 +223,37 @@ class Context:
                                         L.ptr(pk), L.ptr(md), L.ptr(kv), ctypes.byref(info)))
         return PkResult(pk, md, kv, info.n_obj, info.shot_noise, info.normal)
 
+    def cross_power(self, mesh_x, mesh_y, box: float, opts: L.PkOpts, input_type_y=L.INPUT_DENSITY,
+                    want_coeff=False) -> dict:
+        """Cross power spectrum (PowerSpectrumF::compute_cross_power_spectrum_grid,
+        Source/PowerSpectrumF.cpp:549): returns pk (cross power or, with
+        want_coeff, the cross-correlation coefficient), pk_x, pk_y, modes, kvector."""
+        dev = L.is_device(mesh_x)
+        if dev != L.is_device(mesh_y):
+            raise ValueError("both meshes must be on the host or both on the device")
+        n = mesh_x.shape[0]
+        prec = F64 if str(mesh_x.dtype).endswith("float64") else F32
+        if str(mesh_y.dtype) != str(mesh_x.dtype):
+            raise ValueError("both meshes must have one precision")
+        if not dev:
+            mesh_x, mesh_y = np.ascontiguousarray(mesh_x), np.ascontiguousarray(mesh_y)
+        nb = opts.nbins if opts.nbins > 0 else int(n / opts.ndel / 2)
+        pk, px, py, kv = np.empty(nb), np.empty(nb), np.empty(nb), np.empty(nb)
+        md = np.empty(nb, np.int64)
+        g = make_grid(n, box)
+        self._check(self._lib.cam_cross_power(self.h, ctypes.byref(g), L.ptr(mesh_x), L.ptr(mesh_y), prec,
+                                              L.MEM_DEVICE if dev else L.MEM_HOST, ctypes.byref(opts), input_type_y,
+                                              int(want_coeff), L.ptr(pk), L.ptr(px), L.ptr(py), L.ptr(md),
+                                              L.ptr(kv)))
+        return {"pk": pk, "pk_x": px, "pk_y": py, "modes": md, "kvector": kv}
+
     # ---------------------------------------------------------------- T-web
     @staticmethod
-    def tweb_opts(R=0.0, lambda_th=0.0, tie_band=1e-5, input_type=L.INPUT_DENSITY) -> L.TwebOpts:
+    def tweb_opts(R=0.0, lambda_th=0.0, tie_band=1e-5, input_type=L.INPUT_DENSITY, method=L.TWEB_FFT) -> L.TwebOpts:
+        """method: L.TWEB_FFT (tidal tensor k_a k_b / k^2 delta_k) or L.TWEB_FD
+        (finite differences of the potential, the reference's default)."""
         o = L.TwebOpts()
-        o.smoothing_R, o.lambda_th, o.tie_band, o.input_type = R, lambda_th, tie_band, input_type
+        o.smoothing_R, o.lambda_th, o.tie_band, o.input_type, o.method = R, lambda_th, tie_band, input_type, method
         return o
 
     def tweb(self, mesh, box: float, opts: L.TwebOpts, want_lambdas=False) -> TwebResult:
@@ -245,6 +271,76 @@ class Context:
                                        L.ptr(labels), L.ptr(lam), L.MEM_DEVICE if dev else L.MEM_HOST,
                                        ctypes.byref(st)))
         return TwebResult(labels, lam, np.array(st.counts[:], np.int64), int(st.ties), st.mean)
+
+    # ------------------------------------------------- potential / differences
+    def poisson(self, delta, box: float, R: float = 0.0):
+        """PoissonSolver (Source/Miscelanious.cpp:1189): phi with nabla^2 phi =
+        delta (k = 0 mode dropped), optionally Gaussian-smoothed with radius R."""
+        dev = L.is_device(delta)
+        n = delta.shape[0]
+        prec = F64 if str(delta.dtype).endswith("float64") else F32
+        if not dev:
+            delta = np.ascontiguousarray(delta)
+        out = self._empty((n, n, n), np.float64 if prec == F64 else np.float32, dev, delta)
+        g = make_grid(n, box)
+        m = L.MEM_DEVICE if dev else L.MEM_HOST
+        self._check(self._lib.cam_poisson(self.h, ctypes.byref(g), L.ptr(delta), prec, m, R, L.ptr(out), m))
+        return out
+
+    def gradfindif(self, field, box: float, dim: int, out=None):
+        """gradfindif (Source/NumericalMethods.cpp:1123): 4th-order centred
+        difference along dim (1 = x, the slowest axis; 3 = z)."""
+        dev = L.is_device(field)
+        n = field.shape[0]
+        prec = F64 if str(field.dtype).endswith("float64") else F32
+        if not dev:
+            field = np.ascontiguousarray(field)
+        if out is None:
+            out = self._empty((n, n, n), np.float64 if prec == F64 else np.float32, dev, field)
+        g = make_grid(n, box)
+        m = L.MEM_DEVICE if dev else L.MEM_HOST
+        self._check(self._lib.cam_gradfindif(self.h, ctypes.byref(g), L.ptr(field), prec, m, dim, L.ptr(out), m))
+        return out
+
+    # ---------------------------------------------------------------- BAM kernel
+    def bam_kernel_update(self, kernel, box: float, weight, mode=L.KERNEL_SET, DeltaKmin=0.0, ndel=1.0):
+        """The 3D update of Bam::GetKernel (Source/Bam.cpp:786-910) on the
+        half-complex kernel array (N, N, N/2+1), in place.  Returns the bin
+        means of the updated kernel (bin 0 = mean of bins 1..4) and the
+        element count of each bin."""
+        dev = L.is_device(kernel)
+        n = kernel.shape[0]
+        prec = F64 if str(kernel.dtype).endswith("float64") else F32
+        if not dev and not kernel.flags["C_CONTIGUOUS"]:
+            raise ValueError("kernel must be C-contiguous (it is updated in place)")
+        w = np.ascontiguousarray(weight, np.float64)
+        nb = w.size
+        binned = np.empty(nb)
+        modes = np.empty(nb, np.int64)
+        g = make_grid(n, box)
+        self._check(self._lib.cam_bam_kernel_update(self.h, ctypes.byref(g), prec, DeltaKmin, ndel, nb, L.ptr(w),
+                                                    mode, L.ptr(kernel), L.MEM_DEVICE if dev else L.MEM_HOST,
+                                                    L.ptr(binned), L.ptr(modes)))
+        return binned, modes
+
+    def konvolve(self, mesh, box: float, kernel, out=None):
+        """Bam::Konvolve (Source/Bam.cpp:1027): mesh convolved with the
+        half-complex kernel, normalised by 2 sum(kernel) / N^3."""
+        dev = L.is_device(mesh)
+        n = mesh.shape[0]
+        prec = F64 if str(mesh.dtype).endswith("float64") else F32
+        if not dev:
+            mesh = np.ascontiguousarray(mesh)
+        kdev = L.is_device(kernel)
+        if not kdev:
+            kernel = np.ascontiguousarray(kernel)
+        if out is None:
+            out = self._empty((n, n, n), np.float64 if prec == F64 else np.float32, dev, mesh)
+        g = make_grid(n, box)
+        m = L.MEM_DEVICE if dev else L.MEM_HOST
+        self._check(self._lib.cam_konvolve(self.h, ctypes.byref(g), L.ptr(mesh), prec, m, L.ptr(kernel),
+                                           L.MEM_DEVICE if kdev else L.MEM_HOST, L.ptr(out), m))
+        return out
 
     # ---------------------------------------------------------------- job
     def stage(self, x, y, z, w=None) -> "StagedParticles":
@@ -475,24 +571,63 @@ def do_fftw_c2r(Nft, data_in, data_out):
     data_out[...] = res.reshape(data_out.shape)
 
 
+def PoissonSolver(Lbox, Nft, data_in, data_out):
+    """Source/Miscelanious.cpp:1189 -- the potential of ``data_in`` into ``data_out``."""
+    res = default_context().poisson(data_in.reshape(Nft, Nft, Nft), Lbox)
+    data_out[...] = res.reshape(data_out.shape)
+
+
+def gradfindif(N1, N2, N3, L1, L2, L3, data_in, data_out, dim):
+    """Source/NumericalMethods.cpp:1123 -- centred difference along ``dim`` into
+    ``data_out`` (cubic meshes)."""
+    if not (N1 == N2 == N3):
+        raise CamError(L.CAM_E_UNSUPPORTED, "gradfindif: cubic meshes only")
+    res = default_context().gradfindif(data_in.reshape(N1, N2, N3), L1, dim)
+    data_out[...] = res.reshape(data_out.shape)
+
+
+def EigenValuesTweb(Nft, L1, delta, *args):
+    """Both reference overloads, eigenvalues in descending order into the last
+    three arguments:
+    EigenValuesTweb(Nft, L1, delta, out1, out2, out3), Source/Miscelanious.cpp:1772
+        -- tidal tensor of delta by FFTs;
+    EigenValuesTweb(Nft, L1, delta, phi, out1, out2, out3), Source/Miscelanious.cpp:1663
+        -- finite-difference Hessian of the potential phi (the default build)."""
+    if len(args) == 3:
+        mesh, opts = delta, Context.tweb_opts(0.0, 0.0, 0.0, L.INPUT_DELTA, L.TWEB_FFT)
+    elif len(args) == 4:
+        mesh, opts = args[0], Context.tweb_opts(0.0, 0.0, 0.0, L.INPUT_POTENTIAL, L.TWEB_FD)
+        args = args[1:]
+    else:
+        raise TypeError("EigenValuesTweb(Nft, L1, delta, [phi,] out1, out2, out3)")
+    r = default_context().tweb(mesh.reshape(Nft, Nft, Nft), L1, opts, want_lambdas=True)
+    for a, out in enumerate(args):
+        out[...] = r.lambdas[a].reshape(out.shape)
+
+
 @dataclass
 class Params:
     """The Params getters the hot path reads (Headers/Params.h): _Nft, _Lbox,
     _mass_assignment (0 NGP, 1 CIC, 2 TSC), _MAS_correction, _SN_correction,
     _input_type ("density_grid" | "delta_grid"), _ndel_data, _DeltaKmin,
-    _lambdath; smoothing_R is the Gaussian radius applied before the T-web."""
+    _lambdath; smoothing_R is the Gaussian radius applied before the T-web.
+    tweb_method picks the tidal tensor, as the reference's compile-time
+    switch does (Headers/def.h:2657-2658): "fft" (_USE_GFFT_EIGENV_) or
+    "fd" (_USE_GFINDIFF_EIGENV_, the reference's default build)."""
     Nft: int
     Lbox: float
     mass_assignment: int = CIC
     MAS_correction: bool = True
     SN_correction: bool = True
     input_type: str = "density_grid"
+    input_type_two: str = "density_grid"
     ndel_data: float = 1.0
     DeltaKmin: float = 0.0
     Nnp_data: int = 0
     lambdath: float = 0.0
     smoothing_R: float = 0.0
     tie_band: float = 1e-5
+    tweb_method: str = "fft"
     device: int = 0
 
 
@@ -518,6 +653,18 @@ class PowerSpectrumF:
         if write_to_file:
             raise CamError(L.CAM_E_UNSUPPORTED, "file output is not part of the GPU path")
 
+    def compute_cross_power_spectrum_grid(self, dm, X, Y, get_cross_coeff=False):
+        """Source/PowerSpectrumF.cpp:549: X uses input_type, Y input_type_two
+        (Params.input_type_two); fills pk0, modes_g, kvector_data."""
+        p = self.params
+        n = p.Nft
+        it = L.INPUT_DENSITY if p.input_type == "density_grid" else L.INPUT_DELTA
+        it2 = L.INPUT_DENSITY if p.input_type_two == "density_grid" else L.INPUT_DELTA
+        o = Context.pk_opts(p.mass_assignment, p.Nnp_data, p.ndel_data, p.DeltaKmin, p.MAS_correction, False, it)
+        r = default_context(p.device).cross_power(X.reshape(n, n, n), Y.reshape(n, n, n), p.Lbox, o, it2,
+                                                  get_cross_coeff)
+        self.pk0, self.modes_g, self.kvector_data = r["pk"], r["modes"], r["kvector"]
+
     def _pk0(self, i):
         return self.pk0[i]
 
@@ -541,7 +688,8 @@ class Cwclass:
     def get_CWC(self, delta):
         p = self.params
         it = L.INPUT_DELTA if p.input_type == "delta_grid" else L.INPUT_DENSITY
-        o = Context.tweb_opts(p.smoothing_R, p.lambdath, p.tie_band, it)
+        method = {"fft": L.TWEB_FFT, "fd": L.TWEB_FD}[p.tweb_method]
+        o = Context.tweb_opts(p.smoothing_R, p.lambdath, p.tie_band, it, method)
         r = default_context(p.device).tweb(delta.reshape(p.Nft, p.Nft, p.Nft), p.Lbox, o, want_lambdas=True)
         ng = float(p.Nft) ** 3
         self.lambda1, self.lambda2, self.lambda3 = (r.lambdas[0].reshape(-1), r.lambdas[1].reshape(-1),
@@ -552,6 +700,81 @@ class Cwclass:
         self.ties = r.ties
 
     do_CWC = get_CWC
+
+
+class Bam:
+    """The kernel steps of a BAM calibration iteration (Source/Bam.cpp):
+    GetKernel (:529) updates the Fourier-space kernel from the ratio of the
+    reference to the current power spectrum, Konvolve (:1027) convolves a
+    mesh with it.  The kernel lives on the device, (N, N, N/2+1) real_prec,
+    initialised to 1 (:243).  Power_REF, Power_NEW, kvec (h/Mpc) and
+    shot_noise_ref are set by the caller, as the reference's members are."""
+
+    SEED = 55457  # gsl_rng_default_seed of GetKernel (Source/Bam.cpp:594)
+
+    def __init__(self, params: Params):
+        import torch
+        self.params = params
+        n = params.Nft
+        self.Kernel = torch.ones((n, n, n // 2 + 1), dtype=torch.float32, device=f"cuda:{params.device}")
+        nb = params.Nnp_data if params.Nnp_data > 0 else int(n / params.ndel_data / 2)
+        self.kvec = np.zeros(nb)
+        self.Power_REF = np.zeros(nb)
+        self.Power_NEW = np.zeros(nb)
+        self.power_ratio_unsmoothed = np.ones(nb)
+        self.shot_noise_ref = 0.0
+        self.kernel_updated = np.zeros(nb)
+        self.nmodes = np.zeros(nb, np.int64)
+
+    def kernel_weights(self, rejection: bool, exponent: float, uniforms=None):
+        """The per-bin weights of GetKernel (Source/Bam.cpp:604-723), host side
+        (one value per bin).  With rejection, a bin takes its new ratio when a
+        uniform draw is below min(1, chi2_old / chi2_new); `uniforms` are
+        those draws (default: MT19937 seeded with init_genrand(55457), the
+        stream of gsl_rng_mt19937, one 32-bit output / 2^32 per bin)."""
+        nb = self.kvec.size
+        p = self.params
+        weight = np.ones(nb)
+        if rejection and uniforms is None:
+            rs = np.random.RandomState(self.SEED)
+            uniforms = rs.randint(0, 2 ** 32, size=nb, dtype=np.uint64) / 4294967296.0
+        dk = 2.0 * np.pi / p.Lbox
+        sfac = 1.0 / (2.0 * np.pi * dk * p.Lbox ** 3)
+        for i in range(nb):
+            pr, pn = float(self.Power_REF[i]), float(self.Power_NEW[i])
+            if 0 <= exponent < 1.0:
+                ratio = 1.0 if (pn == 0 or pr == 0) else abs(pr / pn) ** exponent
+            else:
+                ratio = 1.0 if pn == 0 else pr / pn
+            if not rejection:
+                weight[i] = ratio
+            else:
+                k2 = self.kvec[i] ** 2
+                inv = sfac / (k2 + dk * dk / 12.0)
+                s_new = 1.0 if pr == 0 else inv * pn * pn
+                new_h = 0.5 * (pr - pn) ** 2 / s_new
+                p_old = pr / self.power_ratio_unsmoothed[i]
+                s_old = 1.0 if pr == 0 else inv * (p_old + self.shot_noise_ref) ** 2
+                old_h = 0.5 * (pr - p_old) ** 2 / s_old
+                with np.errstate(divide="ignore", invalid="ignore"):
+                    ratio_diff = np.float64(old_h) / np.float64(new_h)
+                if uniforms[i] < min(1.0, ratio_diff):
+                    weight[i] = ratio
+            self.power_ratio_unsmoothed[i] = ratio
+        return weight.astype(np.float32).astype(np.float64)
+
+    def GetKernel(self, rejection: bool, exponent: float, uniforms=None):
+        p = self.params
+        w = self.kernel_weights(rejection, exponent, uniforms)
+        mode = L.KERNEL_SCALE if rejection else L.KERNEL_SET
+        self.kernel_updated, self.nmodes = default_context(p.device).bam_kernel_update(
+            self.Kernel, p.Lbox, w, mode, p.DeltaKmin, p.ndel_data)
+
+    def Konvolve(self, data_in, data_out):
+        p = self.params
+        n = p.Nft
+        res = default_context(p.device).konvolve(data_in.reshape(n, n, n), p.Lbox, self.Kernel)
+        data_out[...] = res.reshape(data_out.shape)
 
     def get_Tclassification(self, ig):
         return int(self.CWClass[ig])

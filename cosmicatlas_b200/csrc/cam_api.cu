@@ -654,7 +654,8 @@ int cam_tweb(cam_ctx *ctx, const cam_grid *grid, const void *mesh, int precision
         check_prec(precision);
         check_mem(mem);
         check_mem(out_mem);
-        CAM_REQUIRE(opts->input_type == CAM_INPUT_DENSITY || opts->input_type == CAM_INPUT_DELTA, CAM_E_INVAL,
+        CAM_REQUIRE(opts->input_type == CAM_INPUT_DENSITY || opts->input_type == CAM_INPUT_DELTA ||
+                        opts->input_type == CAM_INPUT_POTENTIAL, CAM_E_INVAL,
                     "unknown input type");
         const int64_t n = grid->n[0], ncell = n * n * n;
         FftPlan *plan = get_plan(ctx, n, precision);
@@ -679,6 +680,201 @@ int cam_tweb(cam_ctx *ctx, const cam_grid *grid, const void *mesh, int precision
         }
         CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
         if (stats) *stats = st;
+    });
+}
+
+int cam_cross_power(cam_ctx *ctx, const cam_grid *grid, const void *mesh_x, const void *mesh_y, int precision,
+                    int mem, const cam_pk_opts *opts, int input_type_y, int want_coeff, double *pk, double *pk_x,
+                    double *pk_y, int64_t *modes, double *kvector)
+{
+    return guarded(ctx, [&] {
+        check_grid_cubic(grid);
+        CAM_REQUIRE(mesh_x && mesh_y, CAM_E_INVAL, "null mesh");
+        check_prec(precision);
+        check_mem(mem);
+        validate_pk(opts);
+        CAM_REQUIRE(input_type_y == CAM_INPUT_DENSITY || input_type_y == CAM_INPUT_DELTA, CAM_E_INVAL,
+                    "unknown input type of the second mesh");
+        const int64_t n = grid->n[0], ncell = n * n * n;
+        FftPlan *plan = get_plan(ctx, n, precision);
+        const size_t bytes = (size_t)ncell * esize(precision);
+        const void *dm[2] = {mesh_x, mesh_y};
+        const int kind[2] = {opts->input_type, input_type_y};
+        auto *dsum = static_cast<double *>(scratch(ctx, "xpk.sum", 4 * sizeof(double)));
+        Spectrum sp[2];
+        for (int a = 0; a < 2; ++a) {
+            const void *d = dm[a];
+            if (mem == CAM_MEM_HOST) {
+                void *t = scratch(ctx, a ? "xpk.mesh1" : "xpk.mesh0", bytes);
+                CAM_CUDA_TRY(cudaMemcpyAsync(t, dm[a], bytes, cudaMemcpyHostToDevice, ctx->stream));
+                d = t;
+            }
+            const double *sub = nullptr;
+            if (kind[a] == CAM_INPUT_DENSITY) {
+                mesh_mean(ctx, d, precision, ncell, dsum + 2 * a);  // [2a] = sum, [2a+1] = mean
+                sub = dsum + 2 * a + 1;
+            }
+            sp[a] = alloc_spectrum(ctx, n, precision, a ? "xpk.spec1" : "xpk.spec0");
+            fft_r2c_split(ctx, plan, d, sub, sp[a]);  // F(rho - mean), or F(delta)
+        }
+        const int nb = nbins_for(*opts, n);
+        const PkDevice xs = power_cross_device(ctx, sp[0], sp[1], *opts, nb);
+        cam_pk_opts oy = *opts;
+        oy.sn_correction = 0;
+        const PkDevice ys = power_bin_device(ctx, sp[1], oy, nb);
+        std::vector<double> hx(2 * (size_t)nb), hy(2 * (size_t)nb), hs(4);
+        std::vector<unsigned long long> hm(nb);
+        CAM_CUDA_TRY(cudaMemcpyAsync(hx.data(), xs.sums, hx.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        CAM_CUDA_TRY(cudaMemcpyAsync(hy.data(), ys.sums, hy.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        CAM_CUDA_TRY(cudaMemcpyAsync(hm.data(), xs.modes, (size_t)nb * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        CAM_CUDA_TRY(cudaMemcpyAsync(hs.data(), dsum, 4 * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        // F(delta) = F(rho - mean) / mean for a density; normal = (L^1.5 / N^3)^-2
+        // for both fields (PowerSpectrumF.cpp:576-577, :605-606)
+        const double fx = kind[0] == CAM_INPUT_DENSITY ? 1.0 / hs[1] : 1.0;
+        const double fy = kind[1] == CAM_INPUT_DENSITY ? 1.0 / hs[3] : 1.0;
+        const double ng = (double)ncell;
+        const double L = grid->L[0];
+        const double normal = ng * ng / (L * L * L);
+        const double kf = 2.0 * M_PI / L;
+        for (int b = 0; b < nb; ++b) {
+            const double m = (double)hm[b];
+            double px = 0.0, pxx = 0.0, pyy = 0.0;
+            if (hm[b] > 0) {
+                px = hx[2 * b] * fx * fy / (m * normal);
+                pxx = hx[2 * b + 1] * fx * fx / (m * normal);
+                pyy = hy[2 * b] * fy * fy / (m * normal);
+            }
+            if (pk) pk[b] = want_coeff ? (hm[b] > 0 ? px / std::sqrt(pxx * pyy) : 0.0) : px;
+            if (pk_x) pk_x[b] = pxx;
+            if (pk_y) pk_y[b] = pyy;
+            if (modes) modes[b] = (int64_t)hm[b];
+            if (kvector) kvector[b] = kf * (opts->DeltaKmin + ((double)b + 0.5) * opts->ndel);
+        }
+    });
+}
+
+int cam_poisson(cam_ctx *ctx, const cam_grid *grid, const void *delta, int precision, int mem, float smoothing_R,
+                void *phi, int out_mem)
+{
+    return guarded(ctx, [&] {
+        check_grid_cubic(grid);
+        CAM_REQUIRE(delta && phi, CAM_E_INVAL, "null mesh");
+        check_prec(precision);
+        check_mem(mem);
+        check_mem(out_mem);
+        CAM_REQUIRE(smoothing_R >= 0.f && std::isfinite(smoothing_R), CAM_E_INVAL, "invalid smoothing radius");
+        const int64_t n = grid->n[0];
+        FftPlan *plan = get_plan(ctx, n, precision);
+        const size_t bytes = (size_t)n * n * n * esize(precision);
+        const void *din = mem == CAM_MEM_DEVICE ? delta : scratch(ctx, "fft.in", bytes);
+        if (mem == CAM_MEM_HOST) CAM_CUDA_TRY(cudaMemcpyAsync((void *)din, delta, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        Spectrum s = alloc_spectrum(ctx, n, precision, "fft.spec");
+        fft_r2c_split(ctx, plan, din, nullptr, s);
+        poisson_device(ctx, s, grid->L[0], smoothing_R);
+        void *dout = out_mem == CAM_MEM_DEVICE ? phi : scratch(ctx, "fd.out", bytes);
+        fft_c2r_split(ctx, plan, s, dout, 1.0 / ((double)n * n * n));
+        if (out_mem == CAM_MEM_HOST) CAM_CUDA_TRY(cudaMemcpyAsync(phi, dout, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+        CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+int cam_gradfindif(cam_ctx *ctx, const cam_grid *grid, const void *in, int precision, int mem, int dim, void *out,
+                   int out_mem)
+{
+    return guarded(ctx, [&] {
+        check_grid_cubic(grid);
+        CAM_REQUIRE(in && out, CAM_E_INVAL, "null mesh");
+        check_prec(precision);
+        check_mem(mem);
+        check_mem(out_mem);
+        CAM_REQUIRE(dim >= 1 && dim <= 3, CAM_E_INVAL, "dim must be 1, 2 or 3");
+        const int64_t n = grid->n[0];
+        const size_t bytes = (size_t)n * n * n * esize(precision);
+        const void *din = in;
+        if (mem == CAM_MEM_HOST || (out_mem == CAM_MEM_DEVICE && in == out)) {
+            // the reference takes `in` by value, so out may be the same array
+            void *t = scratch(ctx, "fd.in", bytes);
+            CAM_CUDA_TRY(cudaMemcpyAsync(t, in, bytes, mem == CAM_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                                         ctx->stream));
+            din = t;
+        }
+        void *dout = out_mem == CAM_MEM_DEVICE ? out : scratch(ctx, "fd.out", bytes);
+        gradfindif_device(ctx, din, dout, n, grid->L[0], dim, precision);
+        if (out_mem == CAM_MEM_HOST) CAM_CUDA_TRY(cudaMemcpyAsync(out, dout, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+        CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+int cam_bam_kernel_update(cam_ctx *ctx, const cam_grid *grid, int precision, double DeltaKmin, double ndel,
+                          int nbins, const double *weight, int mode, void *kernel, int mem, double *kernel_binned,
+                          int64_t *modes)
+{
+    return guarded(ctx, [&] {
+        check_grid_cubic(grid);
+        check_prec(precision);
+        check_mem(mem);
+        CAM_REQUIRE(weight && kernel, CAM_E_INVAL, "null weights or kernel");
+        CAM_REQUIRE(mode == CAM_KERNEL_SET || mode == CAM_KERNEL_SCALE, CAM_E_INVAL, "unknown kernel update mode");
+        CAM_REQUIRE(ndel > 0.0 && std::isfinite(ndel) && DeltaKmin >= 0.0 && std::isfinite(DeltaKmin), CAM_E_INVAL,
+                    "invalid binning");
+        CAM_REQUIRE(nbins >= 5, CAM_E_INVAL, "the kernel update needs nbins >= 5 (bin 0 is the mean of bins 1..4)");
+        const int64_t n = grid->n[0];
+        const size_t kbytes = (size_t)n * n * (n / 2 + 1) * esize(precision);
+        void *dk = mem == CAM_MEM_DEVICE ? kernel : scratch(ctx, "bamk.kernel", kbytes);
+        if (mem == CAM_MEM_HOST) CAM_CUDA_TRY(cudaMemcpyAsync(dk, kernel, kbytes, cudaMemcpyHostToDevice, ctx->stream));
+        auto *dw = static_cast<double *>(scratch(ctx, "bamk.w", (size_t)nbins * sizeof(double)));
+        auto *dsum = static_cast<double *>(scratch(ctx, "bamk.sum", (size_t)nbins * sizeof(double)));
+        auto *dmod = static_cast<unsigned long long *>(scratch(ctx, "bamk.modes", (size_t)nbins * 8));
+        CAM_CUDA_TRY(cudaMemcpyAsync(dw, weight, (size_t)nbins * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        bam_kernel_update_device(ctx, dk, precision, n, grid->L[0], DeltaKmin, ndel, nbins, dw, mode, dsum, dmod);
+        if (mem == CAM_MEM_HOST) CAM_CUDA_TRY(cudaMemcpyAsync(kernel, dk, kbytes, cudaMemcpyDeviceToHost, ctx->stream));
+        std::vector<double> hs(nbins);
+        std::vector<unsigned long long> hm(nbins);
+        CAM_CUDA_TRY(cudaMemcpyAsync(hs.data(), dsum, (size_t)nbins * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        CAM_CUDA_TRY(cudaMemcpyAsync(hm.data(), dmod, (size_t)nbins * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        if (kernel_binned) {
+            // kernel_updated[b] /= nmodes[b]; then bin 0 = mean of bins 1..4
+            for (int b = 0; b < nbins; ++b) kernel_binned[b] = hs[b] / (double)hm[b];
+            kernel_binned[0] = (kernel_binned[1] + kernel_binned[2] + kernel_binned[3] + kernel_binned[4]) / 4.0;
+        }
+        if (modes)
+            for (int b = 0; b < nbins; ++b) modes[b] = (int64_t)hm[b];
+    });
+}
+
+int cam_konvolve(cam_ctx *ctx, const cam_grid *grid, const void *in, int precision, int mem, const void *kernel,
+                 int kernel_mem, void *out, int out_mem)
+{
+    return guarded(ctx, [&] {
+        check_grid_cubic(grid);
+        CAM_REQUIRE(in && out && kernel, CAM_E_INVAL, "null mesh or kernel");
+        check_prec(precision);
+        check_mem(mem);
+        check_mem(kernel_mem);
+        check_mem(out_mem);
+        const int64_t n = grid->n[0], ncell = n * n * n, nh = n * n * (n / 2 + 1);
+        FftPlan *plan = get_plan(ctx, n, precision);
+        const size_t bytes = (size_t)ncell * esize(precision), kbytes = (size_t)nh * esize(precision);
+        const void *din = mem == CAM_MEM_DEVICE ? in : scratch(ctx, "fft.in", bytes);
+        if (mem == CAM_MEM_HOST) CAM_CUDA_TRY(cudaMemcpyAsync((void *)din, in, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        const void *dk = kernel_mem == CAM_MEM_DEVICE ? kernel : scratch(ctx, "bamk.kernel", kbytes);
+        if (kernel_mem == CAM_MEM_HOST)
+            CAM_CUDA_TRY(cudaMemcpyAsync((void *)dk, kernel, kbytes, cudaMemcpyHostToDevice, ctx->stream));
+        auto *dsum = static_cast<double *>(scratch(ctx, "bamk.ksum", 4 * sizeof(double)));
+        mesh_mean(ctx, din, precision, ncell, dsum);     // [0] = sum of in
+        mesh_mean(ctx, dk, precision, nh, dsum + 2);     // [2] = w, the kernel sum
+        Spectrum s = alloc_spectrum(ctx, n, precision, "fft.spec");
+        fft_r2c_split(ctx, plan, din, nullptr, s);
+        konvolve_device(ctx, s, dk, dsum + 2);
+        void *dout = out_mem == CAM_MEM_DEVICE ? out : scratch(ctx, "fd.out", bytes);
+        fft_c2r_split(ctx, plan, s, dout, 1.0 / ((double)n * n * n));
+        if (out_mem == CAM_MEM_HOST) CAM_CUDA_TRY(cudaMemcpyAsync(out, dout, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+        double hsum = 0.0;
+        CAM_CUDA_TRY(cudaMemcpyAsync(&hsum, dsum, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        CAM_REQUIRE(std::isfinite(hsum), CAM_E_NONFINITE, "Konvolve: the input mesh holds a non-finite value");
     });
 }
 
@@ -720,6 +916,8 @@ int cam_job_run(cam_ctx *ctx, const cam_job_desc *job, cam_job_result *res)
         check_prec(job->precision);
         const bool want_pk = job->pk.nbins > 0 || job->pk.ndel > 0.0;
         if (want_pk) validate_pk(&job->pk);
+        CAM_REQUIRE(!job->want_tweb || job->tweb.input_type != CAM_INPUT_POTENTIAL, CAM_E_INVAL,
+                    "a job's T-web input is its density mesh");
         const cam_grid g = resolved_grid(job->grid);
         const int64_t n = g.n[0], ncell = n * n * n;
         const DevParticles d = stage_particles(ctx, &job->parts);

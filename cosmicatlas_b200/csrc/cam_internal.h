@@ -198,6 +198,9 @@ struct PkDevice {
     unsigned long long *modes;
 };
 PkDevice power_bin_device(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins);
+// Cross sums of two spectra of one size: sums [nbins][2] FP64
+// (sum Re(F1 conj F2)/W^2, sum |F1|^2/W^2), modes [nbins]; own buffers.
+PkDevice power_cross_device(cam_ctx *ctx, const Spectrum &s1, const Spectrum &s2, const cam_pk_opts &o, int nbins);
 void power_bin(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins,
                double *h_sum_raw, double *h_sum_sn, int64_t *h_modes);
 
@@ -205,6 +208,21 @@ void power_bin(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins,
 void tweb_device(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const double *d_mean,
                  int input_type, const cam_tweb_opts &o, uint8_t *d_labels, float *d_lambdas,
                  cam_tweb_stats *stats);
+
+// PoissonSolver's multiplier -1/k^2 (times exp(-k^2 R^2 / 2) if R > 0) on a
+// split spectrum, in place (cam_fd.cu).
+void poisson_device(cam_ctx *ctx, Spectrum &s, float L, float R);
+// gradfindif along dim (1 = x, 2 = y, 3 = z) of a real N^3 mesh; in != out.
+void gradfindif_device(cam_ctx *ctx, const void *in, void *out, int64_t n, float L, int dim, int precision);
+
+// BAM kernel (cam_bamkernel.cu): the 3D update of GetKernel on a device
+// half-complex kernel array, bin sums and counts left in d_sum / d_modes
+// [nbins]; and the kernel product of Konvolve on a split spectrum, with the
+// factor 2 w / N^3 (w = *d_w, the kernel sum).
+void bam_kernel_update_device(cam_ctx *ctx, void *kernel, int precision, int64_t n, float L, double kmin_u,
+                              double dK_u, int nbins, const double *d_weight, int mode, double *d_sum,
+                              unsigned long long *d_modes);
+void konvolve_device(cam_ctx *ctx, Spectrum &s, const void *kernel, const double *d_w);
 
 // In-place exclusive prefix sum of uint32 values; *total (device, may be
 // null) receives the sum of all inputs.

@@ -20,6 +20,8 @@
 #include <algorithm>
 #include <cstdio>
 #include <cmath>
+#include <string>
+#include <type_traits>
 #include <vector>
 
 #include "cam_internal.h"
@@ -55,9 +57,13 @@ __device__ __forceinline__ int pk_bin(double q, const double *E2, int nbins, flo
     return b < 0 ? -1 : b;  // b == nbins: above the last edge
 }
 
-template <typename C>
+// CROSS: a second spectrum (main2, nyq2); the two sums become
+// Re(F1 conj F2) / W^2 and |F1|^2 / W^2 (the table's second half is then
+// 1/W^2: the host builds it without shot-noise factors).
+template <typename C, bool CROSS = false>
 __global__ void __launch_bounds__(kPkThreads)
-pk_bin_kernel(const C *__restrict__ main, const C *__restrict__ nyq, int n,
+pk_bin_kernel(const C *__restrict__ main, const C *__restrict__ nyq, const C *__restrict__ main2,
+              const C *__restrict__ nyq2, int n,
               const double *__restrict__ g_tab /* [3][n/2+1]: 1/W^2 axis, C/W^2 axis ; [nbins+1] E2 */,
               int nbins, float m_u, float inv_s, int64_t rows_per_cta,
               double *__restrict__ part /* [grid][nbins][2] */,
@@ -101,8 +107,14 @@ pk_bin_kernel(const C *__restrict__ main, const C *__restrict__ nyq, int n,
                 if (bin >= 0 && bin < nbins && pk_visited(i, j, c, n)) {
                     const C f = main[r * M + c];
                     const double re = (double)f.x, im = (double)f.y;
-                    vraw = (re * re + im * im) * (tab_ab * tw2[c]);
-                    vsn = sn_ab * tsn[c];
+                    if constexpr (CROSS) {
+                        const C g = main2[r * M + c];
+                        vraw = (re * (double)g.x + im * (double)g.y) * (tab_ab * tw2[c]);
+                        vsn = (re * re + im * im) * (sn_ab * tsn[c]);
+                    } else {
+                        vraw = (re * re + im * im) * (tab_ab * tw2[c]);
+                        vsn = sn_ab * tsn[c];
+                    }
                     valid = true;
                 }
             }
@@ -140,8 +152,14 @@ pk_bin_kernel(const C *__restrict__ main, const C *__restrict__ nyq, int n,
             if (bin >= 0 && bin < nbins && pk_visited(i, j, M, n)) {
                 const C f = nyq[r];
                 const double re = (double)f.x, im = (double)f.y;
-                mysum[2 * bin] += (re * re + im * im) * (tab_ab * tw2[M]);
-                mysum[2 * bin + 1] += sn_ab * tsn[M];
+                if constexpr (CROSS) {
+                    const C g = nyq2[r];
+                    mysum[2 * bin] += (re * (double)g.x + im * (double)g.y) * (tab_ab * tw2[M]);
+                    mysum[2 * bin + 1] += (re * re + im * im) * (sn_ab * tsn[M]);
+                } else {
+                    mysum[2 * bin] += (re * re + im * im) * (tab_ab * tw2[M]);
+                    mysum[2 * bin + 1] += sn_ab * tsn[M];
+                }
                 mycnt[bin] += 1ull;
             }
         }
@@ -209,7 +227,12 @@ double sq_factor(int p, double s)
 
 }  // namespace
 
-PkDevice power_bin_device(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins)
+namespace {
+
+// s2 == nullptr: P(k) sums of s.  Otherwise the cross sums of s and s2 into
+// buffers of their own (tag), so that a P(k) of s2 can follow.
+PkDevice power_bin_impl(cam_ctx *ctx, const Spectrum &s, const Spectrum *s2, const cam_pk_opts &o, int nbins,
+                        const char *tag)
 {
     const int n = (int)s.n, h = n / 2;
     CAM_REQUIRE(nbins >= 1 && nbins <= 4096, CAM_E_INVAL, "nbins must be in [1, 4096]");
@@ -254,26 +277,50 @@ PkDevice power_bin_device(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o,
     const int grid = kNumSMs * (smem_need <= 56 * 1024 ? 4 : 2);
     const int64_t nrows = (int64_t)n * n;
     const int64_t rpc = (nrows + grid - 1) / grid;
-    auto *part = static_cast<double *>(scratch(ctx, "pk.part", (size_t)grid * nbins * 2 * sizeof(double)));
-    auto *pm = static_cast<unsigned long long *>(scratch(ctx, "pk.pm", (size_t)grid * nbins * sizeof(unsigned long long)));
-    auto *res = static_cast<double *>(scratch(ctx, "pk.res", (size_t)nbins * 2 * sizeof(double)));
-    auto *resm = static_cast<unsigned long long *>(scratch(ctx, "pk.resm", (size_t)nbins * sizeof(unsigned long long)));
+    const std::string tg(tag);
+    auto *part = static_cast<double *>(scratch(ctx, (tg + ".part").c_str(), (size_t)grid * nbins * 2 * sizeof(double)));
+    auto *pm = static_cast<unsigned long long *>(
+        scratch(ctx, (tg + ".pm").c_str(), (size_t)grid * nbins * sizeof(unsigned long long)));
+    auto *res = static_cast<double *>(scratch(ctx, (tg + ".res").c_str(), (size_t)nbins * 2 * sizeof(double)));
+    auto *resm = static_cast<unsigned long long *>(
+        scratch(ctx, (tg + ".resm").c_str(), (size_t)nbins * sizeof(unsigned long long)));
     const size_t smem = tab_bytes + (size_t)kPkWarps * nbins * (2 * sizeof(double) + sizeof(unsigned long long));
     CAM_REQUIRE(smem <= 220 * 1024, CAM_E_UNSUPPORTED, "too many bins for one CTA");
     const float m_u = (float)o.DeltaKmin, inv_s = (float)(1.0 / o.ndel);
+    auto launch = [&](auto cplx, auto cross) {
+        using C = decltype(cplx);
+        constexpr bool X = decltype(cross)::value;
+        auto kern = pk_bin_kernel<C, X>;
+        smem_at_least(kern, smem);
+        const C *m2 = X ? (const C *)s2->main : nullptr;
+        const C *q2 = X ? (const C *)s2->nyq : nullptr;
+        CAM_LAUNCH_NAMED(ctx, X ? "pk_cross_bin" : "pk_bin", kern, grid, kPkThreads, smem, (const C *)s.main,
+                         (const C *)s.nyq, m2, q2, n, d_tab, nbins, m_u, inv_s, rpc, part, pm);
+    };
     if (s.precision == CAM_F32) {
-        auto kern = pk_bin_kernel<float2>;
-        smem_at_least(kern, smem);
-        CAM_LAUNCH_NAMED(ctx, "pk_bin", kern, grid, kPkThreads, smem, (const float2 *)s.main, (const float2 *)s.nyq, n,
-                   d_tab, nbins, m_u, inv_s, rpc, part, pm);
+        if (s2) launch(float2{}, std::true_type{});
+        else launch(float2{}, std::false_type{});
     } else {
-        auto kern = pk_bin_kernel<double2>;
-        smem_at_least(kern, smem);
-        CAM_LAUNCH_NAMED(ctx, "pk_bin", kern, grid, kPkThreads, smem, (const double2 *)s.main, (const double2 *)s.nyq, n,
-                   d_tab, nbins, m_u, inv_s, rpc, part, pm);
+        if (s2) launch(double2{}, std::true_type{});
+        else launch(double2{}, std::false_type{});
     }
     CAM_LAUNCH(ctx, pk_final_kernel, nbins, 256, 0, part, pm, grid, nbins, res, resm);
     return PkDevice{res, resm};
+}
+
+}  // namespace
+
+PkDevice power_bin_device(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins)
+{
+    return power_bin_impl(ctx, s, nullptr, o, nbins, "pk");
+}
+
+PkDevice power_cross_device(cam_ctx *ctx, const Spectrum &s1, const Spectrum &s2, const cam_pk_opts &o, int nbins)
+{
+    CAM_REQUIRE(s1.n == s2.n && s1.precision == s2.precision, CAM_E_INVAL, "cross spectra differ in size or precision");
+    cam_pk_opts ox = o;
+    ox.sn_correction = 0;  // the second table half is then 1/W^2
+    return power_bin_impl(ctx, s1, &s2, ox, nbins, "pkx");
 }
 
 void power_bin(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins, double *h_sum_raw,

@@ -91,8 +91,9 @@ void validate_job(const cam_job_desc &d)
                         (d.pk.input_type == CAM_INPUT_DENSITY || d.pk.input_type == CAM_INPUT_DELTA),
                     CAM_E_INVAL, "invalid P(k) options");
     if (d.want_tweb)
-        CAM_REQUIRE(d.tweb.input_type == CAM_INPUT_DENSITY || d.tweb.input_type == CAM_INPUT_DELTA, CAM_E_INVAL,
-                    "invalid T-web options");
+        CAM_REQUIRE((d.tweb.input_type == CAM_INPUT_DENSITY || d.tweb.input_type == CAM_INPUT_DELTA) &&
+                        (d.tweb.method == CAM_TWEB_FFT || d.tweb.method == CAM_TWEB_FD),
+                    CAM_E_INVAL, "invalid T-web options");
 }
 
 // Upper estimate of the device bytes a job needs (staged inputs, payload at
@@ -241,12 +242,13 @@ std::string shape_key(const cam_job_desc &d)
     char k[512];
     snprintf(k, sizeof(k),
              "%lld,%lld,%lld|%lld|%d|%d|%d|%d|%.9g,%.9g,%.9g|%.9g,%.9g,%.9g|%.9g,%.9g,%.9g|%d,%d,%d,%d,%d,%.17g,%.17g|"
-             "%d|%.9g,%.17g,%.17g,%d",
+             "%d|%.9g,%.17g,%.17g,%d,%d",
              (long long)d.grid.n[0], (long long)d.grid.n[1], (long long)d.grid.n[2], (long long)d.parts.n,
              d.parts.w != nullptr, d.parts.mem, d.scheme, d.precision, d.grid.L[0], d.grid.L[1], d.grid.L[2],
              d.grid.d[0], d.grid.d[1], d.grid.d[2], d.grid.min[0], d.grid.min[1], d.grid.min[2], d.pk.scheme,
              d.pk.mas_correction, d.pk.sn_correction, d.pk.input_type, d.pk.nbins, d.pk.DeltaKmin, d.pk.ndel,
-             d.want_tweb, d.tweb.smoothing_R, d.tweb.lambda_th, d.tweb.tie_band, d.tweb.input_type);
+             d.want_tweb, d.tweb.smoothing_R, d.tweb.lambda_th, d.tweb.tie_band, d.tweb.input_type,
+             d.tweb.method);
     return k;
 }
 

@@ -30,6 +30,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 
 #include "cam_fft_device.cuh"
 #include "cam_internal.h"
@@ -60,6 +61,22 @@ __host__ __device__ constexpr int slot_of(int p, int q)
     return q == 0 ? p : (p == 0 ? 2 + q : 5);
 }
 
+// Frequency factor of one axis in units of k_f, for signed frequency f and
+// power e = 0, 1, 2: f^e for the FFT tidal tensor; for the finite-difference
+// one (FD), s(f)^e with s the Fourier multiplier of the centred difference,
+// tabulated at sf[f + N/2] (fd_table_kernel).
+template <typename T, bool FD>
+__device__ __forceinline__ T kfac(const double *__restrict__ sf, int h, int f, int e)
+{
+    if constexpr (!FD) {
+        return (T)ipow(f, e);
+    } else {
+        if (e == 0) return (T)1;
+        const double s = __ldg(sf + f + h);
+        return (T)(e == 1 ? s : s * s);
+    }
+}
+
 }  // namespace
 
 
@@ -81,14 +98,25 @@ constexpr int col_min_blocks()
                : 1;
 }
 
-// k_x^p phi / delta_k for signed frequencies (fi, fj, fk).
-template <typename T>
-__device__ __forceinline__ T phi_mult(int p, int fi, int fj, int fk, T gauss_coef, T norm)
+// k_x^p phi / delta_k for signed frequencies (fi, fj, fk).  FD: s(k_x)^p
+// phi / delta_k, or, for a potential input (pot), -s(k_x)^p (the host folds
+// k_f^2 into norm): nabla^2 phi = delta gives phi_k = -delta_k / k^2
+// (PoissonSolver, Source/Miscelanious.cpp:1252-1262), and D_a D_b of phi
+// has the multiplier -s_a s_b.
+template <typename T, bool FD = false>
+__device__ __forceinline__ T phi_mult(int p, int fi, int fj, int fk, T gauss_coef, T norm,
+                                      const double *__restrict__ sf = nullptr, int h = 0, int pot = 0)
 {
     const int q = fi * fi + fj * fj + fk * fk;
     if (q == 0) return (T)0;
     // f^p and q are exact in float up to N = 2048; one rounding each
-    const T ratio = (T)(ipow(fi, p) * (1.0f / (float)q));
+    T ratio;
+    if constexpr (!FD) {
+        ratio = (T)(ipow(fi, p) * (1.0f / (float)q));
+    } else {
+        const T f = kfac<T, true>(sf, h, fi, p);
+        ratio = pot ? -f : f * (T)(1.0f / (float)q);
+    }
     const T g = gauss_coef != (T)0 ? exp(-gauss_coef * (T)q) : (T)1;
     return ratio * g * norm;
 }
@@ -97,12 +125,12 @@ __device__ __forceinline__ T phi_mult(int p, int fi, int fj, int fk, T gauss_coe
 // NYQ = false: main tiles (plane = j, columns = k < N/2, FFT index i with
 // stride N*M).  NYQ = true: the Nyquist plane (columns = j, FFT index i with
 // stride N, k = N/2).
-template <typename T, bool NYQ, int LEN>
+template <typename T, bool NYQ, int LEN, bool FD>
 __global__ void __launch_bounds__(col_threads<T, LEN>(), col_min_blocks<T, LEN>())
 tidal_x_kernel(const typename CTw<T>::t *__restrict__ src, typename CTw<T>::t *__restrict__ dst,
                int n, int ncols, int64_t jstride, int64_t pstride, int64_t ccomp, Radices rd,
                const typename CTw<T>::t *__restrict__ tw, double gauss_coef, const double *__restrict__ d_mean,
-               int density_input, double scale)
+               int density_input, double scale, const double *__restrict__ sf, int pot)
 {
     using C = typename CTw<T>::t;
     constexpr int W = CTw<T>::kCols;
@@ -133,7 +161,7 @@ tidal_x_kernel(const typename CTw<T>::t *__restrict__ src, typename CTw<T>::t *_
                 fj = plane <= h ? plane : plane - n;
                 fk = col0 + cc;
             }
-            const T m = phi_mult<T>(comp, fi, fj, fk, gc, norm);
+            const T m = phi_mult<T, FD>(comp, fi, fj, fk, gc, norm, sf, h, pot);
             tile[e] = C{v.x * m, v.y * m};
         }
     }
@@ -154,10 +182,11 @@ tidal_x_kernel(const typename CTw<T>::t *__restrict__ src, typename CTw<T>::t *_
 // plane*pstride + j*jstride + col*cstride.  k_z = kz_fixed if >= 0 (the
 // Nyquist plane), else the column.  The tile is re-read (from L2) for every
 // q, and (p, 0) is written last, over its own input.
-template <typename T, int LEN>
+template <typename T, int LEN, bool FD>
 __global__ void __launch_bounds__(col_threads<T, LEN>(), col_min_blocks<T, LEN>())
 tidal_y_kernel(typename CTw<T>::t *__restrict__ base, int n, int ncols, int64_t jstride, int64_t cstride,
-               int64_t pstride, int64_t ccomp, Radices rd, const typename CTw<T>::t *__restrict__ tw, int kz_fixed)
+               int64_t pstride, int64_t ccomp, Radices rd, const typename CTw<T>::t *__restrict__ tw, int kz_fixed,
+               const double *__restrict__ sf)
 {
     using C = typename CTw<T>::t;
     constexpr int W = CTw<T>::kCols;
@@ -176,7 +205,11 @@ tidal_y_kernel(typename CTw<T>::t *__restrict__ base, int n, int ncols, int64_t 
             if (cc < nc) {
                 const C v = in[(int64_t)j * jstride + (int64_t)cc * cstride];
                 const int kz = kz_fixed >= 0 ? kz_fixed : col0 + cc;
-                const T m = (T)(ipow(j <= h ? j : j - n, q) * ipow(kz, 2 - p - q));
+                T m;
+                if constexpr (!FD)
+                    m = (T)(ipow(j <= h ? j : j - n, q) * ipow(kz, 2 - p - q));
+                else
+                    m = kfac<T, true>(sf, h, j <= h ? j : j - n, q) * kfac<T, true>(sf, h, kz, 2 - p - q);
                 tile[e] = C{v.x * m, v.y * m};
             }
         }
@@ -218,11 +251,12 @@ constexpr int tpipe_min_blocks()
 // Element (j, col) of a tile sits at (tile base) + j*jstride + col, the
 // unit's tile base at plane*pstride + column tile*W; full tiles only and
 // 16-byte aligned rows (the host checks).
-template <typename T, int MODE, int LEN>
+template <typename T, int MODE, int LEN, bool FD>
 __global__ void __launch_bounds__(col_threads<T, LEN>(), tpipe_min_blocks<T, LEN>())
 tidal_pipe_kernel(const typename CTw<T>::t *src, typename CTw<T>::t *dst, int n, int nct, int64_t nunits,
                   int64_t jstride, int64_t pstride, int64_t ccomp, const typename CTw<T>::t *__restrict__ tw,
-                  double gauss_coef, const double *__restrict__ d_mean, int density_input, double scale)
+                  double gauss_coef, const double *__restrict__ d_mean, int density_input, double scale,
+                  const double *__restrict__ sf, int pot)
 {
     using C = typename CTw<T>::t;
     constexpr int W = CTw<T>::kCols;
@@ -283,7 +317,7 @@ tidal_pipe_kernel(const typename CTw<T>::t *src, typename CTw<T>::t *dst, int n,
             for (int e = threadIdx.x; e < TILE; e += NTHR) {
                 const int j = e / W, cc = e % W;
                 const int fj = j <= h ? j : j - n;
-                const T m = phi_mult<T>(0, fj, fy, ct * W + cc, gc, norm);
+                const T m = phi_mult<T, FD>(0, fj, fy, ct * W + cc, gc, norm, sf, h, pot);
                 const C v = in[e];
                 in[e] = C{v.x * m, v.y * m};
             }
@@ -298,7 +332,7 @@ tidal_pipe_kernel(const typename CTw<T>::t *src, typename CTw<T>::t *dst, int n,
             for (int e = threadIdx.x; e < TILE; e += NTHR) {
                 const int j = e / W;
                 const int fj = j <= h ? j : j - n;
-                const T m = (T)ipow(fj, MODE == 0 ? o : q);
+                const T m = kfac<T, FD>(sf, h, fj, MODE == 0 ? o : q);
                 const C v = in[e];
                 work[e] = C{v.x * m, v.y * m};
             }
@@ -310,7 +344,7 @@ tidal_pipe_kernel(const typename CTw<T>::t *src, typename CTw<T>::t *dst, int n,
             // along y, so it commutes with the transform)
             for (int e = threadIdx.x; e < TILE; e += NTHR) {
                 const C v = work[e];
-                const T mz = MODE == 0 ? (T)1 : (T)ipow(ct * W + e % W, 2 - p - q);
+                const T mz = MODE == 0 ? (T)1 : kfac<T, FD>(sf, h, ct * W + e % W, 2 - p - q);
                 g[(int64_t)(e / W) * jstride + (e % W)] = MODE == 0 ? v : C{v.x * mz, v.y * mz};
             }
             __syncthreads();  // work is refilled by the next output
@@ -670,6 +704,20 @@ tidal_z_pipe_kernel(const typename CTw<T>::t *__restrict__ src, const typename C
     flush_counts(lc0, lc1, lc2, lc3, lties, cnt_s, counts);
 }
 
+// sf[i] = s(f) / k_f, f = i - N/2 (i = 0 .. N): the Fourier multiplier of
+// the centred difference of gradfindif, Source/NumericalMethods.cpp:1123-1218,
+//   D g(x) = (-g(x+2d) + 8 g(x+d) - 8 g(x-d) + g(x-2d)) / (12 d),
+// D e^{ikx} = i s(k) e^{ikx},  s(k) = (8 sin kd - sin 2kd) / (6 d).
+// With k = k_f f and k_f d = 2 pi / N:  s / k_f = N (8 sin t - sin 2t) / (12 pi),
+// t = 2 pi f / N.  s(0) = s(+-N/2) = 0.
+__global__ void fd_table_kernel(double *__restrict__ sf, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > n) return;
+    const double t = 2.0 * (double)(i - n / 2) / (double)n;  // sinpi(t) = sin(2 pi f / N)
+    sf[i] = (double)n * (8.0 * sinpi(t) - sinpi(2.0 * t)) / (12.0 * M_PI);
+}
+
 int threads_for(int points, int ppt, int cap)
 {
     int t = (points + ppt - 1) / ppt;
@@ -680,10 +728,10 @@ int threads_for(int points, int ppt, int cap)
 // Launches the pipelined T-web column kernel for the main planes when it
 // applies (compile-time length, full 16-byte aligned tiles, three tiles
 // within 200 KB of shared memory); returns false otherwise.
-template <typename T, int MODE, int LEN>
+template <typename T, int MODE, int LEN, bool FD>
 bool pipe_launch(cam_ctx *ctx, const char *name, const typename CTw<T>::t *src, typename CTw<T>::t *dst, int64_t n,
                  int64_t M, int64_t jstride, int64_t pstride, int64_t ccomp, const typename CTw<T>::t *tw,
-                 double gcoef, const double *d_mean, int density, double scale)
+                 double gcoef, const double *d_mean, int density, double scale, const double *sf, int pot)
 {
     using C = typename CTw<T>::t;
     constexpr int W = CTw<T>::kCols;
@@ -694,7 +742,7 @@ bool pipe_launch(cam_ctx *ctx, const char *name, const typename CTw<T>::t *src, 
         if (M % W != 0 || (jstride * es) % 16 || (pstride * es) % 16 || (ccomp * es) % 16 ||
             ((uintptr_t)src % 16) || ((uintptr_t)dst % 16))
             return false;
-        auto k = tidal_pipe_kernel<T, MODE, LEN>;
+        auto k = tidal_pipe_kernel<T, MODE, LEN, FD>;
         const size_t smem = 3 * (size_t)LEN * W * sizeof(C);
         smem_at_least(k, smem);
         int per_sm = 0;
@@ -704,7 +752,7 @@ bool pipe_launch(cam_ctx *ctx, const char *name, const typename CTw<T>::t *src, 
         const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>(nunits, (int64_t)kNumSMs * std::max(per_sm, 1)));
         constexpr int nthr = col_threads<T, LEN>();
         CAM_LAUNCH_NAMED(ctx, name, k, g, nthr, smem, src, dst, (int)n, nct, nunits, jstride, pstride, ccomp, tw, gcoef,
-                         d_mean, density, scale);
+                         d_mean, density, scale, sf, pot);
         return true;
     }
 }
@@ -729,28 +777,37 @@ void tweb_impl(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const d
     const double kf = 2.0 * M_PI / (double)L;
     const double R = o.smoothing_R;
     const double gcoef = R > 0 ? 0.5 * kf * kf * R * R : 0.0;
-    const double scale = 1.0 / ((double)n * (double)n * (double)n);  // c2r divides by N^3
     const int density = input_type == CAM_INPUT_DENSITY;
-
+    const int pot = input_type == CAM_INPUT_POTENTIAL;
+    // c2r divides by N^3; a potential input carries the k_f^2 of -k_a k_b
+    const double scale = (pot ? kf * kf : 1.0) / ((double)n * (double)n * (double)n);
+    const double *sf = nullptr;
+    if (o.method == CAM_TWEB_FD) {
+        auto *t = static_cast<double *>(scratch(ctx, "tw.sfac", (size_t)(n + 1) * sizeof(double)));
+        CAM_LAUNCH(ctx, fd_table_kernel, (unsigned)((n + 1 + 127) / 128), 128, 0, t, (int)n);
+        sf = t;
+    }
+    auto passes = [&](auto fdc) {
+    constexpr bool FD = decltype(fdc)::value;
     // 1. x: k_x^p phi + inverse FFT along x, p = 0, 1, 2 (slots 0..2).
     {
         const int nthr = threads_for((int)n * W, CTw<T>::kPPT, 1024);
         const size_t smem = (size_t)n * W * sizeof(C);
         dispatch_fft_len(n, [&](auto lc) {
         constexpr int LEN = decltype(lc)::value;
-        auto k0 = tidal_x_kernel<T, false, LEN>;
-        auto k1 = tidal_x_kernel<T, true, LEN>;
+        auto k0 = tidal_x_kernel<T, false, LEN, FD>;
+        auto k1 = tidal_x_kernel<T, true, LEN, FD>;
         smem_at_least(k1, smem);
-        if (!pipe_launch<T, 0, LEN>(ctx, "tweb_tidal_x", static_cast<const C *>(dk.main), cm, n, M, n * M, (int64_t)M,
-                                    ccomp, tw, gcoef, d_mean, density, scale)) {
+        if (!pipe_launch<T, 0, LEN, FD>(ctx, "tweb_tidal_x", static_cast<const C *>(dk.main), cm, n, M, n * M,
+                                        (int64_t)M, ccomp, tw, gcoef, d_mean, density, scale, sf, pot)) {
             smem_at_least(k0, smem);
             dim3 g0(3, (unsigned)((M + W - 1) / W), (unsigned)n);
             CAM_LAUNCH_NAMED(ctx, "tweb_tidal_x", k0, g0, nthr, smem, static_cast<const C *>(dk.main), cm, (int)n,
-                             (int)M, n * M, (int64_t)M, ccomp, rn, tw, gcoef, d_mean, density, scale);
+                             (int)M, n * M, (int64_t)M, ccomp, rn, tw, gcoef, d_mean, density, scale, sf, pot);
         }
         dim3 g1(3, (unsigned)((n + W - 1) / W), 1);
         CAM_LAUNCH_NAMED(ctx, "tweb_tidal_x_nyq", k1, g1, nthr, smem, static_cast<const C *>(dk.nyq), cn, (int)n, (int)n, n,
-                   (int64_t)0, nn, rn, tw, gcoef, d_mean, density, scale);
+                   (int64_t)0, nn, rn, tw, gcoef, d_mean, density, scale, sf, pot);
         });
     }
     // 2. y: k_y^q and the inverse FFT along y: three fields in, six out.
@@ -759,21 +816,24 @@ void tweb_impl(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const d
         const size_t smem = (size_t)n * W * sizeof(C);
         dispatch_fft_len(n, [&](auto lc) {
         constexpr int LEN = decltype(lc)::value;
-        auto ky = tidal_y_kernel<T, LEN>;
+        auto ky = tidal_y_kernel<T, LEN, FD>;
         smem_at_least(ky, smem);
         // main: planes i, FFT index j (stride M), columns k (stride 1)
-        if (!pipe_launch<T, 1, LEN>(ctx, "tweb_tidal_y", cm, cm, n, M, (int64_t)M, n * M, ccomp, tw, 0.0, nullptr, 0,
-                                    1.0)) {
+        if (!pipe_launch<T, 1, LEN, FD>(ctx, "tweb_tidal_y", cm, cm, n, M, (int64_t)M, n * M, ccomp, tw, 0.0, nullptr,
+                                        0, 1.0, sf, 0)) {
             dim3 g0(3, (unsigned)((M + W - 1) / W), (unsigned)n);
             CAM_LAUNCH_NAMED(ctx, "tweb_tidal_y", ky, g0, nthr, smem, cm, (int)n, (int)M, (int64_t)M, (int64_t)1, n * M,
-                             ccomp, rn, tw, -1);
+                             ccomp, rn, tw, -1, sf);
         }
         // Nyquist plane: columns i (stride N), FFT index j (stride 1)
         dim3 g1(3, (unsigned)((n + W - 1) / W), 1);
         CAM_LAUNCH_NAMED(ctx, "tweb_tidal_y_nyq", ky, g1, nthr, smem, cn, (int)n, (int)n, (int64_t)1, n, (int64_t)0,
-                         nn, rn, tw, (int)M);
+                         nn, rn, tw, (int)M, sf);
         });
     }
+    };
+    if (sf) passes(std::true_type{});
+    else passes(std::false_type{});
     // 3. z: c2r + eigenvalues + labels.
     {
         // Small tiles (<= 4096 complex, 256 threads) so that several CTAs
@@ -827,7 +887,11 @@ void tweb_device(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const
 {
     CAM_REQUIRE(std::isfinite(o.lambda_th) && o.tie_band >= 0.0, CAM_E_INVAL, "invalid T-web threshold");
     CAM_REQUIRE(o.smoothing_R >= 0.f && std::isfinite(o.smoothing_R), CAM_E_INVAL, "invalid smoothing radius");
-    CAM_REQUIRE(input_type == CAM_INPUT_DELTA || d_mean, CAM_E_INVAL, "density input needs the mean");
+    CAM_REQUIRE(o.method == CAM_TWEB_FFT || o.method == CAM_TWEB_FD, CAM_E_INVAL, "unknown T-web method");
+    CAM_REQUIRE(input_type == CAM_INPUT_DENSITY || input_type == CAM_INPUT_DELTA ||
+                    (input_type == CAM_INPUT_POTENTIAL && o.method == CAM_TWEB_FD),
+                CAM_E_INVAL, "T-web input must be a density or delta mesh (or a potential, finite differences only)");
+    CAM_REQUIRE(input_type != CAM_INPUT_DENSITY || d_mean, CAM_E_INVAL, "density input needs the mean");
     if (dk.precision == CAM_F32) tweb_impl<float>(ctx, plan, dk, L, d_mean, input_type, o, d_labels, d_lambdas, stats);
     else tweb_impl<double>(ctx, plan, dk, L, d_mean, input_type, o, d_labels, d_lambdas, stats);
 }

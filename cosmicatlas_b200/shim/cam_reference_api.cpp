@@ -119,3 +119,43 @@ void EigenValuesTweb(ULONG Nft, real_prec L1, std::vector<real_prec> &delta, std
     out2.assign(lam.begin() + ng, lam.begin() + 2 * ng);
     out3.assign(lam.begin() + 2 * ng, lam.end());
 }
+
+void EigenValuesTweb(ULONG Nft, real_prec L1, std::vector<real_prec> & /*delta*/, std::vector<real_prec> &phi,
+                     std::vector<real_prec> &out1, std::vector<real_prec> &out2, std::vector<real_prec> &out3)
+{
+    const size_t ng = (size_t)Nft * Nft * Nft;
+    cam_grid g{};
+    g.n[0] = g.n[1] = g.n[2] = (int64_t)Nft;
+    g.L[0] = g.L[1] = g.L[2] = L1;
+    cam_tweb_opts o{};
+    o.input_type = CAM_INPUT_POTENTIAL;  // the Hessian of phi as given
+    o.method = CAM_TWEB_FD;
+    std::vector<float> lam(3 * ng);
+    cam_tweb_stats st{};
+    const int rc = cam_tweb(ctx(), &g, phi.data(), CAM_F32, CAM_MEM_HOST, &o, nullptr, lam.data(), CAM_MEM_HOST, &st);
+    report(rc, "EigenValuesTweb");
+    out1.assign(lam.begin(), lam.begin() + ng);
+    out2.assign(lam.begin() + ng, lam.begin() + 2 * ng);
+    out3.assign(lam.begin() + 2 * ng, lam.end());
+}
+
+void PoissonSolver(real_prec Lbox, ULONG Nft, std::vector<real_prec> &in, std::vector<real_prec> &out)
+{
+    cam_grid g{};
+    g.n[0] = g.n[1] = g.n[2] = (int64_t)Nft;
+    g.L[0] = g.L[1] = g.L[2] = Lbox;
+    out.resize((size_t)Nft * Nft * Nft);
+    report(cam_poisson(ctx(), &g, in.data(), CAM_F32, CAM_MEM_HOST, 0.f, out.data(), CAM_MEM_HOST), "PoissonSolver");
+}
+
+void gradfindif(ULONG N1, ULONG N2, ULONG N3, real_prec L1, real_prec L2, real_prec L3, std::vector<real_prec> in,
+                std::vector<real_prec> &out, int dim)
+{
+    cam_grid g{};
+    g.n[0] = (int64_t)N1;
+    g.n[1] = (int64_t)N2;
+    g.n[2] = (int64_t)N3;
+    g.L[0] = L1; g.L[1] = L2; g.L[2] = L3;
+    out.resize((size_t)N1 * N2 * N3);
+    report(cam_gradfindif(ctx(), &g, in.data(), CAM_F32, CAM_MEM_HOST, dim, out.data(), CAM_MEM_HOST), "gradfindif");
+}

@@ -42,6 +42,19 @@ enum { CAM_NGP = 0, CAM_CIC = 1, CAM_TSC = 2 };       /* mass assignment  */
 enum { CAM_F32 = 0, CAM_F64 = 1 };                    /* mesh/FFT precision */
 enum { CAM_MEM_HOST = 0, CAM_MEM_DEVICE = 1 };
 enum { CAM_INPUT_DENSITY = 0, CAM_INPUT_DELTA = 1 };  /* P(k)/T-web input  */
+/* T-web only: the mesh is the potential phi (nabla^2 phi = delta) that
+ * Cwclass::get_CWC passes to EigenValuesTweb after PoissonSolver,
+ * Source/Cwclass.cpp:259-277. */
+enum { CAM_INPUT_POTENTIAL = 2 };
+/* Tidal tensor of the T-web:
+ *   CAM_TWEB_FFT  T_ab = c2r(k_a k_b / k^2 delta_k)        (_USE_GFFT_EIGENV_,
+ *                 calc_LapPhiv, Source/NumericalMethods.cpp:2609-2680);
+ *   CAM_TWEB_FD   T_ab = D_b D_a phi, D the 4th-order centred difference
+ *                 (-f[+2] + 8 f[+1] - 8 f[-1] + f[-2]) / (12 d) of gradfindif,
+ *                 Source/NumericalMethods.cpp:1123-1218, and phi from
+ *                 PoissonSolver, Source/Miscelanious.cpp:1189-1275: the
+ *                 reference's default (_USE_GFINDIFF_EIGENV_, Headers/def.h:2657). */
+enum { CAM_TWEB_FFT = 0, CAM_TWEB_FD = 1 };
 
 typedef struct cam_ctx cam_ctx;
 
@@ -96,7 +109,9 @@ typedef struct {
     float smoothing_R;  /* Gaussian exp(-k^2 R^2 / 2); 0 = none            */
     double lambda_th;   /* label = 4 - #{lambda > lambda_th}               */
     double tie_band;    /* cells with |lambda - lambda_th| <= band counted */
-    int input_type;     /* CAM_INPUT_DENSITY (rho -> rho/mean - 1) or DELTA */
+    int input_type;     /* CAM_INPUT_DENSITY (rho -> rho/mean - 1), DELTA
+                           or POTENTIAL                                    */
+    int method;         /* CAM_TWEB_FFT (0) or CAM_TWEB_FD                 */
 } cam_tweb_opts;
 
 typedef struct {
@@ -174,6 +189,20 @@ int cam_power(cam_ctx *ctx, const cam_grid *grid, const void *mesh, int precisio
               int mem, const cam_pk_opts *opts, double *pk, int64_t *modes,
               double *kvector, cam_pk_info *info);
 
+/* Cross power spectrum of two meshes: replaces
+ * PowerSpectrumF::compute_cross_power_spectrum_grid, Source/PowerSpectrumF.cpp:549,
+ * with FftwFunctions::cross_power_spectrum_fkp, Source/FftwFunctions.cpp:645.
+ * mesh_x uses opts->input_type, mesh_y input_type_y (a density becomes
+ * rho/mean - 1).  Over P(k)'s mode set and bins (opts->scheme and
+ * mas_correction give W; no shot noise is subtracted, as in the reference):
+ *   pk_x[b] = sum |F_X|^2 / W^2 / (modes N^6 / L^3), pk_y likewise,
+ *   pk[b]   = sum Re(F_X conj F_Y) / W^2 / (modes N^6 / L^3),
+ *             or, with want_coeff, that divided by sqrt(pk_x pk_y).
+ * Host arrays of nbins; any may be NULL. */
+int cam_cross_power(cam_ctx *ctx, const cam_grid *grid, const void *mesh_x, const void *mesh_y, int precision,
+                    int mem, const cam_pk_opts *opts, int input_type_y, int want_coeff, double *pk,
+                    double *pk_x, double *pk_y, int64_t *modes, double *kvector);
+
 /* ---- T-web -------------------------------------------------------------
  * Replaces Cwclass::get_CWC, Source/Cwclass.cpp:235, with the FFT tidal
  * tensor of EigenValuesTweb, Source/Miscelanious.cpp:1772.  labels (N^3
@@ -182,6 +211,46 @@ int cam_power(cam_ctx *ctx, const cam_grid *grid, const void *mesh, int precisio
 int cam_tweb(cam_ctx *ctx, const cam_grid *grid, const void *mesh, int precision,
              int mem, const cam_tweb_opts *opts, uint8_t *labels, float *lambdas,
              int out_mem, cam_tweb_stats *stats);
+
+/* ---- potential and finite differences --------------------------------
+ * Replaces PoissonSolver(Lbox, Nft, in, out), Source/Miscelanious.cpp:1189:
+ * phi = c2r(-delta_k / k^2) / N^3 (k = 0 mode -> 0), with k from the
+ * signed FFT frequencies times 2 pi / L.  smoothing_R > 0 also multiplies
+ * delta_k by exp(-k^2 R^2 / 2).  delta and phi are N^3 of `precision`; mem
+ * and out_mem say where they live. */
+int cam_poisson(cam_ctx *ctx, const cam_grid *grid, const void *delta, int precision, int mem,
+                float smoothing_R, void *phi, int out_mem);
+
+/* Replaces gradfindif(N1, N2, N3, L1, L2, L3, in, out, dim),
+ * Source/NumericalMethods.cpp:1123: out = (-in[+2] + 8 in[+1] - 8 in[-1] +
+ * in[-2]) / (12 L / N) along dim (1 = x, the slowest index; 3 = z),
+ * periodic.  FP32 results equal the reference loop's bit for bit.  in may
+ * equal out (the reference takes `in` by value). */
+int cam_gradfindif(cam_ctx *ctx, const cam_grid *grid, const void *in, int precision, int mem, int dim,
+                   void *out, int out_mem);
+
+/* ---- BAM kernel ---------------------------------------------------------
+ * The 3D update of Bam::GetKernel, Source/Bam.cpp:529 (:786-910).  kernel is
+ * the real half-complex array [N][N][N/2+1] of `precision`.  Each element
+ * gets the bin b = floor((|k| - kmin) / DeltaK), kmin = DeltaKmin k_f and
+ * DeltaK = ndel k_f, in the reference's real_prec arithmetic; for
+ * 0 <= b < nbins it becomes weight[b] (CAM_KERNEL_SET: GetKernel without
+ * rejection) or is multiplied by it (CAM_KERNEL_SCALE: with rejection).
+ * kernel_binned[b] (may be NULL) = mean of the updated kernel over bin b
+ * (kernel_updated, :905-910; bin 0 = the mean of bins 1..4); modes[b] (may
+ * be NULL) = its element count.  weight, kernel_binned and modes are host
+ * arrays of nbins (1 <= nbins <= 1600). */
+enum { CAM_KERNEL_SET = 0, CAM_KERNEL_SCALE = 1 };
+int cam_bam_kernel_update(cam_ctx *ctx, const cam_grid *grid, int precision, double DeltaKmin, double ndel,
+                          int nbins, const double *weight, int mode, void *kernel, int mem,
+                          double *kernel_binned, int64_t *modes);
+
+/* Replaces Bam::Konvolve, Source/Bam.cpp:1027:
+ * out = c2r(kernel * r2c(in)) / N^3 * 2 w / N^3, w = the sum of the kernel
+ * over its half-complex array.  in may equal out.  A non-finite sum of in
+ * returns CAM_E_NONFINITE (the reference exits, :1060-1067). */
+int cam_konvolve(cam_ctx *ctx, const cam_grid *grid, const void *in, int precision, int mem,
+                 const void *kernel, int kernel_mem, void *out, int out_mem);
 
 /* ---- one mesh job: particles -> mesh -> FFT -> P(k) [-> T-web] ----------
  * The plain per-call GPU path of one BAM iteration: the mesh and its

@@ -49,6 +49,21 @@ void do_fftw_c2r(int Nft, complex_prec *in, std::vector<real_prec> &out);
 void EigenValuesTweb(ULONG Nft, real_prec L1, std::vector<real_prec> &delta, std::vector<real_prec> &out1,
                      std::vector<real_prec> &out2, std::vector<real_prec> &out3);
 
+/* Source/Miscelanious.cpp:1663 (finite differences, the reference's default
+ * _USE_GFINDIFF_EIGENV_ build): eigenvalues of the gradfindif Hessian of the
+ * potential phi, descending, into out1..out3.  delta is not read. */
+void EigenValuesTweb(ULONG Nft, real_prec L1, std::vector<real_prec> &delta, std::vector<real_prec> &phi,
+                     std::vector<real_prec> &out1, std::vector<real_prec> &out2, std::vector<real_prec> &out3);
+
+/* Source/Miscelanious.cpp:1189: out = the potential of in (nabla^2 out = in). */
+void PoissonSolver(real_prec Lbox, ULONG Nft, std::vector<real_prec> &in, std::vector<real_prec> &out);
+
+/* Source/NumericalMethods.cpp:1123: 4th-order centred difference of in along
+ * dim (1 = x, 3 = z), periodic, into out (cubic meshes; bit-identical to the
+ * reference loop). */
+void gradfindif(ULONG N1, ULONG N2, ULONG N3, real_prec L1, real_prec L2, real_prec L3, std::vector<real_prec> in,
+                std::vector<real_prec> &out, int dim);
+
 /* Status of the last call on this thread (CAM_OK or a cam.h code); the
  * reference's functions return void and exit on errors, these never exit. */
 int cam_refapi_last_status();

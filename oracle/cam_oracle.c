@@ -414,6 +414,45 @@ void orc_power_f64(int64_t n, const double *spec, int p, int mas_corr, int sn_co
     free(sr); free(ss); free(md); free(sx); free(cx);
 }
 
+/* Cross power spectrum sums in FP64, FftwFunctions::cross_power_spectrum_fkp,
+ * Source/FftwFunctions.cpp:645-893: over the octant loop's mode set
+ * (pk_visited) and bins (orc_bin), with icorr2 = 1/W^2 when mas_corr
+ * (correction_MAS, :758):
+ *   cross[b] = sum Re(F1 conj F2) icorr2   (the reference's Re1 Re2 + Im1 Im2)
+ *   a1[b]    = sum |F1|^2 icorr2,  a2[b] = sum |F2|^2 icorr2,  modes[b].
+ * No shot noise is subtracted (the reference leaves it out, :653). */
+void orc_cross_f64(int64_t n, const double *s1, const double *s2, int p, int mas_corr, double kmin_u,
+                   double dk_u, int nbins, double *cross, double *a1, double *a2, int64_t *modes)
+{
+    const int64_t nz = n / 2 + 1;
+    for (int b = 0; b < nbins; ++b) { cross[b] = 0.0; a1[b] = 0.0; a2[b] = 0.0; modes[b] = 0; }
+    double *sx = malloc(sizeof(double) * (size_t)n);
+    for (int64_t a = 0; a < n; ++a) sx[a] = sinc_pi(a <= n / 2 ? a : n - a, n);
+    for (int64_t i = 0; i < n; ++i) {
+        int64_t a = i <= n / 2 ? i : n - i;
+        for (int64_t j = 0; j < n; ++j) {
+            int64_t b = j <= n / 2 ? j : n - j;
+            for (int64_t c = 0; c < nz; ++c) {
+                if (!pk_visited(i, j, c, n)) continue;
+                int64_t bin = orc_bin((double)(a * a + b * b + c * c), kmin_u, dk_u, nbins);
+                if (bin < 0) continue;
+                const double *f = s1 + 2 * ((i * n + j) * nz + c);
+                const double *g = s2 + 2 * ((i * n + j) * nz + c);
+                double iw2 = 1.0;
+                if (mas_corr) {
+                    double wk = pow(sx[i] * sx[j] * sx[c], (double)(p + 1));
+                    iw2 = 1.0 / (wk * wk);
+                }
+                cross[bin] += (f[0] * g[0] + f[1] * g[1]) * iw2;
+                a1[bin] += (f[0] * f[0] + f[1] * f[1]) * iw2;
+                a2[bin] += (g[0] * g[0] + g[1] * g[1]) * iw2;
+                modes[bin] += 1;
+            }
+        }
+    }
+    free(sx);
+}
+
 /* The reference's power_spectrum loop as written (FP32, OpenMP atomics,
  * float bins), Source/FftwFunctions.cpp:1660-1876, for the CPU baseline.
  * spec is interleaved complex64.  fix_octant4 selects Re^2+Im^2 for the

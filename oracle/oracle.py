@@ -55,6 +55,8 @@ def lib():
         _LIB.orc_assign_ref.restype = i64
         _LIB.orc_power_f64.argtypes = [i64, P, i32, i32, i32, f64, f64, f64, f64, i32, P, P, P, P]
         _LIB.orc_power_f64.restype = None
+        _LIB.orc_cross_f64.argtypes = [i64, P, P, i32, i32, f64, f64, i32, P, P, P, P]
+        _LIB.orc_cross_f64.restype = None
         _LIB.orc_power_ref.argtypes = [i64, P, i32, i32, i32, f32, f32, f32, f32, f32, i32, i32, P, P]
         _LIB.orc_power_ref.restype = None
         _LIB.orc_bin.argtypes = [f64, f64, f64, i32]
@@ -132,7 +134,7 @@ def rfft3_f64(mesh: np.ndarray) -> np.ndarray:
 def irfft3_f64(spec: np.ndarray, n: int) -> np.ndarray:
     """c2r divided by N^3 as do_fftw_c2r does, Source/NumericalMethods.cpp:1818-1856
     (numpy's irfftn already divides by N^3)."""
-    return np.fft.irfftn(spec, s=(n, n, n))
+    return np.fft.irfftn(spec, s=(n, n, n), axes=(0, 1, 2))
 
 
 @dataclass
@@ -181,6 +183,40 @@ def power_grid(mesh, L, scheme, nbins, kmin_u=0.0, dk_u=1.0, input_type="density
     r = power_from_spectrum(spec, n, L, scheme, nbins, sn, normal, kmin_u, dk_u, mas_corr, sn_corr)
     r.n_obj = ngal
     return r
+
+
+@dataclass
+class CrossResult:
+    pk: np.ndarray      # cross power, or the coefficient with coeff=True
+    pk_x: np.ndarray
+    pk_y: np.ndarray
+    modes: np.ndarray
+
+
+def cross_power_grid(mx, my, L, scheme, nbins, input_x="density", input_y="density", coeff=False,
+                     kmin_u=0.0, dk_u=1.0, mas_corr=True) -> CrossResult:
+    """PowerSpectrumF::compute_cross_power_spectrum_grid, Source/PowerSpectrumF.cpp:549-632,
+    with FftwFunctions::cross_power_spectrum_fkp, Source/FftwFunctions.cpp:645-893, in
+    FP64: density meshes become rho/mean - 1, both normalisations are
+    (L^1.5 / N^3)^-2 = N^6 / L^3, P_X = sum Re(F_X F_Y*) / W^2 / (modes N^6/L^3);
+    coeff=True divides by sqrt(P_XX P_YY) (:885-893)."""
+    n = mx.shape[0]
+    def delta(m, kind):
+        m = np.asarray(m, np.float64)
+        return m / (m.sum() / m.size) - 1.0 if kind == "density" else m
+    s1 = np.ascontiguousarray(rfft3_f64(delta(mx, input_x)), np.complex128)
+    s2 = np.ascontiguousarray(rfft3_f64(delta(my, input_y)), np.complex128)
+    cr, a1, a2 = np.empty(nbins), np.empty(nbins), np.empty(nbins)
+    md = np.empty(nbins, np.int64)
+    lib().orc_cross_f64(n, _p(s1), _p(s2), SCHEME_P[scheme], int(mas_corr), float(kmin_u), float(dk_u), nbins,
+                        _p(cr), _p(a1), _p(a2), _p(md))
+    normal = float(n) ** 6 / float(L) ** 3
+    with np.errstate(divide="ignore", invalid="ignore"):
+        px = np.where(md > 0, cr / (md * normal), 0.0)
+        pxx = np.where(md > 0, a1 / (md * normal), 0.0)
+        pyy = np.where(md > 0, a2 / (md * normal), 0.0)
+        pk = np.where(md > 0, px / np.sqrt(pxx * pyy), 0.0) if coeff else px
+    return CrossResult(pk, pxx, pyy, md)
 
 
 def signed_freq(n: int) -> np.ndarray:
@@ -259,6 +295,150 @@ def tweb_density(mesh, L, R, lth, band=1e-5) -> TwebResult:
     nbar = mesh.sum() / mesh.size
     delta_k = rfft3_f64(mesh / nbar - 1.0)
     return tweb_from_spectrum(delta_k, n, L, R, lth, band)
+
+
+# ---- finite-difference T-web (the reference's default variant) ----------
+
+def poisson_f64(delta_k, n, L, R=0.0) -> np.ndarray:
+    """PoissonSolver, Source/Miscelanious.cpp:1189-1275: phi = c2r(-delta_k / k^2)
+    / N^3 with k from coords[i] = k_f (i <= N/2 ? i : i - N) and the k = 0 mode
+    set to 0 (:1251-1262).  R > 0 also applies the Gaussian filter of
+    kernelcomp, Source/NumericalMethods.cpp:2272-2273, to delta_k."""
+    kf = 2.0 * np.pi / L
+    fx = signed_freq(n)[:, None, None] * kf
+    fy = signed_freq(n)[None, :, None] * kf
+    fz = np.arange(n // 2 + 1, dtype=np.float64)[None, None, :] * kf
+    k2 = fx * fx + fy * fy + fz * fz
+    with np.errstate(divide="ignore", invalid="ignore"):
+        term = np.where(k2 > 0, -1.0 / k2, 0.0)
+    g = np.exp(-0.5 * k2 * R * R) if R > 0 else 1.0
+    return irfft3_f64(delta_k * term * g, n)
+
+
+def gradfindif_f64(f: np.ndarray, axis: int, L: float) -> np.ndarray:
+    """gradfindif, Source/NumericalMethods.cpp:1123-1218: the 4th-order centred
+    difference (-f[+2] + 8 f[+1] - 8 f[-1] + f[-2]) / (12 L / N) along one
+    axis (dim 1 = x = axis 0, the slowest; dim 3 = z = axis 2), periodic."""
+    n = f.shape[axis]
+    ideltaH = 1.0 / (12.0 * (L / n))
+    return (-np.roll(f, -2, axis) + 8.0 * np.roll(f, -1, axis) - 8.0 * np.roll(f, 1, axis)
+            + np.roll(f, 2, axis)) * ideltaH
+
+
+def gradfindif_ref_f32(f: np.ndarray, axis: int, L: float) -> np.ndarray:
+    """gradfindif as the reference evaluates it with real_prec = float
+    (Source/NumericalMethods.cpp:1126-1127, :1153): deltaH = 12.0 * (L1 / N1)
+    from a float quotient, ideltaH = 1.0 / deltaH rounded to float, and
+    (-in[rr] + 8.0*in[r] - 8.0*in[l] + in[ll]) * ideltaH evaluated left to
+    right in double (8.0 is a double literal), rounded to float on
+    assignment."""
+    n = f.shape[axis]
+    d = np.float32(L) / np.float32(n)
+    deltaH = np.float32(12.0 * np.float64(d))
+    ideltaH = np.float32(1.0 / np.float64(deltaH))
+    a = np.asarray(f, np.float32).astype(np.float64)
+    v = ((-np.roll(a, -2, axis) + 8.0 * np.roll(a, -1, axis)) - 8.0 * np.roll(a, 1, axis)) + np.roll(a, 2, axis)
+    return (v * np.float64(ideltaH)).astype(np.float32)
+
+
+def tidal_fd(phi: np.ndarray, L: float) -> np.ndarray:
+    """The (…,6) tensors (xx, yy, zz, xy, xz, yz) of EigenValuesTweb's
+    _USE_GFINDIFF_EIGENV_ branch, Source/Miscelanious.cpp:1681-1700: the
+    first differences of phi along x, y, z, each differenced again.  The
+    off-diagonal entries are the ones gsl_eigen_symmv reads (its lower
+    triangle, in_matrix[1], [2], [5] at :1733-1738): T_xy = D_x(D_y phi),
+    T_xz = D_x(D_z phi), T_yz = D_y(D_z phi)."""
+    gx = gradfindif_f64(phi, 0, L)
+    gy = gradfindif_f64(phi, 1, L)
+    gz = gradfindif_f64(phi, 2, L)
+    out = np.empty(phi.shape + (6,))
+    out[..., 0] = gradfindif_f64(gx, 0, L)
+    out[..., 1] = gradfindif_f64(gy, 1, L)
+    out[..., 2] = gradfindif_f64(gz, 2, L)
+    out[..., 3] = gradfindif_f64(gy, 0, L)
+    out[..., 4] = gradfindif_f64(gz, 0, L)
+    out[..., 5] = gradfindif_f64(gz, 1, L)
+    return out
+
+
+def tweb_fd_potential(phi, L, lth, band=1e-5) -> TwebResult:
+    """EigenValuesTweb(Nft, L, delta, phi, ...) with finite differences
+    (Source/Miscelanious.cpp:1663-1760) and the labels of Cwclass.cpp:875-890."""
+    n = phi.shape[0]
+    lam = eig3_f64(tidal_fd(np.asarray(phi, np.float64), L)).reshape(n, n, n, 3)
+    labels, counts, ties = classify(lam, lth, band)
+    return TwebResult(labels.reshape(n, n, n), lam, counts, ties)
+
+
+def tweb_fd_from_spectrum(delta_k, n, L, R, lth, band=1e-5) -> TwebResult:
+    return tweb_fd_potential(poisson_f64(delta_k, n, L, R), L, lth, band)
+
+
+def tweb_fd_density(mesh, L, R, lth, band=1e-5) -> TwebResult:
+    """Cwclass::get_CWC with the reference's default T-web
+    (Source/Cwclass.cpp:235-277): PoissonSolver on delta = rho/mean - 1,
+    then the finite-difference tidal tensor."""
+    n = mesh.shape[0]
+    mesh = np.asarray(mesh, np.float64)
+    nbar = mesh.sum() / mesh.size
+    return tweb_fd_from_spectrum(rfft3_f64(mesh / nbar - 1.0), n, L, R, lth, band)
+
+
+# ---- BAM kernel (GetKernel's 3D update, Konvolve) ---------------------------
+
+def bam_kernel_bins(n, L, DeltaKmin=0.0, ndel=1.0, dtype=np.float32) -> np.ndarray:
+    """The bin of every half-complex element in Bam::GetKernel,
+    Source/Bam.cpp:829-905, in the reference's real_prec arithmetic:
+    kv = _get_modulo(coords[i]*dk, coords[j]*dk, coords[k]*dk), a macro that
+    expands to sqrt(c_i*dk*c_i*dk + c_j*dk*c_j*dk + c_k*dk*c_k*dk)
+    (Headers/def.h:695), then floor((kv - kmin) / DeltaK).  dk, kmin and
+    DeltaK are Params' double values read through real_prec getters
+    (Source/Params.cpp:4092-4103, Headers/Params.h:4326-4363)."""
+    t = np.dtype(dtype).type
+    deltak = 2.0 * np.pi / np.float64(np.float32(L))
+    dk2 = deltak * deltak
+    deltak0 = np.sqrt((dk2 + dk2) + dk2) / np.sqrt(3.0)
+    dk, kmin, dK = t(deltak), t(DeltaKmin * deltak0), t(ndel * deltak0)
+    c = signed_freq(n).astype(dtype)
+    ck = np.arange(n // 2 + 1).astype(dtype)
+    with np.errstate(over="ignore", invalid="ignore"):
+        tx = ((c * dk) * c) * dk
+        tz = ((ck * dk) * ck) * dk
+        kv = np.sqrt((tx[:, None, None] + tx[None, :, None]) + tz[None, None, :])
+        b = np.floor((kv - kmin) / dK)
+    return b.astype(np.int64)
+
+
+def bam_kernel_update_ref(kernel, L, weight, scale: bool, DeltaKmin=0.0, ndel=1.0):
+    """GetKernel's 3D loops (Source/Bam.cpp:829-905) on a copy of `kernel`
+    (N, N, N/2+1): kernel = weight[b] (no rejection) or kernel *= weight[b]
+    (rejection) for 0 <= b < nbins, in the kernel's precision.  Returns the
+    updated kernel, the bin means of it (FP64 sums; bin 0 = mean of bins
+    1..4, :905-910) and the element counts."""
+    k = np.array(kernel, copy=True)
+    t = k.dtype.type
+    nb = len(weight)
+    b = bam_kernel_bins(k.shape[0], L, DeltaKmin, ndel, k.dtype)
+    inb = (b >= 0) & (b < nb)
+    w = np.asarray(weight, np.float64).astype(k.dtype)
+    if scale:
+        k[inb] = k[inb] * w[b[inb]]
+    else:
+        k[inb] = w[b[inb]]
+    sums = np.bincount(b[inb], weights=k[inb].astype(np.float64), minlength=nb)[:nb]
+    modes = np.bincount(b[inb], minlength=nb)[:nb].astype(np.int64)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        binned = sums / modes
+    binned[0] = (binned[1] + binned[2] + binned[3] + binned[4]) / 4.0
+    return k, binned, modes
+
+
+def konvolve_f64(mesh, kernel, n):
+    """Bam::Konvolve, Source/Bam.cpp:1027-1120, in FP64: c2r(K r2c(in)) / N^3,
+    divided by N^3 / (2 w) with w the sum of K over the half-complex array."""
+    w = np.sum(np.asarray(kernel, np.float64))
+    out = irfft3_f64(rfft3_f64(np.asarray(mesh, np.float64)) * np.asarray(kernel, np.float64), n)
+    return out / (float(n) ** 3 / (2.0 * w))
 
 
 def power_ref(spec_c64, n, L, scheme, nbins, shot_noise, normal, ndel=1.0, fix_octant4=True):

@@ -1,5 +1,6 @@
 // Calls the reference-signature shim the way Bam.cpp / Miscelanious.cpp
-// would: getDensity_CIC, do_fftw_r2c, do_fftw_c2r, EigenValuesTweb.
+// would: getDensity_CIC, do_fftw_r2c, do_fftw_c2r, EigenValuesTweb (both
+// overloads), PoissonSolver, gradfindif.
 // Usage: shim_check <dir>   (reads <dir>/in.bin, writes <dir>/*.bin)
 #include <cstdio>
 #include <string>
@@ -55,5 +56,20 @@ int main(int argc, char **argv)
     if (cam_refapi_last_status()) return 13;
     dump(dir + "/l1.bin", l1.data(), l1.size());
     dump(dir + "/l3.bin", l3.data(), l3.size());
+    // the default build's T-web: the potential, its centred differences and
+    // the eigenvalues of their Hessian (Cwclass::get_CWC, EigenValuesTweb
+    // with _USE_GFINDIFF_EIGENV_)
+    std::vector<real_prec> phi;
+    PoissonSolver(box, N, delta, phi);
+    if (cam_refapi_last_status()) return 14;
+    dump(dir + "/phi.bin", phi.data(), phi.size());
+    std::vector<real_prec> gx;
+    gradfindif(N, N, N, box, box, box, phi, gx, 1);
+    if (cam_refapi_last_status()) return 15;
+    dump(dir + "/gx.bin", gx.data(), gx.size());
+    EigenValuesTweb(N, box, delta, phi, l1, l2, l3);
+    if (cam_refapi_last_status()) return 16;
+    dump(dir + "/fd_l1.bin", l1.data(), l1.size());
+    dump(dir + "/fd_l3.bin", l3.data(), l3.size());
     return 0;
 }

@@ -35,10 +35,13 @@ def test_reference_shim_exports_reference_signatures():
     out = subprocess.run(["nm", "-DC", so], capture_output=True, text=True, check=True).stdout
     names = declared_functions("cam_reference_api.h", "")
     names = {n for n in names if n in ("getDensity_NGP", "getDensity_CIC", "getDensity_TSC", "do_fftw_r2c",
-                                       "do_fftw_c2r", "EigenValuesTweb", "cam_refapi_last_status")}
-    assert len(names) == 7
+                                       "do_fftw_c2r", "EigenValuesTweb", "PoissonSolver", "gradfindif",
+                                       "cam_refapi_last_status")}
+    assert len(names) == 9
     for n in names:
         assert any((" T " + n + "(") in line for line in out.splitlines()), n
+    # both EigenValuesTweb overloads (FFT tensor of delta; FD Hessian of phi)
+    assert sum(1 for line in out.splitlines() if " T EigenValuesTweb(" in line) == 2
 
 
 def test_version_string():

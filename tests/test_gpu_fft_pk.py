@@ -106,3 +106,43 @@ def test_power_deterministic(ctx):
     a = ctx.power(mesh, 1000.0, opts).pk
     b = ctx.power(mesh, 1000.0, opts).pk
     assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
+
+
+# ---------------------------------------------------------------- cross P(k)
+@pytest.mark.parametrize("n,scheme,coeff,prec", [(64, CIC, False, F32), (64, TSC, True, F32), (48, CIC, True, F64)])
+def test_cross_power_vs_oracle(ctx, n, scheme, coeff, prec):
+    # two correlated tracers of one clumped process: the catalogue and a
+    # random half of it, assigned with the same scheme
+    box, nb = 500.0, n // 2
+    x, y, z = synth.clumped(300_000, box, 3_000, 3.0, 0.8, seed=n + scheme)
+    sel = np.random.default_rng(n).random(x.size) < 0.5
+    g = orc.Grid.cubic(n, box)
+    dt = np.float64 if prec == F64 else np.float32
+    mx = orc.assign_f64(scheme, x, y, z, None, g)[0].astype(dt)
+    my = orc.assign_f64(scheme, x[sel], y[sel], z[sel], None, g)[0].astype(dt)
+    got = ctx.cross_power(mx, my, box, Context.pk_opts(scheme, nbins=nb), want_coeff=coeff)
+    ref = orc.cross_power_grid(mx, my, box, scheme, nb, coeff=coeff)
+    assert np.array_equal(got["modes"], ref.modes)
+    has = ref.modes > 0
+    for a, b in ((got["pk"], ref.pk), (got["pk_x"], ref.pk_x), (got["pk_y"], ref.pk_y)):
+        assert np.max(np.abs(a - b)[has] / np.abs(b)[has]) <= 1e-5
+    if coeff:
+        assert np.all(got["pk"][has] <= 1.0 + 1e-6) and np.all(got["pk"][has] > 0.3)
+
+
+def test_cross_power_mixed_inputs_and_mirror(ctx):
+    # X a density, Y an overdensity; and the PowerSpectrumF mirror
+    from cosmicatlas_b200.api import Params, PowerSpectrumF
+    n, box, nb = 32, 300.0, 16
+    x, y, z = synth.clumped(100_000, box, 1_000, 4.0, 0.8, seed=12)
+    m = orc.assign_f64(CIC, x, y, z, None, orc.Grid.cubic(n, box))[0].astype(np.float32)
+    d = (m.astype(np.float64) / m.mean(dtype=np.float64) - 1.0).astype(np.float32)
+    got = ctx.cross_power(m, d, box, Context.pk_opts(CIC, nbins=nb), input_type_y=1)
+    ref = orc.cross_power_grid(m, d, box, CIC, nb, "density", "delta")
+    has = ref.modes > 0
+    assert np.max(np.abs(got["pk"] - ref.pk)[has] / np.abs(ref.pk)[has]) <= 1e-5
+    ps = PowerSpectrumF(Params(Nft=n, Lbox=box, mass_assignment=CIC, Nnp_data=nb, input_type="density_grid",
+                               input_type_two="delta_grid"))
+    ps.compute_cross_power_spectrum_grid(True, m.ravel(), d.ravel(), True)
+    c = orc.cross_power_grid(m, d, box, CIC, nb, "density", "delta", coeff=True)
+    np.testing.assert_allclose(ps.pk0[has], c.pk[has], rtol=1e-5)

@@ -1,6 +1,7 @@
 """The reference-signature shim (libcam_refapi.so) called from C++ the way
-the reference's translation units call getDensity_CIC, do_fftw_r2c/c2r and
-EigenValuesTweb, checked against the oracle."""
+the reference's translation units call getDensity_CIC, do_fftw_r2c/c2r,
+EigenValuesTweb (both overloads), PoissonSolver and gradfindif, checked
+against the oracle."""
 import os
 import struct
 import subprocess
@@ -46,3 +47,17 @@ def test_shim_from_cpp(tmp_path):
     scale = np.abs(tw.lam).max()
     assert np.max(np.abs(l1 - tw.lam[..., 0])) <= 1e-5 * scale
     assert np.max(np.abs(l3 - tw.lam[..., 2])) <= 1e-5 * scale
+    # PoissonSolver, gradfindif and the finite-difference EigenValuesTweb on
+    # the FP32 delta the program formed
+    d32 = delta.astype(np.float32)
+    phi = np.fromfile(tmp_path / "phi.bin", np.float32).reshape(n, n, n)
+    phi_ref = orc.poisson_f64(np.fft.rfftn(d32.astype(np.float64)), n, box)
+    assert np.max(np.abs(phi - phi_ref)) <= 1e-5 * np.abs(phi_ref).max()
+    gx = np.fromfile(tmp_path / "gx.bin", np.float32).reshape(n, n, n)
+    assert np.array_equal(gx, orc.gradfindif_ref_f32(phi, 0, box))
+    fd = orc.tweb_fd_potential(phi.astype(np.float64), box, 0.0)
+    l1 = np.fromfile(tmp_path / "fd_l1.bin", np.float32).reshape(n, n, n)
+    l3 = np.fromfile(tmp_path / "fd_l3.bin", np.float32).reshape(n, n, n)
+    scale = np.abs(fd.lam).max()
+    assert np.max(np.abs(l1 - fd.lam[..., 0])) <= 1e-5 * scale
+    assert np.max(np.abs(l3 - fd.lam[..., 2])) <= 1e-5 * scale

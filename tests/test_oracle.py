@@ -184,3 +184,141 @@ def test_label_truth_table():
     assert labels.tolist() == [1, 2, 3, 4, 4, 2]
     labels, counts, ties = orc.classify(lam[5:], 0.1, 1e-5)
     assert labels.tolist() == [3] and ties == 1
+
+
+# ---------------------------------------------------------------- finite-difference T-web
+def test_gradfindif_known_answer():
+    # gradfindif (Source/NumericalMethods.cpp:1123-1218) of sin(2 pi f x / N)
+    # along each axis: (-f[+2] + 8 f[+1] - 8 f[-1] + f[-2]) / (12 d) gives
+    # (8 sin(t) - sin(2t)) / (6 d) cos(2 pi f x / N), t = 2 pi f / N; the
+    # other axes are untouched.
+    n, box, f = 16, 160.0, 3
+    d = box / n
+    t = 2 * np.pi * f / n
+    x = np.arange(n)
+    wave = np.sin(t * x)
+    amp = (8 * np.sin(t) - np.sin(2 * t)) / (6 * d)
+    for axis in range(3):
+        shape = [1, 1, 1]
+        shape[axis] = n
+        field = np.broadcast_to(wave.reshape(shape), (n, n, n)).copy()
+        want = np.broadcast_to((amp * np.cos(t * x)).reshape(shape), (n, n, n))
+        np.testing.assert_allclose(orc.gradfindif_f64(field, axis, box), want, atol=1e-13)
+    # five-point weights on a single spike: out[x] = (-in[x+2] + 8 in[x+1] - 8 in[x-1] + in[x-2]) / (12 d)
+    spike = np.zeros((n, 1, 1))
+    spike[5] = 1.0
+    g = orc.gradfindif_f64(spike, 0, box)[:, 0, 0] * 12 * d
+    assert np.allclose(g[[3, 4, 6, 7]], [-1.0, 8.0, -8.0, 1.0]) and np.count_nonzero(np.abs(g) > 1e-15) == 4
+
+
+def test_poisson_inverts_laplacian():
+    # PoissonSolver (Source/Miscelanious.cpp:1189-1275): nabla^2 phi = delta for a
+    # zero-mean delta, with the spectral Laplacian -k^2.
+    n, box = 16, 100.0
+    delta = np.random.default_rng(3).normal(size=(n, n, n))
+    delta -= delta.mean()
+    phi = orc.poisson_f64(orc.rfft3_f64(delta), n, box)
+    kf = 2 * np.pi / box
+    f = orc.signed_freq(n)
+    k2 = (f[:, None, None] ** 2 + f[None, :, None] ** 2 + np.arange(n // 2 + 1)[None, None, :] ** 2) * kf * kf
+    np.testing.assert_allclose(orc.irfft3_f64(-k2 * orc.rfft3_f64(phi), n), delta, atol=1e-10)
+
+
+def test_fd_tidal_tensor_is_a_fourier_multiplier():
+    # On a periodic mesh the centred difference is the Fourier multiplier
+    # i s(k), s(k) = (8 sin kd - sin 2kd) / (6 d), so the stencil Hessian of
+    # phi = c2r(-delta_k / k^2) equals c2r(s_a s_b / k^2 delta_k): the form the
+    # GPU T-web computes with its finite-difference method.
+    n, box, R = 24, 300.0, 15.0
+    delta = np.random.default_rng(5).normal(size=(n, n, n))
+    dk = orc.rfft3_f64(delta)
+    t_fd = orc.tidal_fd(orc.poisson_f64(dk, n, box, R), box)
+    kf, d = 2 * np.pi / box, box / n
+    f = orc.signed_freq(n)
+    fz = np.arange(n // 2 + 1, dtype=np.float64)
+    s = lambda fr: (8 * np.sin(fr * kf * d) - np.sin(2 * fr * kf * d)) / (6 * d)
+    sx, sy, sz = s(f)[:, None, None], s(f)[None, :, None], s(fz)[None, None, :]
+    k2 = (f[:, None, None] ** 2 + f[None, :, None] ** 2 + fz[None, None, :] ** 2) * kf * kf
+    with np.errstate(divide="ignore", invalid="ignore"):
+        base = np.where(k2 > 0, dk / k2, 0.0) * np.exp(-0.5 * k2 * R * R)
+    pairs = [(sx, sx), (sy, sy), (sz, sz), (sx, sy), (sx, sz), (sy, sz)]
+    for c, (a, b) in enumerate(pairs):
+        np.testing.assert_allclose(t_fd[..., c], orc.irfft3_f64(base * a * b, n),
+                                   atol=1e-12 * np.abs(t_fd[..., c]).max())
+    # and it differs from the spectral (FFT) tensor by the stencil's truncation error
+    t_fft = orc.tidal_components(dk, n, box, R)
+    assert 0 < np.abs(t_fd - t_fft).max() < 0.2 * np.abs(t_fft).max()
+
+
+def test_gradfindif_as_written_matches_fp64():
+    # the FP32 restatement of the reference's arithmetic agrees with the FP64
+    # stencil to float rounding
+    n, box = 20, 1000.0
+    f = np.random.default_rng(9).normal(size=(n, n, n)).astype(np.float32)
+    for axis in range(3):
+        a = orc.gradfindif_ref_f32(f, axis, box).astype(np.float64)
+        b = orc.gradfindif_f64(f.astype(np.float64), axis, box)
+        assert np.max(np.abs(a - b)) <= 1e-6 * np.abs(b).max()
+
+
+# ---------------------------------------------------------------- BAM kernel
+def test_bam_kernel_bins_follow_float_modulus():
+    # GetKernel's bins (Source/Bam.cpp:829-905) from real_prec arithmetic: the
+    # FP64 floor(|k| / DeltaK) except where |k| / DeltaK sits within float
+    # rounding of an integer; non-decreasing along every row
+    n, box = 32, 700.0
+    for kmin_u, ndel in ((0.0, 1.0), (0.5, 1.5)):
+        b = orc.bam_kernel_bins(n, box, kmin_u, ndel)
+        f = orc.signed_freq(n)
+        q = np.sqrt(f[:, None, None] ** 2 + f[None, :, None] ** 2 + np.arange(n // 2 + 1)[None, None, :] ** 2)
+        x = (q - kmin_u) / ndel
+        exact = np.floor(x).astype(np.int64)
+        near = np.abs(x - np.round(x)) < 1e-5
+        assert np.array_equal(b[~near], exact[~near])
+        assert np.all(np.diff(b, axis=2) >= 0)
+    # the axis modes k = 1..N/2 of unit bins land on their own index or, at a
+    # float rounding below the edge, one lower
+    b = orc.bam_kernel_bins(n, box)
+    assert np.all((b[0, 0, :] == np.arange(n // 2 + 1)) | (b[0, 0, :] == np.arange(n // 2 + 1) - 1))
+
+
+def test_bam_kernel_update_known_answers():
+    n, box, nb = 16, 200.0, 8
+    w = np.linspace(0.5, 2.0, nb)
+    k0 = np.full((n, n, n // 2 + 1), 3.0, np.float32)
+    k1, binned, modes = orc.bam_kernel_update_ref(k0, box, w, scale=False)
+    b = orc.bam_kernel_bins(n, box)
+    inb = b < nb
+    assert np.array_equal(k1[inb], w.astype(np.float32)[b[inb]]) and np.all(k1[~inb] == 3.0)
+    assert modes.sum() == inb.sum()
+    np.testing.assert_allclose(binned[1:], w.astype(np.float32)[1:], rtol=1e-7)
+    assert binned[0] == (binned[1] + binned[2] + binned[3] + binned[4]) / 4.0
+    k2, _, _ = orc.bam_kernel_update_ref(k1, box, w, scale=True)
+    assert np.array_equal(k2[inb], k1[inb] * w.astype(np.float32)[b[inb]])
+
+
+def test_konvolve_with_unit_kernel():
+    # K = 1: c2r(r2c(in)) / N^3 = in, then times 2 w / N^3 with w = N^2 (N/2+1)
+    n = 12
+    m = np.random.default_rng(1).normal(size=(n, n, n))
+    out = orc.konvolve_f64(m, np.ones((n, n, n // 2 + 1)), n)
+    np.testing.assert_allclose(out, m * 2.0 * (n // 2 + 1) / n, rtol=0, atol=1e-12 * np.abs(m).max())
+
+
+# ---------------------------------------------------------------- cross P(k)
+def test_cross_power_of_a_field_with_itself():
+    # X = Y: the cross spectrum is the auto spectrum without shot noise, and
+    # the coefficient is 1 in every bin with modes
+    n, box = 16, 300.0
+    m = np.random.default_rng(4).uniform(0.5, 1.5, size=(n, n, n))
+    x = orc.cross_power_grid(m, m, box, orc.CIC, 8)
+    auto = orc.power_grid(m, box, orc.CIC, 8, sn_corr=False)
+    # the auto spectrum of rho - mean normalised by N_gal^2/V equals that of rho/mean - 1 by N^6/V
+    np.testing.assert_allclose(x.pk, auto.pk, rtol=1e-12)
+    np.testing.assert_allclose(x.pk_x, x.pk_y, rtol=1e-12)
+    c = orc.cross_power_grid(m, m, box, orc.CIC, 8, coeff=True)
+    has = c.modes > 0
+    np.testing.assert_allclose(c.pk[has], 1.0, rtol=1e-12)
+    # -X anticorrelates: coefficient -1
+    c = orc.cross_power_grid(m - 1.0, 1.0 - m, box, orc.CIC, 8, "delta", "delta", coeff=True)
+    np.testing.assert_allclose(c.pk[has], -1.0, rtol=1e-12)
