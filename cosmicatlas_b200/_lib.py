@@ -126,10 +126,14 @@ SIGNATURES = {
                     ctypes.c_int),
     "cam_gradfindif": ([_P, ctypes.POINTER(Grid), _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, ctypes.c_int],
                        ctypes.c_int),
+    "cam_fkp_weights": ([_P, ctypes.c_int64, _P, ctypes.c_double, _P, ctypes.c_int, ctypes.c_double, ctypes.c_int, _P,
+                         ctypes.c_int, _P], ctypes.c_int),
     "cam_bam_kernel_update": ([_P, ctypes.POINTER(Grid), ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                _P, ctypes.c_int, _P, ctypes.c_int, _P, _P], ctypes.c_int),
     "cam_konvolve": ([_P, ctypes.POINTER(Grid), _P, ctypes.c_int, ctypes.c_int, _P, ctypes.c_int, _P, ctypes.c_int],
                      ctypes.c_int),
+    "cam_tweb_invariants": ([_P, ctypes.POINTER(Grid), _P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(TwebOpts), _P,
+                             _P, _P, ctypes.c_int, ctypes.POINTER(TwebStats)], ctypes.c_int),
     "cam_job_run": ([_P, ctypes.POINTER(JobDesc), ctypes.POINTER(JobResult)], ctypes.c_int),
     "cam_particles_stage": ([_P, ctypes.POINTER(Particles), ctypes.POINTER(Particles)], ctypes.c_int),
     "cam_power_noalloc": ([_P, ctypes.c_int64, ctypes.c_int, ctypes.c_float, ctypes.c_double,

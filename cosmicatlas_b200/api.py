@@ -256,6 +256,24 @@ class Context:
         o.smoothing_R, o.lambda_th, o.tie_band, o.input_type, o.method = R, lambda_th, tie_band, input_type, method
         return o
 
+    def tweb_invariants(self, mesh, box: float, opts: L.TwebOpts):
+        """cam_tweb_invariants: (labels, lambdas, invariants) with invariants
+        (4, N, N, N) = I, II, III and the tidal anisotropy per cell."""
+        dev = L.is_device(mesh)
+        n = mesh.shape[0]
+        prec = F64 if str(mesh.dtype).endswith("float64") else F32
+        if not dev:
+            mesh = np.ascontiguousarray(mesh)
+        labels = self._empty((n, n, n), np.uint8, dev, mesh)
+        lam = self._empty((3, n, n, n), np.float32, dev, mesh)
+        inv = self._empty((4, n, n, n), np.float32, dev, mesh)
+        st = L.TwebStats()
+        g = make_grid(n, box)
+        m = L.MEM_DEVICE if dev else L.MEM_HOST
+        self._check(self._lib.cam_tweb_invariants(self.h, ctypes.byref(g), L.ptr(mesh), prec, m, ctypes.byref(opts),
+                                                  L.ptr(labels), L.ptr(lam), L.ptr(inv), m, ctypes.byref(st)))
+        return labels, lam, inv
+
     def tweb(self, mesh, box: float, opts: L.TwebOpts, want_lambdas=False) -> TwebResult:
         dev = L.is_device(mesh)
         n = mesh.shape[0]
@@ -301,6 +319,22 @@ class Context:
         m = L.MEM_DEVICE if dev else L.MEM_HOST
         self._check(self._lib.cam_gradfindif(self.h, ctypes.byref(g), L.ptr(field), prec, m, dim, L.ptr(out), m))
         return out
+
+    # ---------------------------------------------------------------- catalogue
+    def fkp_weights(self, n, nbar=None, nbar_const=0.0, w_in=None, fkp=True, P_est=0.0):
+        """cam_fkp_weights: per-object weights w_in / (1 + P_est nbar) and the sums
+        (n_selected, W_r, S_r, normal) of Catalog.cpp:14120-14190.  Arrays on the
+        host or the device (all alike); returns (weights, sums)."""
+        arrs = [a for a in (nbar, w_in) if a is not None]
+        dev = bool(arrs) and L.is_device(arrs[0])
+        nbar = nbar if (nbar is None or dev) else np.ascontiguousarray(nbar, np.float32)
+        w_in = w_in if (w_in is None or dev) else np.ascontiguousarray(w_in, np.float32)
+        out = self._empty((int(n),), np.float32, dev, arrs[0] if dev else None)
+        sums = np.zeros(4)
+        m = L.MEM_DEVICE if dev else L.MEM_HOST
+        self._check(self._lib.cam_fkp_weights(self.h, int(n), L.ptr(nbar), float(nbar_const), L.ptr(w_in), int(fkp),
+                                              float(P_est), m, L.ptr(out), m, L.ptr(sums)))
+        return out, sums
 
     # ---------------------------------------------------------------- BAM kernel
     def bam_kernel_update(self, kernel, box: float, weight, mode=L.KERNEL_SET, DeltaKmin=0.0, ndel=1.0):
@@ -571,6 +605,36 @@ def do_fftw_c2r(Nft, data_in, data_out):
     data_out[...] = res.reshape(data_out.shape)
 
 
+def write_array(fname, data):
+    """FileOutput::write_array, Source/FileOutput.cpp:858-912: the mesh as raw
+    native-endian float32 (no header) into fname + ".dat"."""
+    a = data.detach().cpu().numpy() if hasattr(data, "detach") else np.asarray(data)
+    np.ascontiguousarray(a, np.float32).tofile(fname + ".dat")
+
+
+def read_array(fname, out):
+    """FileOutput::read_array, Source/FileOutput.cpp:727-752: out.size raw
+    float32 values from fname (the name as given), into out."""
+    a = np.fromfile(fname, np.float32, count=out.size)
+    if a.size != out.size:
+        raise CamError(L.CAM_E_INVAL, f"{fname}: {a.size} values, {out.size} expected")
+    out.reshape(-1)[...] = a
+    return out
+
+
+def get_interpolated_density_field(x, y, z, grid: L.Grid, scheme: int, nbar=None, nbar_const=0.0, weights=None,
+                                   fkp=True, P_est=0.0, precision=F32):
+    """The catalogue's tracer loop, Source/Catalog.cpp:14104-14240: each object
+    weighted by its other weights times the FKP weight 1 / (1 + P_est nbar),
+    assigned with `scheme`; returns (mesh, sums) with sums = (n_selected, W_r,
+    S_r, normal_power).  The assignment is the deterministic one of
+    getDensity_* (the reference's OpenMP loop races on the mesh)."""
+    ctx = default_context()
+    w, sums = ctx.fkp_weights(len(x), nbar, nbar_const, weights, fkp, P_est)
+    res = ctx.assign(x, y, z, w, grid, scheme, precision)
+    return res.mesh, sums
+
+
 def PoissonSolver(Lbox, Nft, data_in, data_out):
     """Source/Miscelanious.cpp:1189 -- the potential of ``data_in`` into ``data_out``."""
     res = default_context().poisson(data_in.reshape(Nft, Nft, Nft), Lbox)
@@ -775,6 +839,19 @@ class Bam:
         n = p.Nft
         res = default_context(p.device).konvolve(data_in.reshape(n, n, n), p.Lbox, self.Kernel)
         data_out[...] = res.reshape(data_out.shape)
+
+    def get_invariants(self, delta):
+        """get_CWC plus the invariant fields of the tidal tensor that BAM's
+        bias binning uses (invariant_field_I/II/III, tidal_anisotropy,
+        Source/Miscelanious.cpp:1460-1492), as members I, II, III, tidal."""
+        p = self.params
+        it = L.INPUT_DELTA if p.input_type == "delta_grid" else L.INPUT_DENSITY
+        method = {"fft": L.TWEB_FFT, "fd": L.TWEB_FD}[p.tweb_method]
+        o = Context.tweb_opts(p.smoothing_R, p.lambdath, p.tie_band, it, method)
+        labels, lam, inv = default_context(p.device).tweb_invariants(delta.reshape(p.Nft, p.Nft, p.Nft), p.Lbox, o)
+        self.CWClass = labels.reshape(-1)
+        self.lambda1, self.lambda2, self.lambda3 = (lam[a].reshape(-1) for a in range(3))
+        self.I, self.II, self.III, self.tidal = (inv[a].reshape(-1) for a in range(4))
 
     def get_Tclassification(self, ig):
         return int(self.CWClass[ig])

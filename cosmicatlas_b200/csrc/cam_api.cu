@@ -162,17 +162,44 @@ void release_all(cam_ctx *ctx)
 
 namespace {
 
-constexpr int kRedBlocks = 2 * kNumSMs;
+constexpr int kRedBlocks = 8 * kNumSMs;
 
 template <typename T>
 __global__ void __launch_bounds__(256) partial_sum_kernel(const T *__restrict__ in, int64_t n, double *__restrict__ part)
 {
     __shared__ double red[8];
-    // Static contiguous chunk per CTA: the summation order is fixed.
-    const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
-    const int64_t beg = (int64_t)blockIdx.x * chunk, end = min(n, beg + chunk);
-    double acc = 0.0;
-    for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) acc += (double)in[i];
+    // Static contiguous chunk per CTA, a multiple of 4 elements: the
+    // summation order is fixed.  16-byte loads when the array is 16-byte
+    // aligned, four (float) or two (double) independent accumulators.
+    const int64_t chunk = (((n + gridDim.x - 1) / gridDim.x) + 3) & ~(int64_t)3;
+    const int64_t beg = min(n, (int64_t)blockIdx.x * chunk), end = min(n, beg + chunk);
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    int64_t tail = beg;
+    if ((reinterpret_cast<uintptr_t>(in) & 15) == 0) {
+        if constexpr (sizeof(T) == 4) {
+            const int64_t nv = (end - beg) / 4;
+            const float4 *v = reinterpret_cast<const float4 *>(in + beg);
+            for (int64_t i = threadIdx.x; i < nv; i += blockDim.x) {
+                const float4 f = __ldg(v + i);
+                a0 += (double)f.x;
+                a1 += (double)f.y;
+                a2 += (double)f.z;
+                a3 += (double)f.w;
+            }
+            tail = beg + 4 * nv;
+        } else {
+            const int64_t nv = (end - beg) / 2;
+            const double2 *v = reinterpret_cast<const double2 *>(in + beg);
+            for (int64_t i = threadIdx.x; i < nv; i += blockDim.x) {
+                const double2 f = __ldg(v + i);
+                a0 += f.x;
+                a1 += f.y;
+            }
+            tail = beg + 2 * nv;
+        }
+    }
+    for (int64_t i = tail + threadIdx.x; i < end; i += blockDim.x) a0 += (double)in[i];
+    double acc = (a0 + a1) + (a2 + a3);
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
@@ -648,6 +675,13 @@ int cam_power(cam_ctx *ctx, const cam_grid *grid, const void *mesh, int precisio
 int cam_tweb(cam_ctx *ctx, const cam_grid *grid, const void *mesh, int precision, int mem,
              const cam_tweb_opts *opts, uint8_t *labels, float *lambdas, int out_mem, cam_tweb_stats *stats)
 {
+    return cam_tweb_invariants(ctx, grid, mesh, precision, mem, opts, labels, lambdas, nullptr, out_mem, stats);
+}
+
+int cam_tweb_invariants(cam_ctx *ctx, const cam_grid *grid, const void *mesh, int precision, int mem,
+                        const cam_tweb_opts *opts, uint8_t *labels, float *lambdas, float *invariants, int out_mem,
+                        cam_tweb_stats *stats)
+{
     return guarded(ctx, [&] {
         check_grid_cubic(grid);
         CAM_REQUIRE(mesh && opts, CAM_E_INVAL, "null mesh or options");
@@ -672,11 +706,16 @@ int cam_tweb(cam_ctx *ctx, const cam_grid *grid, const void *mesh, int precision
         fft_r2c_split(ctx, plan, dm, sub, s);
         uint8_t *dl = labels ? (out_mem == CAM_MEM_DEVICE ? labels : static_cast<uint8_t *>(scratch(ctx, "tw.labels", ncell))) : nullptr;
         float *dlam = lambdas ? (out_mem == CAM_MEM_DEVICE ? lambdas : static_cast<float *>(scratch(ctx, "tw.lam", 3 * ncell * 4))) : nullptr;
+        float *dinv = invariants ? (out_mem == CAM_MEM_DEVICE ? invariants
+                                                              : static_cast<float *>(scratch(ctx, "tw.inv", 4 * ncell * 4)))
+                                 : nullptr;
         cam_tweb_stats st{};
-        tweb_device(ctx, plan, s, grid->L[0], sub, opts->input_type, *opts, dl, dlam, &st);
+        tweb_device(ctx, plan, s, grid->L[0], sub, opts->input_type, *opts, dl, dlam, &st, dinv);
         if (out_mem == CAM_MEM_HOST) {
             if (labels) CAM_CUDA_TRY(cudaMemcpyAsync(labels, dl, ncell, cudaMemcpyDeviceToHost, ctx->stream));
             if (lambdas) CAM_CUDA_TRY(cudaMemcpyAsync(lambdas, dlam, 3 * ncell * 4, cudaMemcpyDeviceToHost, ctx->stream));
+            if (invariants)
+                CAM_CUDA_TRY(cudaMemcpyAsync(invariants, dinv, 4 * ncell * 4, cudaMemcpyDeviceToHost, ctx->stream));
         }
         CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
         if (stats) *stats = st;
@@ -803,6 +842,35 @@ int cam_gradfindif(cam_ctx *ctx, const cam_grid *grid, const void *in, int preci
         gradfindif_device(ctx, din, dout, n, grid->L[0], dim, precision);
         if (out_mem == CAM_MEM_HOST) CAM_CUDA_TRY(cudaMemcpyAsync(out, dout, bytes, cudaMemcpyDeviceToHost, ctx->stream));
         CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+int cam_fkp_weights(cam_ctx *ctx, int64_t n, const float *nbar, double nbar_const, const float *w_in, int fkp,
+                    double P_est, int mem, float *w_out, int out_mem, double *sums)
+{
+    return guarded(ctx, [&] {
+        CAM_REQUIRE(n >= 0 && w_out, CAM_E_INVAL, "invalid object count or null output");
+        check_mem(mem);
+        check_mem(out_mem);
+        CAM_REQUIRE(std::isfinite(nbar_const) && std::isfinite(P_est), CAM_E_INVAL, "non-finite nbar or P_est");
+        const float *dn = stage_in(ctx, "fkp.nbar", nbar, (size_t)n, mem);
+        const float *dw = stage_in(ctx, "fkp.win", w_in, (size_t)n, mem);
+        float *dout = out_mem == CAM_MEM_DEVICE
+                          ? w_out
+                          : static_cast<float *>(scratch(ctx, "fkp.wout", std::max<size_t>(1, (size_t)n) * sizeof(float)));
+        auto *dsum = static_cast<double *>(scratch(ctx, "fkp.sums", 3 * sizeof(double)));
+        fkp_weights_device(ctx, n, dn, nbar_const, dw, fkp, P_est, dout, dsum);
+        if (out_mem == CAM_MEM_HOST && n > 0)
+            CAM_CUDA_TRY(cudaMemcpyAsync(w_out, dout, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+        double h[3] = {0.0, 0.0, 0.0};
+        CAM_CUDA_TRY(cudaMemcpyAsync(h, dsum, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+        CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        if (sums) {
+            sums[0] = (double)n;
+            sums[1] = h[0];
+            sums[2] = h[1];
+            sums[3] = h[2];
+        }
     });
 }
 

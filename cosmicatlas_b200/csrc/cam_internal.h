@@ -205,15 +205,21 @@ void power_bin(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins,
                double *h_sum_raw, double *h_sum_sn, int64_t *h_modes);
 
 // ------------------------------------------------------ T-web
+// d_inv (may be null): 4 planes of N^3 floats, the tidal invariants I, II,
+// III and the anisotropy per cell.
 void tweb_device(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const double *d_mean,
                  int input_type, const cam_tweb_opts &o, uint8_t *d_labels, float *d_lambdas,
-                 cam_tweb_stats *stats);
+                 cam_tweb_stats *stats, float *d_inv = nullptr);
 
 // PoissonSolver's multiplier -1/k^2 (times exp(-k^2 R^2 / 2) if R > 0) on a
 // split spectrum, in place (cam_fd.cu).
 void poisson_device(cam_ctx *ctx, Spectrum &s, float L, float R);
 // gradfindif along dim (1 = x, 2 = y, 3 = z) of a real N^3 mesh; in != out.
 void gradfindif_device(cam_ctx *ctx, const void *in, void *out, int64_t n, float L, int dim, int precision);
+
+// FKP object weights and their sums (cam_fkp.cu): d_sums [3] = W_r, S_r, normal.
+void fkp_weights_device(cam_ctx *ctx, int64_t n, const float *nbar, double nbar_const, const float *w_in, int fkp,
+                        double pest, float *w_out, double *d_sums);
 
 // BAM kernel (cam_bamkernel.cu): the 3D update of GetKernel on a device
 // half-complex kernel array, bin sums and counts left in d_sum / d_modes

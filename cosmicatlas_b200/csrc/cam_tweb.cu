@@ -64,16 +64,17 @@ __host__ __device__ constexpr int slot_of(int p, int q)
 // Frequency factor of one axis in units of k_f, for signed frequency f and
 // power e = 0, 1, 2: f^e for the FFT tidal tensor; for the finite-difference
 // one (FD), s(f)^e with s the Fourier multiplier of the centred difference,
-// tabulated at sf[f + N/2] (fd_table_kernel).
+// tabulated as {s, s^2} (each rounded once from FP64) at sf[f + N/2]
+// (fd_table_kernel).
 template <typename T, bool FD>
-__device__ __forceinline__ T kfac(const double *__restrict__ sf, int h, int f, int e)
+__device__ __forceinline__ T kfac(const typename CTw<T>::t *__restrict__ sf, int h, int f, int e)
 {
     if constexpr (!FD) {
         return (T)ipow(f, e);
     } else {
         if (e == 0) return (T)1;
-        const double s = __ldg(sf + f + h);
-        return (T)(e == 1 ? s : s * s);
+        const typename CTw<T>::t s = __ldg(sf + f + h);
+        return e == 1 ? s.x : s.y;
     }
 }
 
@@ -105,7 +106,7 @@ constexpr int col_min_blocks()
 // has the multiplier -s_a s_b.
 template <typename T, bool FD = false>
 __device__ __forceinline__ T phi_mult(int p, int fi, int fj, int fk, T gauss_coef, T norm,
-                                      const double *__restrict__ sf = nullptr, int h = 0, int pot = 0)
+                                      const typename CTw<T>::t *__restrict__ sf = nullptr, int h = 0, int pot = 0)
 {
     const int q = fi * fi + fj * fj + fk * fk;
     if (q == 0) return (T)0;
@@ -130,7 +131,7 @@ __global__ void __launch_bounds__(col_threads<T, LEN>(), col_min_blocks<T, LEN>(
 tidal_x_kernel(const typename CTw<T>::t *__restrict__ src, typename CTw<T>::t *__restrict__ dst,
                int n, int ncols, int64_t jstride, int64_t pstride, int64_t ccomp, Radices rd,
                const typename CTw<T>::t *__restrict__ tw, double gauss_coef, const double *__restrict__ d_mean,
-               int density_input, double scale, const double *__restrict__ sf, int pot)
+               int density_input, double scale, const typename CTw<T>::t *__restrict__ sf, int pot)
 {
     using C = typename CTw<T>::t;
     constexpr int W = CTw<T>::kCols;
@@ -186,7 +187,7 @@ template <typename T, int LEN, bool FD>
 __global__ void __launch_bounds__(col_threads<T, LEN>(), col_min_blocks<T, LEN>())
 tidal_y_kernel(typename CTw<T>::t *__restrict__ base, int n, int ncols, int64_t jstride, int64_t cstride,
                int64_t pstride, int64_t ccomp, Radices rd, const typename CTw<T>::t *__restrict__ tw, int kz_fixed,
-               const double *__restrict__ sf)
+               const typename CTw<T>::t *__restrict__ sf)
 {
     using C = typename CTw<T>::t;
     constexpr int W = CTw<T>::kCols;
@@ -256,7 +257,7 @@ __global__ void __launch_bounds__(col_threads<T, LEN>(), tpipe_min_blocks<T, LEN
 tidal_pipe_kernel(const typename CTw<T>::t *src, typename CTw<T>::t *dst, int n, int nct, int64_t nunits,
                   int64_t jstride, int64_t pstride, int64_t ccomp, const typename CTw<T>::t *__restrict__ tw,
                   double gauss_coef, const double *__restrict__ d_mean, int density_input, double scale,
-                  const double *__restrict__ sf, int pot)
+                  const typename CTw<T>::t *__restrict__ sf, int pot)
 {
     using C = typename CTw<T>::t;
     constexpr int W = CTw<T>::kCols;
@@ -451,13 +452,14 @@ __device__ __forceinline__ int count_above(double c2, double c1, double c0, doub
 }
 
 // Label of one cell from its six field values (slots 0..5 of t6), written
-// to labels[cell] (and lambdas when LAMBDAS); the label and tie counters
-// of the calling thread are advanced.
+// to labels[cell] (and lambdas when LAMBDAS, and the invariants when
+// LAMBDAS and inv != nullptr); the label and tie counters of the calling
+// thread are advanced.
 template <bool LAMBDAS>
 __device__ __forceinline__ void label_cell(const float t6[6], double lth, double band, int64_t cell, int64_t ncell,
                                            uint8_t *__restrict__ labels, float *__restrict__ lambdas,
-                                           unsigned &lc0, unsigned &lc1, unsigned &lc2, unsigned &lc3,
-                                           unsigned &lties)
+                                           float *__restrict__ inv, unsigned &lc0, unsigned &lc1, unsigned &lc2,
+                                           unsigned &lc3, unsigned &lties)
 {
     // (xx, yy, zz, xy, xz, yz) from slots (2, 4, 0, 5, 1, 3)
     int v = 0, tie = 0;
@@ -472,6 +474,23 @@ __device__ __forceinline__ void label_cell(const float t6[6], double lth, double
         lambdas[cell] = (float)lam[0];
         lambdas[ncell + cell] = (float)lam[1];
         lambdas[2 * ncell + cell] = (float)lam[2];
+        if (inv) {
+            // invariant_field_I/II/III and tidal_anisotropy, Source/Miscelanious.cpp:1460-1492:
+            // I = l1 + l2 + l3, II = l1 l2 + l2 l3 + l1 l3, III = l1 l2 l3 are the
+            // characteristic polynomial's coefficients (FP64 from the tensor);
+            // ((l3-l1)^2 + (l3-l2)^2 + (l2-l1)^2) / 2 = I^2 - 3 II = 3/2 tr(B^2), B
+            // the traceless part of T: a sum of squares, free of cancellation
+            double c2, c1, c0;
+            char_poly(t6[2], t6[4], t6[0], t6[5], t6[1], t6[3], c2, c1, c0);
+            const double q = c2 * (1.0 / 3.0);
+            const double bxx = (double)t6[2] - q, byy = (double)t6[4] - q, bzz = (double)t6[0] - q;
+            const double o2 = (double)t6[5] * t6[5] + (double)t6[1] * t6[1] + (double)t6[3] * t6[3];
+            const double trb2 = bxx * bxx + byy * byy + bzz * bzz + 2.0 * o2;
+            inv[cell] = (float)c2;
+            inv[ncell + cell] = (float)c1;
+            inv[2 * ncell + cell] = (float)c0;
+            inv[3 * ncell + cell] = (float)(sqrt(1.5 * trb2) / (2.0 + c2));
+        }
     } else {
         double c2, c1, c0, a2, a1, a0;
         char_poly(t6[2], t6[4], t6[0], t6[5], t6[1], t6[3], c2, c1, c0);
@@ -517,7 +536,7 @@ __global__ void __launch_bounds__(256, 2)
 tidal_z_kernel(const typename CTw<T>::t *__restrict__ src, const typename CTw<T>::t *__restrict__ nyq,
                int n, int64_t nrows, int rpc, int64_t ccomp, Radices rd,
                const typename CTw<T>::t *__restrict__ tw, double lth, double band,
-               uint8_t *__restrict__ labels, float *__restrict__ lambdas,
+               uint8_t *__restrict__ labels, float *__restrict__ lambdas, float *__restrict__ inv,
                unsigned long long *__restrict__ counts /* [5] */)
 {
     using C = typename CTw<T>::t;
@@ -574,7 +593,8 @@ tidal_z_kernel(const typename CTw<T>::t *__restrict__ src, const typename CTw<T>
 #pragma unroll
         for (int c = 0; c < 6; ++c)
             t6[c] = (float)re[2 * fftdev::sidx<PAD>((c * rpcv + r) * M + (z >> 1)) + (z & 1)];
-        label_cell<LAMBDAS>(t6, lth, band, (row0 + r) * nz + z, ncell, labels, lambdas, lc0, lc1, lc2, lc3, lties);
+        label_cell<LAMBDAS>(t6, lth, band, (row0 + r) * nz + z, ncell, labels, lambdas, inv, lc0, lc1, lc2, lc3,
+                            lties);
     }
     flush_counts(lc0, lc1, lc2, lc3, lties, cnt_s, counts);
 }
@@ -614,7 +634,7 @@ template <typename T, int LEN, bool LAMBDAS>
 __global__ void __launch_bounds__(zpipe_threads<T, LEN>(), zpipe_min_blocks<T, LEN>())
 tidal_z_pipe_kernel(const typename CTw<T>::t *__restrict__ src, const typename CTw<T>::t *__restrict__ nyq, int n,
                     int64_t nrows, int64_t ccomp, const typename CTw<T>::t *__restrict__ tw, double lth, double band,
-                    uint8_t *__restrict__ labels, float *__restrict__ lambdas,
+                    uint8_t *__restrict__ labels, float *__restrict__ lambdas, float *__restrict__ inv,
                     unsigned long long *__restrict__ counts /* [5] */)
 {
     using C = typename CTw<T>::t;
@@ -695,8 +715,8 @@ tidal_z_pipe_kernel(const typename CTw<T>::t *__restrict__ src, const typename C
                 tb[c] = (float)v.y;
             }
             const int64_t cell = (row0 + r) * 2 * M + 2 * m;
-            label_cell<LAMBDAS>(ta, lth, band, cell, ncell, labels, lambdas, lc0, lc1, lc2, lc3, lties);
-            label_cell<LAMBDAS>(tb, lth, band, cell + 1, ncell, labels, lambdas, lc0, lc1, lc2, lc3, lties);
+            label_cell<LAMBDAS>(ta, lth, band, cell, ncell, labels, lambdas, inv, lc0, lc1, lc2, lc3, lties);
+            label_cell<LAMBDAS>(tb, lth, band, cell + 1, ncell, labels, lambdas, inv, lc0, lc1, lc2, lc3, lties);
         }
         __syncthreads();  // tile is refilled next
     }
@@ -710,12 +730,15 @@ tidal_z_pipe_kernel(const typename CTw<T>::t *__restrict__ src, const typename C
 // D e^{ikx} = i s(k) e^{ikx},  s(k) = (8 sin kd - sin 2kd) / (6 d).
 // With k = k_f f and k_f d = 2 pi / N:  s / k_f = N (8 sin t - sin 2t) / (12 pi),
 // t = 2 pi f / N.  s(0) = s(+-N/2) = 0.
-__global__ void fd_table_kernel(double *__restrict__ sf, int n)
+// Stored as {s, s^2} in the transform's precision.
+template <typename T>
+__global__ void fd_table_kernel(typename CTw<T>::t *__restrict__ sf, int n)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i > n) return;
     const double t = 2.0 * (double)(i - n / 2) / (double)n;  // sinpi(t) = sin(2 pi f / N)
-    sf[i] = (double)n * (8.0 * sinpi(t) - sinpi(2.0 * t)) / (12.0 * M_PI);
+    const double v = (double)n * (8.0 * sinpi(t) - sinpi(2.0 * t)) / (12.0 * M_PI);
+    sf[i] = typename CTw<T>::t{(T)v, (T)(v * v)};
 }
 
 int threads_for(int points, int ppt, int cap)
@@ -731,7 +754,8 @@ int threads_for(int points, int ppt, int cap)
 template <typename T, int MODE, int LEN, bool FD>
 bool pipe_launch(cam_ctx *ctx, const char *name, const typename CTw<T>::t *src, typename CTw<T>::t *dst, int64_t n,
                  int64_t M, int64_t jstride, int64_t pstride, int64_t ccomp, const typename CTw<T>::t *tw,
-                 double gcoef, const double *d_mean, int density, double scale, const double *sf, int pot)
+                 double gcoef, const double *d_mean, int density, double scale, const typename CTw<T>::t *sf,
+                 int pot)
 {
     using C = typename CTw<T>::t;
     constexpr int W = CTw<T>::kCols;
@@ -760,7 +784,7 @@ bool pipe_launch(cam_ctx *ctx, const char *name, const typename CTw<T>::t *src, 
 template <typename T>
 void tweb_impl(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const double *d_mean,
                int input_type, const cam_tweb_opts &o, uint8_t *d_labels, float *d_lambdas,
-               cam_tweb_stats *stats)
+               cam_tweb_stats *stats, float *d_inv)
 {
     using C = typename CTw<T>::t;
     constexpr int W = CTw<T>::kCols;
@@ -781,10 +805,11 @@ void tweb_impl(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const d
     const int pot = input_type == CAM_INPUT_POTENTIAL;
     // c2r divides by N^3; a potential input carries the k_f^2 of -k_a k_b
     const double scale = (pot ? kf * kf : 1.0) / ((double)n * (double)n * (double)n);
-    const double *sf = nullptr;
+    const C *sf = nullptr;
     if (o.method == CAM_TWEB_FD) {
-        auto *t = static_cast<double *>(scratch(ctx, "tw.sfac", (size_t)(n + 1) * sizeof(double)));
-        CAM_LAUNCH(ctx, fd_table_kernel, (unsigned)((n + 1 + 127) / 128), 128, 0, t, (int)n);
+        auto *t = static_cast<C *>(scratch(ctx, "tw.sfac", (size_t)(n + 1) * sizeof(C)));
+        CAM_LAUNCH_NAMED(ctx, "fd_table_kernel", fd_table_kernel<T>, (unsigned)((n + 1 + 127) / 128), 128, 0, t,
+                         (int)n);
         sf = t;
     }
     auto passes = [&](auto fdc) {
@@ -857,14 +882,14 @@ void tweb_impl(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const d
             const int64_t ngroups = (nn + tweb_rpc<T>(LEN) - 1) / tweb_rpc<T>(LEN);
             const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ngroups, (int64_t)kNumSMs * std::max(per_sm, 1)));
             CAM_LAUNCH_NAMED(ctx, "tweb_tidal_z_eigen", kp, g, pthr, psmem, cm, cn, (int)n, nn, ccomp, tw, o.lambda_th,
-                             o.tie_band, d_labels, d_lambdas, cnt);
+                             o.tie_band, d_labels, d_lambdas, d_inv, cnt);
             return;
         }
         auto kz = d_lambdas ? tidal_z_kernel<T, LEN, true> : tidal_z_kernel<T, LEN, false>;
         smem_at_least(kz, smem);
         const unsigned grid = (unsigned)((nn + rpc - 1) / rpc);
         CAM_LAUNCH_NAMED(ctx, "tweb_tidal_z_eigen", kz, grid, nthr, smem, cm, cn, (int)n, nn, rpc, ccomp, rm, tw, o.lambda_th,
-                   o.tie_band, d_labels, d_lambdas, cnt);
+                   o.tie_band, d_labels, d_lambdas, d_inv, cnt);
         });
     }
     if (stats) {
@@ -883,7 +908,7 @@ void tweb_impl(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const d
 
 void tweb_device(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const double *d_mean,
                  int input_type, const cam_tweb_opts &o, uint8_t *d_labels, float *d_lambdas,
-                 cam_tweb_stats *stats)
+                 cam_tweb_stats *stats, float *d_inv)
 {
     CAM_REQUIRE(std::isfinite(o.lambda_th) && o.tie_band >= 0.0, CAM_E_INVAL, "invalid T-web threshold");
     CAM_REQUIRE(o.smoothing_R >= 0.f && std::isfinite(o.smoothing_R), CAM_E_INVAL, "invalid smoothing radius");
@@ -892,8 +917,15 @@ void tweb_device(cam_ctx *ctx, FftPlan *plan, const Spectrum &dk, float L, const
                     (input_type == CAM_INPUT_POTENTIAL && o.method == CAM_TWEB_FD),
                 CAM_E_INVAL, "T-web input must be a density or delta mesh (or a potential, finite differences only)");
     CAM_REQUIRE(input_type != CAM_INPUT_DENSITY || d_mean, CAM_E_INVAL, "density input needs the mean");
-    if (dk.precision == CAM_F32) tweb_impl<float>(ctx, plan, dk, L, d_mean, input_type, o, d_labels, d_lambdas, stats);
-    else tweb_impl<double>(ctx, plan, dk, L, d_mean, input_type, o, d_labels, d_lambdas, stats);
+    // the invariants are formed in the eigenvalue path, which needs lambda planes
+    if (d_inv && !d_lambdas) {
+        const int64_t ncell = dk.n * dk.n * dk.n;
+        d_lambdas = static_cast<float *>(scratch(ctx, "tw.lam", (size_t)3 * ncell * sizeof(float)));
+    }
+    if (dk.precision == CAM_F32)
+        tweb_impl<float>(ctx, plan, dk, L, d_mean, input_type, o, d_labels, d_lambdas, stats, d_inv);
+    else
+        tweb_impl<double>(ctx, plan, dk, L, d_mean, input_type, o, d_labels, d_lambdas, stats, d_inv);
 }
 
 }  // namespace cam

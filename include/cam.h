@@ -212,6 +212,16 @@ int cam_tweb(cam_ctx *ctx, const cam_grid *grid, const void *mesh, int precision
              int mem, const cam_tweb_opts *opts, uint8_t *labels, float *lambdas,
              int out_mem, cam_tweb_stats *stats);
 
+/* cam_tweb plus the tidal invariants BAM's bias binning reads, per cell:
+ * invariants = 4 planes of N^3 floats, I = l1 + l2 + l3, II = l1 l2 + l2 l3
+ * + l1 l3, III = l1 l2 l3 (invariant_field_I/II/III,
+ * Source/Miscelanious.cpp:1466-1492) and the tidal anisotropy
+ * sqrt(((l3-l1)^2 + (l3-l2)^2 + (l2-l1)^2) / 2) / (2 + I) (tidal_anisotropy,
+ * :1460), formed in FP64 from the tensor.  labels and lambdas may be NULL. */
+int cam_tweb_invariants(cam_ctx *ctx, const cam_grid *grid, const void *mesh, int precision, int mem,
+                        const cam_tweb_opts *opts, uint8_t *labels, float *lambdas, float *invariants,
+                        int out_mem, cam_tweb_stats *stats);
+
 /* ---- potential and finite differences --------------------------------
  * Replaces PoissonSolver(Lbox, Nft, in, out), Source/Miscelanious.cpp:1189:
  * phi = c2r(-delta_k / k^2) / N^3 (k = 0 mode -> 0), with k from the
@@ -228,6 +238,19 @@ int cam_poisson(cam_ctx *ctx, const cam_grid *grid, const void *delta, int preci
  * equal out (the reference takes `in` by value). */
 int cam_gradfindif(cam_ctx *ctx, const cam_grid *grid, const void *in, int precision, int mem, int dim,
                    void *out, int out_mem);
+
+/* ---- catalogue weights -------------------------------------------------
+ * The per-object weights of the catalogue interpolation with FKP weighting,
+ * Source/Catalog.cpp:14120-14190: w = w_in * (fkp ? 1 / (1 + P_est nbar) : 1)
+ * for n objects, nbar[i] the object's mean density (NULL: nbar_const for
+ * all, the catalogue's mean density without a random catalogue), w_in the
+ * product of its other weights (NULL: 1).  w_out (float, n) is what the
+ * reference passes to grid_assignment_* as the mass; give it to cam_assign
+ * as the particles' w.  sums (host, may be NULL): [0] n_selected,
+ * [1] W_r = sum w, [2] S_r = sum w^2, [3] normal = sum nbar w^2 (FP64, fixed
+ * order).  mem applies to nbar and w_in, out_mem to w_out. */
+int cam_fkp_weights(cam_ctx *ctx, int64_t n, const float *nbar, double nbar_const, const float *w_in, int fkp,
+                    double P_est, int mem, float *w_out, int out_mem, double *sums);
 
 /* ---- BAM kernel ---------------------------------------------------------
  * The 3D update of Bam::GetKernel, Source/Bam.cpp:529 (:786-910).  kernel is

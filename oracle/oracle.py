@@ -280,6 +280,17 @@ def classify(lam, lth, band=1e-5):
     return labels, counts, int(ties[0])
 
 
+def tidal_invariants(lam: np.ndarray) -> np.ndarray:
+    """invariant_field_I/II/III and tidal_anisotropy, Source/Miscelanious.cpp:1460-1492,
+    of descending eigenvalues (…,3), in FP64: (4, …)."""
+    l1, l2, l3 = lam[..., 0], lam[..., 1], lam[..., 2]
+    i1 = l1 + l2 + l3
+    i2 = l1 * l2 + l2 * l3 + l1 * l3
+    i3 = (l1 * l2) * l3
+    ta = np.sqrt(0.5 * ((l3 - l1) ** 2 + (l3 - l2) ** 2 + (l2 - l1) ** 2)) / (2.0 + i1)
+    return np.stack([i1, i2, i3, ta])
+
+
 def tweb_from_spectrum(delta_k, n, L, R, lth, band=1e-5) -> TwebResult:
     t6 = tidal_components(delta_k, n, L, R)
     lam = eig3_f64(t6).reshape(n, n, n, 3)
@@ -382,6 +393,19 @@ def tweb_fd_density(mesh, L, R, lth, band=1e-5) -> TwebResult:
     mesh = np.asarray(mesh, np.float64)
     nbar = mesh.sum() / mesh.size
     return tweb_fd_from_spectrum(rfft3_f64(mesh / nbar - 1.0), n, L, R, lth, band)
+
+
+# ---- catalogue weights -------------------------------------------------------
+
+def fkp_weights_f64(nbar, w_in=None, fkp=True, P_est=0.0):
+    """The tracer loop's weights and sums, Source/Catalog.cpp:14140-14165, in
+    FP64: w = w_in / (1 + P_est nbar) (FKP on); (n_selected, W_r = sum w,
+    S_r = sum w^2, normal = sum nbar w^2)."""
+    nbar = np.asarray(nbar, np.float64)
+    w = np.ones_like(nbar) if w_in is None else np.asarray(w_in, np.float64).copy()
+    if fkp:
+        w = w * (1.0 / (1.0 + P_est * nbar))
+    return w, np.array([float(nbar.size), w.sum(), (w * w).sum(), (nbar * w * w).sum()])
 
 
 # ---- BAM kernel (GetKernel's 3D update, Konvolve) ---------------------------

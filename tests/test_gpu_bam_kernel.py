@@ -117,3 +117,26 @@ def test_bam_iteration_mirror():
     assert np.all(np.isfinite(bam.Kernel.cpu().numpy()))
     changed = np.any(bam.Kernel.cpu().numpy() != k_before)
     assert changed
+
+
+# ---------------------------------------------------------------- catalogue interpolation
+def test_fkp_weights_and_interpolation(ctx):
+    # Catalog.cpp's tracer loop: per-object nbar, an extra weight, FKP on
+    from cosmicatlas_b200.api import get_interpolated_density_field, make_grid
+    n, box, npart = 64, 500.0, 200_000
+    x, y, z = synth.clumped(npart, box, 2_000, 3.0, 0.7, seed=91)
+    rng = np.random.default_rng(92)
+    nbar = rng.uniform(1e-4, 3e-3, npart).astype(np.float32)
+    w1 = rng.uniform(0.5, 2.0, npart).astype(np.float32)
+    w, sums = ctx.fkp_weights(npart, nbar, 0.0, w1, True, 1e4)
+    wref, sref = orc.fkp_weights_f64(nbar, w1, True, 1e4)
+    np.testing.assert_allclose(w, wref.astype(np.float32), rtol=1e-7)
+    np.testing.assert_allclose(sums, sref, rtol=1e-12)
+    mesh, s2 = get_interpolated_density_field(x, y, z, make_grid(n, box), CIC, nbar, 0.0, w1, True, 1e4)
+    ref, _ = orc.assign_f64(CIC, x, y, z, wref.astype(np.float32), orc.Grid.cubic(n, box))
+    from conftest import rel_err_cells
+    assert rel_err_cells(mesh, ref, float(wref.mean())) <= 1e-5
+    # constant nbar (no random catalogue), no extra weights, FKP off: unit weights
+    w, sums = ctx.fkp_weights(1000, None, 2e-3, None, False, 1e4)
+    assert np.all(w == 1.0) and sums[1] == 1000.0 and abs(sums[3] - 2.0) < 1e-12
+

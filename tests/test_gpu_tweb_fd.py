@@ -138,3 +138,21 @@ def test_cwclass_default_build_variant():
     ref = orc.tweb_fd_density(mesh.astype(np.float64), box, 10.0, 0.0, BAND)
     assert label_check(cw.CWClass.reshape(n, n, n), ref.lam, ref.labels, 0.0) == 0
     assert abs(cw.volume_voids - ref.counts[3] / n ** 3) <= (ref.ties + 1) / n ** 3
+
+
+@pytest.mark.parametrize("method", [L.TWEB_FFT, FD])
+def test_tidal_invariants(ctx, method):
+    # invariant_field_I/II/III and tidal_anisotropy of the oracle eigenvalues
+    n, box, R = 48, 600.0, 15.0
+    x, y, z = synth.clumped(300_000, box, 3_000, 4.0, 0.8, seed=81)
+    mesh = orc.assign_f64(CIC, x, y, z, None, orc.Grid.cubic(n, box))[0].astype(np.float32)
+    labels, lam, inv = ctx.tweb_invariants(mesh, box, Context.tweb_opts(R, 0.0, BAND, method=method))
+    ref = (orc.tweb_fd_density if method == FD else orc.tweb_density)(mesh.astype(np.float64), box, R, 0.0, BAND)
+    want = orc.tidal_invariants(ref.lam)
+    scale = np.abs(ref.lam).max()
+    assert np.max(np.abs(inv[0] - want[0])) <= 1e-5 * scale
+    assert np.max(np.abs(inv[1] - want[1])) <= 1e-5 * scale * scale
+    assert np.max(np.abs(inv[2] - want[2])) <= 1e-5 * scale ** 3
+    assert np.max(np.abs(inv[3] - want[3])) <= 1e-4 * np.abs(want[3]).max()
+    assert label_check(labels, ref.lam, ref.labels, 0.0) == 0
+    np.testing.assert_allclose(np.moveaxis(lam, 0, -1), ref.lam, rtol=0, atol=1e-5 * scale)
