@@ -56,6 +56,8 @@ def parse():
                          "calib / stream: served vs plain per-call jobs/s and latency")
     ap.add_argument("--jobs", type=int, default=0, help="calib / stream: number of jobs (0 = the config's)")
     ap.add_argument("--rates", default="50,200,800", help="stream: Poisson arrival rates (jobs/s)")
+    ap.add_argument("--held-gb", type=float, default=24.0,
+                    help="stream: GB of submitted jobs' inputs the client may hold before it waits")
     ap.add_argument("--serving-jobs", type=int, default=1024,
                     help="sweep: jobs of the calibration batch timed served vs per-call on the same line (0: skip)")
     ap.add_argument("--mesh", type=int, default=0, help="single512 only: override N (profiler runs)")
@@ -773,7 +775,10 @@ def run_stream(args):
                        pk=Context.pk_opts(j["scheme"], nbins=n // 2),
                        tweb=Context.tweb_opts(2.0 * j["box"] / n, 0.0, 1e-5) if j["tweb"] else None)
 
-    def one_pass(workers, max_batch, rate, held_gb=24.0):
+    from cosmicatlas_b200.api import alloc_stats
+
+    def one_pass(workers, max_batch, rate, held_gb=None):
+        held_gb = args.held_gb if held_gb is None else held_gb
         rng = np.random.default_rng(99)
         gaps = rng.exponential(1.0 / rate, size=njobs) if rate else np.zeros(njobs)
         with Server(0, hbm_budget=budget, workers=workers, max_batch=max_batch) as srv:
@@ -783,6 +788,8 @@ def run_stream(args):
                 srv.wait(i)
             srv.stats(reset=True)
             srv.trace()
+            alloc_stats(reset=True)
+            retries0 = torch.cuda.memory_stats().get("num_alloc_retries", 0)
             pending = []  # (id, bytes): inputs the client holds until done
             held = 0.0
             t_start = time.perf_counter()
@@ -804,6 +811,8 @@ def run_stream(args):
             wall = time.perf_counter() - t_start
             st = srv.stats()
             tr = srv.trace()
+            al = alloc_stats()
+            torch_retries = torch.cuda.memory_stats().get("num_alloc_retries", 0) - retries0
         tr = tr[-njobs:]
         wait = tr["start_ms"] - tr["submit_ms"]
         run = tr["end_ms"] - tr["start_ms"]
@@ -822,7 +831,9 @@ def run_stream(args):
                                                              - np.unique(np.stack([tr["worker"], tr["start_ms"],
                                                                                    tr["end_ms"]], 1), axis=0)[:, 1])
                                                   / 1e3), 2),
-                          "device_free_gb_after": round(free_gb, 1)}}
+                          "device_free_gb_after": round(free_gb, 1),
+                          "slowest_ms": round(float(np.max(run)), 2) if len(run) else None},
+                "allocations": {"library": al, "torch_alloc_retries": int(torch_retries), "held_gb": held_gb}}
 
     rates = [float(r) for r in args.rates.split(",") if r]
     out = {"workload": f"served mixed stream: {njobs} jobs, N in 64..512, N_p log-uniform [1e5, 5e7], "

@@ -88,6 +88,11 @@ class ServerStats(ctypes.Structure):
                 ("mean_ms", ctypes.c_double), ("max_ms", ctypes.c_double)]
 
 
+class AllocStats(ctypes.Structure):
+    _fields_ = [("allocs", ctypes.c_int64), ("failures", ctypes.c_int64), ("bytes", ctypes.c_int64),
+                ("total_ms", ctypes.c_double), ("max_ms", ctypes.c_double)]
+
+
 class JobTrace(ctypes.Structure):
     _fields_ = [("id", ctypes.c_uint64), ("submit_ms", ctypes.c_double), ("start_ms", ctypes.c_double),
                 ("end_ms", ctypes.c_double), ("worker", ctypes.c_int), ("batch", ctypes.c_int),
@@ -106,6 +111,7 @@ SIGNATURES = {
     "cam_last_error": ([_P], ctypes.c_char_p),
     "cam_kernel_launches": ([_P], ctypes.c_int64),
     "cam_pool_trim": ([ctypes.c_int], ctypes.c_int),
+    "cam_alloc_stats_get": ([ctypes.POINTER(AllocStats), ctypes.c_int], ctypes.c_int),
     "cam_profile_enable": ([_P, ctypes.c_int], ctypes.c_int),
     "cam_profile_read": ([_P, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_int], ctypes.c_int),
     "cam_assign": ([_P, ctypes.POINTER(Particles), ctypes.POINTER(Grid), ctypes.c_int, ctypes.c_int, _P,
@@ -120,6 +126,8 @@ SIGNATURES = {
                    ctypes.POINTER(PkInfo)], ctypes.c_int),
     "cam_tweb": ([_P, ctypes.POINTER(Grid), _P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(TwebOpts), _P, _P,
                   ctypes.c_int, ctypes.POINTER(TwebStats)], ctypes.c_int),
+    "cam_power_multipoles": ([_P, ctypes.POINTER(Grid), _P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(PkOpts),
+                              ctypes.c_int, _P, _P, _P, _P, _P, ctypes.POINTER(PkInfo)], ctypes.c_int),
     "cam_cross_power": ([_P, ctypes.POINTER(Grid), _P, _P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(PkOpts),
                          ctypes.c_int, ctypes.c_int, _P, _P, _P, _P, _P], ctypes.c_int),
     "cam_poisson": ([_P, ctypes.POINTER(Grid), _P, ctypes.c_int, ctypes.c_int, ctypes.c_float, _P, ctypes.c_int],

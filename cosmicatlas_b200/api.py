@@ -223,6 +223,25 @@ class Context:
                                         L.ptr(pk), L.ptr(md), L.ptr(kv), ctypes.byref(info)))
         return PkResult(pk, md, kv, info.n_obj, info.shot_noise, info.normal)
 
+    def power_multipoles(self, mesh, box: float, opts: L.PkOpts, los: int = 2) -> dict:
+        """P(k) and its multipoles l = 2, 4 about axis los (0 x, 1 y, 2 z), as
+        power_spectrum_fkp forms them (Source/FftwFunctions.cpp:958)."""
+        dev = L.is_device(mesh)
+        n = mesh.shape[0]
+        prec = F64 if str(mesh.dtype).endswith("float64") else F32
+        if not dev:
+            mesh = np.ascontiguousarray(mesh)
+        nb = opts.nbins if opts.nbins > 0 else int(n / opts.ndel / 2)
+        p0, p2, p4, kv = np.empty(nb), np.empty(nb), np.empty(nb), np.empty(nb)
+        md = np.empty(nb, np.int64)
+        info = L.PkInfo()
+        g = make_grid(n, box)
+        self._check(self._lib.cam_power_multipoles(self.h, ctypes.byref(g), L.ptr(mesh), prec,
+                                                   L.MEM_DEVICE if dev else L.MEM_HOST, ctypes.byref(opts), los,
+                                                   L.ptr(p0), L.ptr(p2), L.ptr(p4), L.ptr(md), L.ptr(kv),
+                                                   ctypes.byref(info)))
+        return {"p0": p0, "p2": p2, "p4": p4, "modes": md, "kvector": kv}
+
     def cross_power(self, mesh_x, mesh_y, box: float, opts: L.PkOpts, input_type_y=L.INPUT_DENSITY,
                     want_coeff=False) -> dict:
         """Cross power spectrum (PowerSpectrumF::compute_cross_power_spectrum_grid,
@@ -547,6 +566,16 @@ class StagedParticles:
 
 _default: dict[int, Context] = {}
 _default_lock = threading.Lock()
+
+
+def alloc_stats(reset: bool = False) -> dict:
+    """The library's device-allocation counters (cam_alloc_stats_get)."""
+    st = L.AllocStats()
+    rc = L.lib().cam_alloc_stats_get(ctypes.byref(st), int(reset))
+    if rc != L.CAM_OK:
+        raise CamError(rc, "cam_alloc_stats_get")
+    return {"allocs": st.allocs, "failures": st.failures, "bytes": st.bytes, "total_ms": round(st.total_ms, 3),
+            "max_ms": round(st.max_ms, 3)}
 
 
 def default_context(device: int = 0) -> Context:

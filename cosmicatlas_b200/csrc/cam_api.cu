@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -42,6 +44,16 @@ cudaMemPool_t device_pool(int device)
     return pools[device];
 }
 
+// Allocation counters of the process (cam_alloc_stats), all devices.
+struct AllocCounters {
+    std::atomic<int64_t> allocs{0}, failures{0}, bytes{0}, total_us{0}, max_us{0};
+};
+AllocCounters &alloc_counters()
+{
+    static AllocCounters c;
+    return c;
+}
+
 void *scratch(cam_ctx *ctx, const char *name, size_t bytes)
 {
     bytes = std::max<size_t>(bytes, 256);
@@ -63,14 +75,27 @@ void *scratch(cam_ctx *ctx, const char *name, size_t bytes)
         b.cap = 0;
     }
     void *p = nullptr;
+    const auto t0 = std::chrono::steady_clock::now();
     cudaError_t e = cudaMallocFromPoolAsync(&p, want, pool, ctx->stream);
     if (e != cudaSuccess) {
         // idle pool memory may be fragmented or held for other sizes: hand
         // it back to the device and try once more
         cudaGetLastError();
+        alloc_counters().failures++;
         cudaDeviceSynchronize();
         cudaMemPoolTrimTo(pool, 0);
         e = cudaMallocFromPoolAsync(&p, want, pool, ctx->stream);
+    }
+    {
+        AllocCounters &c = alloc_counters();
+        const int64_t us =
+            std::chrono::duration_cast<std::chrono::microseconds>(std::chrono::steady_clock::now() - t0).count();
+        c.allocs++;
+        c.bytes += (int64_t)want;
+        c.total_us += us;
+        int64_t m = c.max_us.load();
+        while (us > m && !c.max_us.compare_exchange_weak(m, us)) {
+        }
     }
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -477,6 +502,25 @@ const char *cam_last_error(cam_ctx *ctx) { return ctx ? ctx->err.c_str() : "null
 
 int64_t cam_kernel_launches(cam_ctx *ctx) { return ctx ? ctx->launches : -1; }
 
+int cam_alloc_stats_get(cam_alloc_stats *out, int reset)
+{
+    if (!out) return CAM_E_INVAL;
+    AllocCounters &c = alloc_counters();
+    out->allocs = c.allocs.load();
+    out->failures = c.failures.load();
+    out->bytes = c.bytes.load();
+    out->total_ms = (double)c.total_us.load() / 1e3;
+    out->max_ms = (double)c.max_us.load() / 1e3;
+    if (reset) {
+        c.allocs = 0;
+        c.failures = 0;
+        c.bytes = 0;
+        c.total_us = 0;
+        c.max_us = 0;
+    }
+    return CAM_OK;
+}
+
 int cam_pool_trim(int device)
 {
     try {
@@ -644,7 +688,16 @@ int cam_fft_c2r(cam_ctx *ctx, int64_t n, int precision, const void *in, void *ou
 int cam_power(cam_ctx *ctx, const cam_grid *grid, const void *mesh, int precision, int mem,
               const cam_pk_opts *opts, double *pk, int64_t *modes, double *kvector, cam_pk_info *info)
 {
+    return cam_power_multipoles(ctx, grid, mesh, precision, mem, opts, -1, pk, nullptr, nullptr, modes, kvector, info);
+}
+
+int cam_power_multipoles(cam_ctx *ctx, const cam_grid *grid, const void *mesh, int precision, int mem,
+                         const cam_pk_opts *opts, int los, double *p0, double *p2, double *p4, int64_t *modes,
+                         double *kvector, cam_pk_info *info)
+{
+    double *pk = p0;
     return guarded(ctx, [&] {
+        CAM_REQUIRE(los >= -1 && los <= 2, CAM_E_INVAL, "line of sight must be 0 (x), 1 (y) or 2 (z)");
         check_grid_cubic(grid);
         CAM_REQUIRE(mesh, CAM_E_INVAL, "null mesh");
         check_prec(precision);
@@ -668,7 +721,25 @@ int cam_power(cam_ctx *ctx, const cam_grid *grid, const void *mesh, int precisio
             CAM_CUDA_TRY(cudaMemcpyAsync(hs, dsum, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
             CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
         }
-        power_from_spectrum(ctx, s, grid->L[0], hs[0], *opts, pk, modes, kvector, info);
+        cam_pk_info inf{};
+        power_from_spectrum(ctx, s, grid->L[0], hs[0], *opts, pk, modes, kvector, &inf);
+        if (info) *info = inf;
+        if (los >= 0 && (p2 || p4)) {
+            // P_l = (2l + 1) sum L_l(mu) |F|^2 / W^2 / (modes normal), no shot
+            // noise for l > 0 (FftwFunctions.cpp:1188-1212, :1614-1625)
+            const int nb = nbins_for(*opts, n);
+            const PkDevice m = power_multipole_device(ctx, s, *opts, nb, los);
+            std::vector<double> hm(2 * (size_t)nb);
+            std::vector<unsigned long long> hc(nb);
+            CAM_CUDA_TRY(cudaMemcpyAsync(hm.data(), m.sums, hm.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+            CAM_CUDA_TRY(cudaMemcpyAsync(hc.data(), m.modes, (size_t)nb * 8, cudaMemcpyDeviceToHost, ctx->stream));
+            CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+            for (int b = 0; b < nb; ++b) {
+                const double den = (double)hc[b] * inf.normal;
+                if (p2) p2[b] = hc[b] ? 5.0 * hm[2 * b] / den : 0.0;
+                if (p4) p4[b] = hc[b] ? 9.0 * hm[2 * b + 1] / den : 0.0;
+            }
+        }
     });
 }
 

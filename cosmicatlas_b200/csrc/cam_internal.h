@@ -201,6 +201,9 @@ PkDevice power_bin_device(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o,
 // Cross sums of two spectra of one size: sums [nbins][2] FP64
 // (sum Re(F1 conj F2)/W^2, sum |F1|^2/W^2), modes [nbins]; own buffers.
 PkDevice power_cross_device(cam_ctx *ctx, const Spectrum &s1, const Spectrum &s2, const cam_pk_opts &o, int nbins);
+// Multipole sums about axis los (0 x, 1 y, 2 z): sums [nbins][2] FP64
+// (sum L_2(mu) |F|^2/W^2, sum L_4(mu) |F|^2/W^2), modes [nbins]; own buffers.
+PkDevice power_multipole_device(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins, int los);
 void power_bin(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins,
                double *h_sum_raw, double *h_sum_sn, int64_t *h_modes);
 

@@ -57,13 +57,26 @@ __device__ __forceinline__ int pk_bin(double q, const double *E2, int nbins, flo
     return b < 0 ? -1 : b;  // b == nbins: above the last edge
 }
 
-// CROSS: a second spectrum (main2, nyq2); the two sums become
-// Re(F1 conj F2) / W^2 and |F1|^2 / W^2 (the table's second half is then
-// 1/W^2: the host builds it without shot-noise factors).
-template <typename C, bool CROSS = false>
+// Legendre polynomials of mu^2 = f^2 / q (FftwFunctions.cpp:1152-1153):
+// L_2 = (3 mu^2 - 1) / 2, L_4 = (35 mu^4 - 30 mu^2 + 3) / 8, both even in mu.
+__device__ __forceinline__ void legendre24(int f, double q, double &l2, double &l4)
+{
+    const double m2 = (double)f * (double)f / q;
+    l2 = 0.5 * (3.0 * m2 - 1.0);
+    l4 = ((35.0 * m2 - 30.0) * m2 + 3.0) * 0.125;
+}
+
+// MODE 0: P(k) sums |F|^2 / W^2 and C / W^2.
+// MODE 1 (cross): a second spectrum (main2, nyq2); the sums become
+// Re(F1 conj F2) / W^2 and |F1|^2 / W^2.
+// MODE 2 (multipoles): L_2(mu) |F|^2 / W^2 and L_4(mu) |F|^2 / W^2, mu the
+// cosine between k and the line of sight (axis `los`: 0 x, 1 y, 2 z).
+// Modes 1 and 2 read the table's second half as 1/W^2: the host builds it
+// without shot-noise factors.
+template <typename C, int MODE = 0>
 __global__ void __launch_bounds__(kPkThreads)
 pk_bin_kernel(const C *__restrict__ main, const C *__restrict__ nyq, const C *__restrict__ main2,
-              const C *__restrict__ nyq2, int n,
+              const C *__restrict__ nyq2, int los, int n,
               const double *__restrict__ g_tab /* [3][n/2+1]: 1/W^2 axis, C/W^2 axis ; [nbins+1] E2 */,
               int nbins, float m_u, float inv_s, int64_t rows_per_cta,
               double *__restrict__ part /* [grid][nbins][2] */,
@@ -107,10 +120,16 @@ pk_bin_kernel(const C *__restrict__ main, const C *__restrict__ nyq, const C *__
                 if (bin >= 0 && bin < nbins && pk_visited(i, j, c, n)) {
                     const C f = main[r * M + c];
                     const double re = (double)f.x, im = (double)f.y;
-                    if constexpr (CROSS) {
+                    if constexpr (MODE == 1) {
                         const C g = main2[r * M + c];
                         vraw = (re * (double)g.x + im * (double)g.y) * (tab_ab * tw2[c]);
                         vsn = (re * re + im * im) * (sn_ab * tsn[c]);
+                    } else if constexpr (MODE == 2) {
+                        double l2, l4;
+                        legendre24(los == 0 ? a : (los == 1 ? b : c), q, l2, l4);
+                        const double pw = (re * re + im * im) * (tab_ab * tw2[c]);
+                        vraw = pw * l2;
+                        vsn = pw * l4;
                     } else {
                         vraw = (re * re + im * im) * (tab_ab * tw2[c]);
                         vsn = sn_ab * tsn[c];
@@ -152,10 +171,16 @@ pk_bin_kernel(const C *__restrict__ main, const C *__restrict__ nyq, const C *__
             if (bin >= 0 && bin < nbins && pk_visited(i, j, M, n)) {
                 const C f = nyq[r];
                 const double re = (double)f.x, im = (double)f.y;
-                if constexpr (CROSS) {
+                if constexpr (MODE == 1) {
                     const C g = nyq2[r];
                     mysum[2 * bin] += (re * (double)g.x + im * (double)g.y) * (tab_ab * tw2[M]);
                     mysum[2 * bin + 1] += (re * re + im * im) * (sn_ab * tsn[M]);
+                } else if constexpr (MODE == 2) {
+                    double l2, l4;
+                    legendre24(los == 0 ? a : (los == 1 ? b : M), q, l2, l4);
+                    const double pw = (re * re + im * im) * (tab_ab * tw2[M]);
+                    mysum[2 * bin] += pw * l2;
+                    mysum[2 * bin + 1] += pw * l4;
                 } else {
                     mysum[2 * bin] += (re * re + im * im) * (tab_ab * tw2[M]);
                     mysum[2 * bin + 1] += sn_ab * tsn[M];
@@ -229,10 +254,11 @@ double sq_factor(int p, double s)
 
 namespace {
 
-// s2 == nullptr: P(k) sums of s.  Otherwise the cross sums of s and s2 into
-// buffers of their own (tag), so that a P(k) of s2 can follow.
+// mode 0: P(k) sums of s; 1: the cross sums of s and s2; 2: the multipole
+// sums of s about axis los.  Modes 1 and 2 use buffers of their own (tag),
+// so that a P(k) can follow.
 PkDevice power_bin_impl(cam_ctx *ctx, const Spectrum &s, const Spectrum *s2, const cam_pk_opts &o, int nbins,
-                        const char *tag)
+                        const char *tag, int mode = 0, int los = 2)
 {
     const int n = (int)s.n, h = n / 2;
     CAM_REQUIRE(nbins >= 1 && nbins <= 4096, CAM_E_INVAL, "nbins must be in [1, 4096]");
@@ -287,23 +313,24 @@ PkDevice power_bin_impl(cam_ctx *ctx, const Spectrum &s, const Spectrum *s2, con
     const size_t smem = tab_bytes + (size_t)kPkWarps * nbins * (2 * sizeof(double) + sizeof(unsigned long long));
     CAM_REQUIRE(smem <= 220 * 1024, CAM_E_UNSUPPORTED, "too many bins for one CTA");
     const float m_u = (float)o.DeltaKmin, inv_s = (float)(1.0 / o.ndel);
-    auto launch = [&](auto cplx, auto cross) {
+    auto launch = [&](auto cplx, auto md) {
         using C = decltype(cplx);
-        constexpr bool X = decltype(cross)::value;
+        constexpr int X = decltype(md)::value;
         auto kern = pk_bin_kernel<C, X>;
         smem_at_least(kern, smem);
-        const C *m2 = X ? (const C *)s2->main : nullptr;
-        const C *q2 = X ? (const C *)s2->nyq : nullptr;
-        CAM_LAUNCH_NAMED(ctx, X ? "pk_cross_bin" : "pk_bin", kern, grid, kPkThreads, smem, (const C *)s.main,
-                         (const C *)s.nyq, m2, q2, n, d_tab, nbins, m_u, inv_s, rpc, part, pm);
+        const C *m2 = X == 1 ? (const C *)s2->main : nullptr;
+        const C *q2 = X == 1 ? (const C *)s2->nyq : nullptr;
+        CAM_LAUNCH_NAMED(ctx, X == 1 ? "pk_cross_bin" : (X == 2 ? "pk_multipole_bin" : "pk_bin"), kern, grid,
+                         kPkThreads, smem, (const C *)s.main, (const C *)s.nyq, m2, q2, los, n, d_tab, nbins, m_u,
+                         inv_s, rpc, part, pm);
     };
-    if (s.precision == CAM_F32) {
-        if (s2) launch(float2{}, std::true_type{});
-        else launch(float2{}, std::false_type{});
-    } else {
-        if (s2) launch(double2{}, std::true_type{});
-        else launch(double2{}, std::false_type{});
-    }
+    auto by_mode = [&](auto cplx) {
+        if (mode == 1) launch(cplx, std::integral_constant<int, 1>{});
+        else if (mode == 2) launch(cplx, std::integral_constant<int, 2>{});
+        else launch(cplx, std::integral_constant<int, 0>{});
+    };
+    if (s.precision == CAM_F32) by_mode(float2{});
+    else by_mode(double2{});
     CAM_LAUNCH(ctx, pk_final_kernel, nbins, 256, 0, part, pm, grid, nbins, res, resm);
     return PkDevice{res, resm};
 }
@@ -320,7 +347,15 @@ PkDevice power_cross_device(cam_ctx *ctx, const Spectrum &s1, const Spectrum &s2
     CAM_REQUIRE(s1.n == s2.n && s1.precision == s2.precision, CAM_E_INVAL, "cross spectra differ in size or precision");
     cam_pk_opts ox = o;
     ox.sn_correction = 0;  // the second table half is then 1/W^2
-    return power_bin_impl(ctx, s1, &s2, ox, nbins, "pkx");
+    return power_bin_impl(ctx, s1, &s2, ox, nbins, "pkx", 1);
+}
+
+PkDevice power_multipole_device(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins, int los)
+{
+    CAM_REQUIRE(los >= 0 && los <= 2, CAM_E_INVAL, "line of sight must be 0 (x), 1 (y) or 2 (z)");
+    cam_pk_opts ox = o;
+    ox.sn_correction = 0;
+    return power_bin_impl(ctx, s, nullptr, ox, nbins, "pkm", 2, los);
 }
 
 void power_bin(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins, double *h_sum_raw,

@@ -134,6 +134,19 @@ int cam_ctx_destroy(cam_ctx *ctx);
  * trimmed automatically when an allocation fails.  cam_pool_trim hands the
  * pool's idle memory back to the device now.  No reference counterpart. */
 int cam_pool_trim(int device);
+/* Device allocations the library made in this process (all devices): how
+ * many, how many first failed and were retried after trimming the pool
+ * (that trim waits for the whole device), bytes, and the host time spent in
+ * them.  reset != 0 zeroes the counters after reading.  No reference
+ * counterpart. */
+typedef struct {
+    int64_t allocs;
+    int64_t failures;
+    int64_t bytes;
+    double total_ms;
+    double max_ms;
+} cam_alloc_stats;
+int cam_alloc_stats_get(cam_alloc_stats *out, int reset);
 /* Sets the CUDA stream (cudaStream_t) the context launches on (NULL = the
  * context's own stream). */
 int cam_ctx_set_stream(cam_ctx *ctx, void *stream);
@@ -188,6 +201,18 @@ int cam_fft_c2r(cam_ctx *ctx, int64_t n, int precision, const void *in, void *ou
 int cam_power(cam_ctx *ctx, const cam_grid *grid, const void *mesh, int precision,
               int mem, const cam_pk_opts *opts, double *pk, int64_t *modes,
               double *kvector, cam_pk_info *info);
+
+/* cam_power plus the multipoles l = 2, 4 about a fixed line of sight (los:
+ * 0 x, 1 y, 2 z; the reference's LOS, Headers/def.h:1714), as
+ * FftwFunctions::power_spectrum_fkp computes them for a box,
+ * Source/FftwFunctions.cpp:1125-1212 and :1614-1625:
+ *   p2[b] = 5 sum L_2(mu) |F|^2 / W^2 / (modes normal),
+ *   p4[b] = 9 sum L_4(mu) |F|^2 / W^2 / (modes normal),
+ * mu = k_los / |k|, no shot noise subtracted for l > 0; p0 is cam_power's
+ * P(k).  Host arrays of nbins; any may be NULL. */
+int cam_power_multipoles(cam_ctx *ctx, const cam_grid *grid, const void *mesh, int precision, int mem,
+                         const cam_pk_opts *opts, int los, double *p0, double *p2, double *p4, int64_t *modes,
+                         double *kvector, cam_pk_info *info);
 
 /* Cross power spectrum of two meshes: replaces
  * PowerSpectrumF::compute_cross_power_spectrum_grid, Source/PowerSpectrumF.cpp:549,

@@ -453,6 +453,45 @@ void orc_cross_f64(int64_t n, const double *s1, const double *s2, int p, int mas
     free(sx);
 }
 
+/* Multipole sums in FP64, FftwFunctions::power_spectrum_fkp,
+ * Source/FftwFunctions.cpp:1125-1212: over the octant loop's mode set and
+ * bins, mu = k_los / |k| with los 0 = x, 1 = y, 2 = z (the reference's
+ * I_LOSX/Y/Z), L_2 = (3 mu^2 - 1)/2, L_4 = (35 mu^4 - 30 mu^2 + 3)/8:
+ *   s2[b] = sum L_2 |F|^2 / W^2,  s4[b] = sum L_4 |F|^2 / W^2,  modes[b]. */
+void orc_multipole_f64(int64_t n, const double *spec, int p, int mas_corr, double kmin_u, double dk_u,
+                       int nbins, int los, double *s2, double *s4, int64_t *modes)
+{
+    const int64_t nz = n / 2 + 1;
+    for (int b = 0; b < nbins; ++b) { s2[b] = 0.0; s4[b] = 0.0; modes[b] = 0; }
+    double *sx = malloc(sizeof(double) * (size_t)n);
+    for (int64_t a = 0; a < n; ++a) sx[a] = sinc_pi(a <= n / 2 ? a : n - a, n);
+    for (int64_t i = 0; i < n; ++i) {
+        int64_t a = i <= n / 2 ? i : n - i;
+        for (int64_t j = 0; j < n; ++j) {
+            int64_t b = j <= n / 2 ? j : n - j;
+            for (int64_t c = 0; c < nz; ++c) {
+                if (!pk_visited(i, j, c, n)) continue;
+                double q = (double)(a * a + b * b + c * c);
+                int64_t bin = orc_bin(q, kmin_u, dk_u, nbins);
+                if (bin < 0) continue;
+                const double *f = spec + 2 * ((i * n + j) * nz + c);
+                double iw2 = 1.0;
+                if (mas_corr) {
+                    double wk = pow(sx[i] * sx[j] * sx[c], (double)(p + 1));
+                    iw2 = 1.0 / (wk * wk);
+                }
+                double fl = (double)(los == 0 ? a : (los == 1 ? b : c));
+                double mu = fl / sqrt(q);
+                double pw = (f[0] * f[0] + f[1] * f[1]) * iw2;
+                s2[bin] += 0.5 * (3.0 * mu * mu - 1.0) * pw;
+                s4[bin] += (35.0 * pow(mu, 4) - 30.0 * mu * mu + 3.0) / 8.0 * pw;
+                modes[bin] += 1;
+            }
+        }
+    }
+    free(sx);
+}
+
 /* The reference's power_spectrum loop as written (FP32, OpenMP atomics,
  * float bins), Source/FftwFunctions.cpp:1660-1876, for the CPU baseline.
  * spec is interleaved complex64.  fix_octant4 selects Re^2+Im^2 for the

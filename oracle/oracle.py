@@ -57,6 +57,8 @@ def lib():
         _LIB.orc_power_f64.restype = None
         _LIB.orc_cross_f64.argtypes = [i64, P, P, i32, i32, f64, f64, i32, P, P, P, P]
         _LIB.orc_cross_f64.restype = None
+        _LIB.orc_multipole_f64.argtypes = [i64, P, i32, i32, f64, f64, i32, i32, P, P, P]
+        _LIB.orc_multipole_f64.restype = None
         _LIB.orc_power_ref.argtypes = [i64, P, i32, i32, i32, f32, f32, f32, f32, f32, i32, i32, P, P]
         _LIB.orc_power_ref.restype = None
         _LIB.orc_bin.argtypes = [f64, f64, f64, i32]
@@ -183,6 +185,25 @@ def power_grid(mesh, L, scheme, nbins, kmin_u=0.0, dk_u=1.0, input_type="density
     r = power_from_spectrum(spec, n, L, scheme, nbins, sn, normal, kmin_u, dk_u, mas_corr, sn_corr)
     r.n_obj = ngal
     return r
+
+
+def power_multipoles(mesh, L, scheme, nbins, los=2, input_type="density", kmin_u=0.0, dk_u=1.0,
+                     mas_corr=True, sn_corr=True):
+    """P(k) (power_grid) and the multipoles of FftwFunctions::power_spectrum_fkp,
+    Source/FftwFunctions.cpp:958-1625, for a box with a fixed line of sight:
+    P_2 = 5 sum L_2 |F|^2/W^2 / (modes normal), P_4 = 9 sum L_4 |F|^2/W^2 / (...),
+    with the normalisation of power_grid and no shot noise for l > 0."""
+    n = mesh.shape[0]
+    p0 = power_grid(mesh, L, scheme, nbins, kmin_u, dk_u, input_type, mas_corr, sn_corr)
+    m = np.asarray(mesh, np.float64)
+    data = m - m.sum() / m.size if input_type == "density" else m
+    spec = np.ascontiguousarray(rfft3_f64(data), np.complex128)
+    s2, s4 = np.empty(nbins), np.empty(nbins)
+    md = np.empty(nbins, np.int64)
+    lib().orc_multipole_f64(n, _p(spec), SCHEME_P[scheme], int(mas_corr), float(kmin_u), float(dk_u), nbins,
+                            int(los), _p(s2), _p(s4), _p(md))
+    den = np.maximum(md, 1) * p0.normal
+    return p0, np.where(md > 0, 5.0 * s2 / den, 0.0), np.where(md > 0, 9.0 * s4 / den, 0.0), md
 
 
 @dataclass

@@ -75,3 +75,12 @@ def test_server_and_batch_reject_bad_arguments_without_device():
     assert lib.cam_server_wait(None, 1, 0) == L.CAM_E_INVAL
     assert lib.cam_server_stats_get(None, None, 0) == L.CAM_E_INVAL
     assert lib.cam_server_destroy(None) == L.CAM_E_INVAL
+
+
+def test_alloc_stats_without_device():
+    # host-side counters: readable (and zero) before any device allocation
+    import ctypes
+    st = L.AllocStats()
+    assert L.lib().cam_alloc_stats_get(ctypes.byref(st), 1) == L.CAM_OK
+    assert st.allocs >= 0 and st.failures >= 0
+    assert L.lib().cam_alloc_stats_get(None, 0) == L.CAM_E_INVAL

@@ -322,3 +322,22 @@ def test_cross_power_of_a_field_with_itself():
     # -X anticorrelates: coefficient -1
     c = orc.cross_power_grid(m - 1.0, 1.0 - m, box, orc.CIC, 8, "delta", "delta", coeff=True)
     np.testing.assert_allclose(c.pk[has], -1.0, rtol=1e-12)
+
+
+def test_multipoles_of_an_isotropic_field_vanish_and_rotate():
+    # a field made isotropic by averaging over the three lines of sight has
+    # sum_los P_2 = 0 (L_2 averages to 0 over the axes: mu_x^2 + mu_y^2 + mu_z^2 = 1);
+    # a field stretched along z has P_2 of opposite sign about z and about x
+    n, box = 24, 400.0
+    rng = np.random.default_rng(6)
+    g = rng.normal(size=(n, n, n))
+    tot = np.zeros(12)
+    for los in range(3):
+        p0, p2, p4, md = orc.power_multipoles(g, box, orc.NGP, 12, los, "delta", mas_corr=False, sn_corr=False)
+        tot += p2
+    np.testing.assert_allclose(tot, 0.0, atol=1e-10 * np.abs(p0.pk).max())
+    k = np.fft.fftfreq(n)[None, None, :n // 2 + 1] * 0 + np.arange(n // 2 + 1)[None, None, :]
+    aniso = orc.irfft3_f64(orc.rfft3_f64(g) * np.exp(-0.02 * k * k), n)  # suppress high k_z only
+    _, p2z, _, _ = orc.power_multipoles(aniso, box, orc.NGP, 12, 2, "delta", mas_corr=False, sn_corr=False)
+    _, p2x, _, _ = orc.power_multipoles(aniso, box, orc.NGP, 12, 0, "delta", mas_corr=False, sn_corr=False)
+    assert p2z[6] < 0 < p2x[6]
