@@ -72,6 +72,30 @@ def dist_env():
             int(os.environ.get("WORLD_SIZE", 1)))
 
 
+def max_over_ranks(ms, device="cuda"):
+    """The slowest rank's time (every rank gets it); one rank: ms itself.
+    Jobs are replicas with no collective in their data path, so this is the
+    only exchange of a timed region."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(ms)
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(jobs_per_rank, world, ms_max):
+    """Throughput of all ranks together: every rank's jobs over the slowest
+    rank's time (weak scaling: per-rank work is fixed as ranks are added)."""
+    return jobs_per_rank * world / (ms_max / 1e3)
+
+
+def rank_seed(base, rank):
+    """Each rank draws its own catalogue (independent jobs per replica)."""
+    return base + 1000 * rank
+
+
 def config_dict(n_particles, extra=None):
     d = {"workload": "scheme sweep: %d clumped weighted particles, L=1000, NGP+CIC+TSC onto 256^3 FP32, "
                      "r2c FFT, P(k) 128 bins" % n_particles,
@@ -225,8 +249,8 @@ def run_ours(args):
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     npart = args.particles
-    x, y, z = synth.clumped(npart, BOX, 200_000, 1.5, 0.8, seed=2 + 1000 * rank)
-    w = synth.halo_masses(npart, seed=1002 + 1000 * rank)
+    x, y, z = synth.clumped(npart, BOX, 200_000, 1.5, 0.8, seed=rank_seed(2, rank))
+    w = synth.halo_masses(npart, seed=rank_seed(1002, rank))
     dev = [torch.from_numpy(v).cuda() for v in (x, y, z, w)]
     pinned = [torch.from_numpy(v).pin_memory() for v in (x, y, z, w)]
     grid = make_grid(NMESH, BOX)
@@ -285,11 +309,7 @@ def run_ours(args):
         # every job has returned its P(k) to the host: all work is done
         t1.record(stream)
         torch.cuda.synchronize()
-        ms = t0.elapsed_time(t1)
-        if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(t0.elapsed_time(t1))
         barrier()
         return ms
 
@@ -302,11 +322,7 @@ def run_ours(args):
             step(arrs, lat)
         t1.record(stream)
         torch.cuda.synchronize()
-        ms = t0.elapsed_time(t1)
-        if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(t0.elapsed_time(t1))
         barrier()
         return ms
 
@@ -334,8 +350,8 @@ def run_ours(args):
     ms_e2e = timed_host_fed(args.steps) if not args.kernels_only else float("nan")
 
     jobs = len(SCHEMES) * args.steps * world
-    value = jobs / (ms / 1e3)
-    e2e = jobs / (ms_e2e / 1e3)
+    value = whole_job_rate(len(SCHEMES) * args.steps, world, ms)
+    e2e = whole_job_rate(len(SCHEMES) * args.steps, world, ms_e2e)
     h2d = npart * 16
     d2h = len(SCHEMES) * NBINS * 24
 
