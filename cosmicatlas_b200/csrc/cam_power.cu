@@ -96,6 +96,8 @@ pk_bin_kernel(const C *__restrict__ main, const C *__restrict__ nyq, const C *__
     __syncthreads();
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // float spectra with an even row length: two elements per lane
+    const bool PAIRED = sizeof(C) == 8 && (M & 1) == 0;
     double *mysum = wsum + (size_t)warp * nbins * 2;
     unsigned long long *mycnt = wcnt + (size_t)warp * nbins;
     const int64_t nrows = (int64_t)n * n;
@@ -109,7 +111,101 @@ pk_bin_kernel(const C *__restrict__ main, const C *__restrict__ nyq, const C *__
         const double tab_ab = tw2[a] * tw2[b];
         const double sn_ab = tsn[a] * tsn[b];
         const int64_t q0 = (int64_t)a * a + (int64_t)b * b;
-        for (int c0 = 0; c0 < M; c0 += 32) {
+        // the two sums of one visited element c (FP64)
+        auto elem = [&](double re, double im, double gre, double gim, int cc, double q, double &vr, double &vs) {
+            if constexpr (MODE == 1) {
+                vr = (re * gre + im * gim) * (tab_ab * tw2[cc]);
+                vs = (re * re + im * im) * (sn_ab * tsn[cc]);
+            } else if constexpr (MODE == 2) {
+                double l2, l4;
+                legendre24(los == 0 ? a : (los == 1 ? b : cc), q, l2, l4);
+                const double pw = (re * re + im * im) * (tab_ab * tw2[cc]);
+                vr = pw * l2;
+                vs = pw * l4;
+            } else {
+                vr = (re * re + im * im) * (tab_ab * tw2[cc]);
+                vs = sn_ab * tsn[cc];
+            }
+        };
+        if (PAIRED) {
+            // Two elements per lane (c, c + 1) from one 16-byte load; M is
+            // even, so both exist together.  Each lane's last element (B,
+            // bin2) enters the warp's run reduction; its first element (A,
+            // bin1 <= bin2), when its bin differs, either joins the previous
+            // lane's B (same bin) or is the only element of its bin in this
+            // chunk and is added by its own lane.
+            for (int c0 = 0; c0 < M; c0 += 64) {
+                const int c = c0 + 2 * lane;
+                double ra = 0.0, sa = 0.0, rb = 0.0, sb = 0.0;
+                int na = 0, nbv = 0;
+                int bin1 = nbins, bin2 = nbins;
+                if (c < M) {
+                    const double q1 = (double)(q0 + (int64_t)c * c);
+                    const double q2 = (double)(q0 + (int64_t)(c + 1) * (c + 1));
+                    bin1 = pk_bin(q1, E2, nbins, m_u, inv_s);
+                    bin2 = pk_bin(q2, E2, nbins, m_u, inv_s);
+                    const float4 f4 = __ldg(reinterpret_cast<const float4 *>(main + r * M + c));
+                    float4 g4 = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if constexpr (MODE == 1) g4 = __ldg(reinterpret_cast<const float4 *>(main2 + r * M + c));
+                    if (bin1 >= 0 && bin1 < nbins && pk_visited(i, j, c, n)) {
+                        elem(f4.x, f4.y, g4.x, g4.y, c, q1, ra, sa);
+                        na = 1;
+                    }
+                    if (bin2 >= 0 && bin2 < nbins && pk_visited(i, j, c + 1, n)) {
+                        elem(f4.z, f4.w, g4.z, g4.w, c + 1, q2, rb, sb);
+                        nbv = 1;
+                    }
+                }
+                const bool split = bin1 != bin2;
+                double vraw = rb, vsn = sb;
+                int cnt = nbv;
+                if (!split) {
+                    vraw = ra + rb;
+                    vsn = sa + sb;
+                    cnt = na + nbv;
+                }
+                // the next lane's A joins this lane's B when their bins agree
+                const int nb1 = __shfl_down_sync(0xffffffffu, bin1, 1);
+                const int nsplit = __shfl_down_sync(0xffffffffu, (int)split, 1);
+                const double nra = __shfl_down_sync(0xffffffffu, ra, 1);
+                const double nsa = __shfl_down_sync(0xffffffffu, sa, 1);
+                const int nna = __shfl_down_sync(0xffffffffu, na, 1);
+                if (lane < 31 && nsplit && nb1 == bin2) {
+                    vraw += nra;
+                    vsn += nsa;
+                    cnt += nna;
+                }
+                const int prev = __shfl_up_sync(0xffffffffu, bin2, 1);
+                const bool a_alone = split && !(lane > 0 && prev == bin1);
+                const bool head = lane == 0 || prev != bin2;
+                const unsigned heads = __ballot_sync(0xffffffffu, head);
+                const unsigned later = heads & ~((2u << lane) - 1u);
+                const int end = later ? __ffs((int)later) - 1 : 32;
+#pragma unroll
+                for (int off = 1; off < 32; off <<= 1) {
+                    const double or_ = __shfl_down_sync(0xffffffffu, vraw, off);
+                    const double os = __shfl_down_sync(0xffffffffu, vsn, off);
+                    const int oc = __shfl_down_sync(0xffffffffu, cnt, off);
+                    if (lane + off < end) {
+                        vraw += or_;
+                        vsn += os;
+                        cnt += oc;
+                    }
+                }
+                if (head && bin2 >= 0 && bin2 < nbins && cnt) {
+                    mysum[2 * bin2] += vraw;
+                    mysum[2 * bin2 + 1] += vsn;
+                    mycnt[bin2] += (unsigned long long)cnt;
+                }
+                if (a_alone && bin1 >= 0 && bin1 < nbins && na) {
+                    mysum[2 * bin1] += ra;
+                    mysum[2 * bin1 + 1] += sa;
+                    mycnt[bin1] += 1ull;
+                }
+                __syncwarp();
+            }
+        }
+        for (int c0 = 0; !PAIRED && c0 < M; c0 += 32) {
             const int c = c0 + lane;
             double vraw = 0.0, vsn = 0.0;
             bool valid = false;
@@ -119,21 +215,9 @@ pk_bin_kernel(const C *__restrict__ main, const C *__restrict__ nyq, const C *__
                 bin = pk_bin(q, E2, nbins, m_u, inv_s);
                 if (bin >= 0 && bin < nbins && pk_visited(i, j, c, n)) {
                     const C f = main[r * M + c];
-                    const double re = (double)f.x, im = (double)f.y;
-                    if constexpr (MODE == 1) {
-                        const C g = main2[r * M + c];
-                        vraw = (re * (double)g.x + im * (double)g.y) * (tab_ab * tw2[c]);
-                        vsn = (re * re + im * im) * (sn_ab * tsn[c]);
-                    } else if constexpr (MODE == 2) {
-                        double l2, l4;
-                        legendre24(los == 0 ? a : (los == 1 ? b : c), q, l2, l4);
-                        const double pw = (re * re + im * im) * (tab_ab * tw2[c]);
-                        vraw = pw * l2;
-                        vsn = pw * l4;
-                    } else {
-                        vraw = (re * re + im * im) * (tab_ab * tw2[c]);
-                        vsn = sn_ab * tsn[c];
-                    }
+                    C g{};
+                    if constexpr (MODE == 1) g = main2[r * M + c];
+                    elem((double)f.x, (double)f.y, (double)g.x, (double)g.y, c, q, vraw, vsn);
                     valid = true;
                 }
             }
