@@ -41,13 +41,6 @@ constexpr int kSmemBricks = 16384;  // per-CTA brick histogram in shared memory 
 // would funnel all bricks through a few slices.
 constexpr int kCursorStride = 32;
 
-__device__ __forceinline__ int wrapi(int v, int n)
-{
-    if (v >= n) v -= n;
-    if (v < 0) v += n;
-    if (v < 0 || v >= n) v = ((v % n) + n) % n;
-    return v;
-}
 
 // Reference FP32 home cell (see orc_keys / ref_home in the oracle).
 // NGP: x on [min, min+L); CIC: x - d/2 wrapped once by +-L then [min, min+L);
@@ -120,6 +113,19 @@ struct Stencil {
     static constexpr int FIRST = SCHEME == CAM_TSC ? -1 : 0;
 };
 
+// First and last stencil cells of a home cell c in [0, n), wrapped
+// periodically: the stencil reaches at most one cell below 0 (TSC) and at
+// most one cell at or above n, so one conditional add or subtract each.
+template <int SCHEME>
+__device__ __forceinline__ void stencil_ends(int c, int n, int &lo, int &hi)
+{
+    using St = Stencil<SCHEME>;
+    lo = c + St::FIRST;
+    hi = c + St::FIRST + St::W - 1;
+    if constexpr (St::FIRST < 0) lo = lo < 0 ? lo + n : lo;
+    if constexpr (St::FIRST + St::W - 1 > 0) hi = hi >= n ? hi - n : hi;
+}
+
 // Payload word per axis: bits 26..31 = home cell relative to the brick + 8,
 // bits 0..25 = round(t * 2^24) + 2^24 (t in [-1, 3)).
 __device__ __forceinline__ uint32_t pack_axis(int cl, float t)
@@ -162,8 +168,8 @@ __device__ __forceinline__ void count_one(float px, float py, float pz, float wt
     bool two[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        const int lo = wrapi(c[a] + St::FIRST, g.n[a]);
-        const int hi = wrapi(c[a] + St::FIRST + St::W - 1, g.n[a]);
+        int lo, hi;
+        stencil_ends<SCHEME>(c[a], g.n[a], lo, hi);
         bl[a] = brick_of(lo, g.b[a], g.bmagic[a]);
         two[a] = St::W > 1 && brick_of(hi, g.b[a], g.bmagic[a]) != bl[a];
     }
@@ -217,8 +223,8 @@ __device__ __forceinline__ void bin_one(float px, float py, float pz, float wt, 
     float t[3] = {0.f, 0.f, 0.f};
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        const int lo = wrapi(c[a] + St::FIRST, g.n[a]);
-        const int hi = wrapi(c[a] + St::FIRST + St::W - 1, g.n[a]);
+        int lo, hi;
+        stencil_ends<SCHEME>(c[a], g.n[a], lo, hi);
         bl[a] = brick_of(lo, g.b[a], g.bmagic[a]);
         nbx[a] = (brick_of(hi, g.b[a], g.bmagic[a]) == bl[a]) ? 1 : 2;
         if (SCHEME != CAM_NGP && SCATTER) t[a] = exact_offset(pos[a], g.mn[a], g.d[a], g.inv_d[a], c[a], g.n[a]);
@@ -313,10 +319,16 @@ bin_kernel(const float *__restrict__ x, const float *__restrict__ y, const float
             const float4 Y = __ldcs(reinterpret_cast<const float4 *>(y + p));
             const float4 Z = __ldcs(reinterpret_cast<const float4 *>(z + p));
             const float4 Wt = weighted ? __ldcs(reinterpret_cast<const float4 *>(w + p)) : make_float4(1.f, 1.f, 1.f, 1.f);
-            one(X.x, Y.x, Z.x, Wt.x);
-            one(X.y, Y.y, Z.y, Wt.y);
-            one(X.z, Y.z, Z.z, Wt.z);
-            one(X.w, Y.w, Z.w, Wt.w);
+            // one copy of the particle body, not four: the inlined body is
+            // large and four copies overflowed the instruction cache
+#pragma unroll 1
+            for (int k = 0; k < 4; ++k) {
+                const float px = k == 0 ? X.x : (k == 1 ? X.y : (k == 2 ? X.z : X.w));
+                const float py = k == 0 ? Y.x : (k == 1 ? Y.y : (k == 2 ? Y.z : Y.w));
+                const float pz = k == 0 ? Z.x : (k == 1 ? Z.y : (k == 2 ? Z.z : Z.w));
+                const float pw = k == 0 ? Wt.x : (k == 1 ? Wt.y : (k == 2 ? Wt.z : Wt.w));
+                one(px, py, pz, pw);
+            }
         }
         ptail = q1;
     }
