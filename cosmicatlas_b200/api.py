@@ -810,6 +810,8 @@ class Bam:
         self.params = params
         n = params.Nft
         self.Kernel = torch.ones((n, n, n // 2 + 1), dtype=torch.float32, device=f"cuda:{params.device}")
+        # filled on torch's stream; the library context launches on its own
+        torch.cuda.synchronize(params.device)
         nb = params.Nnp_data if params.Nnp_data > 0 else int(n / params.ndel_data / 2)
         self.kvec = np.zeros(nb)
         self.Power_REF = np.zeros(nb)

@@ -1,0 +1,124 @@
+"""The configurations at their full sizes on the GPU.
+
+The plain small configuration (2,000,000 particles, CIC onto 128^3 FP64,
+P(k), T-web) is compared with the FP64 oracle in full.  The scheme sweep
+(16,777,216 weighted particles onto 256^3) and the large job (768^3 TSC of
+452,984,832 Zel'dovich-displaced particles) are checked through properties
+that do not depend on size:
+  * every particle is kept, and the mesh holds the total weight (1e-6);
+  * NGP counts sum to the number of particles kept (exact);
+  * the mesh, hence P(k), is bit-identical when the particles are shuffled
+    and when the job is repeated (integer cell sums, fixed-order FP64 bins);
+  * P(k) mode counts equal a direct count of the estimator's mode set;
+  * T-web label counts sum to N^3.
+"""
+import numpy as np
+import pytest
+
+import oracle as orc
+from conftest import pk_rel_err
+from cosmicatlas_b200 import synth
+from cosmicatlas_b200.api import CIC, F32, F64, NGP, TSC, Context, make_grid
+
+pytestmark = pytest.mark.gpu
+
+BAND = 1e-5
+
+
+def mode_counts(n, nbins, kmin_u=0.0, dk_u=1.0):
+    """Modes per bin of the octant loop's mode set (FftwFunctions.cpp:1731-1851:
+    planes i = N/2 and j = N/2 never, one element of each conjugate pair in
+    the k = 0 plane), with |k|^2 = q (units of k_f) in bin b when
+    E2[b] <= q < E2[b + 1], E2[b] = (kmin + b dk)^2 in FP64."""
+    h = n // 2
+    e = kmin_u + np.arange(nbins + 1, dtype=np.float64) * dk_u
+    e2 = e * e
+    j = np.arange(n)[:, None]
+    c = np.arange(h + 1)[None, :]
+    b = np.minimum(j, n - j)
+    out = np.zeros(nbins, np.int64)
+    for i in range(n):
+        if i == h:
+            continue
+        a = min(i, n - i)
+        q = (a * a + b * b + c * c).astype(np.float64)
+        vis = (j != h) & ((c > 0) | ((i != 0) | (j != 0)) & (j <= h) & ~((i > h) & (j == 0)))
+        bins = np.searchsorted(e2, q, side="right") - 1
+        ok = vis & (bins >= 0) & (bins < nbins)
+        out += np.bincount(bins[ok], minlength=nbins)[:nbins]
+    return out
+
+
+def test_mode_count_helper_matches_oracle():
+    # the direct count agrees with the oracle's octant loop on a small mesh
+    n = 24
+    spec = np.zeros((n, n, n // 2 + 1), np.complex128)
+    for nb, du in ((12, 1.0), (8, 1.5)):
+        r = orc.power_from_spectrum(spec, n, 100.0, orc.NGP, nb, 1.0, 1.0, 0.0, du)
+        assert np.array_equal(mode_counts(n, nb, 0.0, du), r.modes)
+
+
+def test_plain_small_config_full_size_vs_oracle(ctx):
+    c = synth.config_c1()
+    n, box = c["n"], c["box"]
+    res = ctx.job(c["x"], c["y"], c["z"], None, make_grid(n, box), CIC, F64, pk=Context.pk_opts(CIC, nbins=64),
+                  tweb=Context.tweb_opts(c["R"], c["lth"], BAND), want_labels=True)
+    mesh, lost = orc.assign_f64(CIC, c["x"], c["y"], c["z"], None, orc.Grid.cubic(n, box))
+    assert res["assign"].n_lost == lost == 0 and res["assign"].n_in == c["x"].size
+    pk = orc.power_grid(mesh, box, CIC, 64)
+    floor = pk.shot_noise * pk.sum_sn / np.maximum(pk.modes, 1)
+    assert np.array_equal(res["pk"].modes, pk.modes)
+    assert pk_rel_err(res["pk"].pk, pk.pk, floor) <= 1e-6
+    tw = orc.tweb_density(mesh, box, c["R"], c["lth"], BAND)
+    near = np.any(np.abs(tw.lam.reshape(-1, 3) - c["lth"]) <= BAND, axis=1).reshape(tw.labels.shape)
+    assert int(((res["tweb"].labels != tw.labels) & ~near).sum()) == 0
+
+
+@pytest.fixture(scope="module")
+def sweep_particles():
+    import torch
+    c = synth.config_c2()
+    return c, [torch.from_numpy(c[k]).cuda() for k in ("x", "y", "z", "w")]
+
+
+@pytest.mark.parametrize("scheme", [NGP, CIC, TSC])
+def test_scheme_sweep_full_size_properties(ctx, sweep_particles, scheme):
+    import torch
+    c, (x, y, z, w) = sweep_particles
+    n, box, nb = c["n"], c["box"], c["nbins"]
+    g = make_grid(n, box)
+    opts = Context.pk_opts(scheme, nbins=nb)
+    r1 = ctx.job(x, y, z, w, g, scheme, F32, pk=opts)
+    r2 = ctx.job(x, y, z, w, g, scheme, F32, pk=opts)
+    perm = torch.randperm(x.numel(), device="cuda", generator=torch.Generator("cuda").manual_seed(scheme))
+    xs, ys, zs, ws = x[perm], y[perm], z[perm], w[perm]
+    # the context launches on its own stream: device inputs must be complete
+    torch.cuda.synchronize()
+    r3 = ctx.job(xs, ys, zs, ws, g, scheme, F32, pk=opts)
+    npart = x.numel()
+    assert r1["assign"].n_lost == 0 and r1["assign"].n_in == npart
+    wsum = float(np.sum(c["w"], dtype=np.float64))
+    assert abs(r1["assign"].sum_mesh - wsum) <= 1e-6 * wsum
+    for r in (r2, r3):
+        assert r["assign"].sum_mesh == r1["assign"].sum_mesh
+        assert np.array_equal(r["pk"].pk, r1["pk"].pk)
+    assert np.array_equal(r1["pk"].modes, mode_counts(n, nb))
+    if scheme == NGP:
+        cnt = ctx.count_ngp(x, y, z, g)
+        assert int(cnt.mesh.sum(dtype=torch.int64)) == cnt.n_in == npart
+
+
+def test_large_job_full_size_properties(ctx):
+    # 768^3 TSC of 452,984,832 particles, P(k) 256 bins of 1.5 k_f, T-web R = 3, lambda_th = 0.1
+    n, box = 768, 1500.0
+    import torch
+    x, y, z, _ = synth.zeldovich_lattice(n, box, device="cuda")
+    torch.cuda.synchronize()  # made by torch on its stream; the context uses its own
+    res = ctx.job(x, y, z, None, make_grid(n, box), TSC, F32, pk=Context.pk_opts(TSC, nbins=256, ndel=1.5),
+                  tweb=Context.tweb_opts(3.0, 0.1, BAND))
+    npart = n ** 3
+    assert res["assign"].n_lost == 0 and res["assign"].n_in == npart
+    assert abs(res["assign"].sum_mesh - npart) <= 1e-6 * npart
+    assert int(res["tweb"].counts.sum()) == npart
+    assert np.array_equal(res["pk"].modes, mode_counts(n, 256, 0.0, 1.5))
+    assert np.all(np.isfinite(res["pk"].pk))
