@@ -77,7 +77,12 @@ class AssignResult:
 
 
 class Context:
-    """A cam_ctx on one device with an optional HBM budget (bytes)."""
+    """A cam_ctx on one device with an optional HBM budget (bytes).
+
+    Device arrays (torch tensors) are read on the context's own stream: ones
+    just produced by torch kernels must be complete first
+    (torch.cuda.synchronize()), or set_stream(torch.cuda.current_stream().cuda_stream)
+    makes the context launch on torch's stream."""
 
     def __init__(self, device: int = 0, hbm_budget: int = 0):
         self._lib = L.lib()

@@ -148,7 +148,9 @@ typedef struct {
 } cam_alloc_stats;
 int cam_alloc_stats_get(cam_alloc_stats *out, int reset);
 /* Sets the CUDA stream (cudaStream_t) the context launches on (NULL = the
- * context's own stream). */
+ * context's own stream).  Device inputs are read on that stream: data that
+ * the caller produced on another stream must be complete before the call,
+ * or the caller sets its own stream here. */
 int cam_ctx_set_stream(cam_ctx *ctx, void *stream);
 int cam_ctx_sync(cam_ctx *ctx);
 /* Message of the last failure on this context ("" if none). */
