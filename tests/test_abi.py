@@ -84,3 +84,17 @@ def test_alloc_stats_without_device():
     assert L.lib().cam_alloc_stats_get(ctypes.byref(st), 1) == L.CAM_OK
     assert st.allocs >= 0 and st.failures >= 0
     assert L.lib().cam_alloc_stats_get(None, 0) == L.CAM_E_INVAL
+
+
+def test_new_entry_points_reject_null_context_without_device():
+    # host-side guards of the finite-difference, BAM-kernel, cross-spectrum,
+    # multipole, invariant and catalogue-weight entry points: no device work
+    lib = L.lib()
+    assert lib.cam_poisson(None, None, None, 0, 0, 0.0, None, 0) == L.CAM_E_INVAL
+    assert lib.cam_gradfindif(None, None, None, 0, 0, 1, None, 0) == L.CAM_E_INVAL
+    assert lib.cam_bam_kernel_update(None, None, 0, 0.0, 1.0, 8, None, 0, None, 0, None, None) == L.CAM_E_INVAL
+    assert lib.cam_konvolve(None, None, None, 0, 0, None, 0, None, 0) == L.CAM_E_INVAL
+    assert lib.cam_cross_power(None, None, None, None, 0, 0, None, 0, 0, None, None, None, None, None) == L.CAM_E_INVAL
+    assert lib.cam_power_multipoles(None, None, None, 0, 0, None, 2, None, None, None, None, None, None) == L.CAM_E_INVAL
+    assert lib.cam_tweb_invariants(None, None, None, 0, 0, None, None, None, None, 0, None) == L.CAM_E_INVAL
+    assert lib.cam_fkp_weights(None, 10, None, 1.0, None, 1, 1e4, 0, None, 0, None) == L.CAM_E_INVAL
