@@ -5,11 +5,17 @@
  * calls this file; only the tests, the smoke check and the CPU-baseline leg of
  * the benchmark do, as the checker or as the timed CPU reference.
  *
- * Parity status: UNPINNED.  The reference (balaguera/COSMICATLAS) cannot be
- * compiled in this environment (FFTW3, GSL, boost, HEALPix, CFITSIO and several
- * of its own headers are absent) and it ships no tests, golden vectors or
- * fixtures.  This file is a restatement of the reference source text; every
- * function names the reference lines it follows.
+ * Parity status.  Mass assignment (getDensity_NGP/CIC/TSC) is PINNED: the
+ * reference's own functions are compiled from Source/massFunctions.cpp by
+ * oracle/Makefile (target ref, stand-in headers in oracle/refstub/), and
+ * tests/test_golden_reference.py checks that orc_assign_ref reproduces their
+ * meshes bit for bit, that the keys of orc_keys give their NGP counts, and
+ * that orc_assign_f64 agrees within 1e-5 (tests/golden/getdensity_ref.npz,
+ * written by tests/golden/make_golden.py).  The P(k) estimator and the T-web
+ * are UNPINNED: their reference code needs FFTW3, GSL and the FftwFunctions
+ * and Cwclass class headers, none of which can be built here, and the
+ * reference ships no tests, golden vectors or fixtures; those functions
+ * restate the reference source text, each naming the lines it follows.
  *
  * Two families of functions live here:
  *   orc_*_f64  : the FP64 oracle with the pinned semantics the GPU path must
@@ -184,13 +190,148 @@ int64_t orc_assign_f64(int scheme, int64_t np, const float *x, const float *y,
     return lost;
 }
 
+/* orc_assign_f64 on all threads, for the full-size configurations (16.8 M
+ * and 453 M particles): particle chunks per thread, every cell update an
+ * atomic FP64 add.  The set of contributions is the serial function's; only
+ * the order of the FP64 additions varies (~1e-16 relative), far inside the
+ * 1e-5 tolerance the oracle checks against. */
+int64_t orc_assign_f64_mt(int scheme, int64_t np, const float *x, const float *y,
+                          const float *z, const float *w, const int64_t n[3],
+                          const float L[3], const float d[3], const float mn[3],
+                          double *mesh)
+{
+    const int64_t ncell = n[0] * n[1] * n[2];
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < ncell; ++i) mesh[i] = 0.0;
+    int64_t lost = 0;
+#pragma omp parallel for schedule(static, 65536) reduction(+ : lost)
+    for (int64_t p = 0; p < np; ++p) {
+        float pos[3] = {x[p], y[p], z[p]};
+        int64_t c[3];
+        if (!ref_home(scheme, pos, n, L, d, mn, c)) { ++lost; continue; }
+        double wa[3][3];
+        int first[3], width[3];
+        for (int a = 0; a < 3; ++a) {
+            double t = (scheme == ORC_NGP) ? 0.0 : exact_offset(pos[a], mn[a], d[a], c[a], n[a], 0.5);
+            width[a] = stencil_f64(scheme, t, wa[a], &first[a]);
+        }
+        const double m = w ? (double)w[p] : 1.0;
+        for (int ia = 0; ia < width[0]; ++ia) {
+            int64_t ii = wrap(c[0] + first[0] + ia, n[0]);
+            for (int ja = 0; ja < width[1]; ++ja) {
+                int64_t jj = wrap(c[1] + first[1] + ja, n[1]);
+                double wij = m * wa[0][ia] * wa[1][ja];
+                for (int ka = 0; ka < width[2]; ++ka) {
+                    int64_t kk = wrap(c[2] + first[2] + ka, n[2]);
+#pragma omp atomic update
+                    mesh[kk + n[2] * (jj + n[1] * ii)] += wij * wa[2][ka];
+                }
+            }
+        }
+    }
+    return lost;
+}
+
 /* ------------------------------------------------------------------------ */
 /* Reference loops as written (FP32) -- the timed CPU baseline.             */
 /* ------------------------------------------------------------------------ */
 
+/* One particle of getDensity_NGP / _CIC / _TSC (Gen A) as written, into the
+ * float mesh delta: Source/massFunctions.cpp:57-76 (NGP), :700-770 (CIC),
+ * :1076-1160 (TSC), including the post-wrap cell used for dx and the float
+ * accumulation.  Returns 0 if the particle is assigned, 1 if it is lost. */
+static inline int ref_one(int scheme, float px, float py, float pz, float mass, int64_t N1, int64_t N2,
+                          int64_t N3, float L1, float L2, float L3, float d1, float d2, float d3, float min1,
+                          float min2, float min3, float *delta)
+{
+#define DELTA(i, j, k) delta[(k) + N3 * ((j) + N2 * (i))]
+    if (scheme == ORC_NGP) {
+        if ((px >= min1 && px < min1 + L1) && (py >= min2 && py < min2 + L2) && (pz >= min3 && pz < min3 + L3)) {
+            uint64_t i = (uint64_t)floorf((px - min1) / d1);
+            uint64_t j = (uint64_t)floorf((py - min2) / d2);
+            uint64_t k = (uint64_t)floorf((pz - min3) / d3);
+            i = (uint64_t)fmodf((float)i, (float)N1);
+            j = (uint64_t)fmodf((float)j, (float)N2);
+            k = (uint64_t)fmodf((float)k, (float)N3);
+            DELTA(i, j, k) += mass;
+            return 0;
+        }
+        return 1;
+    }
+    if (scheme == ORC_CIC) {
+        float xpos = (float)((double)px - 0.5 * (double)d1);
+        float ypos = (float)((double)py - 0.5 * (double)d2);
+        float zpos = (float)((double)pz - 0.5 * (double)d3);
+        if (xpos < 0.f) xpos += L1;
+        if (xpos >= L1) xpos -= L1;
+        if (ypos < 0.f) ypos += L1;
+        if (ypos >= L1) ypos -= L1;
+        if (zpos < 0.f) zpos += L1;
+        if (zpos >= L1) zpos -= L1;
+        if ((xpos >= min1 && xpos < min1 + L1) && (ypos >= min2 && ypos < min2 + L2) &&
+            (zpos >= min3 && zpos < min3 + L3)) {
+            uint64_t i = (uint64_t)floorf((xpos - min1) / d1);
+            uint64_t j = (uint64_t)floorf((ypos - min2) / d2);
+            uint64_t k = (uint64_t)floorf((zpos - min3) / d3);
+            i = (uint64_t)fmodf((float)i, (float)N1);
+            j = (uint64_t)fmodf((float)j, (float)N2);
+            k = (uint64_t)fmodf((float)k, (float)N3);
+            uint64_t ii = (uint64_t)fmodf((float)(i + 1), (float)N1);
+            uint64_t jj = (uint64_t)fmodf((float)(j + 1), (float)N2);
+            uint64_t kk = (uint64_t)fmodf((float)(k + 1), (float)N3);
+            float dx = (xpos - min1) / d1 - (float)i;
+            float dy = (ypos - min2) / d2 - (float)j;
+            float dz = (zpos - min3) / d3 - (float)k;
+            float tx = 1.0f - dx, ty = 1.0f - dy, tz = 1.0f - dz;
+            DELTA(i, j, k) += mass * tx * ty * tz;
+            DELTA(ii, j, k) += mass * dx * ty * tz;
+            DELTA(i, jj, k) += mass * tx * dy * tz;
+            DELTA(i, j, kk) += mass * tx * ty * dz;
+            DELTA(ii, jj, k) += mass * dx * dy * tz;
+            DELTA(ii, j, kk) += mass * dx * ty * dz;
+            DELTA(i, jj, kk) += mass * tx * dy * dz;
+            DELTA(ii, jj, kk) += mass * dx * dy * dz;
+            return 0;
+        }
+        return 1;
+    }
+    if ((px >= min1 && px <= min1 + L1) && (py >= min2 && py <= min2 + L2) && (pz >= min3 && pz <= min3 + L3)) {
+        uint64_t i = (uint64_t)floorf((px - min1) / d1);
+        uint64_t j = (uint64_t)floorf((py - min2) / d2);
+        uint64_t k = (uint64_t)floorf((pz - min3) / d3);
+        i = (uint64_t)fmodf((float)i, (float)N1);
+        j = (uint64_t)fmodf((float)j, (float)N2);
+        k = (uint64_t)fmodf((float)k, (float)N3);
+        uint64_t ii = (uint64_t)fmodf((float)(i + 1), (float)N1);
+        uint64_t jj = (uint64_t)fmodf((float)(j + 1), (float)N2);
+        uint64_t kk = (uint64_t)fmodf((float)(k + 1), (float)N3);
+        uint64_t iii = (uint64_t)fmodf((float)(i - 1 + N1), (float)N1);
+        uint64_t jjj = (uint64_t)fmodf((float)(j - 1 + N2), (float)N2);
+        uint64_t kkk = (uint64_t)fmodf((float)(k - 1 + N3), (float)N3);
+        float xc = (float)i + 0.5f, yc = (float)j + 0.5f, zc = (float)k + 0.5f;
+        float dx = (px - min1) / d1 - xc;
+        float dy = (py - min2) / d2 - yc;
+        float dz = (pz - min3) / d3 - zc;
+        float hx0 = (float)(0.75 - dx * dx), hy0 = (float)(0.75 - dy * dy), hz0 = (float)(0.75 - dz * dz);
+        float hxp1 = (float)(0.5 * (0.5 + dx) * (0.5 + dx));
+        float hyp1 = (float)(0.5 * (0.5 + dy) * (0.5 + dy));
+        float hzp1 = (float)(0.5 * (0.5 + dz) * (0.5 + dz));
+        float hxm1 = (float)(0.5 * (0.5 - dx) * (0.5 - dx));
+        float hym1 = (float)(0.5 * (0.5 - dy) * (0.5 - dy));
+        float hzm1 = (float)(0.5 * (0.5 - dz) * (0.5 - dz));
+        const uint64_t I[3] = {iii, i, ii}, J[3] = {jjj, j, jj}, K[3] = {kkk, k, kk};
+        const float hx[3] = {hxm1, hx0, hxp1}, hy[3] = {hym1, hy0, hyp1}, hz[3] = {hzm1, hz0, hzp1};
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b)
+                for (int c = 0; c < 3; ++c) DELTA(I[a], J[b], K[c]) += mass * hx[a] * hy[b] * hz[c];
+        return 0;
+    }
+    return 1;
+#undef DELTA
+}
+
 /* getDensity_NGP / _CIC / _TSC, Gen A, serial particle loop, float mesh.
- * Source/massFunctions.cpp:35-98, :678-790, :1050-1165.  Kept as written,
- * including the post-wrap cell used for dx and the float accumulation. */
+ * Source/massFunctions.cpp:35-98, :678-790, :1050-1165. */
 int64_t orc_assign_ref(int scheme, int64_t np, const float *xp, const float *yp,
                        const float *zp, const float *w, int64_t N1, int64_t N2,
                        int64_t N3, float L1, float L2, float L3, float d1, float d2,
@@ -200,102 +341,43 @@ int64_t orc_assign_ref(int scheme, int64_t np, const float *xp, const float *yp,
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < ncell; ++i) delta[i] = 0.0f;
     int64_t lost = 0;
-#define DELTA(i, j, k) delta[(k) + N3 * ((j) + N2 * (i))]
-    if (scheme == ORC_NGP) {
-        for (int64_t n = 0; n < np; ++n) {
-            if ((xp[n] >= min1 && xp[n] < min1 + L1) && (yp[n] >= min2 && yp[n] < min2 + L2) &&
-                (zp[n] >= min3 && zp[n] < min3 + L3)) {
-                uint64_t i = (uint64_t)floorf((xp[n] - min1) / d1);
-                uint64_t j = (uint64_t)floorf((yp[n] - min2) / d2);
-                uint64_t k = (uint64_t)floorf((zp[n] - min3) / d3);
-                i = (uint64_t)fmodf((float)i, (float)N1);
-                j = (uint64_t)fmodf((float)j, (float)N2);
-                k = (uint64_t)fmodf((float)k, (float)N3);
-                float mass = w ? w[n] : 1.0f;
-                DELTA(i, j, k) += mass;
-            } else {
-                ++lost;
-            }
+    for (int64_t n = 0; n < np; ++n)
+        lost += ref_one(scheme, xp[n], yp[n], zp[n], w ? w[n] : 1.0f, N1, N2, N3, L1, L2, L3, d1, d2, d3, min1,
+                        min2, min3, delta);
+    return lost;
+}
+
+/* The Gen-B OpenMP form of getDensity_* (Source/Miscelanious.cpp:454-560 CIC,
+ * :693 TSC and the NGP twin): every thread accumulates into its own private
+ * float grid, and the grids are added into delta one thread at a time under
+ * `omp critical`.  As written there, an inner `omp parallel` region wraps the
+ * particle loop without a work-sharing `for`, so every thread processes every
+ * particle and the mesh comes out NTHREADS times too large; here the loop is
+ * shared (`omp for`), which is the fix.  The per-particle arithmetic is Gen
+ * A's (ref_one).  nthreads <= 0: all available threads. */
+int64_t orc_assign_omp(int scheme, int64_t np, const float *xp, const float *yp, const float *zp,
+                       const float *w, int64_t N1, int64_t N2, int64_t N3, float L1, float L2, float L3,
+                       float d1, float d2, float d3, float min1, float min2, float min3, float *delta,
+                       int nthreads)
+{
+    const int64_t ncell = N1 * N2 * N3;
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (int64_t i = 0; i < ncell; ++i) delta[i] = 0.0f;
+    int64_t lost = 0;
+#pragma omp parallel num_threads(nthreads) reduction(+ : lost)
+    {
+        float *priv = (float *)calloc((size_t)ncell, sizeof(float));
+#pragma omp for schedule(static)
+        for (int64_t n = 0; n < np; ++n)
+            lost += ref_one(scheme, xp[n], yp[n], zp[n], w ? w[n] : 1.0f, N1, N2, N3, L1, L2, L3, d1, d2, d3,
+                            min1, min2, min3, priv);
+#pragma omp critical
+        {
+            for (int64_t i = 0; i < ncell; ++i) delta[i] += priv[i];
         }
-    } else if (scheme == ORC_CIC) {
-        for (int64_t n = 0; n < np; ++n) {
-            float xpos = (float)((double)xp[n] - 0.5 * (double)d1);
-            float ypos = (float)((double)yp[n] - 0.5 * (double)d2);
-            float zpos = (float)((double)zp[n] - 0.5 * (double)d3);
-            if (xpos < 0.f) xpos += L1;
-            if (xpos >= L1) xpos -= L1;
-            if (ypos < 0.f) ypos += L1;
-            if (ypos >= L1) ypos -= L1;
-            if (zpos < 0.f) zpos += L1;
-            if (zpos >= L1) zpos -= L1;
-            if ((xpos >= min1 && xpos < min1 + L1) && (ypos >= min2 && ypos < min2 + L2) &&
-                (zpos >= min3 && zpos < min3 + L3)) {
-                uint64_t i = (uint64_t)floorf((xpos - min1) / d1);
-                uint64_t j = (uint64_t)floorf((ypos - min2) / d2);
-                uint64_t k = (uint64_t)floorf((zpos - min3) / d3);
-                i = (uint64_t)fmodf((float)i, (float)N1);
-                j = (uint64_t)fmodf((float)j, (float)N2);
-                k = (uint64_t)fmodf((float)k, (float)N3);
-                uint64_t ii = (uint64_t)fmodf((float)(i + 1), (float)N1);
-                uint64_t jj = (uint64_t)fmodf((float)(j + 1), (float)N2);
-                uint64_t kk = (uint64_t)fmodf((float)(k + 1), (float)N3);
-                float dx = (xpos - min1) / d1 - (float)i;
-                float dy = (ypos - min2) / d2 - (float)j;
-                float dz = (zpos - min3) / d3 - (float)k;
-                float tx = 1.0f - dx, ty = 1.0f - dy, tz = 1.0f - dz;
-                float mass = w ? w[n] : 1.0f;
-                DELTA(i, j, k) += mass * tx * ty * tz;
-                DELTA(ii, j, k) += mass * dx * ty * tz;
-                DELTA(i, jj, k) += mass * tx * dy * tz;
-                DELTA(i, j, kk) += mass * tx * ty * dz;
-                DELTA(ii, jj, k) += mass * dx * dy * tz;
-                DELTA(ii, j, kk) += mass * dx * ty * dz;
-                DELTA(i, jj, kk) += mass * tx * dy * dz;
-                DELTA(ii, jj, kk) += mass * dx * dy * dz;
-            } else {
-                ++lost;
-            }
-        }
-    } else {
-        for (int64_t n = 0; n < np; ++n) {
-            if ((xp[n] >= min1 && xp[n] <= min1 + L1) && (yp[n] >= min2 && yp[n] <= min2 + L2) &&
-                (zp[n] >= min3 && zp[n] <= min3 + L3)) {
-                uint64_t i = (uint64_t)floorf((xp[n] - min1) / d1);
-                uint64_t j = (uint64_t)floorf((yp[n] - min2) / d2);
-                uint64_t k = (uint64_t)floorf((zp[n] - min3) / d3);
-                i = (uint64_t)fmodf((float)i, (float)N1);
-                j = (uint64_t)fmodf((float)j, (float)N2);
-                k = (uint64_t)fmodf((float)k, (float)N3);
-                uint64_t ii = (uint64_t)fmodf((float)(i + 1), (float)N1);
-                uint64_t jj = (uint64_t)fmodf((float)(j + 1), (float)N2);
-                uint64_t kk = (uint64_t)fmodf((float)(k + 1), (float)N3);
-                uint64_t iii = (uint64_t)fmodf((float)(i - 1 + N1), (float)N1);
-                uint64_t jjj = (uint64_t)fmodf((float)(j - 1 + N2), (float)N2);
-                uint64_t kkk = (uint64_t)fmodf((float)(k - 1 + N3), (float)N3);
-                float xc = (float)i + 0.5f, yc = (float)j + 0.5f, zc = (float)k + 0.5f;
-                float dx = (xp[n] - min1) / d1 - xc;
-                float dy = (yp[n] - min2) / d2 - yc;
-                float dz = (zp[n] - min3) / d3 - zc;
-                float hx0 = (float)(0.75 - dx * dx), hy0 = (float)(0.75 - dy * dy), hz0 = (float)(0.75 - dz * dz);
-                float hxp1 = (float)(0.5 * (0.5 + dx) * (0.5 + dx));
-                float hyp1 = (float)(0.5 * (0.5 + dy) * (0.5 + dy));
-                float hzp1 = (float)(0.5 * (0.5 + dz) * (0.5 + dz));
-                float hxm1 = (float)(0.5 * (0.5 - dx) * (0.5 - dx));
-                float hym1 = (float)(0.5 * (0.5 - dy) * (0.5 - dy));
-                float hzm1 = (float)(0.5 * (0.5 - dz) * (0.5 - dz));
-                float mass = w ? w[n] : 1.0f;
-                const uint64_t I[3] = {iii, i, ii}, J[3] = {jjj, j, jj}, K[3] = {kkk, k, kk};
-                const float hx[3] = {hxm1, hx0, hxp1}, hy[3] = {hym1, hy0, hyp1}, hz[3] = {hzm1, hz0, hzp1};
-                for (int a = 0; a < 3; ++a)
-                    for (int b = 0; b < 3; ++b)
-                        for (int c = 0; c < 3; ++c)
-                            DELTA(I[a], J[b], K[c]) += mass * hx[a] * hy[b] * hz[c];
-            } else {
-                ++lost;
-            }
-        }
+        free(priv);
     }
-#undef DELTA
     return lost;
 }
 
@@ -623,4 +705,15 @@ void orc_classify(int64_t ncell, const double *lam, double lth, double band,
     }
     for (int a = 0; a < 4; ++a) counts[a] = cnt[a];
     *ties = nt;
+}
+
+/* Thread count of the OpenMP loops above (CPU-baseline runs at a stated
+ * thread count); n <= 0 restores all available threads. */
+void orc_set_threads(int n)
+{
+#ifdef _OPENMP
+    omp_set_num_threads(n > 0 ? n : omp_get_num_procs());
+#else
+    (void)n;
+#endif
 }

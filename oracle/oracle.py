@@ -3,13 +3,17 @@
 Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
 ``bench.py`` import this module; the product library never does.
 
-Parity status: UNPINNED.  The reference cannot be compiled here (FFTW3, GSL,
-boost, HEALPix, CFITSIO and some of its own headers are missing) and ships no
-golden vectors, so this module restates the reference source text:
+Parity status: mass assignment PINNED, the rest UNPINNED.  The reference's
+own getDensity_NGP/CIC/TSC compile from Source/massFunctions.cpp against
+stand-in headers (oracle/Makefile, target ref -> oracle/_ref/); the golden
+meshes they write (tests/golden/) pin this module's assignment and keys.
+The P(k) estimator and the T-web need FFTW3, GSL and class headers that
+cannot be built here, and the reference ships no golden vectors, so this
+module restates the reference source text:
 
 * mass assignment, keys, P(k) binning, eigenvalues: ``oracle/cam_oracle.c``
   (each function cites the reference lines it follows);
-* FFTs: numpy's pocketfft in FP64 stands in for FFTW3 (unpinned third-party
+* FFTs: pocketfft (scipy's, threaded) in FP64 stands in for FFTW3 (unpinned third-party
   boundary: the reference links an unversioned system FFTW,
   Main/Makefile:42-43);
 * the tidal tensor follows calc_LapPhiv, Source/NumericalMethods.cpp:2609-2680,
@@ -40,6 +44,51 @@ def build() -> str:
     return so
 
 
+REF_SRC = os.environ.get("CAM_REFERENCE_TREE", "/root/reference")
+REF_SO = os.path.join(_HERE, "_ref", "libref_mass.so")
+_REF = None
+
+
+def build_ref() -> str | None:
+    """Compile the reference's own getDensity_NGP/CIC/TSC from its source tree
+    (oracle/Makefile, target ref) into oracle/_ref/ when the tree is present;
+    returns the .so path if it exists (built here, or shipped prebuilt)."""
+    src = os.path.join(REF_SRC, "Source", "massFunctions.cpp")
+    if os.path.exists(src):
+        subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF={REF_SRC}"], check=True)
+    return REF_SO if os.path.exists(REF_SO) else None
+
+
+def ref_lib():
+    """The reference's compiled getDensity_* (None when oracle/_ref is absent)."""
+    global _REF
+    if _REF is None and os.path.exists(REF_SO):
+        _REF = ctypes.CDLL(REF_SO)
+        P = ctypes.c_void_p
+        _REF.ref_assign.argtypes = [ctypes.c_int, ctypes.c_int64, P, P, P, P, ctypes.c_int64, ctypes.c_int64,
+                                    ctypes.c_int64] + [ctypes.c_float] * 9 + [P, P]
+        _REF.ref_assign.restype = ctypes.c_int
+    return _REF
+
+
+def reference_getdensity(scheme, x, y, z, w, grid: "Grid"):
+    """The reference's own getDensity_{NGP,CIC,TSC} (Source/massFunctions.cpp,
+    compiled from source): its float mesh and the seconds the call took."""
+    r = ref_lib()
+    if r is None:
+        raise FileNotFoundError("oracle/_ref/libref_mass.so is not built")
+    x, y, z = _f32(x), _f32(y), _f32(z)
+    w = None if w is None else _f32(w)
+    n, L, d, mn = grid.n, grid.L, grid.d, grid.mn
+    mesh = np.empty(tuple(n), np.float32)
+    sec = ctypes.c_double(0.0)
+    rc = r.ref_assign(scheme, x.size, _p(x), _p(y), _p(z), _p(w), n[0], n[1], n[2], L[0], L[1], L[2],
+                      d[0], d[1], d[2], mn[0], mn[1], mn[2], _p(mesh), ctypes.byref(sec))
+    if rc != 0:
+        raise ValueError("ref_assign failed")
+    return mesh, sec.value
+
+
 def lib():
     global _LIB
     if _LIB is None:
@@ -50,9 +99,16 @@ def lib():
         _LIB.orc_keys.restype = None
         _LIB.orc_assign_f64.argtypes = [i32, i64, P, P, P, P, P, P, P, P, P]
         _LIB.orc_assign_f64.restype = i64
+        _LIB.orc_assign_f64_mt.argtypes = [i32, i64, P, P, P, P, P, P, P, P, P]
+        _LIB.orc_assign_f64_mt.restype = i64
         _LIB.orc_assign_ref.argtypes = [i32, i64, P, P, P, P, i64, i64, i64,
                                         f32, f32, f32, f32, f32, f32, f32, f32, f32, P]
         _LIB.orc_assign_ref.restype = i64
+        _LIB.orc_assign_omp.argtypes = [i32, i64, P, P, P, P, i64, i64, i64,
+                                        f32, f32, f32, f32, f32, f32, f32, f32, f32, P, i32]
+        _LIB.orc_assign_omp.restype = i64
+        _LIB.orc_set_threads.argtypes = [i32]
+        _LIB.orc_set_threads.restype = None
         _LIB.orc_power_f64.argtypes = [i64, P, i32, i32, i32, f64, f64, f64, f64, i32, P, P, P, P]
         _LIB.orc_power_f64.restype = None
         _LIB.orc_cross_f64.argtypes = [i64, P, P, i32, i32, f64, f64, i32, P, P, P, P]
@@ -116,6 +172,18 @@ def assign_f64(scheme, x, y, z, w, grid: Grid):
     return mesh, int(lost)
 
 
+def assign_f64_mt(scheme, x, y, z, w, grid: Grid):
+    """assign_f64 on all host threads (atomic FP64 adds; only the order of the
+    additions differs from the serial loop): for the full-size meshes."""
+    x, y, z = _f32(x), _f32(y), _f32(z)
+    w = None if w is None else _f32(w)
+    n, L, d, mn = grid.arrays()
+    mesh = np.empty(tuple(int(v) for v in n), np.float64)
+    lost = lib().orc_assign_f64_mt(scheme, x.size, _p(x), _p(y), _p(z), _p(w),
+                                   _p(n), _p(L), _p(d), _p(mn), _p(mesh))
+    return mesh, int(lost)
+
+
 def assign_ref(scheme, x, y, z, w, grid: Grid):
     """The reference's FP32 serial loop as written (CPU baseline)."""
     x, y, z = _f32(x), _f32(y), _f32(z)
@@ -127,16 +195,36 @@ def assign_ref(scheme, x, y, z, w, grid: Grid):
     return mesh, int(lost)
 
 
+def set_threads(n: int = 0):
+    """Thread count of the oracle's OpenMP loops (n <= 0: all)."""
+    lib().orc_set_threads(int(n))
+
+
+def assign_omp(scheme, x, y, z, w, grid: Grid, nthreads=0):
+    """The Gen-B OpenMP private-grid form of the reference loops, with its
+    NTHREADS-fold over-count fixed (CPU baseline)."""
+    x, y, z = _f32(x), _f32(y), _f32(z)
+    w = None if w is None else _f32(w)
+    n, L, d, mn = grid.n, grid.L, grid.d, grid.mn
+    mesh = np.empty(tuple(n), np.float32)
+    lost = lib().orc_assign_omp(scheme, x.size, _p(x), _p(y), _p(z), _p(w), n[0], n[1], n[2],
+                                L[0], L[1], L[2], d[0], d[1], d[2], mn[0], mn[1], mn[2], _p(mesh), int(nthreads))
+    return mesh, int(lost)
+
+
 def rfft3_f64(mesh: np.ndarray) -> np.ndarray:
     """Unnormalised forward r2c (FFTW layout [i][j][k<=N/2]); stands in for
-    do_fftw_r2c, Source/NumericalMethods.cpp:1718-1753."""
-    return np.fft.rfftn(np.asarray(mesh, np.float64))
+    do_fftw_r2c, Source/NumericalMethods.cpp:1718-1753.  pocketfft in FP64
+    (scipy's, on all host threads)."""
+    import scipy.fft
+    return scipy.fft.rfftn(np.asarray(mesh, np.float64), workers=-1)
 
 
 def irfft3_f64(spec: np.ndarray, n: int) -> np.ndarray:
     """c2r divided by N^3 as do_fftw_c2r does, Source/NumericalMethods.cpp:1818-1856
-    (numpy's irfftn already divides by N^3)."""
-    return np.fft.irfftn(spec, s=(n, n, n), axes=(0, 1, 2))
+    (the inverse transform already divides by N^3)."""
+    import scipy.fft
+    return scipy.fft.irfftn(spec, s=(n, n, n), axes=(0, 1, 2), workers=-1)
 
 
 @dataclass
@@ -317,6 +405,38 @@ def tweb_from_spectrum(delta_k, n, L, R, lth, band=1e-5) -> TwebResult:
     lam = eig3_f64(t6).reshape(n, n, n, 3)
     labels, counts, ties = classify(lam, lth, band)
     return TwebResult(labels.reshape(n, n, n), lam, counts, ties)
+
+
+def tidal_planes(delta_k, n, L, R, planes) -> np.ndarray:
+    """The six components of tidal_components on the x-planes `planes` only,
+    (len(planes), N, N, 6): the inverse transform along x is evaluated at
+    those planes as a DFT (T(x_p) = sum_kx F[kx] e^{2 pi i kx x_p / N} / N),
+    then the inverse r2c over (y, z).  Equal to tidal_components[planes] up
+    to FP64 rounding; memory O(N^2 (N/2+1)) for one component at a time."""
+    import scipy.fft
+    kf = 2.0 * np.pi / L
+    fx = signed_freq(n)[:, None, None] * kf
+    fy = signed_freq(n)[None, :, None] * kf
+    fz = np.arange(n // 2 + 1, dtype=np.float64)[None, None, :] * kf
+    planes = np.asarray(planes, np.int64)
+    ex = np.exp(2j * np.pi * np.outer(planes, np.arange(n)) / n) / n  # (P, N)
+    pairs = [(0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2)]
+    out = np.empty((planes.size, n, n, 6))
+    chunk = max(1, (1 << 26) // (n * (n // 2 + 1)))
+    for c, (a, b) in enumerate(pairs):
+        acc = np.zeros((planes.size, n, n // 2 + 1), np.complex128)
+        for i0 in range(0, n, chunk):
+            i1 = min(n, i0 + chunk)
+            k = (fx[i0:i1], fy, fz)
+            k2 = k[0] * k[0] + k[1] * k[1] + k[2] * k[2]
+            with np.errstate(divide="ignore", invalid="ignore"):
+                m = np.where(k2 > 0, k[a] * k[b] / k2, 0.0)
+            if R > 0:
+                m = m * np.exp(-0.5 * k2 * R * R)
+            blk = delta_k[i0:i1] * m  # (i1-i0, N, N/2+1)
+            acc += np.tensordot(ex[:, i0:i1], blk, axes=(1, 0))
+        out[..., c] = scipy.fft.irfftn(acc, s=(n, n), axes=(1, 2), workers=-1)
+    return out
 
 
 def tweb_density(mesh, L, R, lth, band=1e-5) -> TwebResult:
