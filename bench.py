@@ -58,8 +58,12 @@ def parse():
     ap.add_argument("--rates", default="50,200,800", help="stream: Poisson arrival rates (jobs/s)")
     ap.add_argument("--held-gb", type=float, default=24.0,
                     help="stream: GB of submitted jobs' inputs the client may hold before it waits")
-    ap.add_argument("--serving-jobs", type=int, default=1024,
+    ap.add_argument("--serving-jobs", type=int, default=4096,
                     help="sweep: jobs of the calibration batch timed served vs per-call on the same line (0: skip)")
+    ap.add_argument("--stream-jobs", type=int, default=2000,
+                    help="sweep: jobs of the mixed stream timed served vs per-call on the same line (0: skip)")
+    ap.add_argument("--stream-rates", default="200",
+                    help="sweep: Poisson arrival rates of the mixed stream on the same line (besides saturation)")
     ap.add_argument("--mesh", type=int, default=0, help="single512 only: override N (profiler runs)")
     ap.add_argument("--tweb-method", default="fft", choices=["fft", "fd"],
                     help="single-job workloads: T-web tidal tensor by FFTs (k_a k_b / k^2) or by the "
@@ -236,6 +240,42 @@ def ncu_traffic():
         return None
 
 
+def cufft_r2c_ms(n, stream, reps=20):
+    """Mean time of torch.fft.rfftn (cuFFT) on an n^3 FP32 device mesh."""
+    import torch
+    m = torch.randn((n, n, n), device="cuda", dtype=torch.float32)
+    for _ in range(3):
+        torch.fft.rfftn(m)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(torch.cuda.current_stream())
+    for _ in range(reps):
+        torch.fft.rfftn(m)
+    e1.record(torch.cuda.current_stream())
+    torch.cuda.synchronize()
+    del m
+    return e0.elapsed_time(e1) / reps
+
+
+def pk_error_vs_oracle(x, y, z, w, pks):
+    """max over bins of |P - P_oracle| / max(|P_oracle|, SN C(k)/W^2) for each
+    scheme's job: the FP64 oracle assigns the same particles and bins the
+    FP64 spectrum (the error metric of the P(k) tests)."""
+    orc = _cpu_oracle()
+    out = {}
+    for s in SCHEMES:
+        mesh, _ = orc.assign_f64_mt(s, x, y, z, w, orc.Grid.cubic(NMESH, BOX))
+        ref = orc.power_grid(mesh, BOX, s, NBINS)
+        floor = np.maximum(np.abs(ref.pk), np.abs(ref.shot_noise * ref.sum_sn / np.maximum(ref.modes, 1)))
+        got = np.asarray(pks[s].pk, np.float64)
+        has = ref.modes > 0
+        out[("ngp", "cic", "tsc")[s]] = float(np.max(np.abs(got - ref.pk)[has] / floor[has]))
+    out["max"] = max(out.values())
+    out["note"] = "last timed step's three jobs vs the FP64 oracle (oracle/), computed after the timed region"
+    return out
+
+
 # -------------------------------------------------------------------------
 def run_ours(args):
     import torch
@@ -259,6 +299,8 @@ def run_ours(args):
     ctx.set_stream(stream.cuda_stream)
     opts = {s: Context.pk_opts(s, nbins=NBINS) for s in SCHEMES}
 
+    last_pk = {}
+
     def step(arrs, lat=None):
         # host arrays: one upload per step serves the three schemes
         src = arrs if arrs[0].is_cuda else [ctx.stage(*arrs)]
@@ -274,6 +316,7 @@ def run_ours(args):
             if lat is not None:
                 e1.record(stream)
                 lat.append((e0, e1))
+            last_pk[s] = r["pk"]
         return r
 
     def barrier():
@@ -349,6 +392,12 @@ def run_ours(args):
     # end to end: pinned host particles in, P(k) out
     ms_e2e = timed_host_fed(args.steps) if not args.kernels_only else float("nan")
 
+    # the FFT stage against cuFFT (torch.fft.rfftn on the device), comparison only
+    cufft_ms = cufft_r2c_ms(NMESH, stream) if rank == 0 else None
+    # P(k) of the last timed step's three jobs against the FP64 oracle
+    # (outside the timed region)
+    pk_err = pk_error_vs_oracle(x, y, z, w, last_pk) if rank == 0 and not args.kernels_only else None
+
     jobs = len(SCHEMES) * args.steps * world
     value = whole_job_rate(len(SCHEMES) * args.steps, world, ms)
     e2e = whole_job_rate(len(SCHEMES) * args.steps, world, ms_e2e)
@@ -412,6 +461,13 @@ def run_ours(args):
             "kernels": kernels,
             "clocks": clk.summary(),
         }
+        if cufft_ms is not None:
+            out["stages"]["fft_r2c"]["cufft_ms"] = round(cufft_ms, 4)
+            out["stages"]["fft_r2c"]["cufft_note"] = ("torch.fft.rfftn of a 256^3 FP32 device mesh (cuFFT), CUDA "
+                                                      "events, comparison only: not on the product path")
+        if pk_err is not None:
+            out["pk_rel_err"] = pk_err["max"]
+            out["pk_rel_err_detail"] = pk_err
     ctx.close()
     if world > 1:
         dist.barrier()
@@ -419,61 +475,113 @@ def run_ours(args):
     return out, (x, y, z, w)
 
 
-def cpu_baseline_sample(x, y, z, w, nsample, cores):
-    """The reference path as written on the host (oracle port): serial FP32
-    scatter, threaded FP32 r2c (scipy pocketfft), the OpenMP P(k) loop."""
+def _cpu_oracle():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
-    import scipy.fft
+    return orc
 
+
+def cpu_job(orc, scheme, x, y, z, w, assign="reference", threads=0):
+    """One scheme-sweep job on the host, as the reference runs it:
+    assign = "reference": the reference's own getDensity_* compiled from its
+    source (oracle/_ref; Gen A, serial particle loop, as Main/Makefile links
+    it), or its FP32 restatement when oracle/_ref is absent ("port");
+    assign = "omp": the Gen-B private-grid OpenMP form (NTHREADS-fold count
+    fixed) on `threads` threads.  Then the threaded r2c (scipy's pocketfft
+    in FP32 standing in for FFTW3, absent here) and the OpenMP P(k) loop as
+    written (octant-4 |delta|^2 fixed).  Returns seconds per stage."""
+    import scipy.fft
+    cores = threads if threads > 0 else (os.cpu_count() or 1)
+    orc.set_threads(cores)
     g = orc.Grid.cubic(NMESH, BOX)
-    t_assign = 0.0
-    t_rest = 0.0
-    for s in SCHEMES:
-        t0 = time.perf_counter()
-        mesh, _ = orc.assign_ref(s, x[:nsample], y[:nsample], z[:nsample], w[:nsample], g)
-        t_assign += time.perf_counter() - t0
-        t0 = time.perf_counter()
-        ngal = float(mesh.sum(dtype=np.float64))
-        data = mesh - np.float32(ngal / mesh.size)
-        spec = scipy.fft.rfftn(data, workers=cores)
-        vol = BOX ** 3
-        orc.power_ref(spec, NMESH, BOX, s, NBINS, vol / ngal, ngal * ngal / vol)
-        t_rest += time.perf_counter() - t0
-    scale = x.size / nsample
-    per_job = (t_assign * scale + t_rest) / len(SCHEMES)
-    return 1.0 / per_job, per_job
+    t0 = time.perf_counter()
+    if assign == "omp":
+        mesh, _ = orc.assign_omp(scheme, x, y, z, w, g, cores)
+        t_assign = time.perf_counter() - t0
+    elif orc.ref_lib() is not None:
+        mesh, t_assign = orc.reference_getdensity(scheme, x, y, z, w, g)
+    else:
+        mesh, _ = orc.assign_ref(scheme, x, y, z, w, g)
+        t_assign = time.perf_counter() - t0
+    t1 = time.perf_counter()
+    ngal = float(mesh.sum(dtype=np.float64))
+    data = mesh - np.float32(ngal / mesh.size)
+    spec = scipy.fft.rfftn(data, workers=cores)
+    t2 = time.perf_counter()
+    vol = BOX ** 3
+    orc.power_ref(spec, NMESH, BOX, scheme, NBINS, vol / ngal, ngal * ngal / vol)
+    t3 = time.perf_counter()
+    orc.set_threads(0)
+    return {"assign": t_assign, "fft": t2 - t1, "power": t3 - t2}
+
+
+def cpu_baseline_block(x, y, z, w):
+    """The CPU baseline on this host, one full-size job per scheme (no
+    sampling): the reference's Gen-A loops (compiled from its source when
+    oracle/_ref is present) with FFT and P(k) on all cores, plus the Gen-B
+    OpenMP assignment on all cores and on the reference's 12 threads
+    (_NTHREADS_, Headers/def.h:278)."""
+    orc = _cpu_oracle()
+    cores = os.cpu_count() or 1
+    kind = "reference" if orc.ref_lib() is not None else "port"
+    per = [cpu_job(orc, s, x, y, z, w) for s in SCHEMES]
+    job_s = sum(sum(t.values()) for t in per) / len(SCHEMES)
+    omp_all = [cpu_job(orc, s, x, y, z, w, "omp", cores) for s in SCHEMES]
+    omp12 = [cpu_job(orc, s, x, y, z, w, "omp", 12) for s in SCHEMES]
+
+    def rate(ts):
+        return round(len(ts) / sum(sum(t.values()) for t in ts), 4)
+    return {
+        "value": round(1.0 / job_s, 4), "unit": "jobs/s", "cores": cores, "kind": kind,
+        "sample": "one full-size job per scheme (16,777,216 particles, 256^3, 128 bins): "
+                  + ("the reference's getDensity_* compiled from its source (Gen A, serial scatter)"
+                     if kind == "reference" else "the oracle's restatement of getDensity_* (Gen A, serial)")
+                  + f", scipy pocketfft r2c on {cores} threads standing in for FFTW3, the OpenMP P(k) loop",
+        "stage_s_per_job": {k: round(sum(t[k] for t in per) / len(per), 3) for k in per[0]},
+        "gen_b_omp_all_cores": {"value": rate(omp_all), "unit": "jobs/s", "threads": cores, "kind": "port",
+                                "note": "Gen-B private-grid OpenMP assignment (NTHREADS-fold count fixed)"},
+        "gen_b_omp_12_threads": {"value": rate(omp12), "unit": "jobs/s", "threads": 12, "kind": "port",
+                                 "note": "the reference's _NTHREADS_ = 12 (Headers/def.h:278); FFT and P(k) "
+                                         "on 12 threads too"},
+    }
 
 
 def run_reference(args):
+    """The reference's own CPU implementation of the path on this host, on
+    the sweep's config: every step is one full-size job (schemes in turn),
+    assignment by the reference's getDensity_* compiled from its source (Gen
+    A, serial, as its Makefile links it; the FP32 restatement if oracle/_ref
+    is absent), r2c on all cores, the OpenMP P(k) loop.  Rank 0 only."""
     rank, local, world = dist_env()
     if rank != 0:
         return None
     from cosmicatlas_b200 import synth
+    orc = _cpu_oracle()
     cores = os.cpu_count() or 1
-    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
     npart = args.particles
     x, y, z = synth.clumped(npart, BOX, 200_000, 1.5, 0.8, seed=2)
     w = synth.halo_masses(npart, seed=1002)
-    nsample = min(npart, 1 << 20)
-    for _ in range(min(args.warmup, 1)):
-        cpu_baseline_sample(x, y, z, w, nsample, cores)
-    vals = []
+    for i in range(min(args.warmup, 1)):
+        cpu_job(orc, SCHEMES[i % 3], x, y, z, w)
+    t_jobs = []
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        v, _ = cpu_baseline_sample(x, y, z, w, nsample, cores)
-        vals.append(v)
+    for i in range(args.steps):
+        t = cpu_job(orc, SCHEMES[i % 3], x, y, z, w)
+        t_jobs.append(sum(t.values()))
     wall = time.perf_counter() - t0
-    value = float(np.median(vals))
-    sample = (f"{nsample} of {npart} particles per scheme (serial scatter time scaled by {npart / nsample:g}), "
-              f"full 256^3 FFT and P(k)")
+    value = len(t_jobs) / sum(t_jobs)
+    kind = "reference" if orc.ref_lib() is not None else "port"
+    sample = (f"one full-size job per step, schemes NGP/CIC/TSC in turn ({npart} particles, 256^3, 128 bins); "
+              + ("getDensity_* compiled from the reference source (Gen A, serial scatter)" if kind == "reference"
+                 else "the oracle's restatement of getDensity_* (Gen A, serial scatter)")
+              + f"; scipy pocketfft r2c on {cores} threads standing in for FFTW3; OpenMP P(k) loop")
     return {
         "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "jobs/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * wall / args.steps, 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded clumped process, halo-like masses)", "config": config_dict(npart),
-        "cpu_baseline": {"value": round(value, 4), "unit": "jobs/s", "cores": cores, "kind": "port",
-                         "sample": sample},
+        "data": "synthetic (seeded clumped process, halo-like masses)",
+        "config": config_dict(npart, {"parallelism": f"job replicas x{world}"}),
+        "cpu_baseline": {"value": round(value, 4), "unit": "jobs/s", "cores": cores, "kind": kind, "sample": sample},
         "e2e": {"value": round(value, 4), "unit": "jobs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -517,19 +625,25 @@ def run_single(args):
     two = Context.tweb_opts(R, lth, 1e-5, method=CL.TWEB_FD if args.tweb_method == "fd" else CL.TWEB_FFT)
     for _ in range(args.warmup):
         ctx.job(arrs[0], arrs[1], arrs[2], None, grid, scheme, prec, pk=pko, tweb=two)
+    times = []
+    with ClockSampler(0) as clk:
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            r = ctx.job(arrs[0], arrs[1], arrs[2], None, grid, scheme, prec, pk=pko, tweb=two)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+    # per-kernel CUDA-event times from a separate pass of the same jobs
     ctx.profile(True)
     ctx.profile_read(reset=True)
-    times = []
     for _ in range(args.steps):
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        r = ctx.job(arrs[0], arrs[1], arrs[2], None, grid, scheme, prec, pk=pko, tweb=two)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        times.append(e0.elapsed_time(e1))
+        ctx.job(arrs[0], arrs[1], arrs[2], None, grid, scheme, prec, pk=pko, tweb=two)
+    torch.cuda.synchronize()
     prof = ctx.profile_read(reset=True)
+    ctx.profile(False)
     hbm, kind = peaks()
     nh = n * n * (n // 2 + 1)
     stage_bytes = {"assign": npart * 12 + 4 * n ** 3, "fft_r2c": 4 * n ** 3 + 8 * nh, "power": 8 * nh,
@@ -555,7 +669,15 @@ def run_single(args):
            "ms_per_job": round(float(np.median(times)), 3),
            "ms_min": round(min(times), 3), "steps": k, "warmup": args.warmup, "peak_gbs": hbm, "peak_kind": kind,
            "stages": stages, "kernels": {a: {"launches": b[0], "ms_total": round(b[1], 3)} for a, b in sorted(prof.items())},
-           "tweb_counts": [int(v) for v in r["tweb"].counts], "n_lost": r["assign"].n_lost}
+           "tweb_counts": [int(v) for v in r["tweb"].counts], "n_lost": r["assign"].n_lost,
+           "clocks": clk.summary(),
+           "timing": "per job: CUDA events around cam_job_run on the launching stream, synchronised on both "
+                     "sides; the per-kernel profile runs on the same jobs"}
+    for st in stages.values():
+        if st["achieved_gbs"]:
+            st["frac"] = round(st["achieved_gbs"] / hbm, 4)
+    if args.workload == "single512":
+        out["stages"]["fft_r2c"]["cufft_ms"] = round(cufft_r2c_ms(n, stream), 4)
     ctx.close()
     if args.workload == "c1":
         out["cpu_ref"] = c1_cpu_reference(x, y, z, n, box, scheme, nb, R, lth)
@@ -886,18 +1008,18 @@ def main():
         return
     rank, local, world = dist_env()
     if world == 1 and not args.kernels_only:
-        cores = os.cpu_count() or 1
-        nsample = min(args.particles, 1 << 20)
-        v, per_job = cpu_baseline_sample(*parts, nsample, cores)
-        out["cpu_baseline"] = {"value": round(v, 4), "unit": "jobs/s", "cores": cores, "kind": "port",
-                               "sample": f"{nsample} of {args.particles} particles per scheme (serial scatter "
-                                         f"scaled by {args.particles / nsample:g}), full 256^3 FFT and P(k), "
-                                         f"FFT on {cores} threads"}
+        out["cpu_baseline"] = cpu_baseline_block(*parts)
         if args.serving_jobs > 0:
             # the metric's "vs plain path" part: the same jobs through the
             # per-call path and through the serving loop, on this GPU
             args.jobs = args.serving_jobs
             out["serving"] = run_calib(args)
+        if args.stream_jobs > 0:
+            # the mixed stream (2,000 jobs, N 64..512): saturation and a
+            # Poisson arrival rate, served against the per-call path
+            args.jobs = args.stream_jobs
+            args.rates = args.stream_rates
+            out["serving_stream"] = run_stream(args)
     print(json.dumps(out), flush=True)
 
 

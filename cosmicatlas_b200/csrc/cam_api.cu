@@ -2,6 +2,8 @@
 // the entry points declared in include/cam.h.
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -107,6 +109,25 @@ void *scratch(cam_ctx *ctx, const char *name, size_t bytes)
     return p;
 }
 
+unsigned *device_error_word(cam_ctx *ctx)
+{
+    if (!ctx->err_word) {
+        auto *w = static_cast<unsigned *>(scratch(ctx, "err.word", 16));
+        CAM_CUDA_TRY(cudaMemsetAsync(w, 0, 16, ctx->stream));
+        ctx->err_word = w;
+    }
+    return ctx->err_word;
+}
+
+void check_device_error(cam_ctx *ctx)
+{
+    if (!ctx->err_word) return;
+    unsigned h = 0;
+    CAM_CUDA_TRY(cudaMemcpyAsync(&h, ctx->err_word, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    CAM_REQUIRE(h == 0u, CAM_E_CUDA, "a kernel's bulk copy did not complete within its wait limit");
+}
+
 void prof_begin(cam_ctx *ctx, const char *name)
 {
     if (!ctx->prof_on || ctx->capturing) return;
@@ -177,6 +198,7 @@ void release_all(cam_ctx *ctx)
         if (kv.second.ptr) cudaFreeAsync(kv.second.ptr, ctx->stream);
     cudaStreamSynchronize(ctx->stream);
     ctx->bufs.clear();
+    ctx->err_word = nullptr;
     ctx->used = 0;
     // The freed blocks stay in the device pool: trimming it here made every
     // later growth map new physical memory while other contexts' jobs ran,
@@ -458,6 +480,8 @@ int cam_ctx_create(int device, size_t hbm_budget, cam_ctx **out)
         return CAM_E_CUDA;
     }
     c->stream = c->own_stream;
+    c->no_tma = std::getenv("CAM_NO_TMA") != nullptr;
+    c->no_stage = std::getenv("CAM_NO_STAGE") != nullptr;
     *out = c;
     return CAM_OK;
 }
@@ -495,7 +519,10 @@ int cam_ctx_set_stream(cam_ctx *ctx, void *stream)
 
 int cam_ctx_sync(cam_ctx *ctx)
 {
-    return guarded(ctx, [&] { CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream)); });
+    return guarded(ctx, [&] {
+        CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        check_device_error(ctx);
+    });
 }
 
 const char *cam_last_error(cam_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
@@ -1064,7 +1091,7 @@ int cam_job_run(cam_ctx *ctx, const cam_job_desc *job, cam_job_result *res)
         const int nb = want_pk ? nbins_for(job->pk, n) : 0;
         // Readback of one run: assignment statistics [4], mesh sum and mean
         // [2], P(k) sums [nb][2] and modes [nb], into a pinned buffer.
-        const size_t pin_bytes = 4 * 8 + 2 * 8 + (size_t)nb * 24;
+        const size_t pin_bytes = 4 * 8 + 2 * 8 + (size_t)nb * 24 + 8;
         if (ctx->job_pin_bytes < pin_bytes) {
             std::lock_guard<std::mutex> lk(alloc_mutex());
             if (ctx->job_pin) CAM_CUDA_TRY(cudaFreeHost(ctx->job_pin));
@@ -1077,6 +1104,8 @@ int cam_job_run(cam_ctx *ctx, const cam_job_desc *job, cam_job_result *res)
         auto *hsum = reinterpret_cast<double *>(ctx->job_pin + 32);
         auto *hpk = reinterpret_cast<double *>(ctx->job_pin + 48);
         auto *hmd = reinterpret_cast<unsigned long long *>(ctx->job_pin + 48 + (size_t)nb * 16);
+        auto *herr = reinterpret_cast<unsigned *>(ctx->job_pin + 48 + (size_t)nb * 24);
+        const unsigned *derr = device_error_word(ctx);
         // One run of the whole job.  defer: the assignment sizes its payload
         // from an estimate and nothing waits for the host until the single
         // readback at the end; returns true if the estimate fell short (the
@@ -1091,16 +1120,17 @@ int cam_job_run(cam_ctx *ctx, const cam_job_desc *job, cam_job_result *res)
             assign_device(ctx, d.x, d.y, d.z, d.w, d.n, g, job->scheme, out);
             // FFT of rho - mean, mean from the deposit's exact per-brick sums.
             Spectrum s = alloc_spectrum(ctx, n, job->precision, "job.spec");
-            fft_r2c_split(ctx, plan, out.mesh, dsum + 1, s);
-            PkDevice pkd{nullptr, nullptr};
-            if (want_pk) pkd = power_bin_device(ctx, s, job->pk, nb);
+            const PkDevice pkd = job_fft_pk(ctx, plan, out.mesh, dsum + 1, s, want_pk ? &job->pk : nullptr, nb,
+                                            job->want_tweb != 0);
             CAM_CUDA_TRY(cudaMemcpyAsync(hstats, assign_stats(ctx), 32, cudaMemcpyDeviceToHost, ctx->stream));
             CAM_CUDA_TRY(cudaMemcpyAsync(hsum, dsum, 16, cudaMemcpyDeviceToHost, ctx->stream));
             if (want_pk) {
                 CAM_CUDA_TRY(cudaMemcpyAsync(hpk, pkd.sums, (size_t)nb * 16, cudaMemcpyDeviceToHost, ctx->stream));
                 CAM_CUDA_TRY(cudaMemcpyAsync(hmd, pkd.modes, (size_t)nb * 8, cudaMemcpyDeviceToHost, ctx->stream));
             }
+            CAM_CUDA_TRY(cudaMemcpyAsync(herr, derr, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
             CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+            CAM_REQUIRE(*herr == 0u, CAM_E_CUDA, "a kernel's bulk copy did not complete within its wait limit");
             if (defer && (hstats[3] & 0xffffffffu)) return true;
             if (d.w) {
                 const unsigned wbits = (unsigned)(hstats[1] & 0xffffffffu);

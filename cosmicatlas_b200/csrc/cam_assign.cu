@@ -151,7 +151,7 @@ __device__ __forceinline__ int brick_linear(const AssignGeom &g, int b0, int b1,
 template <int SCHEME, bool SMEM>
 __device__ __forceinline__ void count_one(float px, float py, float pz, float wt, bool weighted, const AssignGeom &g,
                                           uint32_t *hist, uint32_t *__restrict__ table, unsigned long long &my_lost,
-                                          unsigned int &my_wmax, unsigned int &my_neg)
+                                          unsigned int &my_wmax, unsigned int &my_neg, unsigned int &my_wminc)
 {
     using St = Stencil<SCHEME>;
     const float pos[3] = {px, py, pz};
@@ -163,6 +163,7 @@ __device__ __forceinline__ void count_one(float px, float py, float pz, float wt
     if (weighted) {
         my_wmax = max(my_wmax, __float_as_uint(fabsf(wt)));
         my_neg |= wt < 0.0f;
+        if (wt != 0.0f) my_wminc = max(my_wminc, 0x7fffffffu - __float_as_uint(fabsf(wt)));
     }
     int bl[3];
     bool two[3];
@@ -301,14 +302,15 @@ bin_kernel(const float *__restrict__ x, const float *__restrict__ y, const float
         __syncthreads();
     }
     unsigned long long my_lost = 0;
-    unsigned int my_wmax = 0, my_neg = 0;
+    unsigned int my_wmax = 0, my_neg = 0, my_wminc = 0;
     const bool weighted = w != nullptr;
     auto one = [&](float px, float py, float pz, float wt) {
         if (SCATTER)
             bin_one<SCHEME, true, false>(px, py, pz, wt, weighted, g, G, blk, hist, table, payload, cap, ovf,
                                          my_lost, my_wmax, my_neg);
         else
-            count_one<SCHEME, kHist>(px, py, pz, wt, weighted, g, hist, table, my_lost, my_wmax, my_neg);
+            count_one<SCHEME, kHist>(px, py, pz, wt, weighted, g, hist, table, my_lost, my_wmax, my_neg,
+                                     my_wminc);
     };
     const int64_t p0 = (int64_t)blk * chunk, p1 = min(np, p0 + chunk);
     int64_t ptail = p0;
@@ -341,11 +343,13 @@ bin_kernel(const float *__restrict__ x, const float *__restrict__ y, const float
             my_lost += __shfl_down_sync(0xffffffffu, my_lost, off);
             my_wmax = max(my_wmax, __shfl_down_sync(0xffffffffu, my_wmax, off));
             my_neg |= __shfl_down_sync(0xffffffffu, my_neg, off);
+            my_wminc = max(my_wminc, __shfl_down_sync(0xffffffffu, my_wminc, off));
         }
         if (lane == 0) {
             if (my_lost) atomicAdd(lost, my_lost);
             if (my_wmax) atomicMax(wmax_bits, my_wmax);
             if (my_neg) atomicOr(wmax_bits + 1, 1u);  // some weight is negative
+            if (my_wminc) atomicMax(wmax_bits + 6, my_wminc);  // smallest nonzero |w|
         }
         if (kHist) {
             __syncthreads();
@@ -353,6 +357,173 @@ bin_kernel(const float *__restrict__ x, const float *__restrict__ y, const float
                 if (hist[i]) atomicAdd(table + (int64_t)i * kCursorStride, hist[i]);
         }
     }
+}
+
+// Pass 3, staged form (nb <= kStageBricks).  Each CTA stages the records of
+// a contiguous particle chunk in shared memory and writes them out in
+// flushes: a flush ranks its records by brick (shared-memory counts), takes
+// one global range per brick it holds (one atomic on the brick's cursor per
+// brick and flush instead of one per record) and writes the records in
+// brick order, so a warp's stores land in runs of consecutive slots.
+// Records past the payload's capacity are flagged, not written.
+constexpr int kStageThreads = 1024;
+constexpr int kStageCap = 8192;     // staged records per flush (128 KB)
+constexpr int kStageBricks = 4096;  // bricks whose counts and ranges fit beside them
+constexpr int kStageRankBits = 13;  // kStageCap = 2^13
+
+template <int SCHEME>
+__global__ void __launch_bounds__(kStageThreads, 1)
+scatter_staged_kernel(const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z,
+                      const float *__restrict__ w, int64_t np, int64_t chunk, AssignGeom g, int nb,
+                      uint32_t *__restrict__ table, uint4 *__restrict__ payload, uint64_t cap,
+                      unsigned int *__restrict__ ovf)
+{
+    using St = Stencil<SCHEME>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint4 *srec = reinterpret_cast<uint4 *>(smem_raw);                  // [kStageCap]
+    uint32_t *skey = reinterpret_cast<uint32_t *>(srec + kStageCap);     // [kStageCap] brick << 13 | rank
+    uint16_t *sperm = reinterpret_cast<uint16_t *>(skey + kStageCap);    // [kStageCap] slot -> staged record
+    uint32_t *cnt = reinterpret_cast<uint32_t *>(sperm + kStageCap);     // [nb] records per brick, this flush
+    uint32_t *off = cnt + kStageBricks;                                  // [nb] first slot of each brick
+    uint32_t *gdel = off + kStageBricks;                                 // [nb] global slot - local slot
+    __shared__ uint32_t s_fill, s_need, s_wsum[kStageThreads / 32];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    for (int b = tid; b < nb; b += kStageThreads) cnt[b] = 0u;
+    if (tid == 0) {
+        s_fill = 0u;
+        s_need = 0u;
+    }
+    __syncthreads();
+    const bool weighted = w != nullptr;
+    const int64_t p0 = (int64_t)blockIdx.x * chunk, p1 = min(np, p0 + chunk);
+
+    // Writes the staged records out (every thread takes part).
+    auto flush = [&]() {
+        const uint32_t nst = s_fill;
+        // exclusive scan of the counts: kStageBricks / kStageThreads per thread
+        constexpr int PER = kStageBricks / kStageThreads;
+        uint32_t v[PER];
+        uint32_t tsum = 0;
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const int b = tid * PER + k;
+            v[k] = b < nb ? cnt[b] : 0u;
+            tsum += v[k];
+        }
+        uint32_t incl = tsum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        if (lane == 31) s_wsum[wid] = incl;
+        __syncthreads();
+        if (wid == 0) {
+            const uint32_t ws = s_wsum[lane];
+            uint32_t wi = ws;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
+                if (lane >= o) wi += t;
+            }
+            s_wsum[lane] = wi - ws;
+        }
+        __syncthreads();
+        uint32_t run = s_wsum[wid] + incl - tsum;
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const int b = tid * PER + k;
+            if (b < nb) {
+                off[b] = run;
+                // one global range per brick held in this flush
+                if (v[k]) gdel[b] = atomicAdd(table + (int64_t)b * kCursorStride, v[k]) - run;
+            }
+            run += v[k];
+        }
+        __syncthreads();
+        for (uint32_t i = tid; i < nst; i += kStageThreads) {
+            const uint32_t key = skey[i];
+            sperm[off[key >> kStageRankBits] + (key & ((1u << kStageRankBits) - 1u))] = (uint16_t)i;
+        }
+        __syncthreads();
+        for (uint32_t j = tid; j < nst; j += kStageThreads) {
+            const uint32_t i = sperm[j];
+            const uint32_t slot = gdel[skey[i] >> kStageRankBits] + j;
+            if (slot < cap) payload[slot] = srec[i];
+            else atomicOr(ovf, 1u);
+        }
+        __syncthreads();
+        for (int b = tid; b < nb; b += kStageThreads) cnt[b] = 0u;
+        if (tid == 0) s_fill = 0u;
+        __syncthreads();
+    };
+
+    for (int64_t base = p0; base < p1; base += kStageThreads) {
+        const int64_t p = base + tid;
+        int c[3] = {0, 0, 0}, bl[3] = {0, 0, 0}, nbx[3] = {0, 0, 0};
+        float t[3] = {0.f, 0.f, 0.f};
+        float wt = 1.0f;
+        int nrec = 0;
+        if (p < p1) {
+            const float pos[3] = {__ldcs(x + p), __ldcs(y + p), __ldcs(z + p)};
+            if (weighted) wt = __ldcs(w + p);
+            if (home_cell<SCHEME>(pos, g, c)) {
+                nrec = 1;
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    int lo, hi;
+                    stencil_ends<SCHEME>(c[a], g.n[a], lo, hi);
+                    bl[a] = brick_of(lo, g.b[a], g.bmagic[a]);
+                    nbx[a] = (brick_of(hi, g.b[a], g.bmagic[a]) == bl[a]) ? 1 : 2;
+                    if (SCHEME != CAM_NGP) t[a] = exact_offset(pos[a], g.mn[a], g.d[a], g.inv_d[a], c[a], g.n[a]);
+                    nrec *= nbx[a];
+                }
+            }
+        }
+        // room for this round's records, else flush first
+        if (nrec) atomicAdd(&s_need, (uint32_t)nrec);
+        __syncthreads();
+        const bool full = s_fill + s_need > (uint32_t)kStageCap;
+        __syncthreads();
+        if (full) flush();
+        if (tid == 0) s_need = 0u;
+        if (nrec) {
+            uint32_t dst = atomicAdd(&s_fill, (uint32_t)nrec);
+#pragma unroll
+            for (int i0 = 0; i0 < 2; ++i0) {
+                if (i0 >= nbx[0]) break;
+                const int b0 = (bl[0] + i0 == g.nb[0]) ? 0 : bl[0] + i0;
+#pragma unroll
+                for (int i1 = 0; i1 < 2; ++i1) {
+                    if (i1 >= nbx[1]) break;
+                    const int b1 = (bl[1] + i1 == g.nb[1]) ? 0 : bl[1] + i1;
+#pragma unroll
+                    for (int i2 = 0; i2 < 2; ++i2) {
+                        if (i2 >= nbx[2]) break;
+                        const int b2 = (bl[2] + i2 == g.nb[2]) ? 0 : bl[2] + i2;
+                        const int key = brick_linear(g, b0, b1, b2);
+                        const uint32_t rank = atomicAdd(cnt + key, 1u);
+                        const int o[3] = {b0 * g.b[0], b1 * g.b[1], b2 * g.b[2]};
+                        uint32_t word[3];
+#pragma unroll
+                        for (int a = 0; a < 3; ++a) {
+                            const int e = min(g.b[a], g.n[a] - o[a]);
+                            int cl = c[a] - o[a];
+                            if (cl < -1) cl += g.n[a];
+                            else if (cl > e) cl -= g.n[a];
+                            word[a] = pack_axis(cl, t[a]);
+                        }
+                        srec[dst] = make_uint4(word[0], word[1], word[2], __float_as_uint(wt));
+                        skey[dst] = ((uint32_t)key << kStageRankBits) | rank;
+                        ++dst;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (s_fill) flush();
+    (void)St::W;
 }
 
 // Brick starts in one CTA (nb <= kOffThreads * kOffItems): thread t scans
@@ -456,112 +627,161 @@ __device__ __forceinline__ unsigned div_small(unsigned i, unsigned d, unsigned m
     return d == 1u ? i : __umulhi(i, m);
 }
 
-// Adds round(v) (|v| < 2^32) to the 64-bit fixed-point cell (lo, hi) with
-// 32-bit shared atomics: the low word's old value tells whether the add
-// carried; a negative v adds its two's complement (high word all ones).
+// Adds round(v) to the 64-bit fixed-point cell (lo, hi) with 32-bit shared
+// atomics: the low word's old value tells whether the add carried, and the
+// high word takes the upper 32 bits of the two's complement plus the carry.
+// |v| < 2^31 converts in 32 bits (the common case); larger contributions
+// (heavy particles when light ones set the scale) convert in 64 bits.
 __device__ __forceinline__ void add_fixed(uint32_t *lo, uint32_t *hi, float v)
 {
-    const bool neg = v < 0.0f;
-    const uint32_t m = __float2uint_rn(fabsf(v));
-    const uint32_t ql = neg ? 0u - m : m;
+    uint32_t ql, qh;
+    if (fabsf(v) < 2147483648.0f) {
+        const int q = __float2int_rn(v);
+        ql = (uint32_t)q;
+        qh = q < 0 ? 0xffffffffu : 0u;
+    } else {
+        const long long q = __float2ll_rn(v);
+        ql = (uint32_t)(unsigned long long)q;
+        qh = (uint32_t)((unsigned long long)q >> 32);
+    }
     const uint32_t old = atomicAdd(lo, ql);
     const uint32_t carry = (uint32_t)(old + ql) < old ? 1u : 0u;
-    const uint32_t hadd = (neg && m != 0u ? 0xffffffffu : 0u) + carry;
+    const uint32_t hadd = qh + carry;
     if (hadd) atomicAdd(hi, hadd);
 }
 
-// One payload record into the brick's fixed-point tile.  lc = home cell
-// relative to the brick + FIRST + s is the stencil point's local cell; when
-// the brick has neighbours along an axis (nb > 1) a point outside [0, e)
-// belongs to another brick, and when one brick spans the axis the point
-// wraps periodically inside it.  NONNEG: every particle weight is >= 0, so
-// an add of a non-negative contribution is one 32-bit atomic plus a carry
-// only when the low word overflows.
-template <int SCHEME, bool NONNEG>
-__device__ __forceinline__ void deposit_record(const uint4 v, const AssignGeom &g, const int e[3], const bool whole[3],
-                                               float f1, float f2, uint32_t *lo, uint32_t *hi)
+// The brick's tile has a one-cell halo on every side: tile cell
+// (li + 1, lj + 1, lk + 1) holds brick cell (li, lj, lk), li in [-1, e].  A
+// record deposits its whole stencil with no per-cell test; the halo cells
+// take the contributions that belong to neighbouring bricks (which get the
+// particle's own record) and are discarded.  Per axis, a stencil point
+// further out than the halo (TSC only: home cell -1 or e) gets weight zero
+// and the nearest halo index, so it adds nothing.  Along an axis that one
+// brick spans (nb = 1) the stencil wraps periodically inside the brick.
+template <int SCHEME>
+__device__ __forceinline__ void axis_stencil(uint32_t word, int e, bool whole, float wa[3], int ia[3])
 {
     using St = Stencil<SCHEME>;
-    int cl[3];
-    float t[3];
-    unpack_axis(v.x, cl[0], t[0]);
-    unpack_axis(v.y, cl[1], t[1]);
-    unpack_axis(v.z, cl[2], t[2]);
-    const float ws = (__uint_as_float(v.w) * f1) * f2;
-    float wa[3][St::W];
-    int li[3][St::W];
-    bool ok[3][St::W];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        if (SCHEME == CAM_NGP) {
-            wa[a][0] = 1.0f;
-        } else if (SCHEME == CAM_CIC) {
-            wa[a][0] = 1.0f - t[a];
-            wa[a][St::W - 1] = t[a];
-        } else {
-            const float hm = 0.5f - t[a], hp = 0.5f + t[a];
-            wa[a][0] = 0.5f * hm * hm;
-            wa[a][1] = 0.75f - t[a] * t[a];
-            wa[a][St::W - 1] = 0.5f * hp * hp;
-        }
-#pragma unroll
-        for (int sidx = 0; sidx < St::W; ++sidx) {
-            int lc = cl[a] + St::FIRST + sidx;
-            if (whole[a]) lc += lc < 0 ? e[a] : (lc >= e[a] ? -e[a] : 0);
-            li[a][sidx] = lc;
-            ok[a][sidx] = (unsigned)lc < (unsigned)e[a];
-        }
+    int cl;
+    float t;
+    unpack_axis(word, cl, t);
+    if (SCHEME == CAM_NGP) {
+        wa[0] = 1.0f;
+    } else if (SCHEME == CAM_CIC) {
+        wa[0] = 1.0f - t;
+        wa[1] = t;
+    } else {
+        const float hm = 0.5f - t, hp = 0.5f + t;
+        wa[0] = 0.5f * hm * hm;
+        wa[1] = 0.75f - t * t;
+        wa[2] = 0.5f * hp * hp;
     }
 #pragma unroll
-    for (int ia = 0; ia < St::W; ++ia) {
+    for (int i = 0; i < St::W; ++i) {
+        int lc = cl + St::FIRST + i;
+        if (whole) {
+            lc += lc < 0 ? e : (lc >= e ? -e : 0);
+        } else if (lc < -1 || lc > e) {
+            wa[i] = 0.0f;
+            lc = lc < -1 ? -1 : e;
+        }
+        ia[i] = lc + 1;
+    }
+}
+
+// Adds the non-negative contribution v < 2^32 (units of the quantum) to the
+// cell (lo, hi): one 32-bit atomic, and a carry into the high word when the
+// low word wraps.  v < 2^22 converts by adding 2^23 (the float's mantissa
+// then holds round(v)); larger values convert with cvt.
+template <bool SMALL>
+__device__ __forceinline__ void add_nonneg(uint32_t *lo, uint32_t *hi, float v)
+{
+    uint32_t m;
+    if (SMALL) m = __float_as_uint(__fadd_rn(v, 8388608.0f)) - 0x4b000000u;
+    else m = __float2uint_rn(v);
+    const uint32_t old = atomicAdd(lo, m);
+    if (old + m < old) atomicAdd(hi, 1u);
+}
+
+// TIER 0: every contribution < 2^22 and >= 0; 1: < 2^32 and >= 0; 2: any.
+template <int SCHEME, int TIER>
+__device__ __forceinline__ void deposit_stencil(const float wa[3][3], const int ia[3][3], int S0, int S1, float ws,
+                                                uint32_t *lo, uint32_t *hi)
+{
+    using St = Stencil<SCHEME>;
 #pragma unroll
-        for (int ja = 0; ja < St::W; ++ja) {
-            const float wij = ws * wa[0][ia] * wa[1][ja];
-            const int row = (li[0][ia] * e[1] + li[1][ja]) * e[2];
-            const bool okij = ok[0][ia] && ok[1][ja];
+    for (int i = 0; i < St::W; ++i) {
 #pragma unroll
-            for (int ka = 0; ka < St::W; ++ka) {
-                if (!(okij && ok[2][ka])) continue;
-                const int c = row + li[2][ka];
-                const float val = wij * wa[2][ka];
-                // a stencil weight can dip below zero by ~1e-6 (the FP32 key
-                // and the exact offset disagree near a cell edge): such
-                // contributions take the signed path too
-                if (NONNEG && val >= 0.0f) {
-                    const uint32_t m = __float2uint_rn(val);
-                    const uint32_t old = atomicAdd(lo + c, m);
-                    if (old + m < old) atomicAdd(hi + c, 1u);
-                } else {
-                    add_fixed(lo + c, hi + c, val);
-                }
+        for (int j = 0; j < St::W; ++j) {
+            const float wij = ws * wa[0][i] * wa[1][j];
+            const int row = ia[0][i] * S0 + ia[1][j] * S1;
+#pragma unroll
+            for (int k = 0; k < St::W; ++k) {
+                const int c = row + ia[2][k];
+                const float v = wij * wa[2][k];
+                if (TIER == 0) add_nonneg<true>(lo + c, hi + c, v);
+                else if (TIER == 1) add_nonneg<false>(lo + c, hi + c, v);
+                else add_fixed(lo + c, hi + c, v);
             }
         }
     }
 }
 
-template <int SCHEME, bool NONNEG>
-__device__ __forceinline__ void deposit_range(const uint4 *__restrict__ payload, uint32_t beg, uint32_t end,
-                                              const AssignGeom &g, const int e[3], const bool whole[3], float f1,
-                                              float f2, uint32_t *lo, uint32_t *hi)
+// One payload record into the haloed tile.  ws = weight * 2^s; the stencil
+// weights are <= 1 (a TSC weight can dip below zero by ~1e-7 next to a cell
+// face: such records take the signed path), so |ws| bounds every
+// contribution and picks the conversion once per record.
+template <int SCHEME>
+__device__ __forceinline__ void deposit_record(const uint4 v, const int e[3], const bool whole[3], int S0, int S1,
+                                               float f1, float f2, bool nonneg, uint32_t *lo, uint32_t *hi)
 {
-    // Two records per thread per iteration: both loads are in flight before
-    // the shared-memory atomics of the first one.
-    for (uint32_t p = beg + threadIdx.x; p < end; p += 2 * blockDim.x) {
-        const uint4 va = payload[p];
-        const bool has_b = p + blockDim.x < end;
-        const uint4 vb = has_b ? payload[p + blockDim.x] : make_uint4(0u, 0u, 0u, 0u);
-        deposit_record<SCHEME, NONNEG>(va, g, e, whole, f1, f2, lo, hi);
-        if (has_b) deposit_record<SCHEME, NONNEG>(vb, g, e, whole, f1, f2, lo, hi);
+    float wa[3][3];
+    int ia[3][3];
+    axis_stencil<SCHEME>(v.x, e[0], whole[0], wa[0], ia[0]);
+    axis_stencil<SCHEME>(v.y, e[1], whole[1], wa[1], ia[1]);
+    axis_stencil<SCHEME>(v.z, e[2], whole[2], wa[2], ia[2]);
+    const float ws = (__uint_as_float(v.w) * f1) * f2;
+    bool pos = nonneg;
+    if (SCHEME == CAM_TSC) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) pos = pos && wa[a][0] >= 0.0f && wa[a][2] >= 0.0f;
+    } else if (SCHEME == CAM_CIC) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) pos = pos && wa[a][0] >= 0.0f && wa[a][1] >= 0.0f;
     }
+    if (pos && ws < 4194304.0f) deposit_stencil<SCHEME, 0>(wa, ia, S0, S1, ws, lo, hi);
+    else if (pos && ws < 4294967296.0f) deposit_stencil<SCHEME, 1>(wa, ia, S0, S1, ws, lo, hi);
+    else deposit_stencil<SCHEME, 2>(wa, ia, S0, S1, ws, lo, hi);
 }
 
-// Pass 4: one CTA per brick.  Scale 2^s with max|w| * 2^s < 2^31, so every
-// contribution of a particle (stencil weight <= 1) fits in the low word and
-// the high word only takes carries (and the sign of rare negative weights).
-// Quantum = max|w| / 2^31 per contribution; a cell sum may use all 64 bits.
-// wstat[0] = bits of max |w|, wstat[1] != 0 if some weight is negative.
+// Pass 4: one CTA per brick, cell sums in 64-bit fixed point of quantum
+// 2^-s.  The scale follows the smallest nonzero |w| of the catalogue:
+// 2^-s <= min|w| 2^-21, so every contribution of the lightest particle is
+// rounded to within 2.4e-7 of its own weight, whatever the heaviest one
+// weighs.  It is capped so that no cell of the brick can overflow: a cell
+// takes at most one contribution (stencil weight <= 1) per record of its
+// brick, so max|w| 2^s * nrec < 2^62.  Unit weights use s = 21 (every
+// contribution < 2^22, the cheapest conversion); NGP counts convert by a
+// shift.  wstat[0] = bits of max |w|, wstat[1] != 0 if some
+// weight is negative, wstat[6] = 0x7fffffff - bits of min nonzero |w| (0:
+// no nonzero weight).
+__device__ __forceinline__ int fixed_scale(const unsigned int *wstat, int weighted, uint32_t nrec)
+{
+    float wmax = 1.0f, wmin = 1.0f;
+    if (weighted) {
+        if (wstat[6] == 0u) return 0;  // every weight is zero
+        wmax = __uint_as_float(wstat[0]);
+        wmin = __uint_as_float(0x7fffffffu - wstat[6]);
+    }
+    int emax = 0, emin = 0;
+    frexpf(wmax, &emax);
+    frexpf(wmin, &emin);
+    const int bits = 32 - __clz(nrec | 1u);  // nrec < 2^bits
+    return min(22 - emin, 62 - emax - bits);
+}
+
 template <int SCHEME, typename OutT>
-__global__ void __launch_bounds__(kDepositThreads)
+__global__ void __launch_bounds__(kDepositThreads, 2)
 deposit_kernel(const uint4 *__restrict__ payload, const uint32_t *__restrict__ start, uint32_t nrec,
                AssignGeom g, const unsigned int *__restrict__ wstat, int weighted,
                OutT *__restrict__ mesh, double *__restrict__ brick_sum)
@@ -576,12 +796,13 @@ deposit_kernel(const uint4 *__restrict__ payload, const uint32_t *__restrict__ s
     const int e[3] = {min(g.b[0], g.n[0] - o[0]), min(g.b[1], g.n[1] - o[1]),
                       min(g.b[2], g.n[2] - o[2])};
     const bool whole[3] = {g.nb[0] == 1, g.nb[1] == 1, g.nb[2] == 1};
-    const int ncell = e[0] * e[1] * e[2];
-    const int cap = g.b[0] * g.b[1] * g.b[2];
+    // haloed tile: (b0 + 2) x (b1 + 2) x (b2 + 2) cells, low words then high words
+    const int T2 = g.b[2] + 2, T1 = g.b[1] + 2;
+    const int S1 = T2, S0 = T1 * T2;
+    const int cap = (g.b[0] + 2) * S0;
     uint32_t *lo = tile32;
     uint32_t *hi = tile32 + cap;
     {
-        // both words of all cap cells, 16 bytes a store
         const int nw = 2 * cap;
         uint4 *t4 = reinterpret_cast<uint4 *>(tile32);
         for (int i = threadIdx.x; i < nw / 4; i += blockDim.x) t4[i] = make_uint4(0u, 0u, 0u, 0u);
@@ -591,20 +812,25 @@ deposit_kernel(const uint4 *__restrict__ payload, const uint32_t *__restrict__ s
 
     // records beyond the payload's capacity nrec were not written (overflow flag)
     const uint32_t beg = min(start[B], nrec), end = min(start[B + 1], nrec);
-    const float wmax = weighted ? __uint_as_float(wstat[0]) : 1.0f;
     const bool nonneg = !weighted || wstat[1] == 0u;
-    int ex = 0;
-    frexpf(wmax > 0.f ? wmax : 1.0f, &ex);
-    const int s = 31 - ex;
+    const int s = fixed_scale(wstat, weighted, end - beg);
     // 2^s as two exact factors (s may exceed the float exponent range)
     const float f1 = scalbnf(1.0f, s / 2), f2 = scalbnf(1.0f, s - s / 2);
-    if (nonneg) deposit_range<SCHEME, true>(payload, beg, end, g, e, whole, f1, f2, lo, hi);
-    else deposit_range<SCHEME, false>(payload, beg, end, g, e, whole, f1, f2, lo, hi);
+    // two records per thread per iteration: both loads are in flight before
+    // the shared-memory atomics of the first one
+    for (uint32_t p = beg + threadIdx.x; p < end; p += 2 * blockDim.x) {
+        const uint4 va = payload[p];
+        const bool has_b = p + blockDim.x < end;
+        const uint4 vb = has_b ? payload[p + blockDim.x] : make_uint4(0u, 0u, 0u, 0u);
+        deposit_record<SCHEME>(va, e, whole, S0, S1, f1, f2, nonneg, lo, hi);
+        if (has_b) deposit_record<SCHEME>(vb, e, whole, S0, S1, f1, f2, nonneg, lo, hi);
+    }
     __syncthreads();
 
     long long acc = 0;
     const double sc = ldexp(1.0, -s);
-    // cell i = (li * e1 + lj) * e2 + lk; a tile holds < 2^16 cells
+    // interior cell i = (li * e1 + lj) * e2 + lk; a brick holds < 2^16 cells
+    const int ncell = e[0] * e[1] * e[2];
     const unsigned e2 = (unsigned)e[2], e12 = (unsigned)(e[1] * e[2]);
     const unsigned m2 = e2 > 1u ? (unsigned)((0x100000000ull + e2 - 1) / e2) : 0u;
     const unsigned m12 = e12 > 1u ? (unsigned)((0x100000000ull + e12 - 1) / e12) : 0u;
@@ -614,7 +840,8 @@ deposit_kernel(const uint4 *__restrict__ payload, const uint32_t *__restrict__ s
         const unsigned lk = (unsigned)i - row * e2;
         const unsigned lii = div_small((unsigned)i, e12, m12);
         const unsigned lj = row - lii * e1;
-        const long long q = (long long)(((unsigned long long)hi[i] << 32) | lo[i]);
+        const int c = (int)(lii + 1) * S0 + (int)(lj + 1) * S1 + (int)lk + 1;
+        const long long q = (long long)(((unsigned long long)hi[c] << 32) | lo[c]);
         acc += q;
         const int64_t gidx = ((int64_t)(o[0] + (int)lii) * g.n[1] + (o[1] + (int)lj)) * g.n[2] + (o[2] + (int)lk);
         mesh[gidx] = convert_out<OutT>(q, s, sc);
@@ -794,11 +1021,22 @@ static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const floa
     }
 
     uint4 *payload = static_cast<uint4 *>(scratch(ctx, "asg.payload", std::max<size_t>(total, 1) * sizeof(uint4)));
-    CAM_LAUNCH_NAMED(ctx, "assign_bin_scatter", scatter_k, G2, kScatterThreads, 0, x, y, z, w, np, chunk2, g,
-                     (int)nb, table, payload, d_lost, d_wmax, total, d_ovf);
+    if (nb <= kStageBricks && !ctx->no_stage) {
+        // staged scatter: one CTA per SM over contiguous chunks
+        const int G3 = (int)std::max<int64_t>(1, std::min<int64_t>(kNumSMs, (np + kStageThreads - 1) / kStageThreads));
+        const int64_t chunk3 = (np + G3 - 1) / G3;
+        const size_t ssmem = (size_t)kStageCap * (16 + 4 + 2) + (size_t)kStageBricks * 3 * 4;
+        auto sk = scatter_staged_kernel<SCHEME>;
+        smem_at_least(sk, ssmem);
+        CAM_LAUNCH_NAMED(ctx, "assign_bin_scatter", sk, G3, kStageThreads, ssmem, x, y, z, w, np, chunk3, g, (int)nb,
+                         table, payload, total, d_ovf);
+    } else {
+        CAM_LAUNCH_NAMED(ctx, "assign_bin_scatter", scatter_k, G2, kScatterThreads, 0, x, y, z, w, np, chunk2, g,
+                         (int)nb, table, payload, d_lost, d_wmax, total, d_ovf);
+    }
 
-    const size_t smem = (size_t)g.b[0] * g.b[1] * g.b[2] * 2 * sizeof(uint32_t);
-    CAM_REQUIRE(smem <= 200 * 1024, CAM_E_UNSUPPORTED, "brick tile too large");
+    const size_t smem = (size_t)(g.b[0] + 2) * (g.b[1] + 2) * (g.b[2] + 2) * 2 * sizeof(uint32_t);
+    CAM_REQUIRE(smem <= 110 * 1024, CAM_E_UNSUPPORTED, "brick tile too large");
     const int weighted = w != nullptr;
     auto launch_dep = [&](auto kern, auto *mesh) {
         smem_at_least(kern, smem);

@@ -25,6 +25,8 @@
 
 #include "cam_fft_device.cuh"
 #include "cam_internal.h"
+#include "cam_pk_device.cuh"
+#include "cam_tma.cuh"
 
 namespace cam {
 
@@ -137,6 +139,286 @@ fft_cols_pipe_kernel(typename fftdev::CT<T>::t *base, int nct, int nplanes, int6
         cur ^= 1;
     }
     fftdev::cp_async_wait<0>();
+}
+
+// Column transforms staged by TMA: the persistent, double-buffered column
+// pass with its tiles moved by the tensor memory accelerator.  One thread
+// issues a tile's loads (boxes of 128-byte rows, at most 256 rows each) on
+// the buffer's mbarrier; every thread waits on the mbarrier's phase, the
+// block runs the Stockham stages in shared memory, and the same thread
+// writes the transformed tile back with TMA stores.  A buffer is reloaded
+// only after its previous tile's store has finished reading it.  The tensor
+// map covers this GPU's own memory and the loads use no multicast.
+// Coordinates: (scalar column 2 W ct, row, plane, component); tile t: column
+// tile t % nct, plane (t / nct) % nplanes, component t / (nct * nplanes).
+// err: set to 1 if a tile's copies did not land within the wait bound (the
+// CTA then stops).
+// The tensor map's dimensions 1..3 are (row, plane, component) in order of
+// increasing stride; pos = p_row | p_plane << 2 | p_comp << 4 gives each
+// one's dimension.
+struct TileDims {
+    int pos;
+};
+__device__ __forceinline__ void tile_coords(int pos, int row, int plane, int comp, int &c1, int &c2, int &c3)
+{
+    const int pr = pos & 3, pp = (pos >> 2) & 3;
+    c1 = pr == 1 ? row : (pp == 1 ? plane : comp);
+    c2 = pr == 2 ? row : (pp == 2 ? plane : comp);
+    c3 = pr == 3 ? row : (pp == 3 ? plane : comp);
+}
+
+template <typename T, bool INV, int LEN>
+__global__ void __launch_bounds__(fftdev::ct_threads(LEN, fftdev::CT<T>::kCols, fftdev::CT<T>::kPPT),
+                                  pipe_min_blocks<T, LEN>())
+fft_cols_tma_kernel(const __grid_constant__ CUtensorMap map, TileDims td, int nct, int nplanes, int64_t ntiles,
+                    const typename fftdev::CT<T>::t *__restrict__ tw, unsigned *__restrict__ err)
+{
+    using C = typename fftdev::CT<T>::t;
+    constexpr int W = fftdev::CT<T>::kCols;
+    constexpr int NTHR = fftdev::ct_threads(LEN, W, fftdev::CT<T>::kPPT);
+    constexpr int NBOX = (LEN + 255) / 256;  // boxes of BOXR rows (LEN is a multiple of NBOX)
+    constexpr int BOXR = LEN / NBOX;
+    constexpr unsigned TILE_BYTES = (unsigned)(LEN * W * sizeof(C));
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ uint64_t bar[2];
+    C *const buf0 = reinterpret_cast<C *>(smem_raw);
+    const bool leader = threadIdx.x == 0;
+    auto coords = [&](int64_t t, int &x, int &plane, int &comp) {
+        const int64_t ct = t % nct, r = t / nct;
+        x = (int)(ct * 2 * W);
+        plane = (int)(r % nplanes);
+        comp = (int)(r / nplanes);
+    };
+    auto issue_load = [&](int64_t t, int b) {
+        int x, plane, comp;
+        coords(t, x, plane, comp);
+        tma::mbar_arrive_expect_tx(&bar[b], TILE_BYTES);
+#pragma unroll
+        for (int k = 0; k < NBOX; ++k) {
+            int c1, c2, c3;
+            tile_coords(td.pos, k * BOXR, plane, comp, c1, c2, c3);
+            tma::load_4d(buf0 + b * (LEN * W) + k * BOXR * W, &map, x, c1, c2, c3, &bar[b]);
+        }
+    };
+    if (leader) {
+        tma::mbar_init(&bar[0], 1);
+        tma::mbar_init(&bar[1], 1);
+        tma::fence_mbar_init();
+    }
+    __syncthreads();
+    unsigned phase = 0;  // bit b: parity of buffer b's next completion
+    int cur = 0;
+    int64_t t = blockIdx.x;
+    if (leader && t < ntiles) issue_load(t, 0);
+    bool failed = false;
+    for (; t < ntiles; t += gridDim.x) {
+        C *const here = buf0 + cur * (LEN * W);
+        const int64_t tn = t + gridDim.x;
+        if (leader && tn < ntiles) {
+            tma::bulk_wait_read0();  // the other buffer's last store has read its tile
+            issue_load(tn, cur ^ 1);
+        }
+        const bool ok = tma::mbar_wait(&bar[cur], (phase >> cur) & 1u);
+        phase ^= 1u << cur;
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        fftdev::block_fft_fixed<C, INV, false, W, LEN, NTHR, W, 1, 1>(here, tw);
+        tma::fence_proxy_async_smem();
+        __syncthreads();
+        if (leader) {
+            int x, plane, comp;
+            coords(t, x, plane, comp);
+#pragma unroll
+            for (int k = 0; k < NBOX; ++k) {
+                int c1, c2, c3;
+                tile_coords(td.pos, k * BOXR, plane, comp, c1, c2, c3);
+                tma::store_4d(&map, x, c1, c2, c3, here + k * BOXR * W);
+            }
+            tma::bulk_commit();
+        }
+        cur ^= 1;
+    }
+    if (leader) {
+        if (failed) {
+            atomicOr(err, 1u);
+            // the prefetch of the next tile may still be in flight: give it
+            // the same bound before the shared memory is released
+            const int64_t tn = t + gridDim.x;
+            if (tn < ntiles) tma::mbar_wait(&bar[cur ^ 1], (phase >> (cur ^ 1)) & 1u);
+        }
+        tma::bulk_wait0();
+    }
+}
+
+// The x pass of the r2c with the P(k) binning of its tiles (FP32 spectra):
+// the TMA column pass above, and after a tile's transform -- while its TMA
+// store (if any) reads the tile -- the block bins the tile's modes.  Tile:
+// 16 consecutive k (c0 .. c0 + 15) of all rows i, plane j.  A warp takes two
+// rows at a time (16 lanes each); along a row the bin is non-decreasing in
+// c, so runs of equal bins are contiguous lanes, reduced by a fixed shuffle
+// tree and added by their head lane into the warp's own FP64 bins, the
+// first row's heads before the second's.  Warps and tiles are combined in a
+// fixed order: part[cta][bin] = this CTA's sum of |F|^2 / W^2.  Mode counts
+// and shot-noise sums do not depend on the data; the host takes them from a
+// table.  store = 0: the transformed tiles are not written back (a job that
+// needs only P(k)).
+template <int LEN>
+constexpr int pk_pass_threads()
+{
+    return fftdev::ct_threads(LEN, 16, 16);
+}
+// CTAs per SM the binning pass is built for: two tiles plus the tables and
+// warp bins of N/2 bins in 200 KB, at most 1024 threads.
+template <int LEN>
+constexpr int pk_pass_min_blocks()
+{
+    constexpr int nthr = pk_pass_threads<LEN>();
+    constexpr int by_thr = 1024 / nthr;
+    constexpr int bytes = 2 * LEN * 16 * 8 + (LEN + 2 + (nthr / 32) * (LEN / 2)) * 8;
+    constexpr int by_smem = (200 * 1024) / bytes;
+    constexpr int b = by_thr < by_smem ? by_thr : by_smem;
+    return b > 1 ? b : 1;
+}
+
+template <int LEN>
+__global__ void __launch_bounds__(pk_pass_threads<LEN>(), pk_pass_min_blocks<LEN>())
+fft_cols_tma_pk_kernel(const __grid_constant__ CUtensorMap map, TileDims td, int nct, int nplanes, int64_t ntiles,
+                       const float2 *__restrict__ tw, unsigned *__restrict__ err,
+                       const double *__restrict__ g_tab /* [h+1] 1/W^2, [h+1] C/W^2, [nbins+1] E2 */, int nbins,
+                       float m_u, float inv_s, int store, double *__restrict__ part /* [grid][nbins] */)
+{
+    using C = float2;
+    constexpr int W = 16;
+    constexpr int NTHR = pk_pass_threads<LEN>();
+    constexpr int NWARP = NTHR / 32;
+    constexpr int NBOX = (LEN + 255) / 256;
+    constexpr int BOXR = LEN / NBOX;
+    constexpr unsigned TILE_BYTES = (unsigned)(LEN * W * sizeof(C));
+    constexpr int N = LEN, H = LEN / 2;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ uint64_t bar[2];
+    C *const buf0 = reinterpret_cast<C *>(smem_raw);
+    double *const tw2 = reinterpret_cast<double *>(smem_raw + 2 * (size_t)TILE_BYTES);  // [H + 1]
+    double *const E2 = tw2 + (H + 1);                                                   // [nbins + 1]
+    double *const wsum = E2 + (nbins + 1);                                              // [NWARP][nbins]
+    for (int t = threadIdx.x; t <= H; t += NTHR) tw2[t] = g_tab[t];
+    for (int t = threadIdx.x; t <= nbins; t += NTHR) E2[t] = g_tab[2 * (H + 1) + t];
+    for (int t = threadIdx.x; t < NWARP * nbins; t += NTHR) wsum[t] = 0.0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double *const mysum = wsum + (size_t)warp * nbins;
+    const bool leader = threadIdx.x == 0;
+    auto coords = [&](int64_t t, int &x, int &plane, int &comp) {
+        const int64_t ct = t % nct, r = t / nct;
+        x = (int)(ct * 2 * W);
+        plane = (int)(r % nplanes);
+        comp = (int)(r / nplanes);
+    };
+    auto issue_load = [&](int64_t t, int b) {
+        int x, plane, comp;
+        coords(t, x, plane, comp);
+        tma::mbar_arrive_expect_tx(&bar[b], TILE_BYTES);
+#pragma unroll
+        for (int k = 0; k < NBOX; ++k) {
+            int c1, c2, c3;
+            tile_coords(td.pos, k * BOXR, plane, comp, c1, c2, c3);
+            tma::load_4d(buf0 + b * (LEN * W) + k * BOXR * W, &map, x, c1, c2, c3, &bar[b]);
+        }
+    };
+    if (leader) {
+        tma::mbar_init(&bar[0], 1);
+        tma::mbar_init(&bar[1], 1);
+        tma::fence_mbar_init();
+    }
+    __syncthreads();
+    unsigned phase = 0;
+    int cur = 0;
+    int64_t t = blockIdx.x;
+    if (leader && t < ntiles) issue_load(t, 0);
+    bool failed = false;
+    for (; t < ntiles; t += gridDim.x) {
+        C *const here = buf0 + cur * (LEN * W);
+        const int64_t tn = t + gridDim.x;
+        if (leader && tn < ntiles) {
+            tma::bulk_wait_read0();
+            issue_load(tn, cur ^ 1);
+        }
+        const bool ok = tma::mbar_wait(&bar[cur], (phase >> cur) & 1u);
+        phase ^= 1u << cur;
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        fftdev::block_fft_fixed<C, false, false, W, LEN, NTHR, W, 1, 1>(here, tw);
+        int x, plane, comp;
+        coords(t, x, plane, comp);
+        if (store) {
+            tma::fence_proxy_async_smem();
+            __syncthreads();
+            if (leader) {
+#pragma unroll
+                for (int k = 0; k < NBOX; ++k) {
+                    int c1, c2, c3;
+                    tile_coords(td.pos, k * BOXR, plane, comp, c1, c2, c3);
+                    tma::store_4d(&map, x, c1, c2, c3, here + k * BOXR * W);
+                }
+                tma::bulk_commit();
+            }
+        }
+        // bin the tile: plane = j, columns c0 .. c0 + 15
+        const int j = plane, c0 = x / 2;
+        if (j != H) {
+            const int b = j <= H ? j : N - j;
+            const double tb = tw2[b];
+            const int qb = b * b;
+            const int kk = lane & 15;
+            const int c = c0 + kk;
+            const double tc = tw2[c];
+            for (int pr = warp; pr < LEN / 2; pr += NWARP) {
+                const int i = 2 * pr + (lane >> 4);
+                const int a = i <= H ? i : N - i;
+                const double q = (double)(a * a + qb + c * c);
+                const int bin = pk_bin(q, E2, nbins, m_u, inv_s);
+                double v = 0.0;
+                if (bin >= 0 && bin < nbins && pk_visited(i, j, c, N)) {
+                    const C f = here[i * W + kk];
+                    v = ((double)f.x * (double)f.x + (double)f.y * (double)f.y) * (tw2[a] * tb * tc);
+                }
+                const int prev = __shfl_up_sync(0xffffffffu, bin, 1);
+                const bool head = kk == 0 || prev != bin;
+                const unsigned heads = __ballot_sync(0xffffffffu, head);
+                const unsigned later = heads & ~((2u << lane) - 1u);
+                const int end = later ? __ffs((int)later) - 1 : 32;
+#pragma unroll
+                for (int off = 1; off < 16; off <<= 1) {
+                    const double o = __shfl_down_sync(0xffffffffu, v, off);
+                    if (lane + off < end) v += o;
+                }
+                const bool add = head && bin >= 0 && bin < nbins;
+                if (add && lane < 16) mysum[bin] += v;
+                __syncwarp();
+                if (add && lane >= 16) mysum[bin] += v;
+                __syncwarp();
+            }
+        }
+        __syncthreads();  // the tile is reloaded two iterations on
+        cur ^= 1;
+    }
+    if (leader) {
+        if (failed) {
+            atomicOr(err, 1u);
+            const int64_t tn = t + gridDim.x;
+            if (tn < ntiles) tma::mbar_wait(&bar[cur ^ 1], (phase >> (cur ^ 1)) & 1u);
+        }
+        tma::bulk_wait0();
+    }
+    __syncthreads();
+    for (int bn = threadIdx.x; bn < nbins; bn += NTHR) {
+        double sum = 0.0;
+        for (int w = 0; w < NWARP; ++w) sum += wsum[(size_t)w * nbins + bn];
+        part[(size_t)blockIdx.x * nbins + bn] = sum;
+    }
 }
 
 // Row transforms along the contiguous axis.
@@ -335,6 +617,51 @@ __global__ void fftw_to_split_kernel(const typename fftdev::CT<T>::t *__restrict
     }
 }
 
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled()
+{
+    static const EncodeTiledFn fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+        }
+        return reinterpret_cast<EncodeTiledFn>(p);
+    }();
+    return fn;
+}
+
+// Dimensions of a column-tile tensor map: dim 0 the scalar columns, then
+// (row, plane, component) sorted by increasing byte stride (a component
+// count of 1 gets a stride past the others); box: bw scalars x brows rows.
+// pos receives each one's dimension (see tile_coords).
+void tile_map_layout(int64_t ncol_scalars, int64_t nrows, int64_t rstride, int64_t nplanes, int64_t pstride,
+                     int64_t ncomp, int64_t cstride, uint32_t bw, uint32_t brows, uint64_t dims[4],
+                     uint64_t strides[3], uint32_t box[4], int &pos)
+{
+    struct D {
+        int role;  // 0 row, 1 plane, 2 component
+        int64_t n, st;
+    } d[3] = {{0, nrows, rstride}, {1, nplanes, pstride}, {2, ncomp, cstride}};
+    if (ncomp == 1) d[2].st = std::max(rstride * nrows, pstride * nplanes);
+    if (nplanes == 1) d[1].st = std::max(rstride * nrows, d[2].st * ncomp) + 16;
+    std::sort(d, d + 3, [](const D &a, const D &b) { return a.st < b.st; });
+    dims[0] = (uint64_t)ncol_scalars;
+    box[0] = bw;
+    pos = 0;
+    for (int i = 0; i < 3; ++i) {
+        dims[i + 1] = (uint64_t)d[i].n;
+        strides[i] = (uint64_t)((d[i].st + 15) / 16 * 16);
+        box[i + 1] = d[i].role == 0 ? brows : 1u;
+        pos |= (i + 1) << (2 * d[i].role);
+    }
+}
+
 int threads_for(int points, int ppt)
 {
     int t = (points + ppt - 1) / ppt;
@@ -362,6 +689,26 @@ void cols_impl(cam_ctx *ctx, FftPlan *p, void *base, int64_t len, int64_t ncols,
     dispatch_fft_len(len, [&](auto lc) {
         constexpr int LEN = decltype(lc)::value;
         if constexpr (LEN > 0 && 2 * LEN * W * sizeof(C) <= 200 * 1024) {
+            // TMA tiles: 128-byte rows of a 4D view (scalar column, row,
+            // plane, component) of this GPU's own array
+            CUtensorMap map;
+            TileDims td{0};
+            uint64_t dims[4], strides[3];
+            uint32_t box[4];
+            tile_map_layout(2 * ncols, len, jstride * es, nplanes, pstride * es, ncomp, ccomp * es,
+                            (uint32_t)(2 * W), (uint32_t)(LEN / ((LEN + 255) / 256)), dims, strides, box, td.pos);
+            if (pipe_ok && !ctx->no_tma &&
+                make_tensor_map_4d(&map, sizeof(T) == 8, base, dims, strides, box)) {
+                auto kt = inv ? fft_cols_tma_kernel<T, true, LEN> : fft_cols_tma_kernel<T, false, LEN>;
+                smem_at_least(kt, 2 * smem);
+                int per_sm = 0;
+                CAM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kt, nthr, 2 * smem));
+                const int64_t ntiles = (int64_t)nplanes * ncomp * (ncols / W);
+                const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)kNumSMs * std::max(per_sm, 1)));
+                CAM_LAUNCH_NAMED(ctx, "fft_cols", kt, g, nthr, 2 * smem, map, td, (int)(ncols / W), (int)nplanes, ntiles,
+                                 static_cast<const C *>(p->tw), device_error_word(ctx));
+                return;
+            }
             if (pipe_ok) {
                 auto kp = inv ? fft_cols_pipe_kernel<T, true, LEN> : fft_cols_pipe_kernel<T, false, LEN>;
                 smem_at_least(kp, 2 * smem);
@@ -444,6 +791,73 @@ void c2r_impl(cam_ctx *ctx, FftPlan *p, Spectrum &s, void *out, double scale)
 }  // namespace
 
 const void *plan_twiddles(FftPlan *plan) { return plan->tw; }
+
+bool fft_r2c_pk_fused(cam_ctx *ctx, FftPlan *plan, const void *real_in, const double *d_sub, Spectrum &out,
+                      const PkTables &pt, bool keep, double **d_part, int *nparts)
+{
+    if (plan->precision != CAM_F32 || ctx->no_tma) return false;
+    const int64_t n = plan->n, M = n / 2;
+    if (M % 16 != 0 || ((uintptr_t)out.main % 16) != 0) return false;
+    bool done = false;
+    dispatch_fft_len(n, [&](auto lc) {
+        constexpr int LEN = decltype(lc)::value;
+        if constexpr (LEN >= 32 && 2 * LEN * 16 * 8 <= 200 * 1024) {
+            constexpr int NTHR = pk_pass_threads<LEN>();
+            const size_t smem = (size_t)2 * LEN * 16 * 8 +
+                                (size_t)(LEN / 2 + 1 + pt.nbins + 1 + (NTHR / 32) * pt.nbins) * sizeof(double);
+            if (smem > 220 * 1024) return;
+            // x pass over main: 4D view (scalar column, row i, plane j, 1)
+            CUtensorMap map;
+            TileDims td{0};
+            uint64_t dims[4], strides[3];
+            uint32_t box[4];
+            tile_map_layout(2 * M, n, n * M * 8, n, M * 8, 1, 0, 32u, (uint32_t)(LEN / ((LEN + 255) / 256)), dims,
+                            strides, box, td.pos);
+            if (!make_tensor_map_4d(&map, false, out.main, dims, strides, box)) return;
+            auto kt = fft_cols_tma_pk_kernel<LEN>;
+            smem_at_least(kt, smem);
+            int per_sm = 0;
+            CAM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kt, NTHR, smem));
+            if (per_sm < 1) return;
+            const int64_t ntiles = n * (M / 16);
+            const int g = (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)kNumSMs * per_sm));
+            // rows [0, g) for the column pass, [g, g + kNumSMs) for the Nyquist plane
+            auto *part = static_cast<double *>(
+                scratch(ctx, "pkf.part", (size_t)(g + kNumSMs) * pt.nbins * sizeof(double)));
+            // r2c rows, y columns, the Nyquist plane's y transform, then the
+            // binning x pass and the Nyquist plane's x transform
+            rows_impl<float, 0>(ctx, plan, real_in, out.main, out.nyq, n * n, 1, 0, 0, d_sub, 1.0);
+            cols_impl<float>(ctx, plan, out.main, n, M, M, n, n * M, 1, 0, false);
+            rows_impl<float, 2>(ctx, plan, out.nyq, out.nyq, nullptr, n, 1, 0, 0, nullptr, 1.0);
+            CAM_LAUNCH_NAMED(ctx, "fft_cols_pk", kt, g, NTHR, smem, map, td, (int)(M / 16), (int)n, ntiles,
+                             static_cast<const float2 *>(plan->tw), device_error_word(ctx), pt.tab, pt.nbins, pt.m_u,
+                             pt.inv_s, keep ? 1 : 0, part);
+            cols_impl<float>(ctx, plan, out.nyq, n, n, n, 1, 0, 1, 0, false);
+            *d_part = part;
+            *nparts = g;
+            done = true;
+        }
+    });
+    return done;
+}
+
+bool make_tensor_map_4d(CUtensorMap *map, bool fp64, void *base, const uint64_t dims[4], const uint64_t strides[3],
+                        const uint32_t box[4])
+{
+    const EncodeTiledFn enc = encode_tiled();
+    if (!enc) return false;
+    for (int a = 0; a < 3; ++a)
+        if (strides[a] % 16 != 0 || strides[a] >= (1ull << 40)) return false;
+    if (((uintptr_t)base & 15u) != 0) return false;
+    const cuuint64_t d[4] = {dims[0], dims[1], dims[2], dims[3]};
+    const cuuint64_t st[3] = {strides[0], strides[1], strides[2]};
+    const cuuint32_t bx[4] = {box[0], box[1], box[2], box[3]};
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    const CUresult r = enc(map, fp64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, d, st,
+                           bx, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
 
 void free_plans(cam_ctx *ctx)
 {

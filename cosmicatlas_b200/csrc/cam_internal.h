@@ -85,6 +85,13 @@ struct cam_ctx {
     // captured graphs holding its old addresses can be recognised as stale
     uint64_t gen = 0;
     void *batch = nullptr;  // cam::BatchRunner of cam_batch_run (cam_serve.cu)
+    // Column FFT passes stage tiles with TMA unless CAM_NO_TMA is set in the
+    // environment when the context is created (then the cp.async kernels).
+    bool no_tma = false;
+    // The assignment's scatter stages records in shared memory and writes
+    // them in brick order unless CAM_NO_STAGE is set at context creation.
+    bool no_stage = false;
+    unsigned *err_word = nullptr;  // device word: a bounded wait ran out (see device_error_word)
     // per-kernel timing (cam_profile_enable)
     bool prof_on = false;
     std::vector<cam::ProfRecord> prof_pending;
@@ -96,6 +103,13 @@ namespace cam {
 
 void prof_begin(cam_ctx *ctx, const char *name);
 void prof_end(cam_ctx *ctx);
+
+// Device word of the context where kernels report a bounded wait that ran
+// out (TMA copies that did not land within their limit); zero otherwise.
+// Allocated and cleared on first use; check_device_error reads it (one
+// synchronisation) and throws CAM_E_CUDA if it is set.
+unsigned *device_error_word(cam_ctx *ctx);
+void check_device_error(cam_ctx *ctx);
 
 // Returns a device buffer of at least `bytes`, reallocating (and
 // synchronising the stream) if the cached one is too small.
@@ -206,6 +220,41 @@ PkDevice power_cross_device(cam_ctx *ctx, const Spectrum &s1, const Spectrum &s2
 PkDevice power_multipole_device(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins, int los);
 void power_bin(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins,
                double *h_sum_raw, double *h_sum_sn, int64_t *h_modes);
+
+// Binning tables of a P(k) (cam_power.cu): on the device [h+1] 1/W^2 per
+// axis, [h+1] C/W^2 per axis, [nbins+1] squared bin edges (units of k_f),
+// uploaded once per (N, options, bins); and the FP32 first guess of the bin
+// (m_u, inv_s).
+struct PkTables {
+    const double *tab;
+    int nbins;
+    float m_u, inv_s;
+};
+PkTables pk_tables(cam_ctx *ctx, int64_t n, const cam_pk_opts &o, int nbins);
+// Forward r2c of a real N^3 mesh (FP32) whose last column pass also bins
+// |F|^2 / W^2 of every main-spectrum mode: *d_part receives [*nparts][nbins]
+// partial sums in a fixed order.  keep = false: the x pass does not write
+// its output back (only P(k) is wanted; s.main then holds the y pass).
+// Returns false, having launched nothing, where this path does not apply
+// (FP64, no TMA, sizes without a compile-time stage list, too many bins);
+// callers then run fft_r2c_split and power_bin_device.
+bool fft_r2c_pk_fused(cam_ctx *ctx, FftPlan *plan, const void *real_in, const double *d_sub, Spectrum &out,
+                      const PkTables &pt, bool keep, double **d_part, int *nparts);
+// Completes a fused P(k): bins the Nyquist plane s.nyq into the kNumSMs
+// rows that follow part's nparts rows (the buffer fft_r2c_pk_fused
+// returns has room for them), adds all rows in a fixed order and takes the
+// mode counts and shot-noise sums of the estimator's mode set
+// (data-independent) from a table built once per key.
+PkDevice power_finish_fused(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins, double *part,
+                            int nparts);
+
+// The FFT and P(k) of a job's mesh (cam_job_run and the serving paths use
+// the same kernels, so their results are bit-identical): the r2c of
+// mesh - *d_sub into s and, if pk is non-null, the P(k) sums of nb bins left
+// on the device.  keep = false: the spectrum is not needed after P(k) (no
+// T-web), so the fused x pass need not write it back.
+PkDevice job_fft_pk(cam_ctx *ctx, FftPlan *plan, const void *mesh, const double *d_sub, Spectrum &s,
+                    const cam_pk_opts *pk, int nb, bool keep);
 
 // ------------------------------------------------------ T-web
 // d_inv (may be null): 4 planes of N^3 floats, the tidal invariants I, II,

@@ -14,6 +14,7 @@
 // reads, so nothing is cleared between calls; two calls that overlap on the
 // GPU (different streams or threads) race on it and must be serialised by
 // the caller.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -45,7 +46,15 @@ constexpr size_t kNaScratchBytes = (kTabWords + kPartWords + kModeWords + kResWo
 static __device__ __align__(256) unsigned char g_na_scratch[kNaScratchBytes];
 
 std::mutex g_na_mu;
-void *g_na_ptr[kNaMaxDevices] = {};
+// Per device: the CUDA context the scratch address was looked up in, and the
+// address.  A context that was torn down and created again (cudaDeviceReset)
+// reloads the module, so the address is looked up again when the current
+// context differs from the recorded one.
+struct NaSlot {
+    CUcontext ctx = nullptr;
+    void *ptr = nullptr;
+};
+NaSlot g_na_slot[kNaMaxDevices];
 
 __device__ __forceinline__ bool na_visited(int i, int j, int c, int n)
 {
@@ -198,21 +207,46 @@ double na_sq(int p, double s)
 // Status codes only: the entry point has no context to hold a message.
 int na_fail(int code, const char *) { return code; }
 
-// Device address of the scratch array for the current device: looked up
-// once per device (cudaGetSymbolAddress with that device current).
+// cuCtxGetCurrent through the runtime's driver entry point (the library does
+// not link the driver library itself); null if unavailable.
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+CtxGetCurrentFn ctx_get_current()
+{
+    static const CtxGetCurrentFn fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+        }
+        return reinterpret_cast<CtxGetCurrentFn>(p);
+    }();
+    return fn;
+}
+
+// Device address of the scratch array for the current device, looked up with
+// cudaGetSymbolAddress the first time a device (in its current context) is
+// used, then reused.  Without cuCtxGetCurrent the address is looked up on
+// every call (cheap, and it allocates nothing).
 int na_scratch(int dev, void **out)
 {
+    CUcontext cur = nullptr;
+    const CtxGetCurrentFn get = ctx_get_current();
+    const bool known = get && get(&cur) == CUDA_SUCCESS && cur;
     std::lock_guard<std::mutex> lk(g_na_mu);
-    if (!g_na_ptr[dev]) {
+    NaSlot &slot = g_na_slot[dev];
+    if (!known || !slot.ptr || slot.ctx != cur) {
         void *p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_na_scratch);
         if (e != cudaSuccess || !p) {
             cudaGetLastError();
             return na_fail(CAM_E_CUDA, "cudaGetSymbolAddress of the no-allocation scratch failed");
         }
-        g_na_ptr[dev] = p;
+        slot.ptr = p;
+        slot.ctx = known ? cur : nullptr;
     }
-    *out = g_na_ptr[dev];
+    *out = slot.ptr;
     return CAM_OK;
 }
 

@@ -25,37 +25,13 @@
 #include <vector>
 
 #include "cam_internal.h"
+#include "cam_pk_device.cuh"
 
 namespace cam {
 namespace {
 
 constexpr int kPkThreads = 256;
 constexpr int kPkWarps = kPkThreads / 32;
-
-__device__ __forceinline__ bool pk_visited(int i, int j, int c, int n)
-{
-    const int h = n >> 1;
-    if (i == h || j == h) return false;
-    if (c > 0) return true;
-    if (i == 0 && j == 0) return false;
-    if (j > h) return false;
-    if (i > h && j == 0) return false;
-    return true;
-}
-
-// b with E2[b] <= q < E2[b+1]; -1 below the first edge, nbins at or above
-// the last.  The initial FP32 estimate is refined by exact comparisons with
-// the FP64 squared edges, so the result depends on E2 only.
-__device__ __forceinline__ int pk_bin(double q, const double *E2, int nbins, float m_u, float inv_s)
-{
-    int b = (int)floorf((sqrtf((float)q) - m_u) * inv_s);
-    b = max(-1, min(b, nbins));
-#pragma unroll 1
-    for (int it = 0; it < 8 && b + 1 <= nbins && E2[b + 1] <= q; ++it) ++b;
-#pragma unroll 1
-    for (int it = 0; it < 8 && b >= 0 && E2[b] > q; ++it) --b;
-    return b < 0 ? -1 : b;  // b == nbins: above the last edge
-}
 
 // Legendre polynomials of mu^2 = f^2 / q (FftwFunctions.cpp:1152-1153):
 // L_2 = (3 mu^2 - 1) / 2, L_4 = (35 mu^4 - 30 mu^2 + 3) / 8, both even in mu.
@@ -350,8 +326,55 @@ PkDevice power_bin_impl(cam_ctx *ctx, const Spectrum &s, const Spectrum *s2, con
     CAM_REQUIRE(o.ndel > 0.0 && std::isfinite(o.ndel) && std::isfinite(o.DeltaKmin), CAM_E_INVAL,
                 "bin width must be > 0");
     CAM_REQUIRE(o.scheme >= 0 && o.scheme <= 2, CAM_E_INVAL, "unknown window scheme");
+    const PkTables pt = pk_tables(ctx, n, o, nbins);
+    const double *d_tab = pt.tab;
+    const size_t tab_bytes = (size_t)(2 * (h + 1) + nbins + 1) * sizeof(double);
+    // four CTAs per SM where their shared bins fit (<= 56 KB each), two
+    // otherwise: the loop is latency-bound, more resident warps hide it
+    const size_t smem_need = tab_bytes + (size_t)kPkWarps * nbins * (2 * sizeof(double) + sizeof(unsigned long long));
+    const int grid = kNumSMs * (smem_need <= 56 * 1024 ? 4 : 2);
+    const int64_t nrows = (int64_t)n * n;
+    const int64_t rpc = (nrows + grid - 1) / grid;
+    const std::string tg(tag);
+    auto *part = static_cast<double *>(scratch(ctx, (tg + ".part").c_str(), (size_t)grid * nbins * 2 * sizeof(double)));
+    auto *pm = static_cast<unsigned long long *>(
+        scratch(ctx, (tg + ".pm").c_str(), (size_t)grid * nbins * sizeof(unsigned long long)));
+    auto *res = static_cast<double *>(scratch(ctx, (tg + ".res").c_str(), (size_t)nbins * 2 * sizeof(double)));
+    auto *resm = static_cast<unsigned long long *>(
+        scratch(ctx, (tg + ".resm").c_str(), (size_t)nbins * sizeof(unsigned long long)));
+    const size_t smem = tab_bytes + (size_t)kPkWarps * nbins * (2 * sizeof(double) + sizeof(unsigned long long));
+    CAM_REQUIRE(smem <= 220 * 1024, CAM_E_UNSUPPORTED, "too many bins for one CTA");
+    const float m_u = pt.m_u, inv_s = pt.inv_s;
+    auto launch = [&](auto cplx, auto md) {
+        using C = decltype(cplx);
+        constexpr int X = decltype(md)::value;
+        auto kern = pk_bin_kernel<C, X>;
+        smem_at_least(kern, smem);
+        const C *m2 = X == 1 ? (const C *)s2->main : nullptr;
+        const C *q2 = X == 1 ? (const C *)s2->nyq : nullptr;
+        CAM_LAUNCH_NAMED(ctx, X == 1 ? "pk_cross_bin" : (X == 2 ? "pk_multipole_bin" : "pk_bin"), kern, grid,
+                         kPkThreads, smem, (const C *)s.main, (const C *)s.nyq, m2, q2, los, n, d_tab, nbins, m_u,
+                         inv_s, rpc, part, pm);
+    };
+    auto by_mode = [&](auto cplx) {
+        if (mode == 1) launch(cplx, std::integral_constant<int, 1>{});
+        else if (mode == 2) launch(cplx, std::integral_constant<int, 2>{});
+        else launch(cplx, std::integral_constant<int, 0>{});
+    };
+    if (s.precision == CAM_F32) by_mode(float2{});
+    else by_mode(double2{});
+    CAM_LAUNCH(ctx, pk_final_kernel, nbins, 256, 0, part, pm, grid, nbins, res, resm);
+    return PkDevice{res, resm};
+}
+
+}  // namespace
+
+PkTables pk_tables(cam_ctx *ctx, int64_t n_, const cam_pk_opts &o, int nbins)
+{
+    const int n = (int)n_;
     // Per-axis tables (FP64): 1/W^2 = sinc^(-2(p+1)), C/W^2; squared edges.
     const int p = o.scheme;
+    const int h = (int)(n / 2);
     std::vector<double> tab(2 * (h + 1) + nbins + 1);
     for (int a = 0; a <= h; ++a) {
         const double x = M_PI * (double)a / (double)n;
@@ -381,45 +404,139 @@ PkDevice power_bin_impl(cam_ctx *ctx, const Spectrum &s, const Spectrum *s2, con
     auto *d_tab = static_cast<double *>(scratch(ctx, key, tab_bytes));
     if (fresh) CAM_CUDA_TRY(cudaMemcpyAsync(d_tab, tab.data(), tab_bytes, cudaMemcpyHostToDevice, ctx->stream));
 
-    // four CTAs per SM where their shared bins fit (<= 56 KB each), two
-    // otherwise: the loop is latency-bound, more resident warps hide it
-    const size_t smem_need = tab_bytes + (size_t)kPkWarps * nbins * (2 * sizeof(double) + sizeof(unsigned long long));
-    const int grid = kNumSMs * (smem_need <= 56 * 1024 ? 4 : 2);
+    return PkTables{d_tab, nbins, (float)o.DeltaKmin, (float)(1.0 / o.ndel)};
+}
+
+namespace {
+
+// Nyquist-plane elements (c = N/2) of a fused P(k): each warp takes 32 rows
+// r = i N + j at a time, every lane bins one element, and lane 0 adds the 32
+// values to the warp's own bins in lane order.  part[cta][bin] as the fused
+// column pass writes it.
+constexpr int kNyqThreads = 256;
+__global__ void __launch_bounds__(kNyqThreads)
+pk_nyq_kernel(const float2 *__restrict__ nyq, int n, const double *__restrict__ g_tab, int nbins, float m_u,
+              float inv_s, double *__restrict__ part)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int h = n / 2;
+    double *tw2 = reinterpret_cast<double *>(smem_raw);  // [h+1]
+    double *E2 = tw2 + (h + 1);                          // [nbins+1]
+    double *wsum = E2 + (nbins + 1);                     // [warps][nbins]
+    constexpr int NW = kNyqThreads / 32;
+    for (int t = threadIdx.x; t <= h; t += blockDim.x) tw2[t] = g_tab[t];
+    for (int t = threadIdx.x; t <= nbins; t += blockDim.x) E2[t] = g_tab[2 * (h + 1) + t];
+    for (int t = threadIdx.x; t < NW * nbins; t += blockDim.x) wsum[t] = 0.0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double *mysum = wsum + (size_t)warp * nbins;
     const int64_t nrows = (int64_t)n * n;
-    const int64_t rpc = (nrows + grid - 1) / grid;
-    const std::string tg(tag);
-    auto *part = static_cast<double *>(scratch(ctx, (tg + ".part").c_str(), (size_t)grid * nbins * 2 * sizeof(double)));
-    auto *pm = static_cast<unsigned long long *>(
-        scratch(ctx, (tg + ".pm").c_str(), (size_t)grid * nbins * sizeof(unsigned long long)));
-    auto *res = static_cast<double *>(scratch(ctx, (tg + ".res").c_str(), (size_t)nbins * 2 * sizeof(double)));
-    auto *resm = static_cast<unsigned long long *>(
-        scratch(ctx, (tg + ".resm").c_str(), (size_t)nbins * sizeof(unsigned long long)));
-    const size_t smem = tab_bytes + (size_t)kPkWarps * nbins * (2 * sizeof(double) + sizeof(unsigned long long));
-    CAM_REQUIRE(smem <= 220 * 1024, CAM_E_UNSUPPORTED, "too many bins for one CTA");
-    const float m_u = (float)o.DeltaKmin, inv_s = (float)(1.0 / o.ndel);
-    auto launch = [&](auto cplx, auto md) {
-        using C = decltype(cplx);
-        constexpr int X = decltype(md)::value;
-        auto kern = pk_bin_kernel<C, X>;
-        smem_at_least(kern, smem);
-        const C *m2 = X == 1 ? (const C *)s2->main : nullptr;
-        const C *q2 = X == 1 ? (const C *)s2->nyq : nullptr;
-        CAM_LAUNCH_NAMED(ctx, X == 1 ? "pk_cross_bin" : (X == 2 ? "pk_multipole_bin" : "pk_bin"), kern, grid,
-                         kPkThreads, smem, (const C *)s.main, (const C *)s.nyq, m2, q2, los, n, d_tab, nbins, m_u,
-                         inv_s, rpc, part, pm);
-    };
-    auto by_mode = [&](auto cplx) {
-        if (mode == 1) launch(cplx, std::integral_constant<int, 1>{});
-        else if (mode == 2) launch(cplx, std::integral_constant<int, 2>{});
-        else launch(cplx, std::integral_constant<int, 0>{});
-    };
-    if (s.precision == CAM_F32) by_mode(float2{});
-    else by_mode(double2{});
-    CAM_LAUNCH(ctx, pk_final_kernel, nbins, 256, 0, part, pm, grid, nbins, res, resm);
-    return PkDevice{res, resm};
+    const int64_t chunk = (nrows + gridDim.x - 1) / gridDim.x;
+    const int64_t r0 = (int64_t)blockIdx.x * chunk, r1 = min(nrows, r0 + chunk);
+    for (int64_t rb = r0 + 32 * warp; rb < r1; rb += 32 * NW) {
+        const int64_t r = rb + lane;
+        int bin = -1;
+        double v = 0.0;
+        if (r < r1) {
+            const int i = (int)(r / n), j = (int)(r - (int64_t)i * n);
+            const int a = i <= h ? i : n - i, b = j <= h ? j : n - j;
+            const double q = (double)((int64_t)a * a + (int64_t)b * b + (int64_t)h * h);
+            bin = pk_bin(q, E2, nbins, m_u, inv_s);
+            if (bin >= 0 && bin < nbins && pk_visited(i, j, h, n)) {
+                const float2 f = nyq[r];
+                v = ((double)f.x * (double)f.x + (double)f.y * (double)f.y) * (tw2[a] * tw2[b] * tw2[h]);
+            } else {
+                bin = -1;
+            }
+        }
+        for (int l = 0; l < 32; ++l) {
+            const int bl = __shfl_sync(0xffffffffu, bin, l);
+            const double vl = __shfl_sync(0xffffffffu, v, l);
+            if (lane == 0 && bl >= 0) mysum[bl] += vl;
+        }
+    }
+    __syncthreads();
+    for (int bn = threadIdx.x; bn < nbins; bn += blockDim.x) {
+        double sum = 0.0;
+        for (int w = 0; w < NW; ++w) sum += wsum[(size_t)w * nbins + bn];
+        part[(size_t)blockIdx.x * nbins + bn] = sum;
+    }
+}
+
+// One CTA per bin: the fused partials [nparts][nbins] summed by a fixed
+// tree, with the static shot-noise sums and mode counts of the mode set.
+__global__ void __launch_bounds__(256)
+pk_final_fused_kernel(const double *__restrict__ part, int nparts, int nbins, const double *__restrict__ stat,
+                      const unsigned long long *__restrict__ stat_modes, double *__restrict__ out,
+                      unsigned long long *__restrict__ modes)
+{
+    __shared__ double r0[256];
+    const int bn = blockIdx.x;
+    double s0 = 0.0;
+    for (int p = threadIdx.x; p < nparts; p += blockDim.x) s0 += part[(size_t)p * nbins + bn];
+    r0[threadIdx.x] = s0;
+    __syncthreads();
+    for (int hh = blockDim.x / 2; hh > 0; hh >>= 1) {
+        if (threadIdx.x < hh) r0[threadIdx.x] += r0[threadIdx.x + hh];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[2 * bn] = r0[0];
+        out[2 * bn + 1] = stat[2 * bn + 1];
+        modes[bn] = stat_modes[bn];
+    }
 }
 
 }  // namespace
+
+PkDevice power_finish_fused(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins, double *part,
+                            int nparts)
+{
+    const int n = (int)s.n, h = n / 2;
+    const PkTables pt = pk_tables(ctx, n, o, nbins);
+    // Mode counts and shot-noise sums depend on N, the options and the bins
+    // only: computed once per key by the binning kernel (its sums of |F|^2
+    // are discarded, so the spectrum's contents do not matter) and kept.
+    char key[176];
+    snprintf(key, sizeof(key), "pks.%d.%d.%d.%d.%d.%.17g.%.17g", n, o.scheme, o.mas_correction, o.sn_correction, nbins,
+             o.DeltaKmin, o.ndel);
+    const std::string k(key);
+    const auto found = ctx->bufs.find(k + ".res");
+    PkDevice stat;
+    if (found == ctx->bufs.end() || found->second.ptr == nullptr) {
+        stat = power_bin_impl(ctx, s, nullptr, o, nbins, key);
+    } else {
+        stat.sums = static_cast<double *>(found->second.ptr);
+        stat.modes = static_cast<unsigned long long *>(ctx->bufs[k + ".resm"].ptr);
+    }
+    const int g2 = kNumSMs;
+    const size_t smem = (size_t)(h + 1 + nbins + 1 + (kNyqThreads / 32) * nbins) * sizeof(double);
+    CAM_REQUIRE(smem <= 220 * 1024, CAM_E_UNSUPPORTED, "too many bins for one CTA");
+    double *all = part;  // [nparts + kNumSMs][nbins]: the Nyquist rows follow the column pass's
+    smem_at_least(pk_nyq_kernel, smem);
+    CAM_LAUNCH_NAMED(ctx, "pk_nyq", pk_nyq_kernel, g2, kNyqThreads, smem, static_cast<const float2 *>(s.nyq), n,
+                     pt.tab, nbins, pt.m_u, pt.inv_s, all + (size_t)nparts * nbins);
+    auto *res = static_cast<double *>(scratch(ctx, "pkf.res", (size_t)nbins * 2 * sizeof(double)));
+    auto *resm = static_cast<unsigned long long *>(scratch(ctx, "pkf.resm", (size_t)nbins * sizeof(unsigned long long)));
+    CAM_LAUNCH_NAMED(ctx, "pk_final", pk_final_fused_kernel, nbins, 256, 0, all, nparts + g2, nbins, stat.sums,
+                     stat.modes, res, resm);
+    return PkDevice{res, resm};
+}
+
+PkDevice job_fft_pk(cam_ctx *ctx, FftPlan *plan, const void *mesh, const double *d_sub, Spectrum &s,
+                    const cam_pk_opts *pk, int nb, bool keep)
+{
+    if (pk) {
+        const PkTables pt = pk_tables(ctx, s.n, *pk, nb);
+        double *part = nullptr;
+        int nparts = 0;
+        if (fft_r2c_pk_fused(ctx, plan, mesh, d_sub, s, pt, keep, &part, &nparts))
+            return power_finish_fused(ctx, s, *pk, nb, part, nparts);
+    }
+    fft_r2c_split(ctx, plan, mesh, d_sub, s);
+    if (!pk) return PkDevice{nullptr, nullptr};
+    return power_bin_device(ctx, s, *pk, nb);
+}
 
 PkDevice power_bin_device(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &o, int nbins)
 {

@@ -181,12 +181,8 @@ void enqueue_job(Slot &s, const cam_job_desc &d)
     out.d_sum = static_cast<double *>(scratch(c, "job.sum", 2 * sizeof(double)));
     assign_device(c, s.in[0], s.in[1], s.in[2], d.parts.w ? s.in[3] : nullptr, d.parts.n, g, d.scheme, out);
     Spectrum sp = alloc_spectrum(c, n, d.precision, "job.spec");
-    fft_r2c_split(c, plan, out.mesh, out.d_sum + 1, sp);
-    int nb = 0;
-    if (want_pk(d)) {
-        nb = nbins_for(d.pk, n);
-        power_bin(c, sp, d.pk, nb, nullptr, nullptr, nullptr);
-    }
+    const int nb = want_pk(d) ? nbins_for(d.pk, n) : 0;
+    const PkDevice pkd = job_fft_pk(c, plan, out.mesh, out.d_sum + 1, sp, nb ? &d.pk : nullptr, nb, d.want_tweb != 0);
     if (d.want_tweb) tweb_device(c, plan, sp, g.L[0], out.d_sum + 1, d.tweb.input_type, d.tweb, nullptr, nullptr, nullptr);
     auto *m = reinterpret_cast<MirrorHead *>(s.pin);
     CAM_CUDA_TRY(cudaMemcpyAsync(m->stats, scratch(c, "asg.stats", 64), 3 * sizeof(unsigned long long),
@@ -197,10 +193,10 @@ void enqueue_job(Slot &s, const cam_job_desc &d)
                                      5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
     if (nb) {
         double *pk = reinterpret_cast<double *>(s.pin + sizeof(MirrorHead));
-        CAM_CUDA_TRY(cudaMemcpyAsync(pk, scratch(c, "pk.res", (size_t)nb * 2 * sizeof(double)),
-                                     (size_t)nb * 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-        CAM_CUDA_TRY(cudaMemcpyAsync(pk + 2 * nb, scratch(c, "pk.resm", (size_t)nb * sizeof(unsigned long long)),
-                                     (size_t)nb * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+        CAM_CUDA_TRY(cudaMemcpyAsync(pk, pkd.sums, (size_t)nb * 2 * sizeof(double), cudaMemcpyDeviceToHost,
+                                     c->stream));
+        CAM_CUDA_TRY(cudaMemcpyAsync(pk + 2 * nb, pkd.modes, (size_t)nb * sizeof(unsigned long long),
+                                     cudaMemcpyDeviceToHost, c->stream));
     }
 }
 

@@ -205,3 +205,65 @@ def test_invalid_arguments(ctx):
     with pytest.raises(CamError) as e:
         ctx.assign(x, x, x, None, g, CIC, F32)
     assert e.value.code == -1
+
+
+# ---- against the reference's own getDensity_* (golden fixture) ------------
+def _golden():
+    import os
+    return np.load(os.path.join(os.path.dirname(__file__), "golden", "getdensity_ref.npz"))
+
+
+@pytest.mark.parametrize("case", ["bulk", "shift", "edges"])
+def test_ngp_counts_equal_reference_getdensity(ctx, case):
+    # counts bit-exact against the meshes the reference's getDensity_NGP wrote
+    G = _golden()
+    n, L, mn = G[f"{case}_grid"]
+    n = int(n)
+    g = make_grid(n, float(L), None, float(mn))
+    got = ctx.count_ngp(G[f"{case}_x"], G[f"{case}_y"], G[f"{case}_z"], g).mesh
+    assert np.array_equal(np.asarray(got).astype(np.float32), G[f"{case}_ngp_unit"])
+
+
+@pytest.mark.parametrize("case", ["bulk", "shift"])
+@pytest.mark.parametrize("scheme", SCHEMES)
+@pytest.mark.parametrize("weighted", [False, True])
+def test_mesh_vs_reference_getdensity(ctx, case, scheme, weighted):
+    # within 1e-5 per cell of the reference's own float meshes
+    G = _golden()
+    n, L, mn = G[f"{case}_grid"]
+    g = make_grid(int(n), float(L), None, float(mn))
+    w = G[f"{case}_w"] if weighted else None
+    got = ctx.assign(G[f"{case}_x"], G[f"{case}_y"], G[f"{case}_z"], w, g, scheme, F32).mesh
+    want = G[f"{case}_{('ngp', 'cic', 'tsc')[scheme]}_{'mass' if weighted else 'unit'}"]
+    unit = float(np.mean(w, dtype=np.float64)) if weighted else 1.0
+    assert rel_err_cells(got, want, unit) <= 1e-5
+
+
+def _context_with(env):
+    import os
+    from cosmicatlas_b200.api import Context
+    os.environ[env] = "1"
+    try:
+        return Context(0)
+    finally:
+        del os.environ[env]
+
+
+@pytest.mark.parametrize("scheme", SCHEMES)
+@pytest.mark.parametrize("n", [64, 128, 256])
+def test_staged_scatter_equals_direct_appends(ctx, scheme, n):
+    # the staged scatter (records ranked per brick in shared memory, one
+    # range per brick and flush) fills the same bricks as one append per
+    # record: the integer cell sums, hence the meshes, are bit-identical
+    box = 1000.0
+    x, y, z = synth.clumped(1_500_000, box, 15_000, 2.0, 0.8, seed=n + 10 * scheme)
+    w = synth.halo_masses(x.size, seed=n)
+    c2 = _context_with("CAM_NO_STAGE")
+    try:
+        g = make_grid(n, box)
+        a = ctx.assign(x, y, z, w, g, scheme, F32)
+        b = c2.assign(x, y, z, w, g, scheme, F32)
+        assert np.array_equal(a.mesh, b.mesh)
+        assert a.sum_mesh == b.sum_mesh and a.n_in == b.n_in
+    finally:
+        c2.close()

@@ -45,6 +45,50 @@ def test_c2r_vs_numpy(ctx, n, prec):
     assert rel_rms(got, want) <= (1e-12 if prec == F64 else 2e-6)
 
 
+# The configurations' mesh sizes (384 and 768 need the radix-3 stages)
+LARGE = [(192, F32), (256, F32), (384, F32), (384, F64), (512, F32), (768, F32)]
+
+
+def _rel_rms_chunked(got, want):
+    num = den = 0.0
+    for i in range(0, got.shape[0], 32):
+        a = np.asarray(got[i:i + 32], np.complex128 if np.iscomplexobj(got) else np.float64)
+        b = want[i:i + 32]
+        num += float(np.sum(np.abs(a - b) ** 2))
+        den += float(np.sum(np.abs(b) ** 2))
+    return float(np.sqrt(num / den))
+
+
+@pytest.mark.parametrize("n,prec", LARGE)
+def test_r2c_large_vs_fp64(ctx, n, prec):
+    import torch
+    rng = np.random.default_rng(n)
+    dt = np.float64 if prec == F64 else np.float32
+    x = (rng.standard_normal(size=(n, n, n), dtype=np.float32) + 0.3).astype(dt)
+    got = ctx.fft_r2c(torch.from_numpy(x).cuda()).cpu().numpy()
+    torch.cuda.empty_cache()
+    want = orc.rfft3_f64(x)
+    del x
+    assert got.shape == want.shape
+    assert _rel_rms_chunked(got, want) <= (1e-12 if prec == F64 else 2e-6)
+
+
+@pytest.mark.parametrize("n,prec", [(384, F32), (512, F32), (768, F32), (384, F64)])
+def test_c2r_large_vs_fp64(ctx, n, prec):
+    import torch
+    rng = np.random.default_rng(100 + n)
+    h = n // 2 + 1
+    cdt = np.complex128 if prec == F64 else np.complex64
+    spec = np.empty((n, n, h), cdt)
+    spec.real = rng.standard_normal(size=(n, n, h), dtype=np.float32)
+    spec.imag = rng.standard_normal(size=(n, n, h), dtype=np.float32)
+    got = ctx.fft_c2r(torch.from_numpy(spec).cuda()).cpu().numpy()
+    torch.cuda.empty_cache()
+    want = orc.irfft3_f64(spec, n)
+    del spec
+    assert _rel_rms_chunked(got, want) <= (1e-12 if prec == F64 else 2e-6)
+
+
 @pytest.mark.parametrize("n", [64, 192, 256])
 def test_roundtrip_large(ctx, n):
     rng = np.random.default_rng(n)
@@ -169,3 +213,53 @@ def test_power_multipoles_vs_oracle(ctx, n, scheme, los, prec):
     has = md > 0
     assert np.max(np.abs(got["p2"] - p2)[has] / scale[has]) <= 1e-5
     assert np.max(np.abs(got["p4"] - p4)[has] / scale[has]) <= 1e-5
+
+
+def _context_without_tma():
+    import os
+    os.environ["CAM_NO_TMA"] = "1"
+    try:
+        return Context(0)
+    finally:
+        del os.environ["CAM_NO_TMA"]
+
+
+@pytest.mark.parametrize("n", [64, 256, 384])
+@pytest.mark.parametrize("prec", [F32, F64])
+def test_tma_staged_columns_equal_cp_async(ctx, n, prec):
+    # the column passes staged by TMA compute exactly what the cp.async
+    # kernels compute: only the tile movement differs
+    import torch
+    rng = np.random.default_rng(7 + n)
+    dt = np.float64 if prec == F64 else np.float32
+    x = torch.from_numpy(rng.standard_normal(size=(n, n, n)).astype(dt)).cuda()
+    c2 = _context_without_tma()
+    try:
+        a = ctx.fft_r2c(x)
+        b = c2.fft_r2c(x)
+        torch.cuda.synchronize()
+        assert torch.equal(a, b)
+        assert torch.equal(ctx.fft_c2r(a), c2.fft_c2r(b))
+    finally:
+        c2.close()
+
+
+@pytest.mark.parametrize("scheme", [NGP, CIC, TSC])
+@pytest.mark.parametrize("n,nbins,ndel", [(64, 32, 1.0), (128, 64, 1.0), (96, 30, 1.5)])
+def test_job_pk_binned_in_fft_equals_separate_binning(ctx, scheme, n, nbins, ndel):
+    # cam_job_run bins P(k) inside the FFT's last column pass; the separate
+    # binning kernel over the stored spectrum gives the same sums (up to the
+    # FP64 summation order) and the same mode counts
+    box = 800.0
+    x, y, z = synth.clumped(400_000, box, 4_000, 2.0, 0.8, seed=n + scheme)
+    g = make_grid(n, box)
+    opts = Context.pk_opts(scheme, nbins=nbins, ndel=ndel)
+    job = ctx.job(x, y, z, None, g, scheme, F32, pk=opts)
+    mesh = ctx.assign(x, y, z, None, g, scheme, F32).mesh
+    sep = ctx.power(mesh, box, opts)
+    assert np.array_equal(job["pk"].modes, sep.modes)
+    floor = np.abs(sep.shot_noise) * np.ones(nbins)
+    assert pk_rel_err(job["pk"].pk, sep.pk, floor) <= 1e-9
+    # and with the T-web, where the x pass also writes the spectrum back
+    job2 = ctx.job(x, y, z, None, g, scheme, F32, pk=opts, tweb=Context.tweb_opts(8.0, 0.0, 1e-5))
+    assert np.array_equal(job2["pk"].pk, job["pk"].pk)

@@ -1,22 +1,24 @@
-"""The configurations at their full sizes on the GPU.
+"""The configurations at their full sizes on the GPU, against the FP64 oracle.
 
-The plain small configuration (2,000,000 particles, CIC onto 128^3 FP64,
-P(k), T-web) is compared with the FP64 oracle in full.  The scheme sweep
-(16,777,216 weighted particles onto 256^3) and the large job (768^3 TSC of
-452,984,832 Zel'dovich-displaced particles) are checked through properties
-that do not depend on size:
-  * every particle is kept, and the mesh holds the total weight (1e-6);
-  * NGP counts sum to the number of particles kept (exact);
-  * the mesh, hence P(k), is bit-identical when the particles are shuffled
-    and when the job is repeated (integer cell sums, fixed-order FP64 bins);
-  * P(k) mode counts equal a direct count of the estimator's mode set;
-  * T-web label counts sum to N^3.
+* The plain small configuration (2,000,000 particles, CIC onto 128^3 FP64,
+  P(k), T-web) is compared with the oracle in full.
+* The scheme sweep (16,777,216 weighted particles onto 256^3, 128 bins) is
+  compared with the oracle per cell for NGP, CIC and TSC (NGP counts
+  bit-exact), and its P(k) per bin.
+* The large job (768^3 TSC of 452,984,832 Zel'dovich-displaced particles,
+  256 bins of 1.5 k_f, T-web R = 3, lambda_th = 0.1) is compared with the
+  oracle's P(k) in full and its labels on a fixed set of x-planes.
+Size-independent properties are checked beside them: every particle is kept
+and the mesh holds the total weight (1e-6); the mesh, hence P(k), is
+bit-identical when the particles are shuffled and when the job is repeated
+(integer cell sums, fixed-order FP64 bins); mode counts equal a direct count
+of the estimator's mode set; label counts sum to N^3.
 """
 import numpy as np
 import pytest
 
 import oracle as orc
-from conftest import pk_rel_err
+from conftest import pk_rel_err, rel_err_cells
 from cosmicatlas_b200 import synth
 from cosmicatlas_b200.api import CIC, F32, F64, NGP, TSC, Context, make_grid
 
@@ -122,3 +124,92 @@ def test_large_job_full_size_properties(ctx):
     assert int(res["tweb"].counts.sum()) == npart
     assert np.array_equal(res["pk"].modes, mode_counts(n, 256, 0.0, 1.5))
     assert np.all(np.isfinite(res["pk"].pk))
+
+
+@pytest.mark.parametrize("scheme", [NGP, CIC, TSC])
+def test_scheme_sweep_full_size_vs_oracle(ctx, sweep_particles, scheme):
+    # the benchmarked configuration, per cell and per bin against the FP64 oracle
+    c, (x, y, z, w) = sweep_particles
+    n, box, nb = c["n"], c["box"], c["nbins"]
+    g = make_grid(n, box)
+    a = ctx.assign(x, y, z, w, g, scheme, F32)
+    got = a.mesh.cpu().numpy()
+    ref, lost = orc.assign_f64_mt(scheme, c["x"], c["y"], c["z"], c["w"], orc.Grid.cubic(n, box))
+    assert lost == 0 and a.n_lost == 0 and a.n_in == c["x"].size
+    unit = float(np.mean(c["w"], dtype=np.float64))
+    assert rel_err_cells(got, ref, unit) <= 1e-5
+    if scheme == NGP:
+        cnt = ctx.count_ngp(x, y, z, g).mesh.cpu().numpy().astype(np.int64)
+        keys = orc.keys(NGP, c["x"], c["y"], c["z"], orc.Grid.cubic(n, box))
+        assert np.array_equal(cnt.ravel(), np.bincount(keys, minlength=n ** 3)[: n ** 3])
+    r = ctx.job(x, y, z, w, g, scheme, F32, pk=Context.pk_opts(scheme, nbins=nb))
+    pk = orc.power_grid(ref, box, scheme, nb)
+    floor = pk.shot_noise * pk.sum_sn / np.maximum(pk.modes, 1)
+    assert np.array_equal(r["pk"].modes, pk.modes)
+    assert pk_rel_err(r["pk"].pk, pk.pk, floor) <= 1e-5
+
+
+def test_light_halo_cells_vs_oracle(ctx):
+    # Halo-like masses from 1e11 to 1e15: cells that only light halos reach
+    # are held to 1e-5 of their own value (not to the mean particle mass).
+    n, box, npart = 64, 500.0, 600_000
+    x, y, z = synth.clumped(npart, box, 6_000, 2.0, 0.8, seed=31)
+    w = synth.halo_masses(npart, seed=32)
+    g = orc.Grid.cubic(n, box)
+    heavy = np.where(w >= 1e13, w, 0.0).astype(np.float32)
+    for scheme in (CIC, TSC):
+        got = ctx.assign(x, y, z, w, make_grid(n, box), scheme, F32).mesh
+        ref, _ = orc.assign_f64(scheme, x, y, z, w, g)
+        href, _ = orc.assign_f64(scheme, x, y, z, heavy, g)
+        light = (href == 0.0) & (ref >= 0.5 * 1e11)  # at least half the lightest halo, no heavy halo
+        assert light.sum() > 1000
+        err = np.abs(got.astype(np.float64) - ref)[light] / ref[light]
+        assert float(err.max()) <= 1e-5, float(err.max())
+
+
+def _host_ram_gb():
+    try:
+        import psutil
+        return psutil.virtual_memory().available / 1e9
+    except Exception:
+        return 0.0
+
+
+def test_large_job_full_size_vs_oracle(ctx):
+    # 768^3 TSC of 452,984,832 particles: P(k) (256 bins of 1.5 k_f) against
+    # the FP64 oracle in full; T-web labels (R = 3, lambda_th = 0.1) against
+    # the oracle's FP64 eigenvalues on eight x-planes, ties (an eigenvalue
+    # within 1e-5 of lambda_th) excepted.
+    if _host_ram_gb() < 48:
+        pytest.skip("needs ~48 GB of host memory for the FP64 oracle at 768^3")
+    n, box, R, lth, nb, ndel = 768, 1500.0, 3.0, 0.1, 256, 1.5
+    import torch
+    x, y, z, _ = synth.zeldovich_lattice(n, box, device="cuda")
+    torch.cuda.synchronize()
+    res = ctx.job(x, y, z, None, make_grid(n, box), TSC, F32, pk=Context.pk_opts(TSC, nbins=nb, ndel=ndel),
+                  tweb=Context.tweb_opts(R, lth, BAND), want_labels=True)
+    labels = res["tweb"].labels
+    labels = labels.cpu().numpy() if hasattr(labels, "cpu") else np.asarray(labels)
+    hx, hy, hz = (v.cpu().numpy() for v in (x, y, z))
+    del x, y, z
+    torch.cuda.empty_cache()
+    mesh, lost = orc.assign_f64_mt(TSC, hx, hy, hz, None, orc.Grid.cubic(n, box))
+    del hx, hy, hz
+    assert lost == 0 and res["assign"].n_lost == 0
+    pk = orc.power_grid(mesh, box, TSC, nb, 0.0, ndel)
+    floor = pk.shot_noise * pk.sum_sn / np.maximum(pk.modes, 1)
+    assert np.array_equal(res["pk"].modes, pk.modes)
+    assert pk_rel_err(res["pk"].pk, pk.pk, floor) <= 1e-5
+    nbar = mesh.sum() / mesh.size
+    mesh /= nbar
+    mesh -= 1.0
+    dk = orc.rfft3_f64(mesh)
+    del mesh
+    planes = [0, 97, 200, 383, 384, 511, 640, 767]
+    lam = orc.eig3_f64(orc.tidal_planes(dk, n, box, R, planes))
+    lab, _, _ = orc.classify(lam, lth, BAND)
+    lab = lab.reshape(len(planes), n, n)
+    near = np.any(np.abs(lam - lth) <= BAND, axis=-1)
+    bad = (labels[planes] != lab) & ~near
+    assert int(bad.sum()) == 0, int(bad.sum())
+    assert int(near.sum()) < lab.size // 1000
