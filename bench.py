@@ -51,7 +51,8 @@ def parse():
     ap.add_argument("--particles", type=int, default=N_PARTICLES)
     ap.add_argument("--kernels-only", action="store_true",
                     help="profiler runs: the device-resident pass only (no e2e pass, no CPU baseline)")
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "single512", "large768", "c1", "calib", "stream", "bam"],
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "single512", "large768", "c1", "calib", "calib_pk",
+                                                             "stream", "bam"],
                     help="sweep: the benchmark line (default); single512 / large768 / c1: one-job latency lines; "
                          "calib / stream: served vs plain per-call jobs/s and latency")
     ap.add_argument("--jobs", type=int, default=0, help="calib / stream: number of jobs (0 = the config's)")
@@ -866,6 +867,93 @@ def run_calib(args):
     }
 
 
+def run_calib_pk(args):
+    """The calibration batch without the T-web (4,096 jobs: 64^3 CIC FP32,
+    262,144 clumped particles each, L = 500, P(k) in 32 bins), through the
+    per-call path, graph-packed batches, the job server and the persistent
+    on-device request loop (one CTA per job, no launch per job)."""
+    import torch
+
+    from cosmicatlas_b200 import synth
+    from cosmicatlas_b200.api import CIC, Context, DeviceLoop, JobSpec, Server, make_grid
+    torch.cuda.set_device(0)
+    njobs = args.jobs or 4096
+    grid = make_grid(64, 500.0)
+    pk = Context.pk_opts(CIC, nbins=32)
+    parts = []
+    for j in range(njobs):
+        rng = np.random.default_rng(5 + j)
+        frac, sig = rng.uniform(0.5, 0.9), rng.uniform(1.0, 4.0)
+        parts.append(synth.clumped_torch(262_144, 500.0, 2_000, sig, frac, seed=100_000 + j))
+    torch.cuda.synchronize()
+
+    def specs():
+        return [JobSpec(x, y, z, None, grid=grid, scheme=CIC, precision=0, pk=pk) for x, y, z in parts]
+    stream = torch.cuda.current_stream()
+    ctx = Context(0)
+    ctx.set_stream(stream.cuda_stream)
+
+    def plain():
+        lat = []
+        for x, y, z in parts:
+            t0 = time.perf_counter()
+            ctx.job(x, y, z, None, grid, CIC, 0, pk=pk)
+            lat.append(1e3 * (time.perf_counter() - t0))
+        return lat
+    for x, y, z in parts[:64]:
+        ctx.job(x, y, z, None, grid, CIC, 0, pk=pk)
+    ms_plain, lat_plain = _events_ms(plain, stream)
+    ctx.batch(specs()[:64])
+    sp = specs()
+    ms_batch, _ = _events_ms(lambda: ctx.batch(sp), stream)
+    ctx.close()
+    with Server(0, workers=4, max_batch=32) as srv:
+        for i in [srv.submit(s) for s in specs()[:256]]:
+            srv.wait(i)
+        srv.stats(reset=True)
+        sp = specs()
+
+        def serve():
+            for i in [srv.submit(s) for s in sp]:
+                srv.wait(i)
+        ms_srv, _ = _events_ms(serve, stream)
+        st = srv.stats()
+    with DeviceLoop(0, max_particles=262_144, nslots=njobs, idle_timeout_s=10.0) as lp:
+        for i in [lp.submit(s) for s in specs()[:256]]:
+            lp.wait(i)
+        sp = specs()
+        lat_dl = []
+
+        def devloop():
+            t_sub = {}
+            ids = []
+            for s in sp:
+                t_sub[len(ids)] = time.perf_counter()
+                ids.append(lp.submit(s))
+            for k, i in enumerate(ids):
+                lp.wait(i)
+                lat_dl.append(1e3 * (time.perf_counter() - t_sub[k]))
+        with ClockSampler(0) as clk:
+            ms_dl, _ = _events_ms(devloop, stream)
+    return {
+        "workload": f"calibration batch without the T-web: {njobs} jobs x 262,144 clumped particles, L=500, "
+                    "CIC 64^3 FP32, P(k) 32 bins",
+        "metric": "mesh-jobs/s", "unit": "jobs/s",
+        "plain": {"value": round(njobs / (ms_plain / 1e3), 1), "latency_ms": _latency(lat_plain),
+                  "path": "cam_job_run per job, one context"},
+        "batch": {"value": round(njobs / (ms_batch / 1e3), 1), "path": "cam_batch_run, 32 jobs per graph"},
+        "served": {"value": round(njobs / (ms_srv / 1e3), 1), "path": "cam_server: 4 workers, batches of 32",
+                   "latency_ms": {"p50": round(st["p50_ms"], 3), "p99": round(st["p99_ms"], 3)}},
+        "device_loop": {"value": round(njobs / (ms_dl / 1e3), 1),
+                        "path": "cam_devloop: one resident kernel, one CTA per job, queue in mapped host memory",
+                        "latency_ms": _latency(lat_dl),
+                        "latency_note": "submit -> result with all jobs submitted at t = 0 (queueing included)"},
+        "speedup_device_loop_vs_plain": round(ms_plain / ms_dl, 2),
+        "speedup_served_vs_plain": round(ms_plain / ms_srv, 2),
+        "clocks": clk.summary(),
+    }
+
+
 def stream_jobs(njobs, seed=4):
     """The served mixed stream: N from {64..512} (weights .30/.25/.15/.15/.10
     /.05), N_p log-uniform [1e5, 5e7], L log-uniform [250, 2000], scheme
@@ -989,8 +1077,9 @@ def run_stream(args):
 
 def main():
     args = parse()
-    if args.workload in ("calib", "stream"):
-        print(json.dumps(run_calib(args) if args.workload == "calib" else run_stream(args)), flush=True)
+    if args.workload in ("calib", "calib_pk", "stream"):
+        fn = {"calib": run_calib, "calib_pk": run_calib_pk, "stream": run_stream}[args.workload]
+        print(json.dumps(fn(args)), flush=True)
         return
     if args.workload == "bam":
         print(json.dumps(run_bam(args)), flush=True)
@@ -1014,6 +1103,10 @@ def main():
             # per-call path and through the serving loop, on this GPU
             args.jobs = args.serving_jobs
             out["serving"] = run_calib(args)
+        if args.serving_jobs > 0:
+            # the same batch without the T-web, beside the on-device loop
+            args.jobs = args.serving_jobs
+            out["serving_pk"] = run_calib_pk(args)
         if args.stream_jobs > 0:
             # the mixed stream (2,000 jobs, N 64..512): saturation and a
             # Poisson arrival rate, served against the per-call path

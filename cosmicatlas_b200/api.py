@@ -564,6 +564,70 @@ class Server:
 
 
 @dataclass
+class DeviceLoop:
+    """The persistent on-device request loop (cam_devloop_*): one resident
+    kernel, one CTA of 1024 threads per SM, each running whole small jobs
+    (FP32 cubic meshes of N = 32, 64, 128; device particles; P(k); no
+    T-web) taken from a queue in mapped host memory.  submit() returns an
+    id; wait() returns the job's result as Context.job does."""
+
+    def __init__(self, device: int = 0, max_particles: int = 1 << 20, nslots: int = 4096,
+                 idle_timeout_s: float = 10.0):
+        self._lib = L.lib()
+        h = ctypes.c_void_p()
+        rc = self._lib.cam_devloop_create(device, int(max_particles), int(nslots), float(idle_timeout_s),
+                                          ctypes.byref(h))
+        if rc != L.CAM_OK:
+            raise CamError(rc, "cam_devloop_create")
+        self.h = h
+        self._jobs: dict[int, JobSpec] = {}
+
+    def _err(self, rc, what):
+        msg = self._lib.cam_devloop_last_error(self.h)
+        raise CamError(rc, f"{what}: {msg.decode() if msg else ''}")
+
+    def submit(self, job: "JobSpec") -> int:
+        jid = ctypes.c_uint64()
+        rc = self._lib.cam_devloop_submit(self.h, ctypes.byref(job.desc), ctypes.byref(jid))
+        if rc != L.CAM_OK:
+            self._err(rc, "cam_devloop_submit")
+        self._jobs[jid.value] = job
+        return jid.value
+
+    def wait(self, jid: int, timeout_s: float | None = None) -> dict:
+        job = self._jobs[jid]
+        us = -1 if timeout_s is None else int(timeout_s * 1e6)
+        rc = self._lib.cam_devloop_wait(self.h, jid, us, ctypes.byref(job.desc), ctypes.byref(job.res))
+        if rc != L.CAM_OK:
+            self._err(rc, "cam_devloop_wait")
+        del self._jobs[jid]
+        return job.result()
+
+    def state(self):
+        """(status, running): status CAM_E_TIMEOUT once the kernel has ended
+        on its idle limit."""
+        r = ctypes.c_int()
+        rc = self._lib.cam_devloop_state(self.h, ctypes.byref(r))
+        return rc, r.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._lib.cam_devloop_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class StagedParticles:
     parts: L.Particles
     keep: tuple

@@ -409,6 +409,42 @@ const char *cam_server_last_error(cam_server *s);
 /* Finishes the queued and running jobs, then stops the workers. */
 int cam_server_destroy(cam_server *s);
 
+/* ---- persistent on-device request loop -----------------------------------
+ * No single counterpart in the reference: BAM issues its mesh jobs one
+ * after another from the calibration loop (Source/Bam.cpp:13424,
+ * Bam::bamrunner; get_BAM_DM per iteration, :2102-2303).  Here one kernel
+ * stays resident, one CTA of 1024 threads per SM, and every CTA runs whole
+ * jobs -- assignment, r2c FFT, P(k) -- taking them from a queue in pinned
+ * host memory that the device reads directly, so no kernel is launched per
+ * job.  Jobs: FP32 cubic meshes of N = 32, 64 or 128, NGP/CIC/TSC, unit or
+ * per-particle weights, particles already on the device (CAM_MEM_DEVICE),
+ * density P(k) with at most 128 bins, no T-web (others: CAM_E_UNSUPPORTED).
+ * The mesh sum and the lost count equal cam_job_run's bit for bit (same
+ * assignment functions and fixed-point scale); P(k) agrees to FP64
+ * rounding; a job's results do not depend on the jobs beside it.
+ * Every device-side wait is bounded: with no job for idle_timeout_s the
+ * kernel ends (cam_devloop_state then returns CAM_E_TIMEOUT) and the next
+ * submission or wait relaunches it.  One host thread per loop. */
+typedef struct cam_devloop cam_devloop;
+/* Preallocates, per CTA, a record buffer of 4 * max_particles records and
+ * the mesh and spectrum of N = 128; launches the kernel.  nslots: queued
+ * jobs at most (submit waits, up to 30 s, for a slot). */
+int cam_devloop_create(int device, int64_t max_particles, int nslots, double idle_timeout_s, cam_devloop **out);
+/* Queues a job; the particle arrays must stay valid until it completes. */
+int cam_devloop_submit(cam_devloop *loop, const cam_job_desc *job, uint64_t *id);
+/* Waits up to timeout_us (< 0: no limit) for job `id` and fills res's P(k)
+ * (pk, modes, kvector, pk_info) and assignment statistics as cam_job_run
+ * does; `job` is the descriptor it was submitted with.  CAM_E_TIMEOUT if
+ * it has not completed, CAM_E_NOTFOUND for an unknown or overwritten id. */
+int cam_devloop_wait(cam_devloop *loop, uint64_t id, int64_t timeout_us, const cam_job_desc *job,
+                     cam_job_result *res);
+/* CAM_E_TIMEOUT if the kernel has ended on its idle limit, else CAM_OK;
+ * *running (may be NULL) = 1 while the kernel is resident. */
+int cam_devloop_state(cam_devloop *loop, int *running);
+/* Lets the queued jobs finish, ends the kernel and frees everything. */
+int cam_devloop_destroy(cam_devloop *loop);
+const char *cam_devloop_last_error(cam_devloop *loop);
+
 /* ---- power spectrum without device allocation --------------------------
  * No counterpart in the reference.  For callers that may not allocate
  * device memory -- code running inside a memory pool or arena it does not
