@@ -157,7 +157,8 @@ SIGNATURES = {
     "cam_server_last_error": ([_P], ctypes.c_char_p),
     "cam_server_trace": ([_P, ctypes.POINTER(JobTrace), ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "cam_server_destroy": ([_P], ctypes.c_int),
-    "cam_devloop_create": ([ctypes.c_int, ctypes.c_int64, ctypes.c_int, ctypes.c_double, ctypes.POINTER(_P)],
+    "cam_devloop_create": ([ctypes.c_int, ctypes.c_int64, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                            ctypes.POINTER(_P)],
                            ctypes.c_int),
     "cam_devloop_submit": ([_P, ctypes.POINTER(JobDesc), ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
     "cam_devloop_wait": ([_P, ctypes.c_uint64, ctypes.c_int64, ctypes.POINTER(JobDesc), ctypes.POINTER(JobResult)],

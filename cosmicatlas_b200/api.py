@@ -566,17 +566,18 @@ class Server:
 @dataclass
 class DeviceLoop:
     """The persistent on-device request loop (cam_devloop_*): one resident
-    kernel, one CTA of 1024 threads per SM, each running whole small jobs
+    kernel, one CTA of 1024 threads per SM (max_ctas: fewer, leaving SMs to
+    other work), each running whole small jobs
     (FP32 cubic meshes of N = 32, 64, 128; device particles; P(k); no
     T-web) taken from a queue in mapped host memory.  submit() returns an
     id; wait() returns the job's result as Context.job does."""
 
     def __init__(self, device: int = 0, max_particles: int = 1 << 20, nslots: int = 4096,
-                 idle_timeout_s: float = 10.0):
+                 idle_timeout_s: float = 10.0, max_ctas: int = 0):
         self._lib = L.lib()
         h = ctypes.c_void_p()
         rc = self._lib.cam_devloop_create(device, int(max_particles), int(nslots), float(idle_timeout_s),
-                                          ctypes.byref(h))
+                                          int(max_ctas), ctypes.byref(h))
         if rc != L.CAM_OK:
             raise CamError(rc, "cam_devloop_create")
         self.h = h

@@ -713,11 +713,12 @@ int dl_ensure_running(cam_devloop *l, bool force)
 
 extern "C" {
 
-int cam_devloop_create(int device, int64_t max_particles, int nslots, double idle_timeout_s, cam_devloop **out)
+int cam_devloop_create(int device, int64_t max_particles, int nslots, double idle_timeout_s, int max_ctas,
+                       cam_devloop **out)
 {
     if (!out) return CAM_E_INVAL;
     *out = nullptr;
-    if (max_particles < 1 || max_particles > (1ll << 26) || nslots < 1 || nslots > (1 << 16) ||
+    if (max_particles < 1 || max_particles > (1ll << 26) || nslots < 1 || nslots > (1 << 16) || max_ctas < 0 ||
         !(idle_timeout_s > 0.0) || !(idle_timeout_s <= 3600.0))
         return CAM_E_INVAL;
     auto *l = new (std::nothrow) cam_devloop;
@@ -751,6 +752,7 @@ int cam_devloop_create(int device, int64_t max_particles, int nslots, double idl
         return fail(CAM_E_CUDA);
     }
     l->ctas = sms * per_sm;
+    if (max_ctas > 0) l->ctas = std::min(l->ctas, max_ctas);
     if (cudaStreamCreateWithFlags(&l->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(CAM_E_CUDA);
     if (cudaHostAlloc(reinterpret_cast<void **>(&l->ctl), sizeof(DlControl), cudaHostAllocMapped) != cudaSuccess ||
         cudaHostAlloc(reinterpret_cast<void **>(&l->slots), sizeof(DlSlot) * (size_t)nslots, cudaHostAllocMapped) !=

@@ -428,8 +428,11 @@ int cam_server_destroy(cam_server *s);
 typedef struct cam_devloop cam_devloop;
 /* Preallocates, per CTA, a record buffer of 4 * max_particles records and
  * the mesh and spectrum of N = 128; launches the kernel.  nslots: queued
- * jobs at most (submit waits, up to 30 s, for a slot). */
-int cam_devloop_create(int device, int64_t max_particles, int nslots, double idle_timeout_s, cam_devloop **out);
+ * jobs at most (submit waits, up to 30 s, for a slot).  A CTA holds its
+ * SM's whole register file, so other kernels wait for SMs the loop does
+ * not use: max_ctas (0 = one per SM) leaves the rest free. */
+int cam_devloop_create(int device, int64_t max_particles, int nslots, double idle_timeout_s, int max_ctas,
+                       cam_devloop **out);
 /* Queues a job; the particle arrays must stay valid until it completes. */
 int cam_devloop_submit(cam_devloop *loop, const cam_job_desc *job, uint64_t *id);
 /* Waits up to timeout_us (< 0: no limit) for job `id` and fills res's P(k)

@@ -7,7 +7,8 @@ runs the same stages; P(k) is summed in another fixed FP64 order, so it
 agrees to FP64 rounding (1e-12 here), with identical mode counts.  A job's
 result does not depend on the jobs that ran beside it, and every
 device-side wait is bounded: with no job for the idle limit the kernel
-ends, and the next submission relaunches it.
+ends, and the next submission relaunches it.  The loops here use half the
+SMs, so the cam_job_run references run beside them.
 """
 import time
 
@@ -39,7 +40,8 @@ def _close(a, b):
 
 @pytest.fixture(scope="module")
 def loop():
-    lp = DeviceLoop(0, max_particles=1 << 20, nslots=1024, idle_timeout_s=20.0)
+    # half the SMs: the cam_job_run references run beside it
+    lp = DeviceLoop(0, max_particles=1 << 20, nslots=1024, idle_timeout_s=20.0, max_ctas=74)
     yield lp
     lp.close()
 
@@ -82,7 +84,7 @@ def test_devloop_job_alone_equals_in_mix(loop):
 
 def test_devloop_idle_limit_ends_the_kernel_and_a_submission_relaunches_it(ctx):
     import torch
-    lp = DeviceLoop(0, max_particles=1 << 18, nslots=16, idle_timeout_s=0.2)
+    lp = DeviceLoop(0, max_particles=1 << 18, nslots=16, idle_timeout_s=0.2, max_ctas=74)
     try:
         time.sleep(1.0)  # no job: every CTA's bounded wait runs out
         rc, running = lp.state()
