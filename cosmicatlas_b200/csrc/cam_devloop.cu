@@ -487,6 +487,7 @@ __device__ void dl_pk(const float2 *main, const float2 *nyq, int n, const double
         res->sn[bn] = s1;
         res->modes[bn] = cn;
     }
+    __threadfence_system();  // the host reads them once `done` is set
     __syncthreads();
 }
 
