@@ -173,7 +173,9 @@ void smem_limit(const void *func, size_t bytes)
 {
     static std::mutex m;
     static std::map<std::pair<int, const void *>, size_t> cur;
-    if (bytes <= 48 * 1024) return;  // within the default limit
+    // the default limit (48 KB) also covers a kernel's static shared memory:
+    // sizes near it are raised too
+    if (bytes <= 32 * 1024) return;
     int dev = 0;
     CAM_CUDA_TRY(cudaGetDevice(&dev));
     std::lock_guard<std::mutex> lk(m);

@@ -405,16 +405,17 @@ __device__ __forceinline__ void deposit_record(const uint4 v, const int e[3], co
 }
 
 // Pass 4: one CTA per brick, cell sums in 64-bit fixed point of quantum
-// 2^-s.  The scale follows the smallest nonzero |w| of the catalogue:
-// 2^-s <= min|w| 2^-21, so every contribution of the lightest particle is
-// rounded to within 2.4e-7 of its own weight, whatever the heaviest one
-// weighs.  It is capped so that no cell of the brick can overflow: a cell
-// takes at most one contribution (stencil weight <= 1) per record of its
-// brick, so max|w| 2^s * nrec < 2^62.  Unit weights use s = 21 (every
-// contribution < 2^22, the cheapest conversion); NGP counts convert by a
-// shift.  wstat[0] = bits of max |w|, wstat[1] != 0 if some
-// weight is negative, wstat[6] = 0x7fffffff - bits of min nonzero |w| (0:
-// no nonzero weight).
+// 2^-s.  The scale puts the heaviest weight just below 2^31 (one 32-bit
+// atomic per contribution) unless that leaves the lightest nonzero weight
+// fewer than 2^21 quanta; then the lightest sets it (2^-s <= min|w| 2^-21)
+// and heavy contributions take the 64-bit path.  Either way every
+// contribution of the lightest particle is rounded to within 2.4e-7 of its
+// own weight, whatever the heaviest weighs.  The scale is capped so that no
+// cell of the brick can overflow: a cell takes at most one contribution
+// (stencil weight <= 1) per record of its brick, so max|w| 2^s * nrec <
+// 2^62.  Unit weights use s = 30; NGP counts convert by a shift.
+// wstat[0] = bits of max |w|, wstat[1] != 0 if some weight is negative,
+// wstat[6] = 0x7fffffff - bits of min nonzero |w| (0: no nonzero weight).
 __device__ __forceinline__ int fixed_scale(const unsigned int *wstat, int weighted, uint32_t nrec)
 {
     float wmax = 1.0f, wmin = 1.0f;
@@ -427,7 +428,7 @@ __device__ __forceinline__ int fixed_scale(const unsigned int *wstat, int weight
     frexpf(wmax, &emax);
     frexpf(wmin, &emin);
     const int bits = 32 - __clz(nrec | 1u);  // nrec < 2^bits
-    return min(22 - emin, 62 - emax - bits);
+    return min(max(31 - emax, 22 - emin), 62 - emax - bits);
 }
 
 }  // namespace asg

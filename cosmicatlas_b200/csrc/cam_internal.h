@@ -40,7 +40,12 @@ struct Error {
     do {                                                                            \
         ::cam::prof_begin((ctx), (name));                                           \
         kernel<<<(grid), (block), (smem), (ctx)->stream>>>(__VA_ARGS__);            \
-        CAM_CUDA_TRY(cudaGetLastError());                                           \
+        {                                                                           \
+            const cudaError_t _le = cudaGetLastError();                             \
+            if (_le != cudaSuccess)                                                 \
+                throw ::cam::Error{CAM_E_CUDA, std::string("launch of ") + (name) + \
+                                                   ": " + cudaGetErrorString(_le)}; \
+        }                                                                           \
         ::cam::prof_end(ctx);                                                       \
         (ctx)->launches++;                                                          \
     } while (0)
