@@ -130,7 +130,8 @@ __device__ __forceinline__ int brick_linear(const AssignGeom &g, int b0, int b1,
 template <int SCHEME, bool SMEM>
 __device__ __forceinline__ void count_one(float px, float py, float pz, float wt, bool weighted, const AssignGeom &g,
                                           uint32_t *hist, uint32_t *__restrict__ table, unsigned long long &my_lost,
-                                          unsigned int &my_wmax, unsigned int &my_neg, unsigned int &my_wminc)
+                                          unsigned int &my_wmax, unsigned int &my_neg, unsigned int &my_wminc,
+                                          const AssignGeom *g1 = nullptr, uint32_t *sbh = nullptr)
 {
     using St = Stencil<SCHEME>;
     const float pos[3] = {px, py, pz};
@@ -139,6 +140,13 @@ __device__ __forceinline__ void count_one(float px, float py, float pz, float wt
         ++my_lost;
         return;
     }
+    // two-level scatter: one count per particle for the super-brick of its
+    // home cell (g1's bricks are the super-bricks)
+    if (g1)
+        atomicAdd(sbh + brick_linear(*g1, brick_of(c[0], g1->b[0], g1->bmagic[0]),
+                                     brick_of(c[1], g1->b[1], g1->bmagic[1]),
+                                     brick_of(c[2], g1->b[2], g1->bmagic[2])),
+                  1u);
     if (weighted) {
         my_wmax = max(my_wmax, __float_as_uint(fabsf(wt)));
         my_neg |= wt < 0.0f;

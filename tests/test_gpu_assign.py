@@ -250,11 +250,12 @@ def _context_with(env):
 
 
 @pytest.mark.parametrize("scheme", SCHEMES)
-@pytest.mark.parametrize("n", [64, 128, 256])
+@pytest.mark.parametrize("n", [64, 128, 256, 384, 512])
 def test_staged_scatter_equals_direct_appends(ctx, scheme, n):
     # the staged scatter (records ranked per brick in shared memory, one
-    # range per brick and flush) fills the same bricks as one append per
-    # record: the integer cell sums, hence the meshes, are bit-identical
+    # range per brick and flush; at 384^3 and 512^3 the two-level form,
+    # particles by super-brick first) fills the same bricks as one append
+    # per record: the integer cell sums, hence the meshes, are bit-identical
     box = 1000.0
     x, y, z = synth.clumped(1_500_000, box, 15_000, 2.0, 0.8, seed=n + 10 * scheme)
     w = synth.halo_masses(x.size, seed=n)
@@ -267,3 +268,15 @@ def test_staged_scatter_equals_direct_appends(ctx, scheme, n):
         assert a.sum_mesh == b.sum_mesh and a.n_in == b.n_in
     finally:
         c2.close()
+
+
+@pytest.mark.parametrize("scheme", [CIC, TSC])
+def test_two_level_scatter_mesh_vs_oracle(ctx, scheme):
+    # 384^3 has more bricks than one stage holds: the two-level scatter
+    n, box = 384, 1000.0
+    x, y, z = synth.clumped(3_000_000, box, 30_000, 2.0, 0.8, seed=77 + scheme)
+    w = synth.halo_masses(x.size, seed=78)
+    got = ctx.assign(x, y, z, w, make_grid(n, box), scheme, F32)
+    ref, lost = orc.assign_f64_mt(scheme, x, y, z, w, orc.Grid.cubic(n, box))
+    assert got.n_lost == lost
+    assert rel_err_cells(got.mesh, ref, float(np.mean(w, dtype=np.float64))) <= 1e-5
