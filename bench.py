@@ -417,11 +417,12 @@ def run_ours(args):
             "power": 8 * nh,
         }
         stage_kernels = {
-            "assign": ["assign_bin_count", "assign_starts", "tile_sum_kernel", "tile_offsets_kernel",
+            "assign": ["assign_bin_count", "assign_starts", "assign_partition", "tile_sum_kernel", "tile_offsets_kernel",
                        "tile_scan_kernel", "assign_bin_scatter", "assign_deposit", "partial_sum_kernel<double>",
                        "final_sum_kernel"],
-            "fft_r2c": ["fft_rows_r2c", "fft_cols", "fft_rows_c2c"],
-            "power": ["pk_bin", "pk_final_kernel"],
+            # fft_cols_pk: the x pass that also bins P(k) (the binning adds no traffic)
+            "fft_r2c": ["fft_rows_r2c", "fft_cols", "fft_rows_c2c", "fft_cols_pk"],
+            "power": ["pk_bin", "pk_final_kernel", "pk_nyq", "pk_final"],
         }
         stages = {}
         for st, names in stage_kernels.items():
@@ -650,11 +651,11 @@ def run_single(args):
     stage_bytes = {"assign": npart * 12 + 4 * n ** 3, "fft_r2c": 4 * n ** 3 + 8 * nh, "power": 8 * nh,
                    "tweb": 8 * nh + n ** 3}
     stage_kernels = {
-        "assign": ["assign_bin_count", "assign_scan", "assign_bin_scatter", "assign_deposit",
+        "assign": ["assign_bin_count", "assign_scan", "assign_partition", "assign_bin_scatter", "assign_deposit",
                    "partial_sum_kernel<double>", "final_sum_kernel", "assign_starts", "tile_sum_kernel",
                    "tile_offsets_kernel", "tile_scan_kernel"],
-        "fft_r2c": ["fft_rows_r2c", "fft_cols", "fft_rows_c2c"],
-        "power": ["pk_bin", "pk_final_kernel"],
+        "fft_r2c": ["fft_rows_r2c", "fft_cols", "fft_rows_c2c", "fft_cols_pk"],
+        "power": ["pk_bin", "pk_final_kernel", "pk_nyq", "pk_final"],
         "tweb": ["tweb_tidal_x", "tweb_tidal_x_nyq", "tweb_tidal_y", "tweb_tidal_y_nyq", "tweb_tidal_z_eigen",
                  "fd_table_kernel"],
     }
