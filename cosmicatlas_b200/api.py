@@ -563,7 +563,6 @@ class Server:
             pass
 
 
-@dataclass
 class DeviceLoop:
     """The persistent on-device request loop (cam_devloop_*): one resident
     kernel, one CTA of 1024 threads per SM (max_ctas: fewer, leaving SMs to
@@ -629,6 +628,7 @@ class DeviceLoop:
             pass
 
 
+@dataclass
 class StagedParticles:
     parts: L.Particles
     keep: tuple
