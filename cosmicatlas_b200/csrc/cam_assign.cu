@@ -136,6 +136,30 @@ bin_kernel(const float *__restrict__ x, const float *__restrict__ y, const float
     }
 }
 
+// Warp-aggregated reservations in shared memory (every lane of the warp
+// calls them): the lanes' n add to *counter with one atomic per warp.
+// warp_reserve returns the lane's first slot; warp_add returns nothing.
+__device__ __forceinline__ uint32_t warp_reserve(uint32_t *counter, uint32_t n)
+{
+    const int lane = threadIdx.x & 31;
+    uint32_t incl = n;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    uint32_t base = 0;
+    if (lane == 31 && incl) base = atomicAdd(counter, incl);
+    base = __shfl_sync(0xffffffffu, base, 31);
+    return base + incl - n;
+}
+__device__ __forceinline__ void warp_add(uint32_t *counter, uint32_t n)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) n += __shfl_down_sync(0xffffffffu, n, o);
+    if ((threadIdx.x & 31) == 0 && n) atomicAdd(counter, n);
+}
+
 // Pass 3, staged form (nb <= kStageBricks).  Each CTA stages the records of
 // a contiguous particle chunk in shared memory and writes them out in
 // flushes: a flush ranks its records by brick (shared-memory counts), takes
@@ -259,14 +283,14 @@ scatter_staged_kernel(const float *__restrict__ x, const float *__restrict__ y, 
             }
         }
         // room for this round's records, else flush first
-        if (nrec) atomicAdd(&s_need, (uint32_t)nrec);
+        warp_add(&s_need, (uint32_t)nrec);
         __syncthreads();
         const bool full = s_fill + s_need > (uint32_t)kStageCap;
         __syncthreads();
         if (full) flush();
         if (tid == 0) s_need = 0u;
+        uint32_t dst = warp_reserve(&s_fill, (uint32_t)nrec);
         if (nrec) {
-            uint32_t dst = atomicAdd(&s_fill, (uint32_t)nrec);
 #pragma unroll
             for (int i0 = 0; i0 < 2; ++i0) {
                 if (i0 >= nbx[0]) break;
@@ -414,21 +438,26 @@ partition_kernel(const float *__restrict__ x, const float *__restrict__ y, const
             __syncthreads();
         }
         const int64_t p = base + tid;
+        float px = 0.f, py = 0.f, pz = 0.f, pw = 1.0f;
+        int c[3] = {0, 0, 0};
+        bool ok = false;
         if (p < p1) {
-            const float px = __ldcs(x + p), py = __ldcs(y + p), pz = __ldcs(z + p);
-            const float pw = weighted ? __ldcs(w + p) : 1.0f;
+            px = __ldcs(x + p);
+            py = __ldcs(y + p);
+            pz = __ldcs(z + p);
+            if (weighted) pw = __ldcs(w + p);
             const float pos[3] = {px, py, pz};
-            int c[3];
-            if (home_cell<SCHEME>(pos, g, c)) {
-                const int key = brick_linear(g1, brick_of(c[0], g1.b[0], g1.bmagic[0]),
-                                             brick_of(c[1], g1.b[1], g1.bmagic[1]),
-                                             brick_of(c[2], g1.b[2], g1.bmagic[2]));
-                const uint32_t rank = atomicAdd(cnt + key, 1u);
-                const uint32_t dst = atomicAdd(&s_fill, 1u);
-                srec[dst] = make_uint4(__float_as_uint(px), __float_as_uint(py), __float_as_uint(pz),
-                                       __float_as_uint(pw));
-                skey[dst] = ((uint32_t)key << kStageRankBits) | rank;
-            }
+            ok = home_cell<SCHEME>(pos, g, c);
+        }
+        const uint32_t dst = warp_reserve(&s_fill, ok ? 1u : 0u);
+        if (ok) {
+            const int key = brick_linear(g1, brick_of(c[0], g1.b[0], g1.bmagic[0]),
+                                         brick_of(c[1], g1.b[1], g1.bmagic[1]),
+                                         brick_of(c[2], g1.b[2], g1.bmagic[2]));
+            const uint32_t rank = atomicAdd(cnt + key, 1u);
+            srec[dst] = make_uint4(__float_as_uint(px), __float_as_uint(py), __float_as_uint(pz),
+                                   __float_as_uint(pw));
+            skey[dst] = ((uint32_t)key << kStageRankBits) | rank;
         }
         __syncthreads();
     }
@@ -542,7 +571,7 @@ refine_kernel(const uint4 *__restrict__ raw, const uint32_t *__restrict__ sb_sta
                     }
                 }
             }
-            if (nrec) atomicAdd(&s_need, (uint32_t)nrec);
+            warp_add(&s_need, (uint32_t)nrec);
             __syncthreads();
             const bool full = s_fill + s_need > (uint32_t)kL2Cap;
             __syncthreads();
@@ -552,8 +581,8 @@ refine_kernel(const uint4 *__restrict__ raw, const uint32_t *__restrict__ sb_sta
                 __syncthreads();
             }
             if (tid == 0) s_need = 0u;
+            uint32_t dst = warp_reserve(&s_fill, (uint32_t)nrec);
             if (nrec) {
-                uint32_t dst = atomicAdd(&s_fill, (uint32_t)nrec);
 #pragma unroll
                 for (int i0 = 0; i0 < 2; ++i0) {
                     if (i0 >= nbx[0]) break;

@@ -179,9 +179,9 @@ fft_cols_tma_kernel(const __grid_constant__ CUtensorMap map, TileDims td, int nc
     constexpr int NBOX = (LEN + 255) / 256;  // boxes of BOXR rows (LEN is a multiple of NBOX)
     constexpr int BOXR = LEN / NBOX;
     constexpr unsigned TILE_BYTES = (unsigned)(LEN * W * sizeof(C));
-    extern __shared__ __align__(128) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_tma[];
     __shared__ uint64_t bar[2];
-    C *const buf0 = reinterpret_cast<C *>(smem_raw);
+    C *const buf0 = reinterpret_cast<C *>(smem_tma);
     const bool leader = threadIdx.x == 0;
     auto coords = [&](int64_t t, int &x, int &plane, int &comp) {
         const int64_t ct = t % nct, r = t / nct;
@@ -257,8 +257,8 @@ fft_cols_tma_kernel(const __grid_constant__ CUtensorMap map, TileDims td, int nc
 // store (if any) reads the tile -- the block bins the tile's modes.  Tile:
 // 16 consecutive k (c0 .. c0 + 15) of all rows i, plane j.  A warp takes two
 // rows at a time (16 lanes each); along a row the bin is non-decreasing in
-// c, so runs of equal bins are contiguous lanes, reduced by a fixed shuffle
-// tree and added by their head lane into the warp's own FP64 bins, the
+// c, so runs of equal bins are contiguous lanes (bins from the table of
+// every |k|^2), reduced by a fixed shuffle tree and added by their head lane into the warp's own FP64 bins, the
 // first row's heads before the second's.  Warps and tiles are combined in a
 // fixed order: part[cta][bin] = this CTA's sum of |F|^2 / W^2.  Mode counts
 // and shot-noise sums do not depend on the data; the host takes them from a
@@ -287,7 +287,8 @@ __global__ void __launch_bounds__(pk_pass_threads<LEN>(), pk_pass_min_blocks<LEN
 fft_cols_tma_pk_kernel(const __grid_constant__ CUtensorMap map, TileDims td, int nct, int nplanes, int64_t ntiles,
                        const float2 *__restrict__ tw, unsigned *__restrict__ err,
                        const double *__restrict__ g_tab /* [h+1] 1/W^2, [h+1] C/W^2, [nbins+1] E2 */, int nbins,
-                       float m_u, float inv_s, int store, double *__restrict__ part /* [grid][nbins] */)
+                       const short *__restrict__ btab /* bin of q = |k|^2 / k_f^2 */, int store,
+                       double *__restrict__ part /* [grid][nbins] */)
 {
     using C = float2;
     constexpr int W = 16;
@@ -297,14 +298,12 @@ fft_cols_tma_pk_kernel(const __grid_constant__ CUtensorMap map, TileDims td, int
     constexpr int BOXR = LEN / NBOX;
     constexpr unsigned TILE_BYTES = (unsigned)(LEN * W * sizeof(C));
     constexpr int N = LEN, H = LEN / 2;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_tma[];
     __shared__ uint64_t bar[2];
-    C *const buf0 = reinterpret_cast<C *>(smem_raw);
-    double *const tw2 = reinterpret_cast<double *>(smem_raw + 2 * (size_t)TILE_BYTES);  // [H + 1]
-    double *const E2 = tw2 + (H + 1);                                                   // [nbins + 1]
-    double *const wsum = E2 + (nbins + 1);                                              // [NWARP][nbins]
+    C *const buf0 = reinterpret_cast<C *>(smem_tma);
+    double *const tw2 = reinterpret_cast<double *>(smem_tma + 2 * (size_t)TILE_BYTES);  // [H + 1]
+    double *const wsum = tw2 + (H + 1);                                                 // [NWARP][nbins]
     for (int t = threadIdx.x; t <= H; t += NTHR) tw2[t] = g_tab[t];
-    for (int t = threadIdx.x; t <= nbins; t += NTHR) E2[t] = g_tab[2 * (H + 1) + t];
     for (int t = threadIdx.x; t < NWARP * nbins; t += NTHR) wsum[t] = 0.0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double *const mysum = wsum + (size_t)warp * nbins;
@@ -378,8 +377,7 @@ fft_cols_tma_pk_kernel(const __grid_constant__ CUtensorMap map, TileDims td, int
             for (int pr = warp; pr < LEN / 2; pr += NWARP) {
                 const int i = 2 * pr + (lane >> 4);
                 const int a = i <= H ? i : N - i;
-                const double q = (double)(a * a + qb + c * c);
-                const int bin = pk_bin(q, E2, nbins, m_u, inv_s);
+                const int bin = __ldg(btab + (a * a + qb + c * c));
                 double v = 0.0;
                 if (bin >= 0 && bin < nbins && pk_visited(i, j, c, N)) {
                     const C f = here[i * W + kk];
@@ -803,8 +801,7 @@ bool fft_r2c_pk_fused(cam_ctx *ctx, FftPlan *plan, const void *real_in, const do
         constexpr int LEN = decltype(lc)::value;
         if constexpr (LEN >= 32 && 2 * LEN * 16 * 8 <= 200 * 1024) {
             constexpr int NTHR = pk_pass_threads<LEN>();
-            const size_t smem = (size_t)2 * LEN * 16 * 8 +
-                                (size_t)(LEN / 2 + 1 + pt.nbins + 1 + (NTHR / 32) * pt.nbins) * sizeof(double);
+            const size_t smem = (size_t)2 * LEN * 16 * 8 + (size_t)(LEN / 2 + 1 + (NTHR / 32) * pt.nbins) * sizeof(double);
             if (smem > 220 * 1024) return;
             // x pass over main: 4D view (scalar column, row i, plane j, 1)
             CUtensorMap map;
@@ -830,8 +827,8 @@ bool fft_r2c_pk_fused(cam_ctx *ctx, FftPlan *plan, const void *real_in, const do
             cols_impl<float>(ctx, plan, out.main, n, M, M, n, n * M, 1, 0, false);
             rows_impl<float, 2>(ctx, plan, out.nyq, out.nyq, nullptr, n, 1, 0, 0, nullptr, 1.0);
             CAM_LAUNCH_NAMED(ctx, "fft_cols_pk", kt, g, NTHR, smem, map, td, (int)(M / 16), (int)n, ntiles,
-                             static_cast<const float2 *>(plan->tw), device_error_word(ctx), pt.tab, pt.nbins, pt.m_u,
-                             pt.inv_s, keep ? 1 : 0, part);
+                             static_cast<const float2 *>(plan->tw), device_error_word(ctx), pt.tab, pt.nbins, pt.btab,
+                             keep ? 1 : 0, part);
             cols_impl<float>(ctx, plan, out.nyq, n, n, n, 1, 0, 1, 0, false);
             *d_part = part;
             *nparts = g;

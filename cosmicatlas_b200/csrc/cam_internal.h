@@ -234,6 +234,10 @@ struct PkTables {
     const double *tab;
     int nbins;
     float m_u, inv_s;
+    // bin of every integer |k|^2 / k_f^2 = q in [0, qmax] (pk_bin's result:
+    // -1 below the first edge, nbins at or above the last), int16
+    const short *btab;
+    int qmax;
 };
 PkTables pk_tables(cam_ctx *ctx, int64_t n, const cam_pk_opts &o, int nbins);
 // Forward r2c of a real N^3 mesh (FP32) whose last column pass also bins

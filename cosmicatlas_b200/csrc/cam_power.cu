@@ -369,6 +369,17 @@ PkDevice power_bin_impl(cam_ctx *ctx, const Spectrum &s, const Spectrum *s2, con
 
 }  // namespace
 
+namespace {
+// The bin of every q in [0, qmax] by pk_bin itself, so a table lookup gives
+// exactly what pk_bin gives.
+__global__ void pk_bintab_kernel(const double *__restrict__ E2, int nbins, float m_u, float inv_s, int qmax,
+                                 short *__restrict__ out)
+{
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q <= qmax; q += gridDim.x * blockDim.x)
+        out[q] = (short)pk_bin((double)q, E2, nbins, m_u, inv_s);
+}
+}  // namespace
+
 PkTables pk_tables(cam_ctx *ctx, int64_t n_, const cam_pk_opts &o, int nbins)
 {
     const int n = (int)n_;
@@ -403,8 +414,19 @@ PkTables pk_tables(cam_ctx *ctx, int64_t n_, const cam_pk_opts &o, int nbins)
     const bool fresh = found == ctx->bufs.end() || found->second.ptr == nullptr;
     auto *d_tab = static_cast<double *>(scratch(ctx, key, tab_bytes));
     if (fresh) CAM_CUDA_TRY(cudaMemcpyAsync(d_tab, tab.data(), tab_bytes, cudaMemcpyHostToDevice, ctx->stream));
-
-    return PkTables{d_tab, nbins, (float)o.DeltaKmin, (float)(1.0 / o.ndel)};
+    PkTables pt{d_tab, nbins, (float)o.DeltaKmin, (float)(1.0 / o.ndel), nullptr, 3 * h * h};
+    // the bin table depends on N and the edges only
+    CAM_REQUIRE(nbins < 32767, CAM_E_UNSUPPORTED, "too many bins");
+    char bkey[160];
+    snprintf(bkey, sizeof(bkey), "pk.btab.%d.%d.%.17g.%.17g", n, nbins, o.DeltaKmin, o.ndel);
+    const auto bf = ctx->bufs.find(bkey);
+    const bool bfresh = bf == ctx->bufs.end() || bf->second.ptr == nullptr;
+    auto *d_bt = static_cast<short *>(scratch(ctx, bkey, (size_t)(pt.qmax + 1) * sizeof(short)));
+    if (bfresh)
+        CAM_LAUNCH_NAMED(ctx, "pk_bintab", pk_bintab_kernel, (unsigned)std::min(1024, pt.qmax / 256 + 1), 256, 0,
+                         d_tab + 2 * (h + 1), nbins, pt.m_u, pt.inv_s, pt.qmax, d_bt);
+    pt.btab = d_bt;
+    return pt;
 }
 
 namespace {
@@ -415,8 +437,8 @@ namespace {
 // column pass writes it.
 constexpr int kNyqThreads = 256;
 __global__ void __launch_bounds__(kNyqThreads)
-pk_nyq_kernel(const float2 *__restrict__ nyq, int n, const double *__restrict__ g_tab, int nbins, float m_u,
-              float inv_s, double *__restrict__ part)
+pk_nyq_kernel(const float2 *__restrict__ nyq, int n, const double *__restrict__ g_tab, int nbins,
+              const short *__restrict__ btab, double *__restrict__ part)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int h = n / 2;
@@ -440,8 +462,7 @@ pk_nyq_kernel(const float2 *__restrict__ nyq, int n, const double *__restrict__ 
         if (r < r1) {
             const int i = (int)(r / n), j = (int)(r - (int64_t)i * n);
             const int a = i <= h ? i : n - i, b = j <= h ? j : n - j;
-            const double q = (double)((int64_t)a * a + (int64_t)b * b + (int64_t)h * h);
-            bin = pk_bin(q, E2, nbins, m_u, inv_s);
+            bin = btab[a * a + b * b + h * h];
             if (bin >= 0 && bin < nbins && pk_visited(i, j, h, n)) {
                 const float2 f = nyq[r];
                 v = ((double)f.x * (double)f.x + (double)f.y * (double)f.y) * (tw2[a] * tw2[b] * tw2[h]);
@@ -515,7 +536,7 @@ PkDevice power_finish_fused(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &
     double *all = part;  // [nparts + kNumSMs][nbins]: the Nyquist rows follow the column pass's
     smem_at_least(pk_nyq_kernel, smem);
     CAM_LAUNCH_NAMED(ctx, "pk_nyq", pk_nyq_kernel, g2, kNyqThreads, smem, static_cast<const float2 *>(s.nyq), n,
-                     pt.tab, nbins, pt.m_u, pt.inv_s, all + (size_t)nparts * nbins);
+                     pt.tab, nbins, pt.btab, all + (size_t)nparts * nbins);
     auto *res = static_cast<double *>(scratch(ctx, "pkf.res", (size_t)nbins * 2 * sizeof(double)));
     auto *resm = static_cast<unsigned long long *>(scratch(ctx, "pkf.resm", (size_t)nbins * sizeof(unsigned long long)));
     CAM_LAUNCH_NAMED(ctx, "pk_final", pk_final_fused_kernel, nbins, 256, 0, all, nparts + g2, nbins, stat.sums,
