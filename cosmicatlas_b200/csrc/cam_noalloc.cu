@@ -294,6 +294,18 @@ extern "C" int cam_power_noalloc(const void *spec, int64_t n, int precision, flo
         cudaGetLastError();
         return na_fail(CAM_E_CUDA, "no current CUDA device");
     }
+    // The host-to-device table copy and the final synchronisation cannot be
+    // captured: refuse a capturing stream before touching it, so the
+    // caller's capture stays valid.
+    {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(static_cast<cudaStream_t>(stream), &cs) != cudaSuccess) {
+            cudaGetLastError();
+            return na_fail(CAM_E_CUDA, "cannot query the stream's capture state");
+        }
+        if (cs != cudaStreamCaptureStatusNone)
+            return na_fail(CAM_E_UNSUPPORTED, "the stream is being captured; call outside a capture");
+    }
     void *base = nullptr;
     if (int rc = na_scratch(dev, &base)) return rc;
     double *tab = static_cast<double *>(base);

@@ -459,7 +459,9 @@ const char *cam_devloop_last_error(cam_devloop *loop);
  *   n_obj   sum of the density mesh (CAM_INPUT_DENSITY); ignored for delta
  *   pk, modes  host arrays of nbins (modes may be NULL)
  *   stream  cudaStream_t to run on (NULL = the legacy default stream);
- *           the call returns after that stream has finished its work.
+ *           the call returns after that stream has finished its work.  It
+ *           may not be under stream capture: a capturing stream returns
+ *           CAM_E_UNSUPPORTED and the capture is left untouched.
  * Results equal cam_power's binning of the same spectrum.  Limits: N <= 2048
  * and nbins <= 512; larger inputs return CAM_E_UNSUPPORTED.  The first call
  * on a device looks up the scratch array's device address.  All calls share

@@ -105,3 +105,25 @@ def test_noalloc_rejects_oversize(ctx):
     rc = L.lib().cam_power_noalloc(ctypes.c_void_p(spec.data_ptr()), 4096, L.F32, 100.0, 1.0,
                                    ctypes.byref(opts), pk.ctypes.data, None, None)
     assert rc == L.CAM_E_UNSUPPORTED
+
+
+def test_noalloc_refuses_a_capturing_stream(ctx):
+    """The call copies tables from the host and synchronises its stream, which
+    a CUDA graph cannot record: under capture it must return
+    CAM_E_UNSUPPORTED before touching the stream, and the capture must still
+    end cleanly."""
+    import torch
+    opts = Context.pk_opts(CIC, nbins=8)
+    spec = torch.zeros((16, 16, 9), dtype=torch.complex64, device="cuda")
+    pk = np.empty(8)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        stream = torch.cuda.current_stream().cuda_stream
+        rc = L.lib().cam_power_noalloc(ctypes.c_void_p(spec.data_ptr()), 16, L.F32, 100.0, 1.0,
+                                       ctypes.byref(opts), pk.ctypes.data, None, ctypes.c_void_p(stream))
+        out = spec.real * 2.0
+    assert rc == L.CAM_E_UNSUPPORTED
+    g.replay()
+    torch.cuda.synchronize()
+    assert float(out.abs().sum()) == 0.0
