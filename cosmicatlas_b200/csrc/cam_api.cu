@@ -483,7 +483,6 @@ int cam_ctx_create(int device, size_t hbm_budget, cam_ctx **out)
     }
     c->stream = c->own_stream;
     c->no_tma = std::getenv("CAM_NO_TMA") != nullptr;
-    c->no_stage = std::getenv("CAM_NO_STAGE") != nullptr;
     *out = c;
     return CAM_OK;
 }

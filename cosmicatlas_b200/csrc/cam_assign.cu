@@ -7,14 +7,15 @@
 //   1. bin_count   : each CTA takes a contiguous chunk of particles and
 //                    computes, per particle, the reference's FP32 home cell
 //                    (bit-exact key) and the mesh bricks its stencil
-//                    touches; a shared-memory histogram per CTA gives the
-//                    table count[brick][cta].  Also lost particles, max |w|.
-//   2. scan        : exclusive scan of the table in brick-major order, so
-//                    every (brick, cta) pair owns a contiguous payload range.
-//   3. bin_scatter : the same CTAs re-read their chunks and write one
-//                    16-byte payload per touched brick at their own cursors
-//                    (shared-memory atomics only): home cell relative to the
-//                    brick, exact fractional offset in fixed point, weight.
+//                    touches; a shared-memory histogram per CTA is added to
+//                    per-brick counters.  Also lost particles, max |w|.
+//   2. scan        : exclusive scan of the brick counts: every brick owns a
+//                    contiguous payload range, its counter becomes its
+//                    append cursor.
+//   3. bin_scatter : the particles again; one 16-byte payload per touched
+//                    brick (home cell relative to the brick, exact
+//                    fractional offset in fixed point, weight) at the next
+//                    slot of the brick's cursor (one global atomic each).
 //   4. deposit     : one CTA per brick accumulates its payloads into a
 //                    shared-memory tile of 64-bit fixed-point cell sums kept
 //                    as two 32-bit words (32-bit shared atomics, the carry
@@ -26,6 +27,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 
 #include "cam_assign_device.cuh"
 #include "cam_internal.h"
@@ -40,54 +42,16 @@ constexpr int kSmemBricks = 16384;  // per-CTA brick histogram in shared memory 
 using namespace asg;
 
 
-// Passes 1 and 3.  Block `blk` handles particles [blk * chunk, (blk+1) * chunk)
-// (chunk a multiple of 4).
-//   COUNT   : table[brick * kCursorStride] += number of payloads for the
-//             brick (through a per-CTA shared-memory histogram when SMEM,
-//             nb <= kSmemBricks), plus lost particles and max |w|.
-//   SCATTER : table[brick * kCursorStride] is the brick's append cursor (the
-//             exclusive scan of the counts); every payload takes the next
-//             slot of its brick with one global atomic, and its words are
-//             packed while the atomic is in flight.  A brick's records are appended
-//             contiguously by all CTAs, so its few open 128-byte lines fill
-//             in L2 and are written back whole.  The order of records inside
-//             a brick varies from run to run; the deposit's integer sums do
-//             not depend on it.
-// VEC: 16-byte aligned arrays, four particles per thread per iteration
-// (float4 loads).
-template <int SCHEME, bool SCATTER, bool SMEM, bool VEC>
-__global__ void __launch_bounds__(kBinThreads)
-bin_kernel(const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z,
-           const float *__restrict__ w, int64_t np, int64_t chunk, AssignGeom g, int nb,
-           uint32_t *__restrict__ table, uint4 *__restrict__ payload, unsigned long long *__restrict__ lost,
-           unsigned int *__restrict__ wmax_bits, uint64_t cap, unsigned int *__restrict__ ovf,
-           AssignGeom g1, int nsb, uint32_t *__restrict__ sb_table)
+// Calls one(x, y, z, w) for the particles [p0, p1), the threads of the CTA
+// taking consecutive particles; with VEC (16-byte aligned arrays, p0 a
+// multiple of 4) four per thread per iteration from float4 loads.  Unit
+// weights when w is null.
+template <bool VEC, typename F>
+__device__ __forceinline__ void for_chunk(const float *__restrict__ x, const float *__restrict__ y,
+                                          const float *__restrict__ z, const float *__restrict__ w, int64_t p0,
+                                          int64_t p1, F &one)
 {
-    extern __shared__ uint32_t hist[];
-    constexpr bool kHist = SMEM && !SCATTER;
-    const int G = gridDim.x, blk = blockIdx.x;
-    const int lane = threadIdx.x & 31;
-    // count pass of the two-level scatter (nsb > 0): also one count per
-    // particle for its super-brick, in hist[nb, nb + nsb)
-    // (always in shared memory, after the brick histogram if that is too)
-    const bool coarse = !SCATTER && nsb > 0;
-    uint32_t *sbh = hist + (kHist ? nb : 0);
-    if (kHist || coarse) {
-        for (int i = threadIdx.x; i < (kHist ? nb : 0) + (coarse ? nsb : 0); i += blockDim.x) hist[i] = 0u;
-        __syncthreads();
-    }
-    unsigned long long my_lost = 0;
-    unsigned int my_wmax = 0, my_neg = 0, my_wminc = 0;
     const bool weighted = w != nullptr;
-    auto one = [&](float px, float py, float pz, float wt) {
-        if (SCATTER)
-            bin_one<SCHEME, true, false>(px, py, pz, wt, weighted, g, G, blk, hist, table, payload, cap, ovf,
-                                         my_lost, my_wmax, my_neg);
-        else
-            count_one<SCHEME, kHist>(px, py, pz, wt, weighted, g, hist, table, my_lost, my_wmax, my_neg,
-                                     my_wminc, coarse ? &g1 : nullptr, sbh);
-    };
-    const int64_t p0 = (int64_t)blk * chunk, p1 = min(np, p0 + chunk);
     int64_t ptail = p0;
     if (VEC) {
         const int64_t q1 = p0 + ((p1 - p0) & ~(int64_t)3);
@@ -111,6 +75,51 @@ bin_kernel(const float *__restrict__ x, const float *__restrict__ y, const float
     }
     for (int64_t p = ptail + threadIdx.x; p < p1; p += blockDim.x)
         one(__ldcs(x + p), __ldcs(y + p), __ldcs(z + p), weighted ? __ldcs(w + p) : 1.0f);
+}
+
+
+// Passes 1 and 3.  Block `blk` handles particles [blk * chunk, (blk+1) * chunk)
+// (chunk a multiple of 4).
+//   COUNT   : table[brick * kCursorStride] += number of payloads for the
+//             brick (through a per-CTA shared-memory histogram when SMEM,
+//             nb <= kSmemBricks), plus lost particles and max |w|.
+//   SCATTER : table[brick * kCursorStride] is the brick's append cursor (the
+//             exclusive scan of the counts); every payload takes the next
+//             slot of its brick with one global atomic, and its words are
+//             packed while the atomic is in flight.  A brick's records are appended
+//             contiguously by all CTAs, so its few open 128-byte lines fill
+//             in L2 and are written back whole.  The order of records inside
+//             a brick varies from run to run; the deposit's integer sums do
+//             not depend on it.
+// VEC: 16-byte aligned arrays, four particles per thread per iteration
+// (float4 loads).
+template <int SCHEME, bool SCATTER, bool SMEM, bool VEC>
+__global__ void __launch_bounds__(kBinThreads)
+bin_kernel(const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z,
+           const float *__restrict__ w, int64_t np, int64_t chunk, AssignGeom g, int nb,
+           uint32_t *__restrict__ table, uint4 *__restrict__ payload, unsigned long long *__restrict__ lost,
+           unsigned int *__restrict__ wmax_bits, uint64_t cap, unsigned int *__restrict__ ovf)
+{
+    extern __shared__ uint32_t hist[];
+    constexpr bool kHist = SMEM && !SCATTER;
+    const int G = gridDim.x, blk = blockIdx.x;
+    const int lane = threadIdx.x & 31;
+    if (kHist) {
+        for (int i = threadIdx.x; i < nb; i += blockDim.x) hist[i] = 0u;
+        __syncthreads();
+    }
+    unsigned long long my_lost = 0;
+    unsigned int my_wmax = 0, my_neg = 0, my_wminc = 0;
+    const bool weighted = w != nullptr;
+    auto one = [&](float px, float py, float pz, float wt) {
+        if (SCATTER)
+            bin_one<SCHEME, true, false>(px, py, pz, wt, weighted, g, G, blk, hist, table, payload, cap, ovf,
+                                         my_lost, my_wmax, my_neg);
+        else
+            count_one<SCHEME, kHist>(px, py, pz, wt, weighted, g, hist, table, my_lost, my_wmax, my_neg,
+                                     my_wminc);
+    };
+    for_chunk<VEC>(x, y, z, w, (int64_t)blk * chunk, min(np, (int64_t)blk * chunk + chunk), one);
     if (!SCATTER) {
         // Warp reductions, one atomic per warp.
 #pragma unroll
@@ -126,505 +135,10 @@ bin_kernel(const float *__restrict__ x, const float *__restrict__ y, const float
             if (my_neg) atomicOr(wmax_bits + 1, 1u);  // some weight is negative
             if (my_wminc) atomicMax(wmax_bits + 6, my_wminc);  // smallest nonzero |w|
         }
-        if (kHist || coarse) __syncthreads();
-        if (kHist)
+        if (kHist) {
+            __syncthreads();
             for (int i = threadIdx.x; i < nb; i += blockDim.x)
                 if (hist[i]) atomicAdd(table + (int64_t)i * kCursorStride, hist[i]);
-        if (coarse)
-            for (int i = threadIdx.x; i < nsb; i += blockDim.x)
-                if (sbh[i]) atomicAdd(sb_table + (int64_t)i * kCursorStride, sbh[i]);
-    }
-}
-
-// Warp-aggregated reservations in shared memory (every lane of the warp
-// calls them): the lanes' n add to *counter with one atomic per warp.
-// warp_reserve returns the lane's first slot; warp_add returns nothing.
-__device__ __forceinline__ uint32_t warp_reserve(uint32_t *counter, uint32_t n)
-{
-    const int lane = threadIdx.x & 31;
-    uint32_t incl = n;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += t;
-    }
-    uint32_t base = 0;
-    if (lane == 31 && incl) base = atomicAdd(counter, incl);
-    base = __shfl_sync(0xffffffffu, base, 31);
-    return base + incl - n;
-}
-__device__ __forceinline__ void warp_add(uint32_t *counter, uint32_t n)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) n += __shfl_down_sync(0xffffffffu, n, o);
-    if ((threadIdx.x & 31) == 0 && n) atomicAdd(counter, n);
-}
-
-// Pass 3, staged form (nb <= kStageBricks).  Each CTA stages the records of
-// a contiguous particle chunk in shared memory and writes them out in
-// flushes: a flush ranks its records by brick (shared-memory counts), takes
-// one global range per brick it holds (one atomic on the brick's cursor per
-// brick and flush instead of one per record) and writes the records in
-// brick order, so a warp's stores land in runs of consecutive slots.
-// Records past the payload's capacity are flagged, not written.
-constexpr int kStageThreads = 1024;
-constexpr int kStageCap = 8192;     // staged records per flush (128 KB)
-constexpr int kStageBricks = 4096;  // bricks whose counts and ranges fit beside them
-constexpr int kStagePer = kStageBricks / 1024;  // scan items per thread of a flush
-constexpr int kStageRankBits = 13;  // kStageCap = 2^13
-
-template <int SCHEME>
-__global__ void __launch_bounds__(kStageThreads, 1)
-scatter_staged_kernel(const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z,
-                      const float *__restrict__ w, int64_t np, int64_t chunk, AssignGeom g, int nb,
-                      uint32_t *__restrict__ table, uint4 *__restrict__ payload, uint64_t cap,
-                      unsigned int *__restrict__ ovf)
-{
-    using St = Stencil<SCHEME>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    uint4 *srec = reinterpret_cast<uint4 *>(smem_raw);                  // [kStageCap]
-    uint32_t *skey = reinterpret_cast<uint32_t *>(srec + kStageCap);     // [kStageCap] brick << 13 | rank
-    uint16_t *sperm = reinterpret_cast<uint16_t *>(skey + kStageCap);    // [kStageCap] slot -> staged record
-    uint32_t *cnt = reinterpret_cast<uint32_t *>(sperm + kStageCap);     // [nb] records per brick, this flush
-    uint32_t *off = cnt + kStageBricks;                                  // [nb] first slot of each brick
-    uint32_t *gdel = off + kStageBricks;                                 // [nb] global slot - local slot
-    __shared__ uint32_t s_fill, s_need, s_wsum[kStageThreads / 32];
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    for (int b = tid; b < nb; b += kStageThreads) cnt[b] = 0u;
-    if (tid == 0) {
-        s_fill = 0u;
-        s_need = 0u;
-    }
-    __syncthreads();
-    const bool weighted = w != nullptr;
-    const int64_t p0 = (int64_t)blockIdx.x * chunk, p1 = min(np, p0 + chunk);
-
-    // Writes the staged records out (every thread takes part).
-    auto flush = [&]() {
-        const uint32_t nst = s_fill;
-        // exclusive scan of the counts: kStageBricks / kStageThreads per thread
-        constexpr int PER = kStageBricks / kStageThreads;
-        uint32_t v[PER];
-        uint32_t tsum = 0;
-#pragma unroll
-        for (int k = 0; k < PER; ++k) {
-            const int b = tid * PER + k;
-            v[k] = b < nb ? cnt[b] : 0u;
-            tsum += v[k];
-        }
-        uint32_t incl = tsum;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += t;
-        }
-        if (lane == 31) s_wsum[wid] = incl;
-        __syncthreads();
-        if (wid == 0) {
-            const uint32_t ws = s_wsum[lane];
-            uint32_t wi = ws;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
-                if (lane >= o) wi += t;
-            }
-            s_wsum[lane] = wi - ws;
-        }
-        __syncthreads();
-        uint32_t run = s_wsum[wid] + incl - tsum;
-#pragma unroll
-        for (int k = 0; k < PER; ++k) {
-            const int b = tid * PER + k;
-            if (b < nb) {
-                off[b] = run;
-                // one global range per brick held in this flush
-                if (v[k]) gdel[b] = atomicAdd(table + (int64_t)b * kCursorStride, v[k]) - run;
-            }
-            run += v[k];
-        }
-        __syncthreads();
-        for (uint32_t i = tid; i < nst; i += kStageThreads) {
-            const uint32_t key = skey[i];
-            sperm[off[key >> kStageRankBits] + (key & ((1u << kStageRankBits) - 1u))] = (uint16_t)i;
-        }
-        __syncthreads();
-        for (uint32_t j = tid; j < nst; j += kStageThreads) {
-            const uint32_t i = sperm[j];
-            const uint32_t slot = gdel[skey[i] >> kStageRankBits] + j;
-            if (slot < cap) payload[slot] = srec[i];
-            else atomicOr(ovf, 1u);
-        }
-        __syncthreads();
-        for (int b = tid; b < nb; b += kStageThreads) cnt[b] = 0u;
-        if (tid == 0) s_fill = 0u;
-        __syncthreads();
-    };
-
-    for (int64_t base = p0; base < p1; base += kStageThreads) {
-        const int64_t p = base + tid;
-        int c[3] = {0, 0, 0}, bl[3] = {0, 0, 0}, nbx[3] = {0, 0, 0};
-        float t[3] = {0.f, 0.f, 0.f};
-        float wt = 1.0f;
-        int nrec = 0;
-        if (p < p1) {
-            const float pos[3] = {__ldcs(x + p), __ldcs(y + p), __ldcs(z + p)};
-            if (weighted) wt = __ldcs(w + p);
-            if (home_cell<SCHEME>(pos, g, c)) {
-                nrec = 1;
-#pragma unroll
-                for (int a = 0; a < 3; ++a) {
-                    int lo, hi;
-                    stencil_ends<SCHEME>(c[a], g.n[a], lo, hi);
-                    bl[a] = brick_of(lo, g.b[a], g.bmagic[a]);
-                    nbx[a] = (brick_of(hi, g.b[a], g.bmagic[a]) == bl[a]) ? 1 : 2;
-                    if (SCHEME != CAM_NGP) t[a] = exact_offset(pos[a], g.mn[a], g.d[a], g.inv_d[a], c[a], g.n[a]);
-                    nrec *= nbx[a];
-                }
-            }
-        }
-        // room for this round's records, else flush first
-        warp_add(&s_need, (uint32_t)nrec);
-        __syncthreads();
-        const bool full = s_fill + s_need > (uint32_t)kStageCap;
-        __syncthreads();
-        if (full) flush();
-        if (tid == 0) s_need = 0u;
-        uint32_t dst = warp_reserve(&s_fill, (uint32_t)nrec);
-        if (nrec) {
-#pragma unroll
-            for (int i0 = 0; i0 < 2; ++i0) {
-                if (i0 >= nbx[0]) break;
-                const int b0 = (bl[0] + i0 == g.nb[0]) ? 0 : bl[0] + i0;
-#pragma unroll
-                for (int i1 = 0; i1 < 2; ++i1) {
-                    if (i1 >= nbx[1]) break;
-                    const int b1 = (bl[1] + i1 == g.nb[1]) ? 0 : bl[1] + i1;
-#pragma unroll
-                    for (int i2 = 0; i2 < 2; ++i2) {
-                        if (i2 >= nbx[2]) break;
-                        const int b2 = (bl[2] + i2 == g.nb[2]) ? 0 : bl[2] + i2;
-                        const int key = brick_linear(g, b0, b1, b2);
-                        const uint32_t rank = atomicAdd(cnt + key, 1u);
-                        const int o[3] = {b0 * g.b[0], b1 * g.b[1], b2 * g.b[2]};
-                        uint32_t word[3];
-#pragma unroll
-                        for (int a = 0; a < 3; ++a) {
-                            const int e = min(g.b[a], g.n[a] - o[a]);
-                            int cl = c[a] - o[a];
-                            if (cl < -1) cl += g.n[a];
-                            else if (cl > e) cl -= g.n[a];
-                            word[a] = pack_axis(cl, t[a]);
-                        }
-                        srec[dst] = make_uint4(word[0], word[1], word[2], __float_as_uint(wt));
-                        skey[dst] = ((uint32_t)key << kStageRankBits) | rank;
-                        ++dst;
-                    }
-                }
-            }
-        }
-        __syncthreads();
-    }
-    if (s_fill) flush();
-    (void)St::W;
-}
-
-// ---- two-level scatter (meshes with more bricks than the staged scatter
-// holds).  Level 1 partitions the particles by the super-brick of their
-// home cell (one raw 16-byte record per particle, x, y, z, w); level 2
-// takes each super-brick's particles and writes their brick records, every
-// brick of a window of (sx + 2)(sy + 2)(sz + 2) bricks around the
-// super-brick being one bucket.  Both stage records in shared memory and
-// write them in bucket order, so stores land in runs.
-
-// Flush of a stage: nst records srec[i] with key skey[i] = bucket << 13 |
-// rank, bucket counts cnt[0, nbk); dst(bucket) gives the bucket's global
-// cursor.  Takes one range per bucket, writes the records in bucket order
-// and clears the counts.  Every thread calls it.
-template <typename CursorOf>
-__device__ __forceinline__ void stage_flush(uint4 *srec, uint32_t *skey, uint16_t *sperm, uint32_t *cnt, uint32_t *off,
-                                            uint32_t *gdel, uint32_t *s_wsum, int nbk, uint32_t nst, CursorOf cursor_of,
-                                            uint4 *__restrict__ out, uint64_t cap, unsigned int *__restrict__ ovf)
-{
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    constexpr int PER = kStagePer;
-    uint32_t v[PER];
-    uint32_t tsum = 0;
-#pragma unroll
-    for (int k = 0; k < PER; ++k) {
-        const int b = tid * PER + k;
-        v[k] = b < nbk ? cnt[b] : 0u;
-        tsum += v[k];
-    }
-    uint32_t incl = tsum;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += t;
-    }
-    if (lane == 31) s_wsum[wid] = incl;
-    __syncthreads();
-    if (wid == 0) {
-        const uint32_t ws = s_wsum[lane];
-        uint32_t wi = ws;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
-            if (lane >= o) wi += t;
-        }
-        s_wsum[lane] = wi - ws;
-    }
-    __syncthreads();
-    uint32_t run = s_wsum[wid] + incl - tsum;
-#pragma unroll
-    for (int k = 0; k < PER; ++k) {
-        const int b = tid * PER + k;
-        if (b < nbk) {
-            off[b] = run;
-            if (v[k]) gdel[b] = atomicAdd(cursor_of(b), v[k]) - run;
-        }
-        run += v[k];
-    }
-    __syncthreads();
-    for (uint32_t i = tid; i < nst; i += kStageThreads) {
-        const uint32_t key = skey[i];
-        sperm[off[key >> kStageRankBits] + (key & ((1u << kStageRankBits) - 1u))] = (uint16_t)i;
-    }
-    __syncthreads();
-    for (uint32_t j = tid; j < nst; j += kStageThreads) {
-        const uint32_t i = sperm[j];
-        const uint32_t slot = gdel[skey[i] >> kStageRankBits] + j;
-        if (slot < cap) out[slot] = srec[i];
-        else atomicOr(ovf, 1u);
-    }
-    __syncthreads();
-    for (int b = tid; b < nbk; b += kStageThreads) cnt[b] = 0u;
-    __syncthreads();
-}
-
-constexpr int kL1Cap = 8192;       // staged raw records per flush
-constexpr int kL1Buckets = 1024;   // super-bricks at most
-constexpr int kL2Cap = 8192;
-constexpr int kL2Buckets = 1024;   // window bricks at most
-
-// Level 1: each CTA stages the raw records of a contiguous particle chunk
-// by super-brick (g1's bricks) and flushes them in super-brick order.
-template <int SCHEME>
-__global__ void __launch_bounds__(kStageThreads, 1)
-partition_kernel(const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z,
-                 const float *__restrict__ w, int64_t np, int64_t chunk, AssignGeom g, AssignGeom g1, int nsb,
-                 uint32_t *__restrict__ sb_cursor, uint4 *__restrict__ out, uint64_t cap,
-                 unsigned int *__restrict__ ovf)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    uint4 *srec = reinterpret_cast<uint4 *>(smem_raw);
-    uint32_t *skey = reinterpret_cast<uint32_t *>(srec + kL1Cap);
-    uint16_t *sperm = reinterpret_cast<uint16_t *>(skey + kL1Cap);
-    uint32_t *cnt = reinterpret_cast<uint32_t *>(sperm + kL1Cap);
-    uint32_t *off = cnt + kL1Buckets;
-    uint32_t *gdel = off + kL1Buckets;
-    __shared__ uint32_t s_fill, s_wsum[kStageThreads / 32];
-    const int tid = threadIdx.x;
-    for (int b = tid; b < nsb; b += kStageThreads) cnt[b] = 0u;
-    if (tid == 0) s_fill = 0u;
-    __syncthreads();
-    const bool weighted = w != nullptr;
-    auto cursor_of = [&](int b) { return sb_cursor + (int64_t)b * kCursorStride; };
-    const int64_t p0 = (int64_t)blockIdx.x * chunk, p1 = min(np, p0 + chunk);
-    for (int64_t base = p0; base < p1; base += kStageThreads) {
-        // a round adds at most kStageThreads records
-        if (s_fill + kStageThreads > (uint32_t)kL1Cap) {
-            stage_flush(srec, skey, sperm, cnt, off, gdel, s_wsum, nsb, s_fill, cursor_of, out, cap, ovf);
-            if (tid == 0) s_fill = 0u;
-            __syncthreads();
-        }
-        const int64_t p = base + tid;
-        float px = 0.f, py = 0.f, pz = 0.f, pw = 1.0f;
-        int c[3] = {0, 0, 0};
-        bool ok = false;
-        if (p < p1) {
-            px = __ldcs(x + p);
-            py = __ldcs(y + p);
-            pz = __ldcs(z + p);
-            if (weighted) pw = __ldcs(w + p);
-            const float pos[3] = {px, py, pz};
-            ok = home_cell<SCHEME>(pos, g, c);
-        }
-        const uint32_t dst = warp_reserve(&s_fill, ok ? 1u : 0u);
-        if (ok) {
-            const int key = brick_linear(g1, brick_of(c[0], g1.b[0], g1.bmagic[0]),
-                                         brick_of(c[1], g1.b[1], g1.bmagic[1]),
-                                         brick_of(c[2], g1.b[2], g1.bmagic[2]));
-            const uint32_t rank = atomicAdd(cnt + key, 1u);
-            srec[dst] = make_uint4(__float_as_uint(px), __float_as_uint(py), __float_as_uint(pz),
-                                   __float_as_uint(pw));
-            skey[dst] = ((uint32_t)key << kStageRankBits) | rank;
-        }
-        __syncthreads();
-    }
-    if (s_fill) stage_flush(srec, skey, sperm, cnt, off, gdel, s_wsum, nsb, s_fill, cursor_of, out, cap, ovf);
-}
-
-// Work items of level 2: super-brick sb holds ceil(count / R) items;
-// items[sb] = the first item of sb, items[nsb] = all items.  One CTA of
-// 1024 threads, nsb <= 1024.
-__global__ void __launch_bounds__(1024)
-refine_items_kernel(const uint32_t *__restrict__ sb_start, int nsb, int R, uint32_t *__restrict__ items)
-{
-    __shared__ uint32_t wsum[32];
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    const uint32_t v = tid < nsb ? (sb_start[tid + 1] - sb_start[tid] + R - 1) / R : 0u;
-    uint32_t incl = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += t;
-    }
-    if (lane == 31) wsum[wid] = incl;
-    __syncthreads();
-    if (wid == 0) {
-        const uint32_t ws = wsum[lane];
-        uint32_t wi = ws;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
-            if (lane >= o) wi += t;
-        }
-        wsum[lane] = wi - ws;
-    }
-    __syncthreads();
-    if (tid < nsb) items[tid] = wsum[wid] + incl - v;
-    if (tid == nsb - 1) items[nsb] = wsum[wid] + incl;
-}
-
-// Level 2: CTAs take items (up to R raw records of one super-brick) in
-// turn and write every brick record of those particles inside the
-// super-brick's window, staged with the window's bricks as buckets.
-template <int SCHEME>
-__global__ void __launch_bounds__(kStageThreads, 1)
-refine_kernel(const uint4 *__restrict__ raw, const uint32_t *__restrict__ sb_start,
-              const uint32_t *__restrict__ items, int nsb, int R, AssignGeom g, AssignGeom g1, int ws0, int ws1,
-              int ws2, uint32_t *__restrict__ table, uint4 *__restrict__ payload, uint64_t cap,
-              unsigned int *__restrict__ ovf)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    uint4 *srec = reinterpret_cast<uint4 *>(smem_raw);
-    uint32_t *skey = reinterpret_cast<uint32_t *>(srec + kL2Cap);
-    uint16_t *sperm = reinterpret_cast<uint16_t *>(skey + kL2Cap);
-    uint32_t *cnt = reinterpret_cast<uint32_t *>(sperm + kL2Cap);
-    uint32_t *off = cnt + kL2Buckets;
-    uint32_t *gdel = off + kL2Buckets;
-    __shared__ uint32_t s_fill, s_need, s_wsum[kStageThreads / 32];
-    __shared__ int s_sb;
-    const int tid = threadIdx.x;
-    const int nwin = ws0 * ws1 * ws2;
-    for (int b = tid; b < nwin; b += kStageThreads) cnt[b] = 0u;
-    if (tid == 0) {
-        s_fill = 0u;
-        s_need = 0u;
-    }
-    __syncthreads();
-    const uint32_t nitems = items[nsb];
-    for (uint32_t it = blockIdx.x; it < nitems; it += gridDim.x) {
-        if (tid == 0) {
-            int lo = 0, hi = nsb - 1;  // last sb with items[sb] <= it
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (items[mid] <= it) lo = mid;
-                else hi = mid - 1;
-            }
-            s_sb = lo;
-        }
-        __syncthreads();
-        const int sb = s_sb;
-        const uint32_t r0 = sb_start[sb] + (it - items[sb]) * (uint32_t)R;
-        const uint32_t r1 = min(r0 + (uint32_t)R, sb_start[sb + 1]);
-        // window origin (bricks): the super-brick's first brick - 1 per axis
-        const int S2 = sb % g1.nb[2], S1 = (sb / g1.nb[2]) % g1.nb[1], S0 = sb / (g1.nb[2] * g1.nb[1]);
-        const int w0 = S0 * (g1.b[0] / g.b[0]) - 1, w1 = S1 * (g1.b[1] / g.b[1]) - 1, w2 = S2 * (g1.b[2] / g.b[2]) - 1;
-        // global brick of window bucket k
-        auto cursor_of = [&](int k) {
-            const int l2 = k % ws2, l1 = (k / ws2) % ws1, l0 = k / (ws2 * ws1);
-            const int b0 = (w0 + l0 + g.nb[0]) % g.nb[0], b1 = (w1 + l1 + g.nb[1]) % g.nb[1],
-                      b2 = (w2 + l2 + g.nb[2]) % g.nb[2];
-            return table + (int64_t)brick_linear(g, b0, b1, b2) * kCursorStride;
-        };
-        for (uint32_t base = r0; base < r1; base += kStageThreads) {
-            const uint32_t p = base + tid;
-            int c[3] = {0, 0, 0}, bl[3] = {0, 0, 0}, nbx[3] = {0, 0, 0};
-            float t[3] = {0.f, 0.f, 0.f};
-            float wt = 0.0f;
-            int nrec = 0;
-            if (p < r1) {
-                const uint4 rv = raw[p];
-                const float pos[3] = {__uint_as_float(rv.x), __uint_as_float(rv.y), __uint_as_float(rv.z)};
-                wt = __uint_as_float(rv.w);
-                if (home_cell<SCHEME>(pos, g, c)) {
-                    nrec = 1;
-#pragma unroll
-                    for (int a = 0; a < 3; ++a) {
-                        int lo, hi;
-                        stencil_ends<SCHEME>(c[a], g.n[a], lo, hi);
-                        bl[a] = brick_of(lo, g.b[a], g.bmagic[a]);
-                        nbx[a] = (brick_of(hi, g.b[a], g.bmagic[a]) == bl[a]) ? 1 : 2;
-                        if (SCHEME != CAM_NGP) t[a] = exact_offset(pos[a], g.mn[a], g.d[a], g.inv_d[a], c[a], g.n[a]);
-                        nrec *= nbx[a];
-                    }
-                }
-            }
-            warp_add(&s_need, (uint32_t)nrec);
-            __syncthreads();
-            const bool full = s_fill + s_need > (uint32_t)kL2Cap;
-            __syncthreads();
-            if (full) {
-                stage_flush(srec, skey, sperm, cnt, off, gdel, s_wsum, nwin, s_fill, cursor_of, payload, cap, ovf);
-                if (tid == 0) s_fill = 0u;
-                __syncthreads();
-            }
-            if (tid == 0) s_need = 0u;
-            uint32_t dst = warp_reserve(&s_fill, (uint32_t)nrec);
-            if (nrec) {
-#pragma unroll
-                for (int i0 = 0; i0 < 2; ++i0) {
-                    if (i0 >= nbx[0]) break;
-                    const int b0 = (bl[0] + i0 == g.nb[0]) ? 0 : bl[0] + i0;
-#pragma unroll
-                    for (int i1 = 0; i1 < 2; ++i1) {
-                        if (i1 >= nbx[1]) break;
-                        const int b1 = (bl[1] + i1 == g.nb[1]) ? 0 : bl[1] + i1;
-#pragma unroll
-                        for (int i2 = 0; i2 < 2; ++i2) {
-                            if (i2 >= nbx[2]) break;
-                            const int b2 = (bl[2] + i2 == g.nb[2]) ? 0 : bl[2] + i2;
-                            // window bucket (the stencil's bricks lie within
-                            // one brick of the super-brick)
-                            const int l0 = (b0 - w0 + g.nb[0]) % g.nb[0], l1 = (b1 - w1 + g.nb[1]) % g.nb[1],
-                                      l2 = (b2 - w2 + g.nb[2]) % g.nb[2];
-                            const int key = (l0 * ws1 + l1) * ws2 + l2;
-                            const uint32_t rank = atomicAdd(cnt + key, 1u);
-                            const int o[3] = {b0 * g.b[0], b1 * g.b[1], b2 * g.b[2]};
-                            uint32_t word[3];
-#pragma unroll
-                            for (int a = 0; a < 3; ++a) {
-                                const int e = min(g.b[a], g.n[a] - o[a]);
-                                int cl = c[a] - o[a];
-                                if (cl < -1) cl += g.n[a];
-                                else if (cl > e) cl -= g.n[a];
-                                word[a] = pack_axis(cl, t[a]);
-                            }
-                            srec[dst] = make_uint4(word[0], word[1], word[2], __float_as_uint(wt));
-                            skey[dst] = ((uint32_t)key << kStageRankBits) | rank;
-                            ++dst;
-                        }
-                    }
-                }
-            }
-            __syncthreads();
-        }
-        // a window per super-brick: flush before the next item's window
-        if (s_fill) {
-            stage_flush(srec, skey, sperm, cnt, off, gdel, s_wsum, nwin, s_fill, cursor_of, payload, cap, ovf);
-            if (tid == 0) s_fill = 0u;
-            __syncthreads();
         }
     }
 }
@@ -848,53 +362,12 @@ AssignGeom make_geom(const cam_grid &gr, int scheme, int64_t np)
     return g;
 }
 
-// Super-bricks of the two-level scatter: groups of s0 x s1 x s2 bricks
-// (powers of two), doubled along the axis with the most super-bricks until
-// at most kL1Buckets remain.  g1 is the geometry whose "bricks" are the
-// super-bricks (c / (b s) = (c / b) / s, so a brick lies in one
-// super-brick); ws the window of a super-brick's records in level 2, its
-// bricks plus one on every side.
-struct Coarse {
-    AssignGeom g1;
-    int nsb = 0;
-    int ws[3] = {1, 1, 1};
-};
-
-static Coarse make_coarse(const AssignGeom &g)
-{
-    Coarse c;
-    int s[3] = {1, 1, 1};
-    auto nsb_of = [&](int a) { return (g.nb[a] + s[a] - 1) / s[a]; };
-    for (;;) {
-        const int64_t t = (int64_t)nsb_of(0) * nsb_of(1) * nsb_of(2);
-        if (t <= kL1Buckets) break;
-        int best = -1;
-        for (int a = 0; a < 3; ++a)
-            if (s[a] < g.nb[a] && (best < 0 || nsb_of(a) > nsb_of(best))) best = a;
-        if (best < 0) break;
-        s[best] *= 2;
-    }
-    c.g1 = g;
-    for (int a = 0; a < 3; ++a) {
-        c.g1.b[a] = g.b[a] * s[a];
-        c.g1.nb[a] = (g.n[a] + c.g1.b[a] - 1) / c.g1.b[a];
-        c.g1.bmagic[a] = (unsigned)(((1ull << 32) + (uint64_t)c.g1.b[a] - 1) / (uint64_t)c.g1.b[a]);
-        c.ws[a] = s[a] + 2;
-    }
-    c.nsb = c.g1.nb[0] * c.g1.nb[1] * c.g1.nb[2];
-    return c;
-}
-
 template <int SCHEME>
 static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const float *z,
                         const float *w, int64_t np, const AssignGeom &g, AssignOut &out)
 {
     const int64_t nb = (int64_t)g.nb[0] * g.nb[1] * g.nb[2];
     CAM_REQUIRE(nb < (1ll << 31), CAM_E_UNSUPPORTED, "too many mesh bricks");
-    // CTAs of the binning passes: one per SM (contiguous chunks of >= 4096
-    // particles).  Few CTAs keep the set of partly written payload sectors
-    // (CTAs x bricks x 128 B) inside L2, so sectors are complete before they
-    // are written back.
     // Count pass: one CTA of 1024 threads per SM (its brick histogram in
     // shared memory); scatter pass: two CTAs of 512 threads per SM.  Both
     // take contiguous chunks of >= 4096 particles.
@@ -916,29 +389,14 @@ static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const floa
     unsigned int *d_ovf = reinterpret_cast<unsigned int *>(stats + 3);
     CAM_CUDA_TRY(cudaMemsetAsync(table, 0, (size_t)nb * kCursorStride * sizeof(uint32_t), ctx->stream));
     CAM_CUDA_TRY(cudaMemsetAsync(stats, 0, 64, ctx->stream));
-    // more bricks than the staged scatter holds: the two-level scatter
-    Coarse co;
-    bool two_level = nb > kStageBricks && !ctx->no_stage;
-    if (two_level) {
-        co = make_coarse(g);
-        two_level = co.nsb <= kL1Buckets && co.ws[0] * co.ws[1] * co.ws[2] <= kL2Buckets;
-    }
-    uint32_t *sb_table = nullptr;
-    if (two_level) {
-        sb_table = static_cast<uint32_t *>(
-            scratch(ctx, "asg.sbcur", (size_t)co.nsb * kCursorStride * sizeof(uint32_t)));
-        CAM_CUDA_TRY(cudaMemsetAsync(sb_table, 0, (size_t)co.nsb * kCursorStride * sizeof(uint32_t), ctx->stream));
-    }
-    const int nsb = two_level ? co.nsb : 0;
 
-    const size_t hsmem = (size_t)((smem_hist ? nb : 0) + nsb) * sizeof(uint32_t);
+    const size_t hsmem = smem_hist ? (size_t)nb * sizeof(uint32_t) : 0;
     auto count_k = smem_hist ? (vec ? bin_kernel<SCHEME, false, true, true> : bin_kernel<SCHEME, false, true, false>)
                              : (vec ? bin_kernel<SCHEME, false, false, true> : bin_kernel<SCHEME, false, false, false>);
     auto scatter_k = vec ? bin_kernel<SCHEME, true, false, true> : bin_kernel<SCHEME, true, false, false>;
     smem_at_least(count_k, hsmem);
     CAM_LAUNCH_NAMED(ctx, "assign_bin_count", count_k, G, kBinThreads, hsmem, x, y, z, w, np, chunk, g, (int)nb,
-                     table, (uint4 *)nullptr, d_lost, d_wmax, (uint64_t)0, d_ovf, two_level ? co.g1 : g, nsb,
-                     sb_table);
+                     table, (uint4 *)nullptr, d_lost, d_wmax, (uint64_t)0, d_ovf);
     if (nb <= (int64_t)kOffThreads * kOffItems) {
         CAM_LAUNCH_NAMED(ctx, "assign_starts", brick_offsets_kernel, 1, kOffThreads, 0, table, (int)nb, start, d_total);
     } else {
@@ -996,42 +454,8 @@ static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const floa
     }
 
     uint4 *payload = static_cast<uint4 *>(scratch(ctx, "asg.payload", std::max<size_t>(total, 1) * sizeof(uint4)));
-    if (two_level) {
-        // level 1: particles by super-brick (one raw record each; lost ones
-        // are dropped), then level 2: each super-brick's brick records
-        auto *sb_start = static_cast<uint32_t *>(scratch(ctx, "asg.sbstart", (size_t)(nsb + 1) * sizeof(uint32_t)));
-        auto *sb_total = static_cast<uint32_t *>(scratch(ctx, "asg.sbtotal", 16));
-        auto *items = static_cast<uint32_t *>(scratch(ctx, "asg.items", (size_t)(nsb + 1) * sizeof(uint32_t)));
-        auto *raw = static_cast<uint4 *>(scratch(ctx, "asg.raw", (size_t)std::max<int64_t>(np, 1) * sizeof(uint4)));
-        CAM_LAUNCH_NAMED(ctx, "assign_starts", brick_offsets_kernel, 1, kOffThreads, 0, sb_table, nsb, sb_start,
-                         sb_total);
-        const int G3 = (int)std::max<int64_t>(1, std::min<int64_t>(kNumSMs, (np + kStageThreads - 1) / kStageThreads));
-        const int64_t chunk3 = (np + G3 - 1) / G3;
-        const size_t ssmem1 = (size_t)kL1Cap * (16 + 4 + 2) + (size_t)kL1Buckets * 3 * 4;
-        auto pk1 = partition_kernel<SCHEME>;
-        smem_at_least(pk1, ssmem1);
-        CAM_LAUNCH_NAMED(ctx, "assign_partition", pk1, G3, kStageThreads, ssmem1, x, y, z, w, np, chunk3, g, co.g1,
-                         nsb, sb_table, raw, (uint64_t)std::max<int64_t>(np, 1), d_ovf);
-        const int R = kL2Cap;
-        CAM_LAUNCH_NAMED(ctx, "assign_starts", refine_items_kernel, 1, 1024, 0, sb_start, nsb, R, items);
-        const size_t ssmem2 = (size_t)kL2Cap * (16 + 4 + 2) + (size_t)kL2Buckets * 3 * 4;
-        auto rk = refine_kernel<SCHEME>;
-        smem_at_least(rk, ssmem2);
-        CAM_LAUNCH_NAMED(ctx, "assign_bin_scatter", rk, kNumSMs, kStageThreads, ssmem2, raw, sb_start, items, nsb, R, g,
-                         co.g1, co.ws[0], co.ws[1], co.ws[2], table, payload, total, d_ovf);
-    } else if (nb <= kStageBricks && !ctx->no_stage) {
-        // staged scatter: one CTA per SM over contiguous chunks
-        const int G3 = (int)std::max<int64_t>(1, std::min<int64_t>(kNumSMs, (np + kStageThreads - 1) / kStageThreads));
-        const int64_t chunk3 = (np + G3 - 1) / G3;
-        const size_t ssmem = (size_t)kStageCap * (16 + 4 + 2) + (size_t)kStageBricks * 3 * 4;
-        auto sk = scatter_staged_kernel<SCHEME>;
-        smem_at_least(sk, ssmem);
-        CAM_LAUNCH_NAMED(ctx, "assign_bin_scatter", sk, G3, kStageThreads, ssmem, x, y, z, w, np, chunk3, g, (int)nb,
-                         table, payload, total, d_ovf);
-    } else {
-        CAM_LAUNCH_NAMED(ctx, "assign_bin_scatter", scatter_k, G2, kScatterThreads, 0, x, y, z, w, np, chunk2, g,
-                         (int)nb, table, payload, d_lost, d_wmax, total, d_ovf, g, 0, (uint32_t *)nullptr);
-    }
+    CAM_LAUNCH_NAMED(ctx, "assign_bin_scatter", scatter_k, G2, kScatterThreads, 0, x, y, z, w, np, chunk2, g, (int)nb,
+                     table, payload, d_lost, d_wmax, total, d_ovf);
 
     const size_t smem = (size_t)(g.b[0] + 2) * (g.b[1] + 2) * (g.b[2] + 2) * 2 * sizeof(uint32_t);
     CAM_REQUIRE(smem <= 110 * 1024, CAM_E_UNSUPPORTED, "brick tile too large");

@@ -130,8 +130,7 @@ __device__ __forceinline__ int brick_linear(const AssignGeom &g, int b0, int b1,
 template <int SCHEME, bool SMEM>
 __device__ __forceinline__ void count_one(float px, float py, float pz, float wt, bool weighted, const AssignGeom &g,
                                           uint32_t *hist, uint32_t *__restrict__ table, unsigned long long &my_lost,
-                                          unsigned int &my_wmax, unsigned int &my_neg, unsigned int &my_wminc,
-                                          const AssignGeom *g1 = nullptr, uint32_t *sbh = nullptr)
+                                          unsigned int &my_wmax, unsigned int &my_neg, unsigned int &my_wminc)
 {
     using St = Stencil<SCHEME>;
     const float pos[3] = {px, py, pz};
@@ -140,13 +139,6 @@ __device__ __forceinline__ void count_one(float px, float py, float pz, float wt
         ++my_lost;
         return;
     }
-    // two-level scatter: one count per particle for the super-brick of its
-    // home cell (g1's bricks are the super-bricks)
-    if (g1)
-        atomicAdd(sbh + brick_linear(*g1, brick_of(c[0], g1->b[0], g1->bmagic[0]),
-                                     brick_of(c[1], g1->b[1], g1->bmagic[1]),
-                                     brick_of(c[2], g1->b[2], g1->bmagic[2])),
-                  1u);
     if (weighted) {
         my_wmax = max(my_wmax, __float_as_uint(fabsf(wt)));
         my_neg |= wt < 0.0f;
@@ -230,10 +222,11 @@ __device__ __forceinline__ void bin_one(float px, float py, float pz, float wt, 
                 if (i2 >= nbx[2]) break;
                 const int b2 = (bl[2] + i2 == g.nb[2]) ? 0 : bl[2] + i2;
                 const int key = brick_linear(g, b0, b1, b2);
-                // count: per-CTA shared histogram, or the global counts;
-                // scatter: the brick's global append cursor
-                const uint32_t slot = (SMEM && !SCATTER) ? atomicAdd(hist + key, 1u)
-                                                         : atomicAdd(table + (int64_t)key * CSTRIDE, 1u);
+                // SMEM: the CTA's shared counters (count: its histogram;
+                // scatter: its own cursors into each brick's range);
+                // otherwise the global counts / the brick's append cursor
+                const uint32_t slot = SMEM ? atomicAdd(hist + key, 1u)
+                                           : atomicAdd(table + (int64_t)key * CSTRIDE, 1u);
                 if (SCATTER) {
                     const int o[3] = {b0 * g.b[0], b1 * g.b[1], b2 * g.b[2]};
                     uint32_t word[3];

@@ -93,9 +93,6 @@ struct cam_ctx {
     // Column FFT passes stage tiles with TMA unless CAM_NO_TMA is set in the
     // environment when the context is created (then the cp.async kernels).
     bool no_tma = false;
-    // The assignment's scatter stages records in shared memory and writes
-    // them in brick order unless CAM_NO_STAGE is set at context creation.
-    bool no_stage = false;
     unsigned *err_word = nullptr;  // device word: a bounded wait ran out (see device_error_word)
     // per-kernel timing (cam_profile_enable)
     bool prof_on = false;

@@ -451,12 +451,53 @@ __device__ __forceinline__ int count_above(double c2, double c1, double c0, doub
     return sign_changes(a2, a1, a0);
 }
 
+// Screens one cell in FP32 (labels only): the number of eigenvalues of
+// the tensor above thf = float(lambda_th), from the signs of the
+// coefficients of det(s I - B), B = T - thf I:
+//   a2 = -tr B,  a1 = the sum of B's principal 2x2 minors,  a0 = -det B.
+// Each coefficient is a sum of products of at most three FP32 numbers, one
+// of them rounded once from T - thf, so |fl(a) - a| <= gamma_9 m (gamma_9 =
+// 9u/(1-9u) = 5.4e-7, u = 2^-24), m the same sum over absolute values of
+// the terms (Higham, Accuracy and Stability of Numerical Algorithms, 2nd
+// ed., sec. 3.1); fused multiply-adds only remove roundings.  A sign is
+// taken as certain when |fl(a)| > 2e-6 m, so the count is exact for the
+// exact coefficients.  The cell is also certified free of ties: no root of
+// p within bandp of thf (|p(thf + s) - p(thf)| <= bandp (|a1| + bandp (|a2|
+// + bandp)) for |s| <= bandp), with bandp covering lambda_th +- band.
+// Returns -1 when any test fails (near-zero coefficients, subnormal or
+// non-finite terms, a root near the threshold): the caller then takes the
+// FP64 path.  An eigenvalue between thf and lambda_th (|thf - lambda_th|
+// <= 2^-24 |lambda_th|) lies inside any positive tie band.
+__device__ __forceinline__ int count_above_fp32(const float t6[6], float thf, float bandp)
+{
+    // (xx, yy, zz, xy, xz, yz) from slots (2, 4, 0, 5, 1, 3)
+    const float b0 = t6[2] - thf, b1 = t6[4] - thf, b2 = t6[0] - thf;
+    const float d = t6[5], e = t6[1], f = t6[3];
+    const float dd = d * d, ee = e * e, ff = f * f;
+    const float p01 = b0 * b1, p02 = b0 * b2, p12 = b1 * b2;
+    const float a2 = -(b0 + b1 + b2);
+    const float m2 = fabsf(b0) + fabsf(b1) + fabsf(b2);
+    const float a1 = (p01 + p02 + p12) - (dd + ee + ff);
+    const float m1 = (fabsf(p01) + fabsf(p02) + fabsf(p12)) + (dd + ee + ff);
+    const float t0 = p01 * b2, tdef = 2.0f * (d * e) * f;
+    const float a0 = -(((t0 + tdef) - b0 * ff) - (b1 * ee + b2 * dd));
+    const float m0 = ((fabsf(t0) + fabsf(tdef)) + fabsf(b0) * ff) + (fabsf(b1) * ee + fabsf(b2) * dd);
+    const float r2 = 2e-6f * m2, r1 = 2e-6f * m1, r0 = 2e-6f * m0;
+    // m >= 1e-20: every term's underflow error is far below r
+    if (!(m0 >= 1e-20f && m1 >= 1e-20f && m2 >= 1e-20f && m0 < 1e30f && m1 < 1e30f && m2 < 1e30f)) return -1;
+    if (!(fabsf(a2) > r2 && fabsf(a1) > r1 && fabsf(a0) > r0)) return -1;
+    if (!(fabsf(a0) - r0 > bandp * ((fabsf(a1) + r1) + bandp * ((fabsf(a2) + r2) + bandp)))) return -1;
+    // sign changes of (1, a2, a1, a0), all nonzero
+    return (int)(a2 < 0.0f) + (int)((a1 < 0.0f) != (a2 < 0.0f)) + (int)((a0 < 0.0f) != (a1 < 0.0f));
+}
+
 // Label of one cell from its six field values (slots 0..5 of t6), written
 // to labels[cell] (and lambdas when LAMBDAS, and the invariants when
 // LAMBDAS and inv != nullptr); the label and tie counters of the calling
 // thread are advanced.
 template <bool LAMBDAS>
-__device__ __forceinline__ void label_cell(const float t6[6], double lth, double band, int64_t cell, int64_t ncell,
+__device__ __forceinline__ void label_cell(const float t6[6], double lth, double band, float thf, float bandp,
+                                           int64_t cell, int64_t ncell,
                                            uint8_t *__restrict__ labels, float *__restrict__ lambdas,
                                            float *__restrict__ inv, unsigned &lc0, unsigned &lc1, unsigned &lc2,
                                            unsigned &lc3, unsigned &lties)
@@ -492,15 +533,18 @@ __device__ __forceinline__ void label_cell(const float t6[6], double lth, double
             inv[3 * ncell + cell] = (float)(sqrt(1.5 * trb2) / (2.0 + c2));
         }
     } else {
-        double c2, c1, c0, a2, a1, a0;
-        char_poly(t6[2], t6[4], t6[0], t6[5], t6[1], t6[3], c2, c1, c0);
-        shifted_poly(c2, c1, c0, lth, a2, a1, a0);
-        v = sign_changes(a2, a1, a0);
-        // |p(lth + s) - p(lth)| <= band (|a1| + band (|a2| + band)) for
-        // |s| <= band: above that bound p has no root in the band, and the
-        // counts at its two ends agree.  Only the other cells count again.
-        if (!(fabs(a0) > band * (fabs(a1) + band * (fabs(a2) + band))))
-            tie = count_above(c2, c1, c0, lth - band) != count_above(c2, c1, c0, lth + band);
+        v = count_above_fp32(t6, thf, bandp);
+        if (v < 0) {
+            double c2, c1, c0, a2, a1, a0;
+            char_poly(t6[2], t6[4], t6[0], t6[5], t6[1], t6[3], c2, c1, c0);
+            shifted_poly(c2, c1, c0, lth, a2, a1, a0);
+            v = sign_changes(a2, a1, a0);
+            // |p(lth + s) - p(lth)| <= band (|a1| + band (|a2| + band)) for
+            // |s| <= band: above that bound p has no root in the band, and the
+            // counts at its two ends agree.  Only the other cells count again.
+            if (!(fabs(a0) > band * (fabs(a1) + band * (fabs(a2) + band))))
+                tie = count_above(c2, c1, c0, lth - band) != count_above(c2, c1, c0, lth + band);
+        }
     }
     if (labels) labels[cell] = (uint8_t)(4 - v);
     lc0 += v == 3;  // label 1, knot
@@ -584,6 +628,10 @@ tidal_z_kernel(const typename CTw<T>::t *__restrict__ src, const typename CTw<T>
     }
     // Per cell: 6 components -> eigenvalues -> label.
     unsigned lc0 = 0, lc1 = 0, lc2 = 0, lc3 = 0, lties = 0;
+    // FP32 label screen: the threshold in float, the tie band widened by
+    // that rounding (and by its own)
+    const float thf = (float)lth;
+    const float bandp = (float)((band + fabs(lth - (double)thf)) * (1.0 + 1e-3));
     // real value z of row r of comp c: half z & 1 of complex element (c*rpc + r)*M + z/2
     const T *re = reinterpret_cast<const T *>(tile);
     const int64_t ncell = nn * n;
@@ -593,7 +641,7 @@ tidal_z_kernel(const typename CTw<T>::t *__restrict__ src, const typename CTw<T>
 #pragma unroll
         for (int c = 0; c < 6; ++c)
             t6[c] = (float)re[2 * fftdev::sidx<PAD>((c * rpcv + r) * M + (z >> 1)) + (z & 1)];
-        label_cell<LAMBDAS>(t6, lth, band, (row0 + r) * nz + z, ncell, labels, lambdas, inv, lc0, lc1, lc2, lc3,
+        label_cell<LAMBDAS>(t6, lth, band, thf, bandp, (row0 + r) * nz + z, ncell, labels, lambdas, inv, lc0, lc1, lc2, lc3,
                             lties);
     }
     flush_counts(lc0, lc1, lc2, lc3, lties, cnt_s, counts);
@@ -664,6 +712,10 @@ tidal_z_pipe_kernel(const typename CTw<T>::t *__restrict__ src, const typename C
         }
     };
     unsigned lc0 = 0, lc1 = 0, lc2 = 0, lc3 = 0, lties = 0;
+    // FP32 label screen: the threshold in float, the tie band widened by
+    // that rounding (and by its own)
+    const float thf = (float)lth;
+    const float bandp = (float)((band + fabs(lth - (double)thf)) * (1.0 + 1e-3));
     int64_t gi = blockIdx.x;
     if (gi < ngroups) load(gi, raw);
     fftdev::cp_async_commit();
@@ -715,8 +767,8 @@ tidal_z_pipe_kernel(const typename CTw<T>::t *__restrict__ src, const typename C
                 tb[c] = (float)v.y;
             }
             const int64_t cell = (row0 + r) * 2 * M + 2 * m;
-            label_cell<LAMBDAS>(ta, lth, band, cell, ncell, labels, lambdas, inv, lc0, lc1, lc2, lc3, lties);
-            label_cell<LAMBDAS>(tb, lth, band, cell + 1, ncell, labels, lambdas, inv, lc0, lc1, lc2, lc3, lties);
+            label_cell<LAMBDAS>(ta, lth, band, thf, bandp, cell, ncell, labels, lambdas, inv, lc0, lc1, lc2, lc3, lties);
+            label_cell<LAMBDAS>(tb, lth, band, thf, bandp, cell + 1, ncell, labels, lambdas, inv, lc0, lc1, lc2, lc3, lties);
         }
         __syncthreads();  // tile is refilled next
     }
