@@ -17,11 +17,13 @@
 //
 // Results: the assignment uses the same device functions, brick geometry
 // and 64-bit fixed-point scale as cam_job_run, so the mesh, its sum and the
-// lost-particle count are bit-identical to cam_job_run's.  The FFT runs the
-// same Stockham stages per row and column.  P(k) bins are summed in FP64 in
-// this CTA's fixed order, so they agree with cam_job_run's to FP64 rounding
-// (~1e-15 relative) and a job's results do not depend on which CTA ran it
-// or on what ran beside it.
+// lost-particle count are bit-identical to cam_job_run's.  The FFT holds
+// 8 points per thread and takes radix-8 stages (cam_job_run's kernels hold
+// 16 and take radix-16 stages where that saves a pass), and each mode's
+// power is binned in FP64 (cam_job_run: FP32 per mode, FP64 bins), so P(k)
+// agrees with cam_job_run's to FP32 rounding (~1e-7 relative).  P(k) bins
+// are summed in FP64 in this CTA's fixed order, so a job's results do not
+// depend on which CTA ran it or on what ran beside it.
 //
 // Queue (pinned host memory mapped into the device): a ring of job slots.
 // The host writes a slot's job, then raises `submitted`.  CTA thread 0

@@ -67,7 +67,8 @@ fft_cols_kernel(typename fftdev::CT<T>::t *base, int len, int ncols, int64_t jst
     }
     __syncthreads();
     if constexpr (LEN > 0)
-        fftdev::block_fft_fixed<C, INV, false, W, LEN, fftdev::ct_threads(LEN, W, fftdev::CT<T>::kPPT), W, 1, 1>(
+        fftdev::block_fft_fixed<C, INV, false, W, LEN, fftdev::ct_threads(LEN, W, fftdev::CT<T>::kPPT), W, 1, 1, false,
+                                fftdev::CT<T>::kMaxR>(
             tile, tw);
     else
         fftdev::block_fft<C, fftdev::CT<T>::kPPT, INV, false, W>(tile, len, W, W, 1, rd, tw, twmul);
@@ -132,7 +133,7 @@ fft_cols_pipe_kernel(typename fftdev::CT<T>::t *base, int nct, int nplanes, int6
         fftdev::cp_async_commit();
         fftdev::cp_async_wait<1>();  // this thread's copies of tile t have landed
         __syncthreads();     // ... and everyone's
-        fftdev::block_fft_fixed<C, INV, false, W, LEN, NTHR, W, 1, 1>(here, tw);
+        fftdev::block_fft_fixed<C, INV, false, W, LEN, NTHR, W, 1, 1, false, fftdev::CT<T>::kMaxR>(here, tw);
         C *g = tile_ptr(t);
         for (int e = threadIdx.x; e < LEN * W; e += NTHR) g[(int64_t)(e / W) * jstride + (e % W)] = here[e];
         __syncthreads();  // buf[cur] is refilled by the next iteration's prefetch
@@ -224,7 +225,7 @@ fft_cols_tma_kernel(const __grid_constant__ CUtensorMap map, TileDims td, int nc
             failed = true;
             break;
         }
-        fftdev::block_fft_fixed<C, INV, false, W, LEN, NTHR, W, 1, 1>(here, tw);
+        fftdev::block_fft_fixed<C, INV, false, W, LEN, NTHR, W, 1, 1, false, fftdev::CT<T>::kMaxR>(here, tw);
         tma::fence_proxy_async_smem();
         __syncthreads();
         if (leader) {
@@ -270,14 +271,16 @@ constexpr int pk_pass_threads()
     return fftdev::ct_threads(LEN, 16, 16);
 }
 // CTAs per SM the binning pass is built for: two tiles plus the tables and
-// warp bins of N/2 bins in 200 KB, at most 1024 threads.
+// warp bins of N/2 bins in 222 KB (the SM's 228 KB less 1 KB per CTA), at
+// most 1024 threads: three CTAs of 80 registers at N = 256 (24 warps per SM
+// to hide the binning's latencies), one at 512.
 template <int LEN>
 constexpr int pk_pass_min_blocks()
 {
     constexpr int nthr = pk_pass_threads<LEN>();
     constexpr int by_thr = 1024 / nthr;
-    constexpr int bytes = 2 * LEN * 16 * 8 + (LEN + 2 + (nthr / 32) * (LEN / 2)) * 8;
-    constexpr int by_smem = (200 * 1024) / bytes;
+    constexpr int bytes = 2 * LEN * 16 * 8 + (nthr / 32) * (LEN / 2) * 8 + (LEN / 2 + 1) * 4;
+    constexpr int by_smem = (222 * 1024) / bytes;
     constexpr int b = by_thr < by_smem ? by_thr : by_smem;
     return b > 1 ? b : 1;
 }
@@ -301,9 +304,9 @@ fft_cols_tma_pk_kernel(const __grid_constant__ CUtensorMap map, TileDims td, int
     extern __shared__ __align__(128) unsigned char smem_tma[];
     __shared__ uint64_t bar[2];
     C *const buf0 = reinterpret_cast<C *>(smem_tma);
-    double *const tw2 = reinterpret_cast<double *>(smem_tma + 2 * (size_t)TILE_BYTES);  // [H + 1]
-    double *const wsum = tw2 + (H + 1);                                                 // [NWARP][nbins]
-    for (int t = threadIdx.x; t <= H; t += NTHR) tw2[t] = g_tab[t];
+    double *const wsum = reinterpret_cast<double *>(smem_tma + 2 * (size_t)TILE_BYTES);  // [NWARP][nbins]
+    float *const tw2 = reinterpret_cast<float *>(wsum + (size_t)NWARP * nbins);         // [H + 1]
+    for (int t = threadIdx.x; t <= H; t += NTHR) tw2[t] = (float)g_tab[t];
     for (int t = threadIdx.x; t < NWARP * nbins; t += NTHR) wsum[t] = 0.0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double *const mysum = wsum + (size_t)warp * nbins;
@@ -349,7 +352,7 @@ fft_cols_tma_pk_kernel(const __grid_constant__ CUtensorMap map, TileDims td, int
             failed = true;
             break;
         }
-        fftdev::block_fft_fixed<C, false, false, W, LEN, NTHR, W, 1, 1>(here, tw);
+        fftdev::block_fft_fixed<C, false, false, W, LEN, NTHR, W, 1, 1, false, 16>(here, tw);
         int x, plane, comp;
         coords(t, x, plane, comp);
         if (store) {
@@ -365,23 +368,25 @@ fft_cols_tma_pk_kernel(const __grid_constant__ CUtensorMap map, TileDims td, int
                 tma::bulk_commit();
             }
         }
-        // bin the tile: plane = j, columns c0 .. c0 + 15
+        // bin the tile: plane = j, columns c0 .. c0 + 15.  A mode's
+        // |F|^2 / W^2 is formed in FP32 (one rounding per factor, ~2e-7)
+        // and summed over its run of at most 16 lanes in FP32; each run's
+        // sum is added to the warp's FP64 bin.
         const int j = plane, c0 = x / 2;
         if (j != H) {
             const int b = j <= H ? j : N - j;
-            const double tb = tw2[b];
-            const int qb = b * b;
             const int kk = lane & 15;
             const int c = c0 + kk;
-            const double tc = tw2[c];
+            const int qbc = b * b + c * c;
+            const float wbc = tw2[b] * tw2[c];
             for (int pr = warp; pr < LEN / 2; pr += NWARP) {
                 const int i = 2 * pr + (lane >> 4);
                 const int a = i <= H ? i : N - i;
-                const int bin = __ldg(btab + (a * a + qb + c * c));
-                double v = 0.0;
+                const int bin = __ldg(btab + (a * a + qbc));
+                float v = 0.0f;
                 if (bin >= 0 && bin < nbins && pk_visited(i, j, c, N)) {
                     const C f = here[i * W + kk];
-                    v = ((double)f.x * (double)f.x + (double)f.y * (double)f.y) * (tw2[a] * tb * tc);
+                    v = (f.x * f.x + f.y * f.y) * (tw2[a] * wbc);
                 }
                 const int prev = __shfl_up_sync(0xffffffffu, bin, 1);
                 const bool head = kk == 0 || prev != bin;
@@ -390,13 +395,13 @@ fft_cols_tma_pk_kernel(const __grid_constant__ CUtensorMap map, TileDims td, int
                 const int end = later ? __ffs((int)later) - 1 : 32;
 #pragma unroll
                 for (int off = 1; off < 16; off <<= 1) {
-                    const double o = __shfl_down_sync(0xffffffffu, v, off);
+                    const float o = __shfl_down_sync(0xffffffffu, v, off);
                     if (lane + off < end) v += o;
                 }
                 const bool add = head && bin >= 0 && bin < nbins;
-                if (add && lane < 16) mysum[bin] += v;
+                if (add && lane < 16) mysum[bin] += (double)v;
                 __syncwarp();
-                if (add && lane >= 16) mysum[bin] += v;
+                if (add && lane >= 16) mysum[bin] += (double)v;
                 __syncwarp();
             }
         }
@@ -484,7 +489,7 @@ fft_rows_kernel(const void *in, void *out_main, typename fftdev::CT<T>::t *nyq, 
         // all rpc rows (the unused ones of the last CTA hold garbage and are not stored)
         constexpr int RPC = rows_rpc<T>(LEN);
         fftdev::block_fft_fixed<C, INV, true, RPC, LEN, fftdev::ct_threads(LEN, RPC, fftdev::CT<T>::kPPT), 1, LEN,
-                                (MODE <= 1) ? 2 : 1, PAD>(tile, tw);
+                                (MODE <= 1) ? 2 : 1, PAD, fftdev::CT<T>::kMaxR>(tile, tw);
     } else {
         fftdev::block_fft<C, fftdev::CT<T>::kPPT, INV, true, 0>(tile, len, nr, 1, len, rd, tw, (MODE <= 1) ? 2 : 1);
     }
@@ -566,7 +571,7 @@ fft_rows_r2c_pipe_kernel(const T *__restrict__ in, typename fftdev::CT<T>::t *__
         if (gn < ngroups) load(gn);
         fftdev::cp_async_commit();
         // all RPC rows (the unused ones of the last group hold stale data and are not stored)
-        fftdev::block_fft_fixed<C, false, true, RPC, LEN, NTHR, 1, LEN, 2, true>(tile, tw);
+        fftdev::block_fft_fixed<C, false, true, RPC, LEN, NTHR, 1, LEN, 2, true, fftdev::CT<T>::kMaxR>(tile, tw);
         C *dm = out_main + row0 * M;
         C *dn = nyq + row0;
         for (int e = threadIdx.x; e < nr * (M + 1); e += NTHR) {
@@ -801,7 +806,8 @@ bool fft_r2c_pk_fused(cam_ctx *ctx, FftPlan *plan, const void *real_in, const do
         constexpr int LEN = decltype(lc)::value;
         if constexpr (LEN >= 32 && 2 * LEN * 16 * 8 <= 200 * 1024) {
             constexpr int NTHR = pk_pass_threads<LEN>();
-            const size_t smem = (size_t)2 * LEN * 16 * 8 + (size_t)(LEN / 2 + 1 + (NTHR / 32) * pt.nbins) * sizeof(double);
+            const size_t smem = (size_t)2 * LEN * 16 * 8 + (size_t)(NTHR / 32) * pt.nbins * sizeof(double) +
+                                (size_t)(LEN / 2 + 1) * sizeof(float);
             if (smem > 220 * 1024) return;
             // x pass over main: 4D view (scalar column, row i, plane j, 1)
             CUtensorMap map;

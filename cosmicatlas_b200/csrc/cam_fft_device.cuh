@@ -1,5 +1,5 @@
 // Device-side FFT building blocks shared by the FFT and T-web kernels:
-// complex helpers, radix-2/3/4/8 butterflies and a Stockham stage that runs
+// complex helpers, radix-2/3/4/8/16 butterflies and a Stockham stage that runs
 // over many independent transforms held in shared memory.
 //
 // Stage (Stockham autosort, radix R, Ns = product of the radices already
@@ -64,12 +64,14 @@ struct CT<float> {
     using t = float2;
     static constexpr int kCols = 16;  // 128-byte column tiles
     static constexpr int kPPT = 16;   // complex points per thread
+    static constexpr int kMaxR = 16;  // largest radix of the compile-time stage lists
 };
 template <>
 struct CT<double> {
     using t = double2;
     static constexpr int kCols = 8;
     static constexpr int kPPT = 8;
+    static constexpr int kMaxR = 8;
 };
 
 template <typename C>
@@ -81,6 +83,13 @@ __device__ __forceinline__ C cmul(C a, C b) { return C{a.x * b.x - a.y * b.y, a.
 // multiply by -i (forward) or +i (inverse)
 template <typename C, bool INV>
 __device__ __forceinline__ C rot(C a) { return INV ? C{-a.y, a.x} : C{a.y, -a.x}; }
+
+// a * exp(-+ i t) given c = cos t, s = sin t (forward: -, inverse: +)
+template <typename C, bool INV, typename T>
+__device__ __forceinline__ C twid(C a, T c, T s)
+{
+    return INV ? C{a.x * c - a.y * s, a.x * s + a.y * c} : C{a.x * c + a.y * s, a.y * c - a.x * s};
+}
 
 template <typename C, bool INV>
 __device__ __forceinline__ void dft2(C &a, C &b)
@@ -128,6 +137,36 @@ __device__ __forceinline__ void dft(C *v)
         for (int k = 0; k < 4; ++k) {
             v[k] = cadd(e[k], o[k]);
             v[k + 4] = csub(e[k], o[k]);
+        }
+    } else if (R == 16) {
+        // 4 x 4: n = n2 + 4 n1, k = k1 + 4 k2,
+        //   X[k1 + 4 k2] = sum_n2 W4^(n2 k2) W16^(n2 k1) sum_n1 x[n2 + 4 n1] W4^(n1 k1)
+        const T c1 = (T)0.92387953251128675613;  // cos(pi/8)
+        const T s1 = (T)0.38268343236508977173;  // sin(pi/8)
+        const T h = (T)0.70710678118654752440;   // cos(pi/4)
+        C a[4][4];
+#pragma unroll
+        for (int n2 = 0; n2 < 4; ++n2) {
+#pragma unroll
+            for (int n1 = 0; n1 < 4; ++n1) a[n2][n1] = v[n2 + 4 * n1];
+            dft<C, 4, INV>(a[n2]);  // a[n2][k1]
+        }
+        // W16^(n2 k1), angle 2 pi m / 16 for m = n2 k1
+        a[1][1] = twid<C, INV>(a[1][1], c1, s1);   // m = 1
+        a[1][2] = twid<C, INV>(a[1][2], h, h);     // m = 2
+        a[1][3] = twid<C, INV>(a[1][3], s1, c1);   // m = 3
+        a[2][1] = twid<C, INV>(a[2][1], h, h);     // m = 2
+        a[2][2] = rot<C, INV>(a[2][2]);            // m = 4
+        a[2][3] = twid<C, INV>(a[2][3], -h, h);    // m = 6
+        a[3][1] = twid<C, INV>(a[3][1], s1, c1);   // m = 3
+        a[3][2] = twid<C, INV>(a[3][2], -h, h);    // m = 6
+        a[3][3] = twid<C, INV>(a[3][3], -c1, -s1); // m = 9
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1) {
+            C b[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
+            dft<C, 4, INV>(b);
+#pragma unroll
+            for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = b[k2];
         }
     }
 }
@@ -212,21 +251,33 @@ __device__ __forceinline__ void block_fft(C *buf, int len, int ncol, int jstride
 // Same factorisation as factor_radices, evaluated at compile time, so that
 // each stage of a known length is inlined with constant Ns and len; the
 // register allocator then sees one stage at a time (the runtime stage loop
-// above spills on sm_100a).
-constexpr int ct_num_stages(int len)
+// above spills on sm_100a).  With MAXR = 16 a length takes radix-16 stages
+// first when that needs fewer stages than radix 8 (16, 48, 128, 256, 384,
+// 768, 1024): every stage is a full pass through shared memory with two
+// barriers, so fewer stages is less traffic and fewer barriers.
+constexpr int ct_stages_of(int len, int first)
 {
     int n = 0, m = len;
-    while (m % 8 == 0 && m > 8) { ++n; m /= 8; }
+    while (m % first == 0 && m > 8) { ++n; m /= first; }
     while (m % 3 == 0) { ++n; m /= 3; }
-    if (m == 8 || m == 4 || m == 2) ++n;
+    if (m == 16 || m == 8 || m == 4 || m == 2) ++n;
     return n;
 }
-constexpr int ct_radix(int len, int s)
+constexpr int ct_first_radix(int len, int maxr)
 {
+    return maxr >= 16 && len % 16 == 0 && ct_stages_of(len, 16) < ct_stages_of(len, 8) ? 16 : 8;
+}
+constexpr int ct_num_stages(int len, int maxr = 8)
+{
+    return ct_stages_of(len, ct_first_radix(len, maxr));
+}
+constexpr int ct_radix(int len, int s, int maxr = 8)
+{
+    const int f = ct_first_radix(len, maxr);
     int k = 0, m = len;
-    while (m % 8 == 0 && m > 8) { if (k == s) return 8; ++k; m /= 8; }
+    while (m % f == 0 && m > 8) { if (k == s) return f; ++k; m /= f; }
     while (m % 3 == 0) { if (k == s) return 3; ++k; m /= 3; }
-    return m;  // the final 8, 4 or 2
+    return m;  // the final 16, 8, 4 or 2
 }
 constexpr unsigned ct_magic(int d) { return d <= 1 ? 0u : (unsigned)(((1ull << 32) + (unsigned long long)d - 1) / (unsigned long long)d); }
 
@@ -323,14 +374,15 @@ __device__ __forceinline__ void stage_ct(C *buf, const C *__restrict__ tw)
 
 // All stages of a length-LEN transform, layout and thread count fixed at
 // compile time (the CTA must run exactly NTHR threads).
+// MAXR: largest radix (8, or 16 for kernels whose threads hold 16 points).
 template <typename C, bool INV, bool JFAST, int NCOL, int LEN, int NTHR, int JSTRIDE, int CSTRIDE, int TWMUL,
-          bool PAD = false, int S = 0, int NS = 1>
+          bool PAD = false, int MAXR = 8, int S = 0, int NS = 1>
 __device__ __forceinline__ void block_fft_fixed(C *buf, const C *__restrict__ tw)
 {
-    if constexpr (S < ct_num_stages(LEN)) {
-        constexpr int R = ct_radix(LEN, S);
+    if constexpr (S < ct_num_stages(LEN, MAXR)) {
+        constexpr int R = ct_radix(LEN, S, MAXR);
         stage_ct<C, R, INV, JFAST, NCOL, LEN, NS, NTHR, JSTRIDE, CSTRIDE, TWMUL, PAD>(buf, tw);
-        block_fft_fixed<C, INV, JFAST, NCOL, LEN, NTHR, JSTRIDE, CSTRIDE, TWMUL, PAD, S + 1, NS * R>(buf, tw);
+        block_fft_fixed<C, INV, JFAST, NCOL, LEN, NTHR, JSTRIDE, CSTRIDE, TWMUL, PAD, MAXR, S + 1, NS * R>(buf, tw);
     }
 }
 

@@ -168,7 +168,8 @@ tidal_x_kernel(const typename CTw<T>::t *__restrict__ src, typename CTw<T>::t *_
     }
     __syncthreads();
     if constexpr (LEN > 0)
-        fftdev::block_fft_fixed<C, true, false, W, LEN, fftdev::ct_threads(LEN, W, CTw<T>::kPPT), W, 1, 1>(tile, tw);
+        fftdev::block_fft_fixed<C, true, false, W, LEN, fftdev::ct_threads(LEN, W, CTw<T>::kPPT), W, 1, 1, false,
+                                    CTw<T>::kMaxR>(tile, tw);
     else
         fftdev::block_fft<C, CTw<T>::kPPT, true, false, W>(tile, n, W, W, 1, rd, tw, 1);
     for (int e = threadIdx.x; e < tot; e += blockDim.x) {
@@ -216,7 +217,8 @@ tidal_y_kernel(typename CTw<T>::t *__restrict__ base, int n, int ncols, int64_t 
         }
         __syncthreads();
         if constexpr (LEN > 0)
-            fftdev::block_fft_fixed<C, true, false, W, LEN, fftdev::ct_threads(LEN, W, CTw<T>::kPPT), W, 1, 1>(tile, tw);
+            fftdev::block_fft_fixed<C, true, false, W, LEN, fftdev::ct_threads(LEN, W, CTw<T>::kPPT), W, 1, 1, false,
+                                    CTw<T>::kMaxR>(tile, tw);
         else
             fftdev::block_fft<C, CTw<T>::kPPT, true, false, W>(tile, n, W, W, 1, rd, tw, 1);
         C *o = base + (int64_t)slot_of(p, q) * ccomp + off;
@@ -338,7 +340,7 @@ tidal_pipe_kernel(const typename CTw<T>::t *src, typename CTw<T>::t *dst, int n,
                 work[e] = C{v.x * m, v.y * m};
             }
             __syncthreads();
-            fftdev::block_fft_fixed<C, true, false, W, LEN, NTHR, W, 1, 1>(work, tw);
+            fftdev::block_fft_fixed<C, true, false, W, LEN, NTHR, W, 1, 1, false, CTw<T>::kMaxR>(work, tw);
             const int slot = MODE == 0 ? pp : slot_of(p, q);
             C *g = dst + (int64_t)slot * ccomp + (int64_t)plane * pstride + (int64_t)ct * W;
             // the y pass: k_z^r, r = 2 - p - q, k_z = the column (constant
@@ -622,7 +624,7 @@ tidal_z_kernel(const typename CTw<T>::t *__restrict__ src, const typename CTw<T>
     if constexpr (LEN > 0) {
         constexpr int RPCZ = tweb_rpc<T>(LEN);
         fftdev::block_fft_fixed<C, true, true, 6 * RPCZ, LEN, fftdev::ct_threads(LEN, 6 * RPCZ, CTw<T>::kPPT), 1, LEN, 2,
-                                true>(tile, tw);
+                                true, CTw<T>::kMaxR>(tile, tw);
     } else {
         fftdev::block_fft<C, CTw<T>::kPPT, true, true, 0>(tile, M, 6 * rpc, 1, M, rd, tw, 2);
     }
@@ -755,7 +757,7 @@ tidal_z_pipe_kernel(const typename CTw<T>::t *__restrict__ src, const typename C
         const int64_t gn = gi + gridDim.x;
         if (gn < ngroups) load(gn, raw);
         fftdev::cp_async_commit();
-        fftdev::block_fft_fixed<C, true, true, 6 * RPC, LEN, NTHR, 1, LEN, 2, true>(tile, tw);
+        fftdev::block_fft_fixed<C, true, true, 6 * RPC, LEN, NTHR, 1, LEN, 2, true, CTw<T>::kMaxR>(tile, tw);
         // complex element m of a row holds the real values at z = 2m, 2m + 1
         for (int e = threadIdx.x; e < nr * M; e += NTHR) {
             const int r = e / M, m = e % M;

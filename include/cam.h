@@ -420,8 +420,9 @@ int cam_server_destroy(cam_server *s);
  * per-particle weights, particles already on the device (CAM_MEM_DEVICE),
  * density P(k) with at most 128 bins, no T-web (others: CAM_E_UNSUPPORTED).
  * The mesh sum and the lost count equal cam_job_run's bit for bit (same
- * assignment functions and fixed-point scale); P(k) agrees to FP64
- * rounding; a job's results do not depend on the jobs beside it.
+ * assignment functions and fixed-point scale); P(k) agrees to FP32
+ * rounding (its FFT takes radix-8 stages, its binning FP64 per mode); a
+ * job's results do not depend on the jobs beside it.
  * Every device-side wait is bounded: with no job for idle_timeout_s the
  * kernel ends (cam_devloop_state then returns CAM_E_TIMEOUT) and the next
  * submission or wait relaunches it.  One host thread per loop. */

@@ -2,9 +2,11 @@
 
 The loop runs whole jobs inside one resident kernel, one CTA per job.  Its
 assignment uses the same device functions and fixed-point scale as
-cam_job_run, so the lost count and the mesh sum are bit-identical; the FFT
-runs the same stages; P(k) is summed in another fixed FP64 order, so it
-agrees to FP64 rounding (1e-12 here), with identical mode counts.  A job's
+cam_job_run, so the lost count and the mesh sum are bit-identical.  Its
+FFT holds 8 points per thread (radix-8 stages; cam_job_run's 16-point
+threads take radix-16 stages where that saves a pass) and it bins each
+mode's power in FP64 (cam_job_run: FP32 per mode, FP64 bins), so P(k)
+agrees to FP32 rounding (2e-6 here), with identical mode counts.  A job's
 result does not depend on the jobs that ran beside it, and every
 device-side wait is bounded: with no job for the idle limit the kernel
 ends, and the next submission relaunches it.  The loops here use half the
@@ -35,7 +37,7 @@ def _close(a, b):
     assert a["assign"].sum_mesh == b["assign"].sum_mesh
     assert np.array_equal(a["pk"].modes, b["pk"].modes)
     floor = np.abs(b["pk"].shot_noise) * np.ones(len(b["pk"].pk))
-    assert pk_rel_err(a["pk"].pk, b["pk"].pk, floor) <= 1e-12
+    assert pk_rel_err(a["pk"].pk, b["pk"].pk, floor) <= 2e-6
 
 
 @pytest.fixture(scope="module")

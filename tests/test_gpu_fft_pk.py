@@ -248,8 +248,11 @@ def test_tma_staged_columns_equal_cp_async(ctx, n, prec):
 @pytest.mark.parametrize("n,nbins,ndel", [(64, 32, 1.0), (128, 64, 1.0), (96, 30, 1.5)])
 def test_job_pk_binned_in_fft_equals_separate_binning(ctx, scheme, n, nbins, ndel):
     # cam_job_run bins P(k) inside the FFT's last column pass; the separate
-    # binning kernel over the stored spectrum gives the same sums (up to the
-    # FP64 summation order) and the same mode counts
+    # binning kernel over the stored spectrum gives the same mode counts and
+    # the same sums up to rounding: the fused pass forms each mode's
+    # |F|^2 / W^2 in FP32 and sums runs of at most 16 modes in FP32 (a few
+    # units of 2^-24 per run) before its FP64 bins; the separate one is FP64
+    # throughout
     box = 800.0
     x, y, z = synth.clumped(400_000, box, 4_000, 2.0, 0.8, seed=n + scheme)
     g = make_grid(n, box)
@@ -259,7 +262,7 @@ def test_job_pk_binned_in_fft_equals_separate_binning(ctx, scheme, n, nbins, nde
     sep = ctx.power(mesh, box, opts)
     assert np.array_equal(job["pk"].modes, sep.modes)
     floor = np.abs(sep.shot_noise) * np.ones(nbins)
-    assert pk_rel_err(job["pk"].pk, sep.pk, floor) <= 1e-9
+    assert pk_rel_err(job["pk"].pk, sep.pk, floor) <= 2e-6
     # and with the T-web, where the x pass also writes the spectrum back
     job2 = ctx.job(x, y, z, None, g, scheme, F32, pk=opts, tweb=Context.tweb_opts(8.0, 0.0, 1e-5))
     assert np.array_equal(job2["pk"].pk, job["pk"].pk)
