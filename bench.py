@@ -259,6 +259,29 @@ def cufft_r2c_ms(n, stream, reps=20):
     return e0.elapsed_time(e1) / reps
 
 
+def ours_r2c_ms(ctx, n, reps=20):
+    """Mean time of the library's own r2c alone (cam_fft_r2c on an n^3 FP32
+    device mesh: no P(k) binning; its FFTW-layout output costs one layout
+    copy more than the jobs' internal layout), CUDA events on the launching
+    stream: the like-for-like counterpart of cufft_r2c_ms.  The context
+    launches on torch's current stream (set by the caller)."""
+    import torch
+    m = torch.randn((n, n, n), device="cuda", dtype=torch.float32)
+    st = torch.cuda.current_stream()
+    for _ in range(3):
+        ctx.fft_r2c(m)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(reps):
+        ctx.fft_r2c(m)
+    e1.record(st)
+    torch.cuda.synchronize()
+    del m
+    return e0.elapsed_time(e1) / reps
+
+
 def pk_error_vs_oracle(x, y, z, w, pks):
     """max over bins of |P - P_oracle| / max(|P_oracle|, SN C(k)/W^2) for each
     scheme's job: the FP64 oracle assigns the same particles and bins the
@@ -395,6 +418,7 @@ def run_ours(args):
 
     # the FFT stage against cuFFT (torch.fft.rfftn on the device), comparison only
     cufft_ms = cufft_r2c_ms(NMESH, stream) if rank == 0 else None
+    plain_fft_ms = ours_r2c_ms(ctx, NMESH) if rank == 0 else None
     # P(k) of the last timed step's three jobs against the FP64 oracle
     # (outside the timed region)
     pk_err = pk_error_vs_oracle(x, y, z, w, last_pk) if rank == 0 and not args.kernels_only else None
@@ -467,6 +491,10 @@ def run_ours(args):
             out["stages"]["fft_r2c"]["cufft_ms"] = round(cufft_ms, 4)
             out["stages"]["fft_r2c"]["cufft_note"] = ("torch.fft.rfftn of a 256^3 FP32 device mesh (cuFFT), CUDA "
                                                       "events, comparison only: not on the product path")
+            out["stages"]["fft_r2c"]["plain_ms"] = round(plain_fft_ms, 4)
+            out["stages"]["fft_r2c"]["plain_note"] = ("cam_fft_r2c alone on the same mesh (no P(k) binning, "
+                                                      "FFTW-layout output), CUDA events; ms_per_job above is the "
+                                                      "jobs' r2c with P(k) binned in its last pass")
         if pk_err is not None:
             out["pk_rel_err"] = pk_err["max"]
             out["pk_rel_err_detail"] = pk_err
@@ -680,6 +708,7 @@ def run_single(args):
             st["frac"] = round(st["achieved_gbs"] / hbm, 4)
     if args.workload == "single512":
         out["stages"]["fft_r2c"]["cufft_ms"] = round(cufft_r2c_ms(n, stream), 4)
+        out["stages"]["fft_r2c"]["plain_ms"] = round(ours_r2c_ms(ctx, n), 4)
     ctx.close()
     if args.workload == "c1":
         out["cpu_ref"] = c1_cpu_reference(x, y, z, n, box, scheme, nb, R, lth)

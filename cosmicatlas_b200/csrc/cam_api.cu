@@ -128,6 +128,26 @@ void check_device_error(cam_ctx *ctx)
     CAM_REQUIRE(h == 0u, CAM_E_CUDA, "a kernel's bulk copy did not complete within its wait limit");
 }
 
+cudaStream_t aux_fork(cam_ctx *ctx)
+{
+    aux_join(ctx);  // a fork left open by an earlier failure
+    CAM_CUDA_TRY(cudaEventRecord(ctx->ev_fork, ctx->stream));
+    CAM_CUDA_TRY(cudaStreamWaitEvent(ctx->aux_stream, ctx->ev_fork, 0));
+    ctx->aux_open = true;
+    return ctx->aux_stream;
+}
+
+void aux_join(cam_ctx *ctx)
+{
+    if (!ctx->aux_open) return;
+    ctx->aux_open = false;
+    CAM_CUDA_TRY(cudaEventRecord(ctx->ev_join, ctx->aux_stream));
+    CAM_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
+}
+
+StreamScope::StreamScope(cam_ctx *ctx, cudaStream_t s) : c(ctx), saved(ctx->stream) { ctx->stream = s; }
+StreamScope::~StreamScope() { c->stream = saved; }
+
 void prof_begin(cam_ctx *ctx, const char *name)
 {
     if (!ctx->prof_on || ctx->capturing) return;
@@ -476,8 +496,14 @@ int cam_ctx_create(int device, size_t hbm_budget, cam_ctx **out)
     c->device = device;
     c->budget = hbm_budget;
     if (cudaSetDevice(device) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->aux_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
         cudaGetLastError();
+        if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+        if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
+        if (c->own_stream) cudaStreamDestroy(c->own_stream);
         delete c;
         return CAM_E_CUDA;
     }
@@ -507,6 +533,12 @@ int cam_ctx_destroy(cam_ctx *ctx)
             cudaFreeHost(ctx->job_pin);
             ctx->job_pin = nullptr;
         }
+        if (ctx->aux_stream) {
+            cudaStreamSynchronize(ctx->aux_stream);
+            cudaStreamDestroy(ctx->aux_stream);
+        }
+        if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+        if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
         if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     }
     delete ctx;

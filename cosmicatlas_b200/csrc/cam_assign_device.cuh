@@ -409,8 +409,15 @@ __device__ __forceinline__ void deposit_record(const uint4 v, const int e[3], co
 #pragma unroll
         for (int a = 0; a < 3; ++a) pos = pos && wa[a][0] >= 0.0f && wa[a][1] >= 0.0f;
     }
-    if (pos && ws < 4194304.0f) deposit_stencil<SCHEME, 0>(wa, ia, in_x, in_y, S0, S1, ws, lo, hi);
-    else if (pos && ws < 4294967296.0f) deposit_stencil<SCHEME, 1>(wa, ia, in_x, in_y, S0, S1, ws, lo, hi);
+    // One conversion path for all lanes of the warp here (the most general
+    // one any of them needs): lanes of a warp hold unrelated records, and
+    // per-lane paths would run one after the other.  Every path gives the
+    // same integer sums.
+    const int tier = (pos && ws < 4194304.0f) ? 0 : ((pos && ws < 4294967296.0f) ? 1 : 2);
+    const unsigned act = __activemask();
+    const int wt = __reduce_max_sync(act, (unsigned)tier);
+    if (wt == 0) deposit_stencil<SCHEME, 0>(wa, ia, in_x, in_y, S0, S1, ws, lo, hi);
+    else if (wt == 1) deposit_stencil<SCHEME, 1>(wa, ia, in_x, in_y, S0, S1, ws, lo, hi);
     else deposit_stencil<SCHEME, 2>(wa, ia, in_x, in_y, S0, S1, ws, lo, hi);
 }
 

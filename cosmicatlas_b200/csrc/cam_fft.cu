@@ -14,7 +14,7 @@
 //           complex FFT plus the r2c untangling (or its inverse for c2r);
 //   cols  : along y or x, tiles of 16 (float) / 8 (double) consecutive
 //           columns x N rows staged in shared memory.
-// Inside a CTA the 1D transforms are mixed-radix (8, 4, 2, 3) Stockham
+// Inside a CTA the 1D transforms are mixed-radix (16, 8, 4, 2, 3) Stockham
 // stages in shared memory.  Each thread keeps its butterflies' inputs in
 // registers across a barrier, so a stage reads and writes the same buffer.
 #include <cuda_runtime.h>
@@ -827,15 +827,21 @@ bool fft_r2c_pk_fused(cam_ctx *ctx, FftPlan *plan, const void *real_in, const do
             // rows [0, g) for the column pass, [g, g + kNumSMs) for the Nyquist plane
             auto *part = static_cast<double *>(
                 scratch(ctx, "pkf.part", (size_t)(g + kNumSMs) * pt.nbins * sizeof(double)));
-            // r2c rows, y columns, the Nyquist plane's y transform, then the
-            // binning x pass and the Nyquist plane's x transform
+            // r2c rows; then the y columns and the binning x pass, and beside
+            // them, on the side stream, the Nyquist plane's y and x
+            // transforms (it is independent of the main planes; its binning,
+            // also on the side stream, and the join are power_finish_fused's)
+            unsigned *errw = device_error_word(ctx);
             rows_impl<float, 0>(ctx, plan, real_in, out.main, out.nyq, n * n, 1, 0, 0, d_sub, 1.0);
+            {
+                StreamScope side(ctx, aux_fork(ctx));
+                rows_impl<float, 2>(ctx, plan, out.nyq, out.nyq, nullptr, n, 1, 0, 0, nullptr, 1.0);
+                cols_impl<float>(ctx, plan, out.nyq, n, n, n, 1, 0, 1, 0, false);
+            }
             cols_impl<float>(ctx, plan, out.main, n, M, M, n, n * M, 1, 0, false);
-            rows_impl<float, 2>(ctx, plan, out.nyq, out.nyq, nullptr, n, 1, 0, 0, nullptr, 1.0);
             CAM_LAUNCH_NAMED(ctx, "fft_cols_pk", kt, g, NTHR, smem, map, td, (int)(M / 16), (int)n, ntiles,
-                             static_cast<const float2 *>(plan->tw), device_error_word(ctx), pt.tab, pt.nbins, pt.btab,
-                             keep ? 1 : 0, part);
-            cols_impl<float>(ctx, plan, out.nyq, n, n, n, 1, 0, 1, 0, false);
+                             static_cast<const float2 *>(plan->tw), errw, pt.tab, pt.nbins, pt.btab, keep ? 1 : 0,
+                             part);
             *d_part = part;
             *nparts = g;
             done = true;

@@ -74,6 +74,12 @@ struct cam_ctx {
     size_t used = 0;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
+    // Side stream for independent work inside one call (the Nyquist plane
+    // of the fused r2c + P(k)), forked from and joined back into `stream`
+    // with two events (see aux_fork / aux_join); created with the context.
+    cudaStream_t aux_stream = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    bool aux_open = false;
     std::string err;
     std::recursive_mutex mu;
     int64_t launches = 0;
@@ -105,6 +111,24 @@ namespace cam {
 
 void prof_begin(cam_ctx *ctx, const char *name);
 void prof_end(cam_ctx *ctx);
+
+// Forks the side stream from the context's stream (the side stream then
+// runs after everything enqueued so far) and returns it; aux_join makes the
+// context's stream wait for everything enqueued on the side stream since.
+// Both are plain event record / wait, so they also work under stream
+// capture.
+cudaStream_t aux_fork(cam_ctx *ctx);
+void aux_join(cam_ctx *ctx);
+// Launches made while a StreamScope lives go to `s` instead of the
+// context's stream.
+struct StreamScope {
+    cam_ctx *c;
+    cudaStream_t saved;
+    StreamScope(cam_ctx *ctx, cudaStream_t s);
+    ~StreamScope();
+    StreamScope(const StreamScope &) = delete;
+    StreamScope &operator=(const StreamScope &) = delete;
+};
 
 // Device word of the context where kernels report a bounded wait that ran
 // out (TMA copies that did not land within their limit); zero otherwise.

@@ -514,7 +514,20 @@ PkDevice power_finish_fused(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &
                             int nparts)
 {
     const int n = (int)s.n, h = n / 2;
-    const PkTables pt = pk_tables(ctx, n, o, nbins);
+    const PkTables pt = pk_tables(ctx, n, o, nbins);  // built before the column pass
+    const int g2 = kNumSMs;
+    const size_t smem = (size_t)(h + 1 + nbins + 1 + (kNyqThreads / 32) * nbins) * sizeof(double);
+    CAM_REQUIRE(smem <= 220 * 1024, CAM_E_UNSUPPORTED, "too many bins for one CTA");
+    double *all = part;  // [nparts + kNumSMs][nbins]: the Nyquist rows follow the column pass's
+    smem_at_least(pk_nyq_kernel, smem);
+    {
+        // on the side stream when the Nyquist plane was transformed there
+        // (fft_r2c_pk_fused), then joined back before anything else reads it
+        StreamScope side(ctx, ctx->aux_open ? ctx->aux_stream : ctx->stream);
+        CAM_LAUNCH_NAMED(ctx, "pk_nyq", pk_nyq_kernel, g2, kNyqThreads, smem, static_cast<const float2 *>(s.nyq), n,
+                         pt.tab, nbins, pt.btab, all + (size_t)nparts * nbins);
+    }
+    aux_join(ctx);
     // Mode counts and shot-noise sums depend on N, the options and the bins
     // only: computed once per key by the binning kernel (its sums of |F|^2
     // are discarded, so the spectrum's contents do not matter) and kept.
@@ -530,13 +543,6 @@ PkDevice power_finish_fused(cam_ctx *ctx, const Spectrum &s, const cam_pk_opts &
         stat.sums = static_cast<double *>(found->second.ptr);
         stat.modes = static_cast<unsigned long long *>(ctx->bufs[k + ".resm"].ptr);
     }
-    const int g2 = kNumSMs;
-    const size_t smem = (size_t)(h + 1 + nbins + 1 + (kNyqThreads / 32) * nbins) * sizeof(double);
-    CAM_REQUIRE(smem <= 220 * 1024, CAM_E_UNSUPPORTED, "too many bins for one CTA");
-    double *all = part;  // [nparts + kNumSMs][nbins]: the Nyquist rows follow the column pass's
-    smem_at_least(pk_nyq_kernel, smem);
-    CAM_LAUNCH_NAMED(ctx, "pk_nyq", pk_nyq_kernel, g2, kNyqThreads, smem, static_cast<const float2 *>(s.nyq), n,
-                     pt.tab, nbins, pt.btab, all + (size_t)nparts * nbins);
     auto *res = static_cast<double *>(scratch(ctx, "pkf.res", (size_t)nbins * 2 * sizeof(double)));
     auto *resm = static_cast<unsigned long long *>(scratch(ctx, "pkf.resm", (size_t)nbins * sizeof(unsigned long long)));
     CAM_LAUNCH_NAMED(ctx, "pk_final", pk_final_fused_kernel, nbins, 256, 0, all, nparts + g2, nbins, stat.sums,

@@ -230,13 +230,29 @@ tidal_y_kernel(typename CTw<T>::t *__restrict__ base, int n, int ncols, int64_t 
     }
 }
 
+// Columns per tile of the pipelined T-web column kernel: the transform
+// precision's 128-byte rows, halved (down to 64-byte rows) until its three
+// tiles fit 200 KB of shared memory (N = 768: 8 float columns, 144 KB).
+template <typename T, int LEN>
+constexpr int tpipe_cols()
+{
+    int w = CTw<T>::kCols;
+    while (w * (int)sizeof(typename CTw<T>::t) > 64 && 3 * LEN * w * (int)sizeof(typename CTw<T>::t) > 200 * 1024)
+        w /= 2;
+    return w;
+}
+template <typename T, int LEN>
+constexpr int tpipe_threads()
+{
+    return LEN > 0 ? fftdev::ct_threads(LEN, tpipe_cols<T, LEN>(), CTw<T>::kPPT) : 1024;
+}
 // CTAs per SM the pipelined T-web column kernel is built for: as many as
 // fit 1024 threads and three tiles each in 200 KB of shared memory.
 template <typename T, int LEN>
 constexpr int tpipe_min_blocks()
 {
-    constexpr int by_thr = 1024 / col_threads<T, LEN>();
-    constexpr int by_smem = (200 * 1024) / (3 * LEN * CTw<T>::kCols * (int)sizeof(typename CTw<T>::t));
+    constexpr int by_thr = 1024 / tpipe_threads<T, LEN>();
+    constexpr int by_smem = (200 * 1024) / (3 * LEN * tpipe_cols<T, LEN>() * (int)sizeof(typename CTw<T>::t));
     constexpr int b = by_thr < by_smem ? by_thr : by_smem;
     return b > 1 ? b : 1;
 }
@@ -255,15 +271,15 @@ constexpr int tpipe_min_blocks()
 // unit's tile base at plane*pstride + column tile*W; full tiles only and
 // 16-byte aligned rows (the host checks).
 template <typename T, int MODE, int LEN, bool FD>
-__global__ void __launch_bounds__(col_threads<T, LEN>(), tpipe_min_blocks<T, LEN>())
+__global__ void __launch_bounds__(tpipe_threads<T, LEN>(), tpipe_min_blocks<T, LEN>())
 tidal_pipe_kernel(const typename CTw<T>::t *src, typename CTw<T>::t *dst, int n, int nct, int64_t nunits,
                   int64_t jstride, int64_t pstride, int64_t ccomp, const typename CTw<T>::t *__restrict__ tw,
                   double gauss_coef, const double *__restrict__ d_mean, int density_input, double scale,
                   const typename CTw<T>::t *__restrict__ sf, int pot)
 {
     using C = typename CTw<T>::t;
-    constexpr int W = CTw<T>::kCols;
-    constexpr int NTHR = col_threads<T, LEN>();
+    constexpr int W = tpipe_cols<T, LEN>();
+    constexpr int NTHR = tpipe_threads<T, LEN>();
     constexpr int CPR = W * (int)sizeof(C) / 16;  // 16-byte chunks per tile row
     constexpr int EPC = 16 / (int)sizeof(C);
     constexpr int TILE = LEN * W;
@@ -357,46 +373,49 @@ tidal_pipe_kernel(const typename CTw<T>::t *src, typename CTw<T>::t *dst, int n,
     fftdev::cp_async_wait<0>();
 }
 
-// FP32 trigonometric eigenvalues of a symmetric 3x3 matrix (O.K. Smith,
-// CACM 4(4):168, 1961), each refined by one Newton step on the FP64
-// characteristic polynomial; returned in descending order.
-__device__ __forceinline__ void eig3(float a00, float a11, float a22, float a01, float a02, float a12,
+// Trigonometric eigenvalues of a symmetric 3x3 matrix (O.K. Smith, CACM
+// 4(4):168, 1961) in FP64 from the FP32 entries, each refined by one Newton
+// step on the FP64 characteristic polynomial; returned in descending
+// order.  FP64 throughout because acos is ill-conditioned next to r = +-1
+// (two equal eigenvalues): an error e in r moves phi by ~sqrt(2e), which
+// for FP32 (e ~ 6e-8) is ~3e-4 of the spread; in FP64 it is ~2e-8.  Only
+// the eigenvalue planes take this path; labels alone use the sign count.
+__device__ __forceinline__ void eig3(float a00f, float a11f, float a22f, float a01f, float a02f, float a12f,
                                      double lam[3])
 {
-    const float p1 = a01 * a01 + a02 * a02 + a12 * a12;
-    const float q = (a00 + a11 + a22) * (1.0f / 3.0f);
-    const float b00 = a00 - q, b11 = a11 - q, b22 = a22 - q;
-    const float p2 = b00 * b00 + b11 * b11 + b22 * b22 + 2.0f * p1;
-    float l[3];
-    if (!(p2 > 0.0f)) {
+    const double a00 = a00f, a11 = a11f, a22 = a22f, a01 = a01f, a02 = a02f, a12 = a12f;
+    const double p1 = a01 * a01 + a02 * a02 + a12 * a12;
+    const double q = (a00 + a11 + a22) * (1.0 / 3.0);
+    const double b00 = a00 - q, b11 = a11 - q, b22 = a22 - q;
+    const double p2 = b00 * b00 + b11 * b11 + b22 * b22 + 2.0 * p1;
+    double l[3];
+    if (!(p2 > 0.0)) {
         l[0] = l[1] = l[2] = q;
     } else {
-        const float pp = sqrtf(p2 * (1.0f / 6.0f));
-        const float det = b00 * (b11 * b22 - a12 * a12) - a01 * (a01 * b22 - a12 * a02) +
-                          a02 * (a01 * a12 - b11 * a02);
-        float r = det / (2.0f * pp * pp * pp);
-        r = fminf(1.0f, fmaxf(-1.0f, r));
-        const float phi = acosf(r) * (1.0f / 3.0f);  // in [0, pi/3]
-        l[0] = q + 2.0f * pp * __cosf(phi);
-        l[2] = q + 2.0f * pp * __cosf(phi + 2.0943951023931954923f);
-        l[1] = 3.0f * q - l[0] - l[2];
+        const double pp = sqrt(p2 * (1.0 / 6.0));
+        const double det = b00 * (b11 * b22 - a12 * a12) - a01 * (a01 * b22 - a12 * a02) +
+                           a02 * (a01 * a12 - b11 * a02);
+        double r = det / (2.0 * pp * pp * pp);
+        r = fmin(1.0, fmax(-1.0, r));
+        const double phi = acos(r) * (1.0 / 3.0);  // in [0, pi/3]
+        l[0] = q + 2.0 * pp * cos(phi);
+        l[2] = q + 2.0 * pp * cos(phi + 2.0943951023931954923);
+        l[1] = 3.0 * q - l[0] - l[2];
     }
     // det(x I - A) = x^3 - c2 x^2 + c1 x - c0, coefficients in FP64 from the
     // FP32 entries (products of two floats are exact in double).
-    const double A00 = a00, A11 = a11, A22 = a22, A01 = a01, A02 = a02, A12 = a12;
-    const double c2 = A00 + A11 + A22;
-    const double c1 = A00 * A11 + A00 * A22 + A11 * A22 - A01 * A01 - A02 * A02 - A12 * A12;
-    const double c0 = A00 * (A11 * A22 - A12 * A12) - A01 * (A01 * A22 - A12 * A02) + A02 * (A01 * A12 - A11 * A02);
-    const double sc = fmax(fabs((double)l[0]), fabs((double)l[2])) + 1e-30;
+    const double c2 = a00 + a11 + a22;
+    const double c1 = a00 * a11 + a00 * a22 + a11 * a22 - a01 * a01 - a02 * a02 - a12 * a12;
+    const double c0 = a00 * (a11 * a22 - a12 * a12) - a01 * (a01 * a22 - a12 * a02) + a02 * (a01 * a12 - a11 * a02);
+    const double sc = fmax(fabs(l[0]), fabs(l[2])) + 1e-30;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         double x = l[k];
         const double f = ((x - c2) * x + c1) * x - c0;
         const double fp = (3.0 * x - 2.0 * c2) * x + c1;
+        // a Newton step only where the root is simple enough to gain from it
         if (fabs(fp) > 1e-6 * sc * sc) {
-            // f is O(eps_f32) relative, so a float reciprocal of f' keeps the
-            // correction accurate to ~1e-7 of itself
-            const double dx = f * (double)__frcp_rn((float)fp);
+            const double dx = f / fp;
             if (fabs(dx) < 1e-4 * sc) x -= dx;
         }
         lam[k] = x;
@@ -812,7 +831,7 @@ bool pipe_launch(cam_ctx *ctx, const char *name, const typename CTw<T>::t *src, 
                  int pot)
 {
     using C = typename CTw<T>::t;
-    constexpr int W = CTw<T>::kCols;
+    constexpr int W = LEN > 0 ? tpipe_cols<T, LEN>() : CTw<T>::kCols;
     if constexpr (LEN == 0 || 3 * LEN * W * sizeof(C) > 200 * 1024) {
         return false;
     } else {
@@ -824,11 +843,11 @@ bool pipe_launch(cam_ctx *ctx, const char *name, const typename CTw<T>::t *src, 
         const size_t smem = 3 * (size_t)LEN * W * sizeof(C);
         smem_at_least(k, smem);
         int per_sm = 0;
-        CAM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, col_threads<T, LEN>(), smem));
+        CAM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, tpipe_threads<T, LEN>(), smem));
         const int nct = (int)(M / W);
         const int64_t nunits = (int64_t)nct * n * (MODE == 0 ? 1 : 3);
         const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>(nunits, (int64_t)kNumSMs * std::max(per_sm, 1)));
-        constexpr int nthr = col_threads<T, LEN>();
+        constexpr int nthr = tpipe_threads<T, LEN>();
         CAM_LAUNCH_NAMED(ctx, name, k, g, nthr, smem, src, dst, (int)n, nct, nunits, jstride, pstride, ccomp, tw, gcoef,
                          d_mean, density, scale, sf, pot);
         return true;
