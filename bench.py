@@ -448,12 +448,20 @@ def run_ours(args):
             "fft_r2c": ["fft_rows_r2c", "fft_cols", "fft_rows_c2c", "fft_cols_pk"],
             "power": ["pk_bin", "pk_final_kernel", "pk_nyq", "pk_final"],
         }
+        # kernels on the side stream run beside the stage's main-stream
+        # kernels: reported per stage, not added to its time
+        side_kernels = {"fft_r2c": ["side.fft_rows_c2c", "side.fft_cols"], "power": ["side.pk_nyq"]}
         stages = {}
         for st, names in stage_kernels.items():
             t = sum(prof.get(nm, (0, 0.0))[1] for nm in names) / jobs_rank
             ach = stage_bytes[st] / (t / 1e3) / 1e9 if t > 0 else 0.0
             stages[st] = {"ms_per_job": round(t, 4), "algorithmic_bytes": stage_bytes[st],
                           "achieved_gbs": round(ach, 1), "frac": round(ach / hbm, 4)}
+            ov = sum(prof.get(nm, (0, 0.0))[1] for nm in side_kernels.get(st, [])) / jobs_rank
+            if ov > 0:
+                stages[st]["overlapped_ms_per_job"] = round(ov, 4)
+                stages[st]["overlapped_note"] = ("the Nyquist plane's kernels, on a side stream beside the "
+                                                 "main-stream kernels above")
         dom = max(stages, key=lambda s: stages[s]["ms_per_job"])
         traffic = ncu_traffic()
         dom_traffic = traffic.get(dom) if isinstance(traffic, dict) else None
@@ -688,11 +696,15 @@ def run_single(args):
                  "fd_table_kernel"],
     }
     k = args.steps
+    side_kernels = {"fft_r2c": ["side.fft_rows_c2c", "side.fft_cols"], "power": ["side.pk_nyq"]}
     stages = {}
     for st, names in stage_kernels.items():
         t = sum(prof.get(nm, (0, 0.0))[1] for nm in names) / k
         stages[st] = {"ms": round(t, 3), "algorithmic_bytes": stage_bytes[st],
                       "achieved_gbs": round(stage_bytes[st] / (t / 1e3) / 1e9, 1) if t > 0 else None}
+        ov = sum(prof.get(nm, (0, 0.0))[1] for nm in side_kernels.get(st, [])) / k
+        if ov > 0:
+            stages[st]["overlapped_ms"] = round(ov, 3)
     # the T-web's y-pass runs through fft_cols too: attribute by launch counts is not possible
     # from totals, so report the raw kernel table alongside
     out = {"workload": args.workload, "tweb_method": args.tweb_method, "mesh": n, "particles": npart,

@@ -161,7 +161,7 @@ void prof_begin(cam_ctx *ctx, const char *name)
         }
         return e;
     };
-    ProfRecord r{name, take(), take()};
+    ProfRecord r{name, take(), take(), ctx->stream == ctx->aux_stream};
     CAM_CUDA_TRY(cudaEventRecord(r.start, ctx->stream));
     ctx->prof_pending.push_back(r);
 }
@@ -180,7 +180,7 @@ static void prof_collect(cam_ctx *ctx)
     for (auto &r : ctx->prof_pending) {
         float ms = 0.f;
         CAM_CUDA_TRY(cudaEventElapsedTime(&ms, r.start, r.stop));
-        auto &acc = ctx->prof_acc[r.name];
+        auto &acc = ctx->prof_acc[r.side ? std::string("side.") + r.name : std::string(r.name)];
         acc.first += 1;
         acc.second += ms;
         ctx->prof_pool.push_back(r.start);

@@ -64,6 +64,7 @@ struct FftPlan;  // cam_fft.cu
 struct ProfRecord {
     const char *name;
     cudaEvent_t start, stop;
+    bool side;  // launched on the side stream (reported as "side.<name>")
 };
 
 }  // namespace cam
