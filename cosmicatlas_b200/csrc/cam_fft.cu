@@ -265,10 +265,17 @@ fft_cols_tma_kernel(const __grid_constant__ CUtensorMap map, TileDims td, int nc
 // and shot-noise sums do not depend on the data; the host takes them from a
 // table.  store = 0: the transformed tiles are not written back (a job that
 // needs only P(k)).
+// Columns per tile: 16 (128-byte rows); 8 from N = 512 on, so that two
+// CTAs of the longer transforms share an SM.
+template <int LEN>
+constexpr int pk_pass_cols()
+{
+    return LEN >= 512 ? 8 : 16;
+}
 template <int LEN>
 constexpr int pk_pass_threads()
 {
-    return fftdev::ct_threads(LEN, 16, 16);
+    return fftdev::ct_threads(LEN, pk_pass_cols<LEN>(), 16);
 }
 // CTAs per SM the binning pass is built for: two tiles plus the tables and
 // warp bins of N/2 bins in 222 KB (the SM's 228 KB less 1 KB per CTA), at
@@ -279,7 +286,7 @@ constexpr int pk_pass_min_blocks()
 {
     constexpr int nthr = pk_pass_threads<LEN>();
     constexpr int by_thr = 1024 / nthr;
-    constexpr int bytes = 2 * LEN * 16 * 8 + (nthr / 32) * (LEN / 2) * 8 + (LEN / 2 + 1) * 4;
+    constexpr int bytes = 2 * LEN * pk_pass_cols<LEN>() * 8 + (nthr / 32) * (LEN / 2) * 8 + (LEN / 2 + 1) * 4;
     constexpr int by_smem = (222 * 1024) / bytes;
     constexpr int b = by_thr < by_smem ? by_thr : by_smem;
     return b > 1 ? b : 1;
@@ -294,7 +301,8 @@ fft_cols_tma_pk_kernel(const __grid_constant__ CUtensorMap map, TileDims td, int
                        double *__restrict__ part /* [grid][nbins] */)
 {
     using C = float2;
-    constexpr int W = 16;
+    constexpr int W = pk_pass_cols<LEN>();
+    constexpr int RPW = 32 / W;  // rows a warp bins at a time
     constexpr int NTHR = pk_pass_threads<LEN>();
     constexpr int NWARP = NTHR / 32;
     constexpr int NBOX = (LEN + 255) / 256;
@@ -368,19 +376,20 @@ fft_cols_tma_pk_kernel(const __grid_constant__ CUtensorMap map, TileDims td, int
                 tma::bulk_commit();
             }
         }
-        // bin the tile: plane = j, columns c0 .. c0 + 15.  A mode's
+        // bin the tile: plane = j, columns c0 .. c0 + W - 1.  A mode's
         // |F|^2 / W^2 is formed in FP32 (one rounding per factor, ~2e-7)
-        // and summed over its run of at most 16 lanes in FP32; each run's
-        // sum is added to the warp's FP64 bin.
+        // and summed over its run of at most W lanes in FP32; each run's
+        // sum is added to the warp's FP64 bin, the rows' heads one row at a
+        // time (two rows' runs may share a bin).
         const int j = plane, c0 = x / 2;
         if (j != H) {
             const int b = j <= H ? j : N - j;
-            const int kk = lane & 15;
+            const int kk = lane % W;
             const int c = c0 + kk;
             const int qbc = b * b + c * c;
             const float wbc = tw2[b] * tw2[c];
-            for (int pr = warp; pr < LEN / 2; pr += NWARP) {
-                const int i = 2 * pr + (lane >> 4);
+            for (int pr = warp; pr < LEN / RPW; pr += NWARP) {
+                const int i = RPW * pr + lane / W;
                 const int a = i <= H ? i : N - i;
                 const int bin = __ldg(btab + (a * a + qbc));
                 float v = 0.0f;
@@ -394,15 +403,16 @@ fft_cols_tma_pk_kernel(const __grid_constant__ CUtensorMap map, TileDims td, int
                 const unsigned later = heads & ~((2u << lane) - 1u);
                 const int end = later ? __ffs((int)later) - 1 : 32;
 #pragma unroll
-                for (int off = 1; off < 16; off <<= 1) {
+                for (int off = 1; off < W; off <<= 1) {
                     const float o = __shfl_down_sync(0xffffffffu, v, off);
                     if (lane + off < end) v += o;
                 }
                 const bool add = head && bin >= 0 && bin < nbins;
-                if (add && lane < 16) mysum[bin] += (double)v;
-                __syncwarp();
-                if (add && lane >= 16) mysum[bin] += (double)v;
-                __syncwarp();
+#pragma unroll
+                for (int r = 0; r < RPW; ++r) {
+                    if (add && lane / W == r) mysum[bin] += (double)v;
+                    __syncwarp();
+                }
             }
         }
         __syncthreads();  // the tile is reloaded two iterations on
@@ -804,25 +814,26 @@ bool fft_r2c_pk_fused(cam_ctx *ctx, FftPlan *plan, const void *real_in, const do
     bool done = false;
     dispatch_fft_len(n, [&](auto lc) {
         constexpr int LEN = decltype(lc)::value;
-        if constexpr (LEN >= 32 && 2 * LEN * 16 * 8 <= 200 * 1024) {
+        if constexpr (LEN >= 32 && 2 * LEN * pk_pass_cols<LEN>() * 8 <= 200 * 1024) {
             constexpr int NTHR = pk_pass_threads<LEN>();
-            const size_t smem = (size_t)2 * LEN * 16 * 8 + (size_t)(NTHR / 32) * pt.nbins * sizeof(double) +
-                                (size_t)(LEN / 2 + 1) * sizeof(float);
+            const size_t smem = (size_t)2 * LEN * pk_pass_cols<LEN>() * 8 +
+                                (size_t)(NTHR / 32) * pt.nbins * sizeof(double) + (size_t)(LEN / 2 + 1) * sizeof(float);
             if (smem > 220 * 1024) return;
             // x pass over main: 4D view (scalar column, row i, plane j, 1)
             CUtensorMap map;
             TileDims td{0};
             uint64_t dims[4], strides[3];
             uint32_t box[4];
-            tile_map_layout(2 * M, n, n * M * 8, n, M * 8, 1, 0, 32u, (uint32_t)(LEN / ((LEN + 255) / 256)), dims,
-                            strides, box, td.pos);
+            constexpr int WC = pk_pass_cols<LEN>();
+            tile_map_layout(2 * M, n, n * M * 8, n, M * 8, 1, 0, (uint32_t)(2 * WC), (uint32_t)(LEN / ((LEN + 255) / 256)),
+                            dims, strides, box, td.pos);
             if (!make_tensor_map_4d(&map, false, out.main, dims, strides, box)) return;
             auto kt = fft_cols_tma_pk_kernel<LEN>;
             smem_at_least(kt, smem);
             int per_sm = 0;
             CAM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kt, NTHR, smem));
             if (per_sm < 1) return;
-            const int64_t ntiles = n * (M / 16);
+            const int64_t ntiles = n * (M / WC);
             const int g = (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)kNumSMs * per_sm));
             // rows [0, g) for the column pass, [g, g + kNumSMs) for the Nyquist plane
             auto *part = static_cast<double *>(
@@ -839,7 +850,7 @@ bool fft_r2c_pk_fused(cam_ctx *ctx, FftPlan *plan, const void *real_in, const do
                 cols_impl<float>(ctx, plan, out.nyq, n, n, n, 1, 0, 1, 0, false);
             }
             cols_impl<float>(ctx, plan, out.main, n, M, M, n, n * M, 1, 0, false);
-            CAM_LAUNCH_NAMED(ctx, "fft_cols_pk", kt, g, NTHR, smem, map, td, (int)(M / 16), (int)n, ntiles,
+            CAM_LAUNCH_NAMED(ctx, "fft_cols_pk", kt, g, NTHR, smem, map, td, (int)(M / WC), (int)n, ntiles,
                              static_cast<const float2 *>(plan->tw), errw, pt.tab, pt.nbins, pt.btab, keep ? 1 : 0,
                              part);
             *d_part = part;

@@ -233,6 +233,8 @@ tidal_y_kernel(typename CTw<T>::t *__restrict__ base, int n, int ncols, int64_t 
 // Columns per tile of the pipelined T-web column kernel: the transform
 // precision's 128-byte rows, halved (down to 64-byte rows) until its three
 // tiles fit 200 KB of shared memory (N = 768: 8 float columns, 144 KB).
+// Halving them at N = 512 too, for two CTAs per SM, measured slower (x pass
+// 0.87 -> 0.95 ms, y pass 1.60 -> 1.68 ms at 512^3).
 template <typename T, int LEN>
 constexpr int tpipe_cols()
 {

@@ -245,12 +245,13 @@ def test_tma_staged_columns_equal_cp_async(ctx, n, prec):
 
 
 @pytest.mark.parametrize("scheme", [NGP, CIC, TSC])
-@pytest.mark.parametrize("n,nbins,ndel", [(64, 32, 1.0), (128, 64, 1.0), (96, 30, 1.5)])
+@pytest.mark.parametrize("n,nbins,ndel", [(64, 32, 1.0), (128, 64, 1.0), (96, 30, 1.5),
+                                          (512, 256, 1.0), (768, 256, 1.5)])  # 8-column tiles from 512 on
 def test_job_pk_binned_in_fft_equals_separate_binning(ctx, scheme, n, nbins, ndel):
     # cam_job_run bins P(k) inside the FFT's last column pass; the separate
     # binning kernel over the stored spectrum gives the same mode counts and
     # the same sums up to rounding: the fused pass forms each mode's
-    # |F|^2 / W^2 in FP32 and sums runs of at most 16 modes in FP32 (a few
+    # |F|^2 / W^2 in FP32 and sums runs of at most one tile row (16 or 8 modes) in FP32 (a few
     # units of 2^-24 per run) before its FP64 bins; the separate one is FP64
     # throughout
     box = 800.0
