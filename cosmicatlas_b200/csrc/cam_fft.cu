@@ -265,12 +265,13 @@ fft_cols_tma_kernel(const __grid_constant__ CUtensorMap map, TileDims td, int nc
 // and shot-noise sums do not depend on the data; the host takes them from a
 // table.  store = 0: the transformed tiles are not written back (a job that
 // needs only P(k)).
-// Columns per tile: 16 (128-byte rows); 8 from N = 512 on, so that two
-// CTAs of the longer transforms share an SM.
+// Columns per tile: 16 (128-byte rows); 8 from N = 768 on, where two
+// 16-column tiles and the warps' bins would not fit one CTA's shared memory
+// (8 at N = 512, for two CTAs per SM, measured 0.585 -> 0.600 ms).
 template <int LEN>
 constexpr int pk_pass_cols()
 {
-    return LEN >= 512 ? 8 : 16;
+    return LEN >= 768 ? 8 : 16;
 }
 template <int LEN>
 constexpr int pk_pass_threads()

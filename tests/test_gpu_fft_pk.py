@@ -246,7 +246,7 @@ def test_tma_staged_columns_equal_cp_async(ctx, n, prec):
 
 @pytest.mark.parametrize("scheme", [NGP, CIC, TSC])
 @pytest.mark.parametrize("n,nbins,ndel", [(64, 32, 1.0), (128, 64, 1.0), (96, 30, 1.5),
-                                          (512, 256, 1.0), (768, 256, 1.5)])  # 8-column tiles from 512 on
+                                          (512, 256, 1.0), (768, 256, 1.5)])  # 8-column tiles at 768
 def test_job_pk_binned_in_fft_equals_separate_binning(ctx, scheme, n, nbins, ndel):
     # cam_job_run bins P(k) inside the FFT's last column pass; the separate
     # binning kernel over the stored spectrum gives the same mode counts and
