@@ -310,7 +310,7 @@ __device__ __forceinline__ void add_fixed(uint32_t *lo, uint32_t *hi, float v)
 // and the nearest halo index, so it adds nothing.  Along an axis that one
 // brick spans (nb = 1) the stencil wraps periodically inside the brick.
 template <int SCHEME>
-__device__ __forceinline__ void axis_stencil(uint32_t word, int e, bool whole, float wa[3], int ia[3], int &inside)
+__device__ __forceinline__ void axis_stencil(uint32_t word, int e, bool whole, float wa[3], int ia[3])
 {
     using St = Stencil<SCHEME>;
     int cl;
@@ -327,7 +327,6 @@ __device__ __forceinline__ void axis_stencil(uint32_t word, int e, bool whole, f
         wa[1] = 0.75f - t * t;
         wa[2] = 0.5f * hp * hp;
     }
-    inside = 0;
 #pragma unroll
     for (int i = 0; i < St::W; ++i) {
         int lc = cl + St::FIRST + i;
@@ -337,7 +336,6 @@ __device__ __forceinline__ void axis_stencil(uint32_t word, int e, bool whole, f
             wa[i] = 0.0f;
             lc = lc < -1 ? -1 : e;
         }
-        if (whole || (lc >= 0 && lc < e)) inside |= 1 << i;
         ia[i] = lc + 1;
     }
 }
@@ -357,20 +355,19 @@ __device__ __forceinline__ void add_nonneg(uint32_t *lo, uint32_t *hi, float v)
 }
 
 // TIER 0: every contribution < 2^22 and >= 0; 1: < 2^32 and >= 0; 2: any.
-// Stencil rows (i, j) that lie in the halo along x or y are skipped
-// (inside_x, inside_y: bit i set if point i is inside the brick); along z
-// the halo cells are written and discarded.
+// The whole stencil is written, halo cells included (they are discarded):
+// skipping the stencil rows that lie in the halo along x or y saved
+// atomics but cost more in branches (TSC deposit 0.257 -> 0.304 ms per
+// 256^3 job with the skip).
 template <int SCHEME, int TIER>
-__device__ __forceinline__ void deposit_stencil(const float wa[3][3], const int ia[3][3], int inside_x, int inside_y,
-                                                int S0, int S1, float ws, uint32_t *lo, uint32_t *hi)
+__device__ __forceinline__ void deposit_stencil(const float wa[3][3], const int ia[3][3], int S0, int S1, float ws,
+                                                uint32_t *lo, uint32_t *hi)
 {
     using St = Stencil<SCHEME>;
 #pragma unroll
     for (int i = 0; i < St::W; ++i) {
-        if (!((inside_x >> i) & 1)) continue;
 #pragma unroll
         for (int j = 0; j < St::W; ++j) {
-            if (!((inside_y >> j) & 1)) continue;
             const float wij = ws * wa[0][i] * wa[1][j];
             const int row = ia[0][i] * S0 + ia[1][j] * S1;
 #pragma unroll
@@ -395,11 +392,9 @@ __device__ __forceinline__ void deposit_record(const uint4 v, const int e[3], co
 {
     float wa[3][3];
     int ia[3][3];
-    int in_x, in_y, in_z;
-    axis_stencil<SCHEME>(v.x, e[0], whole[0], wa[0], ia[0], in_x);
-    axis_stencil<SCHEME>(v.y, e[1], whole[1], wa[1], ia[1], in_y);
-    axis_stencil<SCHEME>(v.z, e[2], whole[2], wa[2], ia[2], in_z);
-    (void)in_z;
+    axis_stencil<SCHEME>(v.x, e[0], whole[0], wa[0], ia[0]);
+    axis_stencil<SCHEME>(v.y, e[1], whole[1], wa[1], ia[1]);
+    axis_stencil<SCHEME>(v.z, e[2], whole[2], wa[2], ia[2]);
     const float ws = (__uint_as_float(v.w) * f1) * f2;
     bool pos = nonneg;
     if (SCHEME == CAM_TSC) {
@@ -416,9 +411,9 @@ __device__ __forceinline__ void deposit_record(const uint4 v, const int e[3], co
     const int tier = (pos && ws < 4194304.0f) ? 0 : ((pos && ws < 4294967296.0f) ? 1 : 2);
     const unsigned act = __activemask();
     const int wt = __reduce_max_sync(act, (unsigned)tier);
-    if (wt == 0) deposit_stencil<SCHEME, 0>(wa, ia, in_x, in_y, S0, S1, ws, lo, hi);
-    else if (wt == 1) deposit_stencil<SCHEME, 1>(wa, ia, in_x, in_y, S0, S1, ws, lo, hi);
-    else deposit_stencil<SCHEME, 2>(wa, ia, in_x, in_y, S0, S1, ws, lo, hi);
+    if (wt == 0) deposit_stencil<SCHEME, 0>(wa, ia, S0, S1, ws, lo, hi);
+    else if (wt == 1) deposit_stencil<SCHEME, 1>(wa, ia, S0, S1, ws, lo, hi);
+    else deposit_stencil<SCHEME, 2>(wa, ia, S0, S1, ws, lo, hi);
 }
 
 // Pass 4: one CTA per brick, cell sums in 64-bit fixed point of quantum
