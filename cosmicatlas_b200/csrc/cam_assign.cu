@@ -253,14 +253,16 @@ deposit_kernel(const uint4 *__restrict__ payload, const uint32_t *__restrict__ s
     const int s = fixed_scale(wstat, weighted, end - beg);
     // 2^s as two exact factors (s may exceed the float exponent range)
     const float f1 = scalbnf(1.0f, s / 2), f2 = scalbnf(1.0f, s - s / 2);
-    // two records per thread per iteration: both loads are in flight before
-    // the shared-memory atomics of the first one
-    for (uint32_t p = beg + threadIdx.x; p < end; p += 2 * blockDim.x) {
-        const uint4 va = payload[p];
-        const bool has_b = p + blockDim.x < end;
-        const uint4 vb = has_b ? payload[p + blockDim.x] : make_uint4(0u, 0u, 0u, 0u);
-        deposit_record<SCHEME>(va, e, whole, S0, S1, f1, f2, nonneg, lo, hi);
-        if (has_b) deposit_record<SCHEME>(vb, e, whole, S0, S1, f1, f2, nonneg, lo, hi);
+    // one record per iteration, the next one's load in flight meanwhile; a
+    // single inlined copy of the stencil (three conversion paths of up to 27
+    // cells each) keeps the loop within the instruction cache
+    uint32_t p = beg + threadIdx.x;
+    uint4 v = p < end ? payload[p] : make_uint4(0u, 0u, 0u, 0u);
+    for (; p < end; p += blockDim.x) {
+        const uint32_t pn = p + blockDim.x;
+        const uint4 vn = pn < end ? payload[pn] : make_uint4(0u, 0u, 0u, 0u);
+        deposit_record<SCHEME>(v, e, whole, S0, S1, f1, f2, nonneg, lo, hi);
+        v = vn;
     }
     __syncthreads();
 
