@@ -1164,7 +1164,12 @@ int cam_job_run(cam_ctx *ctx, const cam_job_desc *job, cam_job_result *res)
             CAM_CUDA_TRY(cudaMemcpyAsync(herr, derr, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
             CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
             CAM_REQUIRE(*herr == 0u, CAM_E_CUDA, "a kernel's bulk copy did not complete within its wait limit");
-            if (defer && (hstats[3] & 0xffffffffu)) return true;
+            if (defer && (hstats[3] & 0xffffffffu)) {
+                // a slab (or the payload estimate) was too small: larger
+                // slabs for the next jobs of this context, and an exact run
+                ctx->slab_ratio = std::min(64.0, ctx->slab_ratio * 2.0);
+                return true;
+            }
             if (d.w) {
                 const unsigned wbits = (unsigned)(hstats[1] & 0xffffffffu);
                 CAM_REQUIRE(wbits < 0x7f800000u, CAM_E_NONFINITE, "a particle weight is NaN or infinite");

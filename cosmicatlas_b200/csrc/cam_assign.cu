@@ -93,12 +93,14 @@ __device__ __forceinline__ void for_chunk(const float *__restrict__ x, const flo
 //             not depend on it.
 // VEC: 16-byte aligned arrays, four particles per thread per iteration
 // (float4 loads).
-template <int SCHEME, bool SCATTER, bool SMEM, bool VEC>
+// SLAB (scatter only): records into per-brick slabs of `slab` records, the
+// weight statistics and lost count gathered here (no count pass).
+template <int SCHEME, bool SCATTER, bool SMEM, bool VEC, bool SLAB = false>
 __global__ void __launch_bounds__(kBinThreads)
 bin_kernel(const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z,
            const float *__restrict__ w, int64_t np, int64_t chunk, AssignGeom g, int nb,
            uint32_t *__restrict__ table, uint4 *__restrict__ payload, unsigned long long *__restrict__ lost,
-           unsigned int *__restrict__ wmax_bits, uint64_t cap, unsigned int *__restrict__ ovf)
+           unsigned int *__restrict__ wmax_bits, uint64_t cap, unsigned int *__restrict__ ovf, uint32_t slab)
 {
     extern __shared__ uint32_t hist[];
     constexpr bool kHist = SMEM && !SCATTER;
@@ -114,14 +116,15 @@ bin_kernel(const float *__restrict__ x, const float *__restrict__ y, const float
     auto one = [&](float px, float py, float pz, float wt) {
         if (SCATTER)
             bin_one<SCHEME, true, false>(px, py, pz, wt, weighted, g, G, blk, hist, table, payload, cap, ovf,
-                                         my_lost, my_wmax, my_neg);
+                                         my_lost, my_wmax, my_neg, SLAB ? &my_wminc : nullptr, SLAB ? slab : 0u);
         else
             count_one<SCHEME, kHist>(px, py, pz, wt, weighted, g, hist, table, my_lost, my_wmax, my_neg,
                                      my_wminc);
     };
     for_chunk<VEC>(x, y, z, w, (int64_t)blk * chunk, min(np, (int64_t)blk * chunk + chunk), one);
-    if (!SCATTER) {
-        // Warp reductions, one atomic per warp.
+    if (!SCATTER || SLAB) {
+        // Warp reductions, one atomic per warp (the scatter's when it writes
+        // slabs: there is no count pass then).
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) {
             my_lost += __shfl_down_sync(0xffffffffu, my_lost, off);
@@ -198,6 +201,19 @@ brick_offsets_kernel(uint32_t *__restrict__ padded, int nb, uint32_t *__restrict
 }
 
 // counts[b] = padded[b * kCursorStride] (contiguous, for the scan).
+// The largest brick record count, start[b + 1] - start[b], into *out
+// (atomicMax; *out zeroed before).
+__global__ void __launch_bounds__(256)
+brick_max_kernel(const uint32_t *__restrict__ start, int nb, unsigned int *__restrict__ out)
+{
+    unsigned m = 0u;
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x)
+        m = max(m, start[b + 1] - start[b]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
+}
+
 __global__ void compact_counts_kernel(const uint32_t *__restrict__ padded, int nb, uint32_t *__restrict__ counts)
 {
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x)
@@ -221,7 +237,8 @@ template <int SCHEME, typename OutT>
 __global__ void __launch_bounds__(kDepositThreads, 2)
 deposit_kernel(const uint4 *__restrict__ payload, const uint32_t *__restrict__ start, uint32_t nrec,
                AssignGeom g, const unsigned int *__restrict__ wstat, int weighted,
-               OutT *__restrict__ mesh, double *__restrict__ brick_sum)
+               OutT *__restrict__ mesh, double *__restrict__ brick_sum, uint32_t slab,
+               const uint32_t *__restrict__ slab_count)
 {
     extern __shared__ uint32_t tile32[];
     __shared__ long long red[kDepositThreads / 32];
@@ -247,8 +264,11 @@ deposit_kernel(const uint4 *__restrict__ payload, const uint32_t *__restrict__ s
     }
     __syncthreads();
 
-    // records beyond the payload's capacity nrec were not written (overflow flag)
-    const uint32_t beg = min(start[B], nrec), end = min(start[B + 1], nrec);
+    // records beyond the payload's capacity nrec were not written (overflow
+    // flag); with slabs, the brick's records are the first of its slab (the
+    // host keeps every slab index below 2^32)
+    const uint32_t beg = slab ? (uint32_t)B * slab : min(start[B], nrec);
+    const uint32_t end = slab ? beg + min(slab_count[(int64_t)B * kCursorStride], slab) : min(start[B + 1], nrec);
     const bool nonneg = !weighted || wstat[1] == 0u;
     const int s = fixed_scale(wstat, weighted, end - beg);
     // 2^s as two exact factors (s may exceed the float exponent range)
@@ -392,32 +412,64 @@ static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const floa
     CAM_CUDA_TRY(cudaMemsetAsync(table, 0, (size_t)nb * kCursorStride * sizeof(uint32_t), ctx->stream));
     CAM_CUDA_TRY(cudaMemsetAsync(stats, 0, 64, ctx->stream));
 
+    // Expected records per particle of a uniform catalogue: a stencil
+    // crosses a face of a brick of extent b with probability (W-1)/b per
+    // axis; at most two bricks per axis.
+    double f = 1.0;
+    uint64_t per = 1;
+    for (int a = 0; a < 3; ++a) {
+        if (SCHEME == CAM_NGP || g.nb[a] == 1) continue;
+        f *= 1.0 + std::min(1.0, (double)(Stencil<SCHEME>::W - 1) / g.b[a]);
+        per *= 2;
+    }
+    // Slabs (deferred jobs): every brick gets a fixed slab of the payload,
+    // sized from the uniform expectation times a ratio that grows when a
+    // slab overflows (the job then reruns exactly) and from the largest
+    // brick an exact run has seen; no count pass and no scan then, and the
+    // scatter gathers the statistics.  Only while the slabs stay within four
+    // times the expected payload and 2^32 records.
+    uint32_t slab = 0;
+    if (out.defer && !ctx->sync_free && np > 0) {
+        const double est_brick = (double)np * f / (double)nb;
+        uint64_t cap = (uint64_t)std::ceil(ctx->slab_ratio * est_brick);
+        cap = std::max<uint64_t>(cap, ctx->slab_hint + ctx->slab_hint / 8);
+        cap = (cap + 16 + 3) & ~(uint64_t)3;
+        const uint64_t est_total = (uint64_t)((double)np * f * 1.25) + 65536;
+        if ((uint64_t)nb * cap < (1ull << 32) && (uint64_t)nb * cap <= 4 * est_total) slab = (uint32_t)cap;
+    }
+
     const size_t hsmem = smem_hist ? (size_t)nb * sizeof(uint32_t) : 0;
     auto count_k = smem_hist ? (vec ? bin_kernel<SCHEME, false, true, true> : bin_kernel<SCHEME, false, true, false>)
                              : (vec ? bin_kernel<SCHEME, false, false, true> : bin_kernel<SCHEME, false, false, false>);
-    auto scatter_k = vec ? bin_kernel<SCHEME, true, false, true> : bin_kernel<SCHEME, true, false, false>;
-    smem_at_least(count_k, hsmem);
-    CAM_LAUNCH_NAMED(ctx, "assign_bin_count", count_k, G, kBinThreads, hsmem, x, y, z, w, np, chunk, g, (int)nb,
-                     table, (uint4 *)nullptr, d_lost, d_wmax, (uint64_t)0, d_ovf);
-    if (nb <= (int64_t)kOffThreads * kOffItems) {
-        CAM_LAUNCH_NAMED(ctx, "assign_starts", brick_offsets_kernel, 1, kOffThreads, 0, table, (int)nb, start, d_total);
-    } else {
-        auto *counts = static_cast<uint32_t *>(scratch(ctx, "asg.counts", (size_t)nb * sizeof(uint32_t)));
-        const unsigned sg = (unsigned)std::min<int64_t>((nb + 256) / 256, 1024);
-        CAM_LAUNCH_NAMED(ctx, "assign_starts", compact_counts_kernel, sg, 256, 0, table, (int)nb, counts);
-        exclusive_scan_u32(ctx, counts, nb, d_total);
-        CAM_LAUNCH_NAMED(ctx, "assign_starts", brick_starts_kernel, sg, 256, 0, counts, (int)nb, d_total, start,
-                         table);
+    auto scatter_k = slab ? (vec ? bin_kernel<SCHEME, true, false, true, true> : bin_kernel<SCHEME, true, false, false, true>)
+                          : (vec ? bin_kernel<SCHEME, true, false, true> : bin_kernel<SCHEME, true, false, false>);
+    if (!slab) {
+        smem_at_least(count_k, hsmem);
+        CAM_LAUNCH_NAMED(ctx, "assign_bin_count", count_k, G, kBinThreads, hsmem, x, y, z, w, np, chunk, g, (int)nb,
+                         table, (uint4 *)nullptr, d_lost, d_wmax, (uint64_t)0, d_ovf, 0u);
+        if (nb <= (int64_t)kOffThreads * kOffItems) {
+            CAM_LAUNCH_NAMED(ctx, "assign_starts", brick_offsets_kernel, 1, kOffThreads, 0, table, (int)nb, start,
+                             d_total);
+        } else {
+            auto *counts = static_cast<uint32_t *>(scratch(ctx, "asg.counts", (size_t)nb * sizeof(uint32_t)));
+            const unsigned sg = (unsigned)std::min<int64_t>((nb + 256) / 256, 1024);
+            CAM_LAUNCH_NAMED(ctx, "assign_starts", compact_counts_kernel, sg, 256, 0, table, (int)nb, counts);
+            exclusive_scan_u32(ctx, counts, nb, d_total);
+            CAM_LAUNCH_NAMED(ctx, "assign_starts", brick_starts_kernel, sg, 256, 0, counts, (int)nb, d_total, start,
+                             table);
+        }
     }
 
     uint64_t total = 0;
-    if (ctx->sync_free) {
+    if (slab) {
+        total = (uint64_t)nb * slab;
+        out.n_lost = -1;
+        out.n_in = -1;
+    } else if (ctx->sync_free) {
         // No host round trip (stream capture): size the payload for the
         // provable bound, one record per touched brick and at most two
         // bricks per axis.  Lost count and max |w| stay on the device
         // (asg.stats) for the caller to read back with the results.
-        int per = 1;
-        for (int a = 0; a < 3; ++a) per *= (SCHEME == CAM_NGP || g.nb[a] == 1) ? 1 : 2;
         total = (uint64_t)np * per;
         CAM_REQUIRE(total < (1ull << 32), CAM_E_UNSUPPORTED, "payload bound exceeds 2^32 records");
         out.n_lost = -1;
@@ -428,13 +480,6 @@ static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const floa
         // probability (W-1)/b per axis) with a 25% margin, never below what
         // this context used before nor above the provable bound.  The
         // scatter flags records past it; the caller then reruns.
-        double f = 1.0;
-        uint64_t per = 1;
-        for (int a = 0; a < 3; ++a) {
-            if (SCHEME == CAM_NGP || g.nb[a] == 1) continue;
-            f *= 1.0 + std::min(1.0, (double)(Stencil<SCHEME>::W - 1) / g.b[a]);
-            per *= 2;
-        }
         const uint64_t bound = (uint64_t)np * per;
         uint64_t est = (uint64_t)((double)np * f * 1.25) + 65536;
         est = std::min(bound, std::max(est, ctx->asg_cap));
@@ -443,12 +488,16 @@ static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const floa
         out.n_lost = -1;
         out.n_in = -1;
     } else {
-        // Payload size and diagnostics back to the host (one synchronisation).
-        unsigned long long hstats[3] = {0, 0, 0};
+        // Payload size and diagnostics back to the host (one synchronisation),
+        // with the largest brick's record count for later slabs.
+        CAM_LAUNCH_NAMED(ctx, "assign_starts", brick_max_kernel, 64, 256, 0, start, (int)nb,
+                         reinterpret_cast<unsigned int *>(stats + 5));
+        unsigned long long hstats[6] = {0, 0, 0, 0, 0, 0};
         CAM_CUDA_TRY(cudaMemcpyAsync(hstats, stats, sizeof(hstats), cudaMemcpyDeviceToHost, ctx->stream));
         CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
         total = (uint32_t)(hstats[2] & 0xffffffffu);
         ctx->asg_cap = std::max<uint64_t>(ctx->asg_cap, total);  // deferred runs size from it
+        ctx->slab_hint = std::max<uint64_t>(ctx->slab_hint, hstats[5] & 0xffffffffu);
         const unsigned int wmax_bits = (unsigned int)(hstats[1] & 0xffffffffu);
         CAM_REQUIRE(!w || wmax_bits < 0x7f800000u, CAM_E_NONFINITE, "a particle weight is NaN or infinite");
         out.n_lost = (int64_t)hstats[0];
@@ -457,7 +506,7 @@ static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const floa
 
     uint4 *payload = static_cast<uint4 *>(scratch(ctx, "asg.payload", std::max<size_t>(total, 1) * sizeof(uint4)));
     CAM_LAUNCH_NAMED(ctx, "assign_bin_scatter", scatter_k, G2, kScatterThreads, 0, x, y, z, w, np, chunk2, g, (int)nb,
-                     table, payload, d_lost, d_wmax, total, d_ovf);
+                     table, payload, d_lost, d_wmax, total, d_ovf, slab);
 
     const size_t smem = (size_t)(g.b[0] + 2) * (g.b[1] + 2) * (g.b[2] + 2) * 2 * sizeof(uint32_t);
     CAM_REQUIRE(smem <= 110 * 1024, CAM_E_UNSUPPORTED, "brick tile too large");
@@ -465,7 +514,8 @@ static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const floa
     auto launch_dep = [&](auto kern, auto *mesh) {
         smem_at_least(kern, smem);
         CAM_LAUNCH_NAMED(ctx, "assign_deposit", kern, (unsigned)nb, kDepositThreads, smem, payload, start,
-                         (uint32_t)std::min<uint64_t>(total, 0xffffffffull), g, d_wmax, weighted, mesh, bsum);
+                         (uint32_t)std::min<uint64_t>(total, 0xffffffffull), g, d_wmax, weighted, mesh, bsum, slab,
+                         table);
     };
     if (out.precision == CAM_F32)
         launch_dep(deposit_kernel<SCHEME, float>, static_cast<float *>(out.mesh));

@@ -179,13 +179,17 @@ __device__ __forceinline__ void count_one(float px, float py, float pz, float wt
     }
 }
 
-// One particle of pass 3 (see bin_kernel).
+// One particle of pass 3 (see bin_kernel).  slab > 0: the brick's records
+// go to its own slab of `slab` records (payload[key * slab + slot], the
+// counter starting at 0), and the weight statistics are gathered here
+// (there is no count pass); my_wminc then receives the smallest nonzero
+// |w| as count_one keeps it.
 template <int SCHEME, bool SCATTER, bool SMEM, int CSTRIDE = kCursorStride>
 __device__ __forceinline__ void bin_one(float px, float py, float pz, float wt, bool weighted,
                                         const AssignGeom &g, int G, int blk, uint32_t *hist,
                                         uint32_t *__restrict__ table, uint4 *__restrict__ payload, uint64_t cap,
                                         unsigned int *ovf, unsigned long long &my_lost, unsigned int &my_wmax,
-                                        unsigned int &my_neg)
+                                        unsigned int &my_neg, unsigned int *my_wminc = nullptr, uint32_t slab = 0)
 {
     using St = Stencil<SCHEME>;
     const float pos[3] = {px, py, pz};
@@ -194,9 +198,10 @@ __device__ __forceinline__ void bin_one(float px, float py, float pz, float wt, 
         ++my_lost;
         return;
     }
-    if (!SCATTER && weighted) {
+    if (weighted && (!SCATTER || my_wminc)) {
         my_wmax = max(my_wmax, __float_as_uint(fabsf(wt)));
         my_neg |= wt < 0.0f;
+        if (SCATTER && wt != 0.0f) *my_wminc = max(*my_wminc, 0x7fffffffu - __float_as_uint(fabsf(wt)));
     }
     // Bricks touched along each axis: 1 or 2.
     int bl[3], nbx[3];
@@ -242,8 +247,11 @@ __device__ __forceinline__ void bin_one(float px, float py, float pz, float wt, 
                         word[a] = pack_axis(cl, t[a]);
                     }
                     // records past the payload's capacity (a deferred
-                    // estimate that fell short) are flagged, not written
-                    if (slot < cap) payload[slot] = make_uint4(word[0], word[1], word[2], __float_as_uint(wt));
+                    // estimate that fell short) or past a full slab are
+                    // flagged, not written
+                    const bool fits = slab ? slot < slab : slot < cap;
+                    const uint64_t at = slab ? (uint64_t)key * slab + slot : (uint64_t)slot;
+                    if (fits) payload[at] = make_uint4(word[0], word[1], word[2], __float_as_uint(wt));
                     else atomicOr(ovf, 1u);
                 }
             }

@@ -91,6 +91,11 @@ struct cam_ctx {
     bool sync_free = false;
     bool capturing = false;  // inside stream capture: no allocation, no events
     uint64_t asg_cap = 0;    // payload records of deferred assignments (grow-only)
+    // Slabs of deferred assignments: per-brick capacity = slab_ratio times
+    // the uniform expectation, at least the largest brick an exact run has
+    // seen (slab_hint, records); the ratio doubles when a slab overflows.
+    double slab_ratio = 2.0;
+    uint64_t slab_hint = 0;
     unsigned char *job_pin = nullptr;  // pinned readback buffer of cam_job_run
     size_t job_pin_bytes = 0;
     // bumped whenever a scratch buffer is (re)allocated or freed, so that
