@@ -1122,9 +1122,9 @@ int cam_job_run(cam_ctx *ctx, const cam_job_desc *job, cam_job_result *res)
         const DevParticles d = stage_particles(ctx, &job->parts);
         FftPlan *plan = get_plan(ctx, n, job->precision);
         const int nb = want_pk ? nbins_for(job->pk, n) : 0;
-        // Readback of one run: assignment statistics [4], mesh sum and mean
+        // Readback of one run: assignment statistics [6], mesh sum and mean
         // [2], P(k) sums [nb][2] and modes [nb], into a pinned buffer.
-        const size_t pin_bytes = 4 * 8 + 2 * 8 + (size_t)nb * 24 + 8;
+        const size_t pin_bytes = 6 * 8 + 2 * 8 + (size_t)nb * 24 + 8;
         if (ctx->job_pin_bytes < pin_bytes) {
             std::lock_guard<std::mutex> lk(alloc_mutex());
             if (ctx->job_pin) CAM_CUDA_TRY(cudaFreeHost(ctx->job_pin));
@@ -1134,10 +1134,10 @@ int cam_job_run(cam_ctx *ctx, const cam_job_desc *job, cam_job_result *res)
             ctx->job_pin_bytes = pin_bytes;
         }
         auto *hstats = reinterpret_cast<unsigned long long *>(ctx->job_pin);
-        auto *hsum = reinterpret_cast<double *>(ctx->job_pin + 32);
-        auto *hpk = reinterpret_cast<double *>(ctx->job_pin + 48);
-        auto *hmd = reinterpret_cast<unsigned long long *>(ctx->job_pin + 48 + (size_t)nb * 16);
-        auto *herr = reinterpret_cast<unsigned *>(ctx->job_pin + 48 + (size_t)nb * 24);
+        auto *hsum = reinterpret_cast<double *>(ctx->job_pin + 48);
+        auto *hpk = reinterpret_cast<double *>(ctx->job_pin + 64);
+        auto *hmd = reinterpret_cast<unsigned long long *>(ctx->job_pin + 64 + (size_t)nb * 16);
+        auto *herr = reinterpret_cast<unsigned *>(ctx->job_pin + 64 + (size_t)nb * 24);
         const unsigned *derr = device_error_word(ctx);
         // One run of the whole job.  defer: the assignment sizes its payload
         // from an estimate and nothing waits for the host until the single
@@ -1155,7 +1155,7 @@ int cam_job_run(cam_ctx *ctx, const cam_job_desc *job, cam_job_result *res)
             Spectrum s = alloc_spectrum(ctx, n, job->precision, "job.spec");
             const PkDevice pkd = job_fft_pk(ctx, plan, out.mesh, dsum + 1, s, want_pk ? &job->pk : nullptr, nb,
                                             job->want_tweb != 0);
-            CAM_CUDA_TRY(cudaMemcpyAsync(hstats, assign_stats(ctx), 32, cudaMemcpyDeviceToHost, ctx->stream));
+            CAM_CUDA_TRY(cudaMemcpyAsync(hstats, assign_stats(ctx), 48, cudaMemcpyDeviceToHost, ctx->stream));
             CAM_CUDA_TRY(cudaMemcpyAsync(hsum, dsum, 16, cudaMemcpyDeviceToHost, ctx->stream));
             if (want_pk) {
                 CAM_CUDA_TRY(cudaMemcpyAsync(hpk, pkd.sums, (size_t)nb * 16, cudaMemcpyDeviceToHost, ctx->stream));
@@ -1164,12 +1164,13 @@ int cam_job_run(cam_ctx *ctx, const cam_job_desc *job, cam_job_result *res)
             CAM_CUDA_TRY(cudaMemcpyAsync(herr, derr, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
             CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
             CAM_REQUIRE(*herr == 0u, CAM_E_CUDA, "a kernel's bulk copy did not complete within its wait limit");
-            if (defer && (hstats[3] & 0xffffffffu)) {
-                // a slab (or the payload estimate) was too small: larger
-                // slabs for the next jobs of this context, and an exact run
-                ctx->slab_ratio = std::min(64.0, ctx->slab_ratio * 2.0);
-                return true;
-            }
+            // An exact run measured its fullest brick: later deferred jobs
+            // of this context and mesh shape size their slabs from it.
+            const uint64_t bmax = defer ? (hstats[5] & 0xffffffffu) : out.brick_max;
+            if (bmax && out.brick_est > 0.0) ctx->slab_clump[out.brick_shape] = slab_clump_of(bmax, out.brick_est);
+            // a slab (or the payload estimate) was too small: an exact run,
+            // which also measures the bricks again
+            if (defer && (hstats[3] & 0xffffffffu)) return true;
             if (d.w) {
                 const unsigned wbits = (unsigned)(hstats[1] & 0xffffffffu);
                 CAM_REQUIRE(wbits < 0x7f800000u, CAM_E_NONFINITE, "a particle weight is NaN or infinite");

@@ -423,19 +423,23 @@ static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const floa
         per *= 2;
     }
     // Slabs (deferred jobs): every brick gets a fixed slab of the payload,
-    // sized from the uniform expectation times a ratio that grows when a
-    // slab overflows (the job then reruns exactly) and from the largest
-    // brick an exact run has seen; no count pass and no scan then, and the
-    // scatter gathers the statistics.  Only while the slabs stay within four
-    // times the expected payload and 2^32 records.
+    // sized from the clumping the last exact job run of this mesh shape
+    // measured (a slab that overflows makes the job rerun exactly, which
+    // measures again); no count pass and no scan then, and the scatter
+    // gathers the statistics.  Only while the slabs stay within 1.6 times
+    // the expected records (or 2^20 records): the scatter slows as the slabs
+    // spread its appends over more memory (256^3: 0.37 ms per job densely
+    // packed, 0.48 in slabs of twice, 0.55 of four times the mean brick).
+    const double est_brick = (double)np * f / (double)nb;
+    const int64_t shape = ((int64_t)g.n[0] << 32) | ((int64_t)g.n[1] << 16) | (int64_t)g.n[2];
     uint32_t slab = 0;
-    if (out.defer && !ctx->sync_free && np > 0) {
-        const double est_brick = (double)np * f / (double)nb;
-        uint64_t cap = (uint64_t)std::ceil(ctx->slab_ratio * est_brick);
-        cap = std::max<uint64_t>(cap, ctx->slab_hint + ctx->slab_hint / 8);
-        cap = (cap + 16 + 3) & ~(uint64_t)3;
-        const uint64_t est_total = (uint64_t)((double)np * f * 1.25) + 65536;
-        if ((uint64_t)nb * cap < (1ull << 32) && (uint64_t)nb * cap <= 4 * est_total) slab = (uint32_t)cap;
+    if (out.defer && !ctx->sync_free && !ctx->slabs_off && np > 0) {
+        const auto it = ctx->slab_clump.find(shape);
+        if (it != ctx->slab_clump.end()) {
+            const uint64_t cap = slab_capacity(it->second * est_brick);
+            const double room = std::max(1.6 * (double)np * f, (double)(1u << 20));
+            if ((double)nb * (double)cap <= room && (uint64_t)nb * cap < (1ull << 32)) slab = (uint32_t)cap;
+        }
     }
 
     const size_t hsmem = smem_hist ? (size_t)nb * sizeof(uint32_t) : 0;
@@ -457,6 +461,13 @@ static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const floa
             exclusive_scan_u32(ctx, counts, nb, d_total);
             CAM_LAUNCH_NAMED(ctx, "assign_starts", brick_starts_kernel, sg, 256, 0, counts, (int)nb, d_total, start,
                              table);
+        }
+        // the fullest brick, for the slabs of later deferred jobs
+        if (!ctx->sync_free) {
+            CAM_LAUNCH_NAMED(ctx, "assign_starts", brick_max_kernel, 64, 256, 0, start, (int)nb,
+                             reinterpret_cast<unsigned int *>(stats + 5));
+            out.brick_est = est_brick;
+            out.brick_shape = shape;
         }
     }
 
@@ -489,15 +500,13 @@ static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const floa
         out.n_in = -1;
     } else {
         // Payload size and diagnostics back to the host (one synchronisation),
-        // with the largest brick's record count for later slabs.
-        CAM_LAUNCH_NAMED(ctx, "assign_starts", brick_max_kernel, 64, 256, 0, start, (int)nb,
-                         reinterpret_cast<unsigned int *>(stats + 5));
+        // with the fullest brick's record count for later slabs.
         unsigned long long hstats[6] = {0, 0, 0, 0, 0, 0};
         CAM_CUDA_TRY(cudaMemcpyAsync(hstats, stats, sizeof(hstats), cudaMemcpyDeviceToHost, ctx->stream));
         CAM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
         total = (uint32_t)(hstats[2] & 0xffffffffu);
         ctx->asg_cap = std::max<uint64_t>(ctx->asg_cap, total);  // deferred runs size from it
-        ctx->slab_hint = std::max<uint64_t>(ctx->slab_hint, hstats[5] & 0xffffffffu);
+        out.brick_max = hstats[5] & 0xffffffffu;
         const unsigned int wmax_bits = (unsigned int)(hstats[1] & 0xffffffffu);
         CAM_REQUIRE(!w || wmax_bits < 0x7f800000u, CAM_E_NONFINITE, "a particle weight is NaN or infinite");
         out.n_lost = (int64_t)hstats[0];

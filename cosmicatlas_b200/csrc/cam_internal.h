@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+#include <cmath>
 #include <map>
 #include <mutex>
 #include <string>
@@ -91,11 +93,14 @@ struct cam_ctx {
     bool sync_free = false;
     bool capturing = false;  // inside stream capture: no allocation, no events
     uint64_t asg_cap = 0;    // payload records of deferred assignments (grow-only)
-    // Slabs of deferred assignments: per-brick capacity = slab_ratio times
-    // the uniform expectation, at least the largest brick an exact run has
-    // seen (slab_hint, records); the ratio doubles when a slab overflows.
-    double slab_ratio = 2.0;
-    uint64_t slab_hint = 0;
+    // Slabs of deferred assignments (cam_job_run), per mesh shape: the
+    // fullest brick's expected records over those of a uniform catalogue,
+    // as the last exact job run of that shape measured them (Poisson noise
+    // taken out).  No entry until a job of the shape has run exactly.
+    // slabs_off: always the exact path (the server's contexts, whose
+    // admission budgets the exact payload).
+    std::map<int64_t, double> slab_clump;
+    bool slabs_off = false;
     unsigned char *job_pin = nullptr;  // pinned readback buffer of cam_job_run
     size_t job_pin_bytes = 0;
     // bumped whenever a scratch buffer is (re)allocated or freed, so that
@@ -190,11 +195,35 @@ struct AssignOut {
     // written and raise the overflow word of the device statistics, in
     // which case the caller reruns without defer.  n_in / n_lost are -1.
     bool defer = false;
+    // Set by exact (non-slab) runs: the records a brick of a uniform
+    // catalogue expects, and (without defer) the fullest brick's records;
+    // with defer the fullest brick is word [5] of the device statistics.
+    double brick_est = 0.0;
+    uint64_t brick_max = 0;
+    int64_t brick_shape = 0;  // slab_clump key of the mesh
 };
+
+// Records per brick (noise included) that hold the fullest brick of a
+// catalogue whose fullest brick expects mu records: 9/8 of mu plus 4.5
+// Poisson standard deviations plus 16.
+inline uint64_t slab_capacity(double mu)
+{
+    const uint64_t cap = (uint64_t)std::ceil(1.125 * mu + 4.5 * std::sqrt(mu)) + 16;
+    return (cap + 3) & ~(uint64_t)3;
+}
+
+// The clumping an exact run measured: a fullest brick of m records where a
+// uniform brick expects est, less four standard deviations of noise.
+inline double slab_clump_of(uint64_t m, double est)
+{
+    const double md = (double)m;
+    return std::max(1.0, (md - 4.0 * std::sqrt(md)) / est);
+}
 
 // Device statistics of the last assignment of a context (asg.stats):
 // [0] lost particles, [1] low word: bits of max |w|, [2] low word: payload
-// records, [3] low word: nonzero if the deferred payload overflowed.
+// records, [3] low word: nonzero if the deferred payload overflowed,
+// [5] low word: records of the fullest brick (exact runs; 0 with slabs).
 unsigned long long *assign_stats(cam_ctx *ctx);
 
 // Runs the assignment pipeline on device particle arrays.  Writes the mesh

@@ -667,6 +667,7 @@ int cam_server_create(int device, size_t hbm_budget, int nworkers, int max_batch
     {
         const int rc = cam_ctx_create(device, 0, &s->big_ctx);
         if (rc != CAM_OK) return rc;
+        s->big_ctx->slabs_off = true;  // admission budgets the exact payload
     }
     for (int i = 0; i < nworkers; ++i) {
         std::unique_ptr<cam_server::Worker> w(new cam_server::Worker);
@@ -677,6 +678,7 @@ int cam_server_create(int device, size_t hbm_budget, int nworkers, int max_batch
             cam_ctx_destroy(s->big_ctx);
             return rc;
         }
+        w->ctx->slabs_off = true;
         s->workers.push_back(std::move(w));
     }
     cam_server *sp = s.release();

@@ -304,7 +304,13 @@ int cam_konvolve(cam_ctx *ctx, const cam_grid *grid, const void *in, int precisi
 
 /* ---- one mesh job: particles -> mesh -> FFT -> P(k) [-> T-web] ----------
  * The plain per-call GPU path of one BAM iteration: the mesh and its
- * spectrum stay resident on the device between the stages. */
+ * spectrum stay resident on the device between the stages, and the host
+ * waits once, for the statistics and P(k) at the end.  A context's first
+ * job of a mesh shape sorts the particles into mesh bricks exactly (count,
+ * scan, scatter) and measures its fullest brick; later jobs of that shape
+ * write every brick's records into a fixed slab sized from it and skip the
+ * count.  A job whose records do not fit (its slabs or the payload
+ * estimate) runs again exactly, so results never depend on the path. */
 typedef struct {
     cam_particles parts;
     cam_grid grid;
@@ -339,8 +345,9 @@ int cam_particles_stage(cam_ctx *ctx, const cam_particles *host, cam_particles *
  * No single counterpart in the reference: BAM issues its mesh jobs one
  * after another from the calibration loop (Source/Bam.cpp:13424,
  * Bam::bamrunner), one cam_job_run each.  Both entry points below return,
- * per job, exactly what cam_job_run returns for it (same kernels, every job
- * on its own buffers), except that labels are not returned by batches.
+ * per job, exactly what cam_job_run returns for it (the same mesh,
+ * transform and binning; every job on its own buffers), except that labels
+ * are not returned by batches.
  *
  * cam_batch_run: consecutive jobs of one shape (mesh, particle count,
  * weights or not, scheme, precision, box and all P(k)/T-web options equal)

@@ -114,9 +114,10 @@ def test_job_fp64_mesh_c1_shape(ctx):
 def test_job_payload_estimate_overflow_reruns():
     # Every particle's CIC stencil crosses a brick face along all three axes
     # (home cell 31 ends a brick for every power-of-two brick extent <= 32),
-    # so each gives 8 records, far above the job's payload estimate: the
-    # first job of a fresh context overflows it and reruns exactly; the
-    # second finds the grown capacity and runs once.
+    # so each gives 8 records and one brick receives all 60,000 of its
+    # particles: the first job of a fresh context overflows the payload
+    # estimate and reruns exactly; the second finds the grown payload, but
+    # slabs of the fullest brick too costly, and runs once on the exact path.
     n, box, nbins = 64, 64.0, 24
     rng = np.random.default_rng(41)
     npart = 60_000
@@ -145,3 +146,49 @@ def test_job_payload_estimate_overflow_reruns():
     floor = opk.shot_noise * opk.sum_sn / np.maximum(opk.modes, 1)
     assert np.array_equal(r1["pk"].modes, opk.modes)
     assert pk_rel_err(r1["pk"].pk, opk.pk, floor) <= 1e-5
+
+
+def test_job_slabs_measured_overflow_reruns():
+    # A context's first job of a mesh shape runs exactly and measures its
+    # fullest brick; later jobs write per-brick slabs sized from it (no
+    # count pass).  A more concentrated catalogue overflows them: the job
+    # reruns exactly, measures again, and the next job fits its slabs.
+    # Every result equals a fresh context's exact run bit for bit.
+    n, box, nbins = 128, 1000.0, 32
+    npart = 400_000
+    rng = np.random.default_rng(5)
+    ux, uy, uz = (rng.uniform(0.0, box, npart).astype(np.float32) for _ in range(3))
+    # density rising towards x = 0: the fullest brick holds 2,942 TSC
+    # records against 2,229 of the uniform catalogue (2,101 expected), past
+    # the uniform catalogue's slabs of 2,588
+    cx = (box * (ux.astype(np.float64) / box) ** 1.2).astype(np.float32)
+    w = synth.halo_masses(npart, seed=6)
+    g = make_grid(n, box)
+    opts = Context.pk_opts(TSC, nbins=nbins)
+    c = Context(0)
+    try:
+        launches = []
+        res = []
+        for xs in (ux, ux, cx, cx):
+            l0 = c.kernel_launches
+            res.append(c.job(xs, uy, uz, w, g, TSC, F32, pk=opts))
+            launches.append(c.kernel_launches - l0)
+    finally:
+        c.close()
+    exact, slab, rerun, slab2 = launches
+    assert slab < exact          # no count pass, scan or brick measure
+    assert rerun > exact         # the slab run, then the exact one
+    assert slab2 == slab         # the measured slabs hold the new catalogue
+    assert np.array_equal(res[0]["pk"].pk, res[1]["pk"].pk)
+    assert np.array_equal(res[2]["pk"].pk, res[3]["pk"].pk)
+    f = Context(0)
+    try:
+        fresh = f.job(cx, uy, uz, w, g, TSC, F32, pk=opts)
+    finally:
+        f.close()
+    assert np.array_equal(fresh["pk"].pk, res[3]["pk"].pk)
+    assert np.array_equal(fresh["pk"].modes, res[3]["pk"].modes)
+    assert res[3]["assign"].n_lost == 0 and res[3]["assign"].n_in == npart
+    _, lost, opk, _ = oracle_job(cx, uy, uz, w, n, box, TSC, nbins, None, 0.0, F32)
+    floor = opk.shot_noise * opk.sum_sn / np.maximum(opk.modes, 1)
+    assert pk_rel_err(res[3]["pk"].pk, opk.pk, floor) <= 1e-5
