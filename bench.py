@@ -499,6 +499,7 @@ def run_ours(args):
                          "frac": stages[dom]["frac"], "traffic": dom_traffic,
                          "note": "stage = the kernels that implement one assignment (algorithmic bytes "
                                  "N_p*16 + 4*N^3 per job); traffic = their ncu DRAM bytes per job",
+                         "traffic_path": (traffic or {}).get("path"),
                          "dominant_kernel": dominant_kernel},
             "stages": stages,
             "kernels": kernels,

@@ -426,8 +426,8 @@ static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const floa
     // sized from the clumping the last exact job run of this mesh shape
     // measured (a slab that overflows makes the job rerun exactly, which
     // measures again); no count pass and no scan then, and the scatter
-    // gathers the statistics.  Only while the slabs stay within 1.6 times
-    // the expected records (or 2^20 records): the scatter slows as the slabs
+    // gathers the statistics.  Only while the slabs stay within twice the
+    // expected records (or 2^20 records): the scatter slows as the slabs
     // spread its appends over more memory (256^3: 0.37 ms per job densely
     // packed, 0.48 in slabs of twice, 0.55 of four times the mean brick).
     const double est_brick = (double)np * f / (double)nb;
@@ -437,7 +437,7 @@ static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const floa
         const auto it = ctx->slab_clump.find(shape);
         if (it != ctx->slab_clump.end()) {
             const uint64_t cap = slab_capacity(it->second * est_brick);
-            const double room = std::max(1.6 * (double)np * f, (double)(1u << 20));
+            const double room = std::max(2.0 * (double)np * f, (double)(1u << 20));
             if ((double)nb * (double)cap <= room && (uint64_t)nb * cap < (1ull << 32)) slab = (uint32_t)cap;
         }
     }
