@@ -430,10 +430,12 @@ static void assign_impl(cam_ctx *ctx, const float *x, const float *y, const floa
     // expected records (or 2^20 records): the scatter slows as the slabs
     // spread its appends over more memory (256^3: 0.37 ms per job densely
     // packed, 0.48 in slabs of twice, 0.55 of four times the mean brick).
+    // A context with an HBM budget keeps the exact path, whose payload the
+    // budget was sized for.
     const double est_brick = (double)np * f / (double)nb;
     const int64_t shape = ((int64_t)g.n[0] << 32) | ((int64_t)g.n[1] << 16) | (int64_t)g.n[2];
     uint32_t slab = 0;
-    if (out.defer && !ctx->sync_free && !ctx->slabs_off && np > 0) {
+    if (out.defer && !ctx->sync_free && !ctx->slabs_off && !ctx->budget && np > 0) {
         const auto it = ctx->slab_clump.find(shape);
         if (it != ctx->slab_clump.end()) {
             const uint64_t cap = slab_capacity(it->second * est_brick);

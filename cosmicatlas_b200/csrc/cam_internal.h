@@ -98,7 +98,8 @@ struct cam_ctx {
     // as the last exact job run of that shape measured them (Poisson noise
     // taken out).  No entry until a job of the shape has run exactly.
     // slabs_off: always the exact path (the server's contexts, whose
-    // admission budgets the exact payload).
+    // admission budgets the exact payload); so does a context with an HBM
+    // budget.
     std::map<int64_t, double> slab_clump;
     bool slabs_off = false;
     unsigned char *job_pin = nullptr;  // pinned readback buffer of cam_job_run
