@@ -200,7 +200,6 @@ brick_offsets_kernel(uint32_t *__restrict__ padded, int nb, uint32_t *__restrict
     }
 }
 
-// counts[b] = padded[b * kCursorStride] (contiguous, for the scan).
 // The largest brick record count, start[b + 1] - start[b], into *out
 // (atomicMax; *out zeroed before).
 __global__ void __launch_bounds__(256)
@@ -214,6 +213,7 @@ brick_max_kernel(const uint32_t *__restrict__ start, int nb, unsigned int *__res
     if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
 }
 
+// counts[b] = padded[b * kCursorStride] (contiguous, for the scan).
 __global__ void compact_counts_kernel(const uint32_t *__restrict__ padded, int nb, uint32_t *__restrict__ counts)
 {
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x)
